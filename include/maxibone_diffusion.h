@@ -1,0 +1,130 @@
+/*
+ * maxibone_diffusion.h -- C ABI of the B200 (sm_100a) mask-diffusion library.
+ *
+ * The path: a uint8 binary mask becomes a {0,1} field; each repetition applies
+ * a 1-D kernel along z, then y, then x with a zero boundary, and re-illuminates
+ * the mask voxels to exactly 1.0; the final field is quantised to uint16 as
+ * floor(v * 65535) in FP32.  All entry points return a maxi_status; a nonzero
+ * code comes with a message from maxi_last_error() (per calling thread).
+ *
+ * Plain C types only: pointers, sizes, enums.  No ownership crosses the
+ * boundary; the caller owns every buffer it passes in.  Calls are synchronous
+ * unless the entry point takes a `stream` (a cudaStream_t; NULL = the legacy
+ * default stream), in which case work is enqueued on that stream.
+ */
+#ifndef MAXIBONE_DIFFUSION_H
+#define MAXIBONE_DIFFUSION_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum maxi_status {
+    MAXI_OK = 0,
+    MAXI_ERR_INVALID_ARGUMENT = 1, /* bad shape, kernel length, dtype, pointer */
+    MAXI_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+    MAXI_ERR_OUT_OF_MEMORY = 3,    /* device or pinned host allocation failed */
+    MAXI_ERR_IO = 4,               /* file open / read / write failed (on-disk form) */
+    MAXI_ERR_UNSUPPORTED = 5,      /* a valid request this build does not serve */
+    MAXI_ERR_NO_DEVICE = 6         /* no CUDA device visible */
+} maxi_status;
+
+/* How the field is stored in HBM between passes.  Accumulation is always FP32
+ * (FP64 for MAXI_FIELD_F64). */
+typedef enum maxi_field_type {
+    MAXI_FIELD_F32 = 0,
+    MAXI_FIELD_BF16 = 1,
+    MAXI_FIELD_F16 = 2,
+    MAXI_FIELD_F64 = 3 /* FP64 storage and arithmetic: the error reference form */
+} maxi_field_type;
+
+/* Mask encodings accepted by the device entry points. */
+typedef enum maxi_mask_format {
+    MAXI_MASK_U8 = 0,       /* one byte per voxel, voxel is set when > 0 */
+    MAXI_MASK_BITPACKED = 1 /* uint32 words over the flat voxel order, 32 voxels each,
+                               most significant bit first (the reference bitpacking
+                               layout); ceil(nz*ny*nx / 32) words */
+} maxi_mask_format;
+
+/* Option bits for maxi_diffusion_device(). */
+#define MAXI_FLAG_REFERENCE_ROUNDING 0x1 /* FP32 only: separate multiply and add in the
+                                            reference's tap order, bit-identical to the
+                                            reference OpenMP backend */
+
+const char *maxi_last_error(void);
+const char *maxi_version(void);
+
+/* Kernel kinds reported by maxi_profile_read(). */
+typedef enum maxi_kernel_kind {
+    MAXI_KERNEL_INIT = 0,    /* mask -> field */
+    MAXI_KERNEL_Z = 1,       /* z pass */
+    MAXI_KERNEL_Y = 2,       /* y pass */
+    MAXI_KERNEL_X = 3,       /* x pass + re-illumination */
+    MAXI_KERNEL_X_FINAL = 4, /* last x pass + re-illumination + uint16 quantisation */
+    MAXI_KERNEL_YX = 5,      /* fused y and x passes + re-illumination */
+    MAXI_KERNEL_OTHER = 6,
+    MAXI_KERNEL_KINDS = 8
+} maxi_kernel_kind;
+
+/*
+ * Per-launch timing of this library's kernels (no reference counterpart; the
+ * reference times slabs with wall clocks behind a PROFILE constant,
+ * src/lib/cpp/gpu/diffusion.cc:854-933).  When enabled, every kernel launch is
+ * bracketed by CUDA events on its stream.  maxi_profile_read() waits for the
+ * recorded events, writes the summed device milliseconds and launch counts per
+ * maxi_kernel_kind (n_kinds entries) and clears the record.
+ */
+int maxi_profile_enable(int on);
+int maxi_profile_read(double *ms_by_kind, int64_t *launches_by_kind, int32_t n_kinds);
+
+/*
+ * In-memory diffusion on HOST buffers (the reference-facing call).
+ * Replaces NS::diffusion_in_memory, src/lib/cpp/include/diffusion.hh:36, as
+ * bound by python_api::diffusion_in_memory, src/pybind/diffusion-pybind.cc:27-53.
+ * voxels: uint8[nz][ny][nx] (set when > 0); kernel: float[kernel_size], odd
+ * length; output: uint16[nz][ny][nx], written in place.  FP32 field.
+ */
+int maxi_diffusion_in_memory(const uint8_t *voxels, int64_t nz, int64_t ny, int64_t nx,
+                             const float *kernel, int64_t kernel_size, int64_t repititions,
+                             uint16_t *output, int verbose);
+
+/*
+ * Working memory (bytes) that maxi_diffusion_device() needs for one volume:
+ * two field buffers of the storage type plus the bit-packed mask.
+ */
+int64_t maxi_diffusion_workspace_size(int64_t nz, int64_t ny, int64_t nx, int32_t field_type);
+
+/*
+ * In-memory diffusion on DEVICE buffers, enqueued on `stream`.  The device
+ * form of diffusion.hh:36 (no reference counterpart for the extra options).
+ *   mask: device mask in `mask_format`;
+ *   kernel: HOST float[kernel_size] (copied into the launch parameters);
+ *   output: device uint16[nz][ny][nx], or NULL;
+ *   field_out: device buffer for the final field before quantisation, or NULL:
+ *              float[N] for F32/BF16/F16 (taken from the FP32 accumulator),
+ *              double[N] for F64;
+ *   workspace: device memory of at least maxi_diffusion_workspace_size() bytes,
+ *              or NULL to let the library allocate (and free) it per call;
+ *   flags: MAXI_FLAG_* bits.
+ */
+int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,
+                          const float *kernel, int64_t kernel_size, int64_t repititions,
+                          uint16_t *output, void *field_out, int32_t field_type, int32_t flags,
+                          void *workspace, int64_t workspace_bytes, void *stream);
+
+/*
+ * Bit-packing of a device mask to uint32 words, MSB first.  Replaces the
+ * reference `bitpacking.encode` / `decode` (src/pybind/bitpacking-pybind.cc:17-48,
+ * src/lib/cpp/cpu_seq/bitpacking.cc:9-42); n must be a multiple of 32.
+ * encode keeps bit 0 of each byte (`mask & 1`), as the reference does.
+ */
+int maxi_bitpack_encode(const uint8_t *mask, int64_t n, uint32_t *packed, void *stream);
+int maxi_bitpack_decode(const uint32_t *packed, int64_t n, uint8_t *mask, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MAXIBONE_DIFFUSION_H */

@@ -1,0 +1,72 @@
+"""ctypes binding of the in-tree CUDA library ``libmaxibone_diffusion.so``.
+
+The library is the product: every diffusion call goes through it.  If it is
+missing the import fails loudly (there is no CPU fallback); build it with
+``python -m maxibone_b200.build`` or ``__graft_entry__.build()``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmaxibone_diffusion.so")
+
+MAXI_OK = 0
+STATUS_NAMES = {
+    0: "MAXI_OK", 1: "MAXI_ERR_INVALID_ARGUMENT", 2: "MAXI_ERR_CUDA", 3: "MAXI_ERR_OUT_OF_MEMORY",
+    4: "MAXI_ERR_IO", 5: "MAXI_ERR_UNSUPPORTED", 6: "MAXI_ERR_NO_DEVICE",
+}
+FIELD_TYPES = {"f32": 0, "bf16": 1, "f16": 2, "f64": 3}
+MASK_FORMATS = {"u8": 0, "bitpacked": 1}
+FLAG_REFERENCE_ROUNDING = 0x1
+
+# Every symbol include/maxibone_diffusion.h declares, with (restype, argtypes).
+_i64, _i32, _p, _int = ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int
+SIGNATURES = {
+    "maxi_last_error": (ctypes.c_char_p, []),
+    "maxi_version": (ctypes.c_char_p, []),
+    "maxi_diffusion_in_memory": (_int, [_p, _i64, _i64, _i64, _p, _i64, _i64, _p, _int]),
+    "maxi_diffusion_workspace_size": (_i64, [_i64, _i64, _i64, _i32]),
+    "maxi_diffusion_device": (_int, [_p, _i32, _i64, _i64, _i64, _p, _i64, _i64, _p, _p, _i32, _i32, _p, _i64, _p]),
+    "maxi_bitpack_encode": (_int, [_p, _i64, _p, _p]),
+    "maxi_bitpack_decode": (_int, [_p, _i64, _p, _p]),
+    "maxi_profile_enable": (_int, [_int]),
+    "maxi_profile_read": (_int, [_p, _p, _i32]),
+}
+KERNEL_KINDS = ["init", "z", "y", "x", "x_final", "yx", "other", "spare"]
+
+
+class MaxiError(RuntimeError):
+    """A nonzero maxi_status, with the library's message."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+_LIB = None
+
+
+def lib() -> ctypes.CDLL:
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run `python -m maxibone_b200.build`")
+        handle = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = handle
+    return _LIB
+
+
+def check(code: int) -> None:
+    if code != MAXI_OK:
+        msg = lib().maxi_last_error()
+        msg = msg.decode() if msg else ""
+        if code == 1:
+            raise ValueError(f"{STATUS_NAMES[code]}: {msg}")
+        if code == 3:
+            raise MemoryError(f"{STATUS_NAMES[code]}: {msg}")
+        raise MaxiError(code, msg)

@@ -1,0 +1,221 @@
+// Host orchestration and C ABI of the mask-diffusion library.
+//
+// The reference entry points this file replaces:
+//   NS::diffusion_in_memory  src/lib/cpp/include/diffusion.hh:36
+//                            (CPU body src/lib/cpp/cpu/diffusion.cc:339-374,
+//                             OpenACC body src/lib/cpp/gpu/diffusion.cc:758-806)
+//   python_api::diffusion_in_memory  src/pybind/diffusion-pybind.cc:27-53
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "passes.cuh"
+#include "host_util.h"
+#include "unrolled.h"
+#include "profiler.h"
+
+namespace maxi {
+
+// Generic passes: FP64 form, reference rounding, radii beyond the unrolled set.
+template <typename S, bool EXACT, int MF>
+static cudaError_t run_generic_fmt(const Volume &v, const void *mask, const float *kernel, int radius,
+                                   int64_t reps, S *b0, S *b1, uint16_t *out_u16, void *field_out,
+                                   cudaStream_t st) {
+    using Acc = typename FieldIO<S>::Acc;
+    auto *taps = new GenericTaps<Acc>();
+    for (int i = 0; i < 2 * radius + 1; i++) taps->k[i] = (Acc) kernel[i];
+    const int64_t n = v.n();
+    const int threads = 256;
+    const int64_t blocks = ceil_div(n, threads);
+    {
+        ProfScope ps(MAXI_KERNEL_INIT, st);
+        mask_to_field<S, MF, false><<<std::min<int64_t>(blocks, 148 * 64), threads, 0, st>>>(mask, b0, nullptr, nullptr, n);
+    }
+    for (int64_t rep = 0; rep < reps; rep++) {
+        {
+            ProfScope ps(MAXI_KERNEL_Z, st);
+            generic_pass<S, EXACT, false, MF, false><<<blocks, threads, 0, st>>>(b0, b1, mask, nullptr, nullptr, n, v.nz, v.ny * v.nx, radius, *taps);
+        }
+        {
+            ProfScope ps(MAXI_KERNEL_Y, st);
+            generic_pass<S, EXACT, false, MF, false><<<blocks, threads, 0, st>>>(b1, b0, mask, nullptr, nullptr, n, v.ny, v.nx, radius, *taps);
+        }
+        if (rep + 1 < reps) {
+            ProfScope ps(MAXI_KERNEL_X, st);
+            generic_pass<S, EXACT, true, MF, false><<<blocks, threads, 0, st>>>(b0, b1, mask, nullptr, nullptr, n, v.nx, 1, radius, *taps);
+            std::swap(b0, b1);
+        } else {
+            ProfScope ps(MAXI_KERNEL_X_FINAL, st);
+            generic_pass<S, EXACT, true, MF, true><<<blocks, threads, 0, st>>>(b0, b1, mask, out_u16, field_out, n, v.nx, 1, radius, *taps);
+        }
+    }
+    delete taps;
+    return cudaGetLastError();
+}
+
+template <typename S, bool EXACT>
+static cudaError_t run_generic(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
+                               int64_t reps, S *b0, S *b1, uint16_t *out_u16, void *field_out, cudaStream_t st) {
+    if (mask_fmt == MAXI_MASK_U8)
+        return run_generic_fmt<S, EXACT, MAXI_MASK_U8>(v, mask, kernel, radius, reps, b0, b1, out_u16, field_out, st);
+    return run_generic_fmt<S, EXACT, MAXI_MASK_BITPACKED>(v, mask, kernel, radius, reps, b0, b1, out_u16, field_out, st);
+}
+
+template <typename S>
+static cudaError_t zero_reps(const Volume &v, const void *mask, int mask_fmt, uint16_t *out_u16, void *field_out,
+                             cudaStream_t st) {
+    const int64_t n = v.n();
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148 * 64);
+    ProfScope ps(MAXI_KERNEL_X_FINAL, st);
+    if (mask_fmt == MAXI_MASK_U8)
+        mask_to_field<S, MAXI_MASK_U8, true><<<blocks, 256, 0, st>>>(mask, nullptr, out_u16, field_out, n);
+    else
+        mask_to_field<S, MAXI_MASK_BITPACKED, true><<<blocks, 256, 0, st>>>(mask, nullptr, out_u16, field_out, n);
+    return cudaGetLastError();
+}
+
+static size_t field_bytes(int32_t ft) {
+    switch (ft) {
+    case MAXI_FIELD_F32: return 4;
+    case MAXI_FIELD_BF16: return 2;
+    case MAXI_FIELD_F16: return 2;
+    case MAXI_FIELD_F64: return 8;
+    default: return 0;
+    }
+}
+
+static int64_t workspace_bytes_for(int64_t n, int32_t ft) {
+    return 2 * round_up((int64_t) field_bytes(ft) * n, 256);
+}
+
+template <typename S>
+static cudaError_t run_typed(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
+                             int64_t reps, uint16_t *out_u16, void *field_out, int32_t flags, char *ws,
+                             cudaStream_t st) {
+    if (reps == 0) return zero_reps<S>(v, mask, mask_fmt, out_u16, field_out, st);
+    S *b0 = reinterpret_cast<S *>(ws);
+    S *b1 = reinterpret_cast<S *>(ws + round_up((int64_t) sizeof(S) * v.n(), 256));
+    constexpr bool is_f64 = std::is_same<S, double>::value;
+    const bool exact = (flags & MAXI_FLAG_REFERENCE_ROUNDING) != 0;
+    if (is_f64 || exact || radius_bucket(radius) < 0) {
+        if (exact) return run_generic<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, st);
+        return run_generic<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, st);
+    }
+    if constexpr (!is_f64)
+        return dispatch_unrolled<S>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16,
+                                    static_cast<float *>(field_out), st);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace maxi
+
+using namespace maxi;
+
+extern "C" {
+
+const char *maxi_version(void) { return "maxibone_b200 diffusion 0.1 (sm_100a)"; }
+
+const char *maxi_last_error(void) { return last_error_cstr(); }
+
+int64_t maxi_diffusion_workspace_size(int64_t nz, int64_t ny, int64_t nx, int32_t field_type) {
+    if (nz <= 0 || ny <= 0 || nx <= 0 || field_bytes(field_type) == 0) return -1;
+    return workspace_bytes_for(nz * ny * nx, field_type);
+}
+
+int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,
+                          const float *kernel, int64_t kernel_size, int64_t repititions,
+                          uint16_t *output, void *field_out, int32_t field_type, int32_t flags,
+                          void *workspace, int64_t workspace_bytes, void *stream) {
+    clear_error();
+    int rc = validate_common(mask, nz, ny, nx, kernel, kernel_size, repititions);
+    if (rc) return rc;
+    if (mask_format != MAXI_MASK_U8 && mask_format != MAXI_MASK_BITPACKED)
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "unknown mask_format %d", mask_format);
+    if (field_bytes(field_type) == 0)
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "unknown field_type %d", field_type);
+    if ((flags & MAXI_FLAG_REFERENCE_ROUNDING) && field_type != MAXI_FIELD_F32)
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "reference rounding is defined for the FP32 field only");
+    if (!output && !field_out)
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "neither output nor field_out given");
+    if ((rc = require_device())) return rc;
+
+    const Volume v{nz, ny, nx};
+    const int radius = (int) (kernel_size / 2);
+    const int64_t need = workspace_bytes_for(v.n(), field_type);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    char *ws = static_cast<char *>(workspace);
+    bool owned = false;
+    if (repititions > 0) {
+        if (ws && workspace_bytes < need)
+            return set_error(MAXI_ERR_INVALID_ARGUMENT, "workspace of %lld bytes is smaller than the %lld needed",
+                             (long long) workspace_bytes, (long long) need);
+        if (!ws) {
+            if (cudaMallocAsync(reinterpret_cast<void **>(&ws), need, st) != cudaSuccess) {
+                cudaGetLastError();
+                return set_error(MAXI_ERR_OUT_OF_MEMORY, "could not allocate %lld bytes of device workspace",
+                                 (long long) need);
+            }
+            owned = true;
+        }
+    }
+    cudaError_t e;
+    switch (field_type) {
+    case MAXI_FIELD_F32: e = run_typed<float>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st); break;
+    case MAXI_FIELD_BF16: e = run_typed<__nv_bfloat16>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st); break;
+    case MAXI_FIELD_F16: e = run_typed<__half>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st); break;
+    default: e = run_typed<double>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st); break;
+    }
+    if (owned) cudaFreeAsync(ws, st);
+    if (e != cudaSuccess) return set_cuda_error(e, "diffusion launch");
+    return MAXI_OK;
+}
+
+int maxi_diffusion_in_memory(const uint8_t *voxels, int64_t nz, int64_t ny, int64_t nx,
+                             const float *kernel, int64_t kernel_size, int64_t repititions,
+                             uint16_t *output, int verbose) {
+    clear_error();
+    int rc = validate_common(voxels, nz, ny, nx, kernel, kernel_size, repititions);
+    if (rc) return rc;
+    if (!output) return set_error(MAXI_ERR_INVALID_ARGUMENT, "output is NULL");
+    if ((rc = require_device())) return rc;
+    const int64_t n = nz * ny * nx;
+    const int64_t need = workspace_bytes_for(n, MAXI_FIELD_F32);
+    if (verbose >= 1)
+        printf("Diffusion: shape (%lld, %lld, %lld), kernel size %lld, %lld repetitions, FP32 field on the GPU\n",
+               (long long) nz, (long long) ny, (long long) nx, (long long) kernel_size, (long long) repititions);
+    cudaStream_t st;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+        return set_cuda_error(cudaGetLastError(), "stream creation");
+    uint8_t *d_mask = nullptr;
+    uint16_t *d_out = nullptr;
+    char *ws = nullptr;
+    cudaError_t e = cudaSuccess;
+    do {
+        if ((e = cudaMallocAsync(reinterpret_cast<void **>(&d_mask), n, st)) != cudaSuccess) break;
+        if ((e = cudaMallocAsync(reinterpret_cast<void **>(&d_out), 2 * n, st)) != cudaSuccess) break;
+        if (repititions > 0 && (e = cudaMallocAsync(reinterpret_cast<void **>(&ws), need, st)) != cudaSuccess) break;
+        if ((e = cudaMemcpyAsync(d_mask, voxels, n, cudaMemcpyHostToDevice, st)) != cudaSuccess) break;
+        rc = maxi_diffusion_device(d_mask, MAXI_MASK_U8, nz, ny, nx, kernel, kernel_size, repititions, d_out,
+                                   nullptr, MAXI_FIELD_F32, 0, ws, need, st);
+        if (rc) break;
+        if ((e = cudaMemcpyAsync(output, d_out, 2 * n, cudaMemcpyDeviceToHost, st)) != cudaSuccess) break;
+        e = cudaStreamSynchronize(st);
+    } while (0);
+    if (d_mask) cudaFreeAsync(d_mask, st);
+    if (d_out) cudaFreeAsync(d_out, st);
+    if (ws) cudaFreeAsync(ws, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (rc) return rc;
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return set_error(MAXI_ERR_OUT_OF_MEMORY, "device allocation failed for a %lld-voxel volume", (long long) n);
+    }
+    if (e != cudaSuccess) return set_cuda_error(e, "in-memory diffusion");
+    if (verbose >= 1) printf("Diffusion is complete!\n");
+    return MAXI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,228 @@
+// CUDA-core convolution passes of the diffusion step (sm_100a).
+//
+// One repetition of the reference step (src/lib/cpp/cpu/diffusion.cc:314-320)
+// is three 1-D zero-boundary convolutions -- z, then y, then x -- followed by
+// re-illumination of the mask voxels.  Here:
+//
+//   * strided_pass   : the z and y passes.  The volume is viewed as
+//                      [outer][axis][inner] with `inner` contiguous; a CTA stages
+//                      a tile of (TA + 2R) axis rows x TI inner columns in shared
+//                      memory and each thread produces M consecutive outputs
+//                      along the axis for one column.
+//   * contig_pass    : the x pass fused with re-illumination (and, on the last
+//                      repetition, with the uint16 quantisation).  A CTA stages
+//                      32 rows x (TX + 2R) voxels; lane = row, warp = x segment.
+//
+// Both are register-blocked: each thread reads M + 2R staged values and issues
+// M * (2R + 1) FMAs whose coefficients are compile-time indices into the launch
+// parameters (constant bank operands), in increasing tap order -- the
+// reference's summation order (src/lib/cpp/cpu/diffusion.cc:41-54).  Taps
+// outside the volume read zeros, which leave the FP32 sum unchanged, so the
+// zero boundary needs no clipping of the tap range.
+#pragma once
+
+#include "common.cuh"
+
+namespace maxi {
+
+template <int R> struct Taps { float k[2 * R + 1]; };
+
+// ---- strided (z / y) pass -------------------------------------------------
+constexpr int kStrTI = 32;    // inner columns per CTA (one warp wide)
+constexpr int kStrTA = 128;   // axis outputs per CTA
+constexpr int kStrM = 16;     // axis outputs per thread
+constexpr int kStrThreads = kStrTI * (kStrTA / kStrM);  // 256
+
+template <int R> constexpr int strided_smem_bytes() { return (kStrTA + 2 * R) * kStrTI * 4; }
+
+template <int R, typename S>
+__global__ void __launch_bounds__(kStrThreads)
+strided_pass(const S *__restrict__ in, S *__restrict__ out, int64_t A, int64_t I,
+             int64_t n_axis_tiles, int64_t n_inner_tiles, const Taps<R> taps) {
+    constexpr int ROWS = kStrTA + 2 * R;
+    extern __shared__ __align__(16) float s_tile[];  // [ROWS][kStrTI]
+
+    int64_t b = blockIdx.x;
+    const int64_t at = b % n_axis_tiles;  b /= n_axis_tiles;   // axis tile fastest: halos hit L2
+    const int64_t it = b % n_inner_tiles;
+    const int64_t o = b / n_inner_tiles;
+    const int64_t a0 = at * kStrTA, i0 = it * kStrTI;
+    const int col = threadIdx.x % kStrTI;
+    const int seg = threadIdx.x / kStrTI;
+    const bool col_ok = i0 + col < I;
+    const S *src = in + o * A * I + i0 + col;
+
+    for (int r = seg; r < ROWS; r += kStrThreads / kStrTI) {
+        const int64_t a = a0 - R + r;
+        float v = 0.0f;
+        if (col_ok && a >= 0 && a < A) v = FieldIO<S>::load(src + a * I);
+        s_tile[r * kStrTI + col] = v;
+    }
+    __syncthreads();
+
+    float acc[kStrM];
+#pragma unroll
+    for (int i = 0; i < kStrM; i++) acc[i] = 0.0f;
+    const float *s = s_tile + seg * kStrM * kStrTI + col;
+#pragma unroll
+    for (int j = 0; j < kStrM + 2 * R; j++) {
+        const float v = s[j * kStrTI];
+#pragma unroll
+        for (int i = 0; i < kStrM; i++) {
+            const int t = j - i;
+            if (t >= 0 && t <= 2 * R) acc[i] = fmaf(taps.k[t], v, acc[i]);
+        }
+    }
+
+    if (!col_ok) return;
+    S *dst = out + o * A * I + i0 + col;
+#pragma unroll
+    for (int i = 0; i < kStrM; i++) {
+        const int64_t a = a0 + seg * kStrM + i;
+        if (a < A) dst[a * I] = FieldIO<S>::narrow(acc[i]);
+    }
+}
+
+// ---- contiguous (x) pass + illumination ------------------------------------
+constexpr int kConTR = 32;   // rows per CTA (lane = row)
+constexpr int kConM = 32;    // x outputs per thread
+constexpr int kConWarps = 8;
+constexpr int kConTX = kConWarps * kConM;  // 256 x outputs per CTA
+constexpr int kConThreads = kConWarps * 32;
+
+template <int R> constexpr int contig_width() { return ((kConTX + 2 * R) + 3) / 4 * 4; }
+// Row stride = 4 (mod 32) words: float4 reads by 32 lanes on 32 rows are conflict-free.
+template <int R> constexpr int contig_stride() {
+    return contig_width<R>() + ((4 - contig_width<R>() % 32) + 32) % 32;
+}
+template <int R> constexpr int contig_smem_bytes() { return kConTR * contig_stride<R>() * 4; }
+
+// FINAL: last repetition -- write the uint16 output (and optionally the FP32
+// field) instead of the storage-type field.
+template <int R, typename S, int MASK_FMT, bool FINAL>
+__global__ void __launch_bounds__(kConThreads)
+contig_pass(const S *__restrict__ in, S *__restrict__ out, const void *__restrict__ mask,
+            uint16_t *__restrict__ out_u16, float *__restrict__ field_out,
+            int64_t rows, int64_t nx, int64_t n_x_tiles, const Taps<R> taps) {
+    constexpr int W = contig_width<R>();
+    constexpr int STRIDE = contig_stride<R>();
+    constexpr int NJ = (kConM + 2 * R + 3) / 4 * 4;  // staged values read per thread
+    extern __shared__ __align__(16) float s_tile[];  // [kConTR][STRIDE]
+
+    const int64_t xt = blockIdx.x % n_x_tiles;
+    const int64_t r0 = (blockIdx.x / n_x_tiles) * kConTR;
+    const int64_t x0 = xt * kConTX;
+    const int tid = threadIdx.x;
+
+    for (int e = tid; e < kConTR * W; e += kConThreads) {
+        const int r = e / W, c = e % W;
+        const int64_t row = r0 + r, x = x0 - R + c;
+        float v = 0.0f;
+        if (row < rows && x >= 0 && x < nx) v = FieldIO<S>::load(in + row * nx + x);
+        s_tile[r * STRIDE + c] = v;
+    }
+    __syncthreads();
+
+    const int lane = tid & 31, warp = tid >> 5;
+    float acc[kConM];
+#pragma unroll
+    for (int i = 0; i < kConM; i++) acc[i] = 0.0f;
+    const float *s = s_tile + lane * STRIDE + warp * kConM;
+#pragma unroll
+    for (int j4 = 0; j4 < NJ; j4 += 4) {
+        const float4 q = *reinterpret_cast<const float4 *>(s + j4);
+        const float vv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int j = j4 + u;
+#pragma unroll
+            for (int i = 0; i < kConM; i++) {
+                const int t = j - i;
+                if (t >= 0 && t <= 2 * R) acc[i] = fmaf(taps.k[t], vv[u], acc[i]);
+            }
+        }
+    }
+    __syncthreads();
+    float *so = s_tile + lane * STRIDE + warp * kConM;
+#pragma unroll
+    for (int i = 0; i < kConM; i += 4)
+        *reinterpret_cast<float4 *>(so + i) = make_float4(acc[i], acc[i + 1], acc[i + 2], acc[i + 3]);
+    __syncthreads();
+
+    for (int e = tid; e < kConTR * kConTX; e += kConThreads) {
+        const int r = e / kConTX, c = e % kConTX;
+        const int64_t row = r0 + r, x = x0 + c;
+        if (row >= rows || x >= nx) continue;
+        const int64_t idx = row * nx + x;
+        float v = s_tile[r * STRIDE + c];
+        if (MaskIO<MASK_FMT>::get(mask, idx)) v = 1.0f;  // re-illumination
+        if (FINAL) {
+            out_u16[idx] = quantise_u16(v);
+            if (field_out) field_out[idx] = v;
+        } else {
+            out[idx] = FieldIO<S>::narrow(v);
+        }
+    }
+}
+
+// ---- generic pass (any radius, FP64, reference rounding) -------------------
+// One output per thread, direct reads along the axis.  Used for the FP64
+// error-reference form, for bit-identical reference rounding (separate
+// multiply and add, tap range clipped as in diffusion.cc:41-54) and for radii
+// above kMaxUnrolledRadius.
+template <typename Acc> struct GenericTaps { Acc k[2 * kMaxRadius + 1]; };
+
+// Rounded multiply and add that the compiler may not fuse into an FMA.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
+template <typename S, bool EXACT, bool X_PASS, int MASK_FMT, bool FINAL>
+__global__ void __launch_bounds__(256)
+generic_pass(const S *__restrict__ in, S *__restrict__ out, const void *__restrict__ mask,
+             uint16_t *__restrict__ out_u16, void *__restrict__ field_out,
+             int64_t n, int64_t A, int64_t stride, int radius,
+             const GenericTaps<typename FieldIO<S>::Acc> taps) {
+    using Acc = typename FieldIO<S>::Acc;
+    const int64_t idx = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const int64_t a = (idx / stride) % A;
+    const int64_t lo = -(a < radius ? a : (int64_t) radius);
+    const int64_t hi = (A - a - 1 < radius) ? A - a - 1 : (int64_t) radius;
+    Acc sum = Acc(0);
+    for (int64_t t = lo; t <= hi; t++) {
+        const Acc v = FieldIO<S>::load(in + idx + t * stride);
+        if (EXACT) sum = add_rn(sum, mul_rn(v, taps.k[radius + t]));
+        else sum = fma(taps.k[radius + t], v, sum);
+    }
+    if (X_PASS) {
+        if (MaskIO<MASK_FMT>::get(mask, idx)) sum = Acc(1);
+        if (FINAL) {
+            out_u16[idx] = quantise_u16(sum);
+            if (field_out) static_cast<Acc *>(field_out)[idx] = sum;
+            return;
+        }
+    }
+    out[idx] = FieldIO<S>::narrow(sum);
+}
+
+// mask -> {0, 1} field (src/lib/cpp/cpu/diffusion.cc:243-247); with FINAL set
+// (zero repetitions) the quantised output and field are written directly.
+template <typename S, int MASK_FMT, bool FINAL>
+__global__ void mask_to_field(const void *__restrict__ mask, S *__restrict__ field,
+                              uint16_t *__restrict__ out_u16, void *__restrict__ field_out, int64_t n) {
+    using Acc = typename FieldIO<S>::Acc;
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t) gridDim.x * blockDim.x) {
+        const bool m = MaskIO<MASK_FMT>::get(mask, i);
+        if (FINAL) {
+            if (out_u16) out_u16[i] = m ? 65535 : 0;
+            if (field_out) static_cast<Acc *>(field_out)[i] = m ? Acc(1) : Acc(0);
+        } else {
+            field[i] = FieldIO<S>::narrow(m ? Acc(1) : Acc(0));
+        }
+    }
+}
+
+}  // namespace maxi

@@ -1,0 +1,9 @@
+// Instantiation of the unrolled passes for the bf16 field storage type.
+#include "unrolled_impl.cuh"
+
+namespace maxi {
+
+template cudaError_t dispatch_unrolled<__nv_bfloat16>(const Volume &, const void *, int, const float *, int, int64_t,
+                                           __nv_bfloat16 *, __nv_bfloat16 *, uint16_t *, float *, cudaStream_t);
+
+}  // namespace maxi

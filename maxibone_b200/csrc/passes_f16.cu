@@ -1,0 +1,9 @@
+// Instantiation of the unrolled passes for the f16 field storage type.
+#include "unrolled_impl.cuh"
+
+namespace maxi {
+
+template cudaError_t dispatch_unrolled<__half>(const Volume &, const void *, int, const float *, int, int64_t,
+                                           __half *, __half *, uint16_t *, float *, cudaStream_t);
+
+}  // namespace maxi

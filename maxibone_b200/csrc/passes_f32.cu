@@ -1,0 +1,11 @@
+// Instantiation of the unrolled passes for the f32 field storage type.
+#include "unrolled_impl.cuh"
+
+namespace maxi {
+
+int radius_bucket(int r) { return radius_bucket_impl(r); }
+
+template cudaError_t dispatch_unrolled<float>(const Volume &, const void *, int, const float *, int, int64_t,
+                                           float *, float *, uint16_t *, float *, cudaStream_t);
+
+}  // namespace maxi

@@ -1,0 +1,25 @@
+// Unrolled CUDA-core repetition loop, instantiated per field storage type in
+// passes_<type>.cu so that the instantiations compile in parallel.
+#pragma once
+
+#include "common.cuh"
+#include "host_util.h"
+
+namespace maxi {
+
+struct Volume {
+    int64_t nz, ny, nx;
+    int64_t n() const { return nz * ny * nx; }
+};
+
+// Smallest radius with an unrolled instantiation that is >= r, or -1.
+int radius_bucket(int r);
+
+// Runs `reps` repetitions (reps >= 1) of the unrolled passes: buf0 receives
+// the initial field, buf0/buf1 ping-pong, the last x pass writes out_u16 and
+// field_out (either may be NULL).
+template <typename S>
+cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
+                              int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, cudaStream_t st);
+
+}  // namespace maxi

@@ -1,0 +1,108 @@
+// Unrolled CUDA-core repetition loop (template definitions); included by the
+// per-type instantiation units passes_f32.cu, passes_bf16.cu, passes_f16.cu.
+#pragma once
+
+#include "passes.cuh"
+#include "unrolled.h"
+#include "profiler.h"
+
+namespace maxi {
+
+// Radii with an unrolled instantiation; a radius between two of these runs
+// with the next larger one and zero-padded taps (FMAs with a zero coefficient
+// leave the FP32 sum unchanged).
+static const int kRadiusBuckets[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128};
+
+inline int radius_bucket_impl(int r) {
+    for (int b : kRadiusBuckets)
+        if (r <= b) return b;
+    return -1;
+}
+
+template <int R>
+static Taps<R> make_taps(const float *kernel, int radius) {
+    Taps<R> t;
+    for (int i = 0; i < 2 * R + 1; i++) {
+        const int off = i - R;
+        t.k[i] = (off >= -radius && off <= radius) ? kernel[radius + off] : 0.0f;
+    }
+    return t;
+}
+
+template <typename F>
+static cudaError_t set_smem(F *f, int bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+// One repetition loop on the unrolled CUDA-core passes for bucket radius R.
+template <int R, typename S>
+static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel,
+                                int radius, int64_t reps, S *buf0, S *buf1, uint16_t *out_u16,
+                                float *field_out, cudaStream_t st) {
+    const Taps<R> taps = make_taps<R>(kernel, radius);
+    const int str_smem = strided_smem_bytes<R>();
+    const int con_smem = contig_smem_bytes<R>();
+    auto *zy = strided_pass<R, S>;
+    cudaError_t e = set_smem(zy, str_smem);
+    if (e != cudaSuccess) return e;
+    auto *xu8 = contig_pass<R, S, MAXI_MASK_U8, false>;
+    auto *xu8f = contig_pass<R, S, MAXI_MASK_U8, true>;
+    auto *xbp = contig_pass<R, S, MAXI_MASK_BITPACKED, false>;
+    auto *xbpf = contig_pass<R, S, MAXI_MASK_BITPACKED, true>;
+    for (auto *f : {xu8, xu8f, xbp, xbpf})
+        if ((e = set_smem(f, con_smem)) != cudaSuccess) return e;
+    auto *xpass = mask_fmt == MAXI_MASK_U8 ? xu8 : xbp;
+    auto *xfinal = mask_fmt == MAXI_MASK_U8 ? xu8f : xbpf;
+
+    const int64_t n = v.n();
+    {
+        const int threads = 256;
+        const int64_t blocks = std::min<int64_t>((n + threads - 1) / threads, 148 * 64);
+        ProfScope ps(MAXI_KERNEL_INIT, st);
+        if (mask_fmt == MAXI_MASK_U8)
+            mask_to_field<S, MAXI_MASK_U8, false><<<blocks, threads, 0, st>>>(mask, buf0, nullptr, nullptr, n);
+        else
+            mask_to_field<S, MAXI_MASK_BITPACKED, false><<<blocks, threads, 0, st>>>(mask, buf0, nullptr, nullptr, n);
+    }
+    // z pass: [1][nz][ny*nx]; y pass: [nz][ny][nx]
+    const int64_t zI = v.ny * v.nx, zA = v.nz, zat = ceil_div(zA, kStrTA), zit = ceil_div(zI, kStrTI);
+    const int64_t yI = v.nx, yA = v.ny, yO = v.nz, yat = ceil_div(yA, kStrTA), yit = ceil_div(yI, kStrTI);
+    const int64_t rows = v.nz * v.ny, xt = ceil_div(v.nx, kConTX), xrb = ceil_div(rows, kConTR);
+    for (int64_t rep = 0; rep < reps; rep++) {
+        {
+            ProfScope ps(MAXI_KERNEL_Z, st);
+            zy<<<zat * zit, kStrThreads, str_smem, st>>>(buf0, buf1, zA, zI, zat, zit, taps);
+        }
+        {
+            ProfScope ps(MAXI_KERNEL_Y, st);
+            zy<<<yat * yit * yO, kStrThreads, str_smem, st>>>(buf1, buf0, yA, yI, yat, yit, taps);
+        }
+        if (rep + 1 < reps) {
+            ProfScope ps(MAXI_KERNEL_X, st);
+            xpass<<<xt * xrb, kConThreads, con_smem, st>>>(buf0, buf1, mask, nullptr, nullptr, rows, v.nx, xt, taps);
+            std::swap(buf0, buf1);
+        } else {
+            ProfScope ps(MAXI_KERNEL_X_FINAL, st);
+            xfinal<<<xt * xrb, kConThreads, con_smem, st>>>(buf0, buf1, mask, out_u16, field_out, rows, v.nx, xt, taps);
+        }
+    }
+    return cudaGetLastError();
+}
+
+template <typename S>
+cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel,
+                                     int radius, int64_t reps, S *b0, S *b1, uint16_t *out_u16,
+                                     float *field_out, cudaStream_t st) {
+    switch (radius_bucket_impl(radius)) {
+#define MAXI_CASE(RB) \
+    case RB: return run_unrolled<RB, S>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, st);
+        MAXI_CASE(1) MAXI_CASE(2) MAXI_CASE(3) MAXI_CASE(4) MAXI_CASE(6) MAXI_CASE(8) MAXI_CASE(12)
+        MAXI_CASE(16) MAXI_CASE(24) MAXI_CASE(32) MAXI_CASE(48) MAXI_CASE(64) MAXI_CASE(96) MAXI_CASE(128)
+#undef MAXI_CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+
+}  // namespace maxi

@@ -1,0 +1,115 @@
+"""Device-resident API: the diffusion on torch CUDA tensors, enqueued on the
+current torch stream (torch supplies device memory and streams; the work is
+the library's CUDA kernels).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+
+_FIELD_OUT_DTYPE = {"f32": torch.float32, "bf16": torch.float32, "f16": torch.float32, "f64": torch.float64}
+
+
+def workspace_bytes(shape, field: str = "f32") -> int:
+    nz, ny, nx = shape
+    n = _lib.lib().maxi_diffusion_workspace_size(nz, ny, nx, _lib.FIELD_TYPES[field])
+    if n < 0:
+        raise ValueError(f"invalid shape {shape} or field type {field}")
+    return int(n)
+
+
+def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor | None = None,
+            field: str = "f32", field_out: torch.Tensor | None = None, shape=None,
+            reference_rounding: bool = False, workspace: torch.Tensor | None = None,
+            stream: torch.cuda.Stream | None = None) -> None:
+    """Run the diffusion on device buffers.
+
+    mask: uint8 [nz, ny, nx] CUDA tensor (set when > 0), or a bit-packed int32/uint32
+          tensor of ceil(N/32) words (MSB first) together with `shape`.
+    kernel: 1-D array-like of odd length (host values; cast to float32).
+    output: uint16 CUDA tensor of the volume's shape, or None.
+    field: storage type between passes: "f32", "bf16", "f16" or "f64".
+    field_out: final field before quantisation (float32; float64 for "f64"), or None.
+    workspace: uint8 CUDA tensor of at least workspace_bytes(shape, field), or None.
+    """
+    if not mask.is_cuda:
+        raise ValueError("mask must be a CUDA tensor")
+    if mask.dtype == torch.uint8:
+        if mask.dim() != 3:
+            raise ValueError(f"uint8 mask must be 3-D, got {tuple(mask.shape)}")
+        fmt, (nz, ny, nx) = _lib.MASK_FORMATS["u8"], mask.shape
+    elif mask.dtype in (torch.int32, torch.uint32):
+        if shape is None:
+            raise ValueError("a bit-packed mask needs `shape`")
+        nz, ny, nx = shape
+        if mask.numel() < (nz * ny * nx + 31) // 32:
+            raise ValueError("bit-packed mask has too few words for the shape")
+        fmt = _lib.MASK_FORMATS["bitpacked"]
+    else:
+        raise ValueError(f"unsupported mask dtype {mask.dtype}")
+    if not mask.is_contiguous():
+        raise ValueError("mask must be contiguous")
+    k = np.ascontiguousarray(kernel, dtype=np.float32)
+    if k.ndim != 1:
+        raise ValueError("kernel must be 1-D")
+    n = nz * ny * nx
+    if output is not None:
+        if output.dtype != torch.uint16 or not output.is_cuda or not output.is_contiguous() or output.numel() != n:
+            raise ValueError("output must be a contiguous CUDA uint16 tensor with one element per voxel")
+    if field_out is not None:
+        want = _FIELD_OUT_DTYPE[field]
+        if field_out.dtype != want or not field_out.is_cuda or not field_out.is_contiguous() or field_out.numel() != n:
+            raise ValueError(f"field_out must be a contiguous CUDA {want} tensor with one element per voxel")
+    ws_ptr, ws_bytes = None, 0
+    if workspace is not None:
+        ws_ptr, ws_bytes = workspace.data_ptr(), workspace.numel() * workspace.element_size()
+    st = stream if stream is not None else torch.cuda.current_stream(mask.device)
+    flags = _lib.FLAG_REFERENCE_ROUNDING if reference_rounding else 0
+    with torch.cuda.device(mask.device):
+        _lib.check(_lib.lib().maxi_diffusion_device(
+            mask.data_ptr(), fmt, nz, ny, nx, k.ctypes.data, k.shape[0], int(repititions),
+            output.data_ptr() if output is not None else None,
+            field_out.data_ptr() if field_out is not None else None,
+            _lib.FIELD_TYPES[field], flags, ws_ptr, ws_bytes, st.cuda_stream))
+
+
+def bitpack(mask: torch.Tensor, stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+    """uint8 CUDA mask -> int32 words (uint32 bit patterns), MSB first, `mask & 1`
+    per voxel (the reference bitpacking.encode).  The mask is padded with zeros
+    to a multiple of 32 voxels."""
+    flat = mask.reshape(-1)
+    n = flat.numel()
+    if n % 32:
+        flat = torch.cat([flat, flat.new_zeros(32 - n % 32)])
+    out = torch.empty(flat.numel() // 32, dtype=torch.int32, device=mask.device)
+    st = stream if stream is not None else torch.cuda.current_stream(mask.device)
+    with torch.cuda.device(mask.device):
+        _lib.check(_lib.lib().maxi_bitpack_encode(flat.data_ptr(), flat.numel(), out.data_ptr(), st.cuda_stream))
+    return out
+
+
+def bitunpack(packed: torch.Tensor, n: int, stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+    """int32/uint32 words -> uint8 {0,1} per voxel (the reference bitpacking.decode)."""
+    n32 = (n + 31) // 32 * 32
+    out = torch.empty(n32, dtype=torch.uint8, device=packed.device)
+    st = stream if stream is not None else torch.cuda.current_stream(packed.device)
+    with torch.cuda.device(packed.device):
+        _lib.check(_lib.lib().maxi_bitpack_decode(packed.data_ptr(), n32, out.data_ptr(), st.cuda_stream))
+    return out[:n]
+
+
+def profile_enable(on: bool = True) -> None:
+    """Bracket every library kernel launch with CUDA events (see maxi_profile_read)."""
+    _lib.check(_lib.lib().maxi_profile_enable(1 if on else 0))
+
+
+def profile_read() -> dict:
+    """{kind: (total device ms, launches)} since the last read; waits for the events."""
+    import ctypes
+    n = len(_lib.KERNEL_KINDS)
+    ms = (ctypes.c_double * n)()
+    cnt = (ctypes.c_int64 * n)()
+    _lib.check(_lib.lib().maxi_profile_read(ctypes.addressof(ms), ctypes.addressof(cnt), n))
+    return {k: (ms[i], cnt[i]) for i, k in enumerate(_lib.KERNEL_KINDS) if cnt[i]}

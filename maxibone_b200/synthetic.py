@@ -1,0 +1,74 @@
+"""Seeded synthetic masks standing in for maxibone's implant masks.
+
+The reference's tomograms are not available, so the workloads use masks with
+the stated shapes and foreground fractions:
+
+* ``spheres_mask``: union of random spheres (radii uniform in a range, centres
+  uniform in the box), numpy ``default_rng(seed)``.
+* ``bone_implant_mask``: a solid cylinder along z through the centre (the
+  implant) plus thresholded two-octave value noise (trabecular-like sheets and
+  struts), topped up to a target foreground fraction.  Built with torch on the
+  given device so a 1024^3 mask takes well under a second on a GPU.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def spheres_mask(shape, n_spheres: int = 40, r_range=(4, 20), seed: int = 0) -> np.ndarray:
+    nz, ny, nx = shape
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(0, 1, size=(n_spheres, 3)) * np.array([nz, ny, nx])
+    radii = rng.uniform(r_range[0], r_range[1], size=n_spheres)
+    mask = np.zeros(shape, dtype=np.uint8)
+    for (cz, cy, cx), r in zip(centres, radii):
+        z0, z1 = max(0, int(cz - r)), min(nz, int(cz + r) + 1)
+        y0, y1 = max(0, int(cy - r)), min(ny, int(cy + r) + 1)
+        x0, x1 = max(0, int(cx - r)), min(nx, int(cx + r) + 1)
+        if z0 >= z1 or y0 >= y1 or x0 >= x1:
+            continue
+        z = np.arange(z0, z1)[:, None, None] - cz
+        y = np.arange(y0, y1)[None, :, None] - cy
+        x = np.arange(x0, x1)[None, None, :] - cx
+        mask[z0:z1, y0:y1, x0:x1] |= (z * z + y * y + x * x <= r * r).astype(np.uint8)
+    return mask
+
+
+def random_mask(shape, fraction: float, seed: int = 0) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return (rng.random(shape) < fraction).astype(np.uint8)
+
+
+def bone_implant_mask(shape, seed: int = 0, foreground: float = 0.25, implant_radius: float = 120.0,
+                      device="cpu"):
+    """uint8 torch tensor [nz, ny, nx] on `device`: implant cylinder + noise structures."""
+    import torch
+    import torch.nn.functional as F
+
+    nz, ny, nx = shape
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    field = None
+    for cells, weight in ((16, 1.0), (48, 0.5)):
+        coarse = torch.rand((1, 1, max(2, nz * cells // 1024 + 2), max(2, ny * cells // 1024 + 2),
+                             max(2, nx * cells // 1024 + 2)), generator=g)
+        coarse = coarse.to(device=device, dtype=torch.float32)
+        up = F.interpolate(coarse, size=(nz, ny, nx), mode="trilinear", align_corners=True)[0, 0]
+        field = up * weight if field is None else field.add_(up, alpha=weight)
+        del up
+    # Ridge structure: voxels near the noise's median level form thin sheets.
+    flat = field.reshape(-1)
+    idx = torch.randint(0, flat.numel(), (1 << 20,), generator=g).to(device)
+    sample = flat[idx]
+    median = sample.median()
+    dist = (field - median).abs_()
+    del field
+    yy = torch.arange(ny, device=device, dtype=torch.float32)[:, None] - (ny - 1) / 2
+    xx = torch.arange(nx, device=device, dtype=torch.float32)[None, :] - (nx - 1) / 2
+    cyl = (yy * yy + xx * xx) <= implant_radius * implant_radius
+    cyl_frac = cyl.float().mean().item()
+    want = max(0.0, (foreground - cyl_frac) / max(1e-9, 1.0 - cyl_frac))
+    thr = torch.quantile(dist.reshape(-1)[idx].float(), want).item() if want > 0 else -1.0
+    mask = (dist <= thr)
+    del dist
+    mask |= cyl[None, :, :]
+    return mask.to(torch.uint8)

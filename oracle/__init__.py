@@ -1,0 +1,166 @@
+"""Test oracle for the mask-diffusion path (test infrastructure only).
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this package, and only as the checker or the timed CPU
+baseline.  The product (``maxibone_b200``) never imports it.
+
+Three oracles live here:
+
+* ``diffusion_in_memory``: ctypes binding of ``diffusion_oracle.c``, a C
+  restatement of the reference OpenMP backend
+  (src/lib/cpp/cpu/diffusion.cc:31-57,191-195,243-247,295-302,314-320,339-374).
+  It is bit-identical to the reference's own module (pinned by the golden
+  vectors in tests/golden and, where the reference tree is present, by running
+  the reference module built into ``oracle/_ref``).
+* ``scipy_chain``: the oracle of the reference's own unit test,
+  src/test/test_diffusion.py:49-59 (scipy ``convolve1d`` with mode='constant').
+* ``diffusion_f64``: the same algorithm in FP64, the error reference for the
+  reduced-precision field forms.
+
+``reference_module()`` imports the reference's own ``diffusion`` pybind module
+from ``oracle/_ref`` when it has been built (``make -C oracle ref``).
+"""
+from __future__ import annotations
+
+import ctypes
+import importlib.util
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def build() -> None:
+    """Compile the C restatement (and the reference modules where the reference tree exists)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    if os.path.isdir(os.environ.get("MAXI_REFERENCE_SRC", "/root/reference/src")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle_diffusion.so")
+        if not os.path.exists(path):
+            subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+        lib = ctypes.CDLL(path)
+        i64, p = ctypes.c_int64, ctypes.c_void_p
+        lib.oracle_diffusion_in_memory.argtypes = [p, i64, i64, i64, p, i64, i64, p, p]
+        lib.oracle_diffusion_in_memory.restype = ctypes.c_int
+        lib.oracle_diffusion_f64.argtypes = [p, i64, i64, i64, p, i64, i64, p]
+        lib.oracle_diffusion_f64.restype = ctypes.c_int
+        lib.oracle_diffusion_on_disk_semantics.argtypes = [p, i64, i64, i64, p, i64, i64, p]
+        lib.oracle_diffusion_on_disk_semantics.restype = ctypes.c_int
+        lib.oracle_convolve_axis_f32.argtypes = [p, p, p, i64, i64, i64, ctypes.c_int, i64]
+        lib.oracle_convolve_axis_f32.restype = None
+        lib.oracle_bitpack_encode_u32.argtypes = [p, i64, p]
+        lib.oracle_bitpack_encode_u32.restype = None
+        lib.oracle_bitpack_decode_u32.argtypes = [p, i64, p]
+        lib.oracle_bitpack_decode_u32.restype = None
+        _LIB = lib
+    return _LIB
+
+
+def _ptr(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def diffusion_in_memory(mask: np.ndarray, kernel: np.ndarray, repititions: int):
+    """FP32 reference semantics. Returns (uint16 output, float32 final field)."""
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    k = np.ascontiguousarray(kernel, dtype=np.float32)
+    nz, ny, nx = m.shape
+    out = np.empty(m.shape, np.uint16)
+    field = np.empty(m.shape, np.float32)
+    rc = _lib().oracle_diffusion_in_memory(_ptr(m), nz, ny, nx, _ptr(k), k.shape[0], int(repititions),
+                                           _ptr(out), _ptr(field))
+    if rc != 0:
+        raise MemoryError("oracle could not allocate its working buffers")
+    return out, field
+
+
+def diffusion_f64(mask: np.ndarray, kernel: np.ndarray, repititions: int) -> np.ndarray:
+    """FP64 field after `repititions` steps (kernel promoted to FP64 as given)."""
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    k = np.ascontiguousarray(kernel, dtype=np.float64)
+    nz, ny, nx = m.shape
+    field = np.empty(m.shape, np.float64)
+    rc = _lib().oracle_diffusion_f64(_ptr(m), nz, ny, nx, _ptr(k), k.shape[0], int(repititions), _ptr(field))
+    if rc != 0:
+        raise MemoryError("oracle could not allocate its working buffers")
+    return field
+
+
+def diffusion_on_disk_semantics(mask: np.ndarray, kernel: np.ndarray, repititions: int) -> np.ndarray:
+    """uint16 output of the reference's on-disk variant (mask rebuilt as field == 1.0f each step)."""
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    k = np.ascontiguousarray(kernel, dtype=np.float32)
+    nz, ny, nx = m.shape
+    out = np.empty(m.shape, np.uint16)
+    rc = _lib().oracle_diffusion_on_disk_semantics(_ptr(m), nz, ny, nx, _ptr(k), k.shape[0],
+                                                   int(repititions), _ptr(out))
+    if rc != 0:
+        raise MemoryError("oracle could not allocate its working buffers")
+    return out
+
+
+def convolve_axis(field: np.ndarray, kernel: np.ndarray, dim: int) -> np.ndarray:
+    """One zero-boundary FP32 pass along axis `dim` (reference diffusion_core)."""
+    f = np.ascontiguousarray(field, dtype=np.float32)
+    k = np.ascontiguousarray(kernel, dtype=np.float32)
+    out = np.empty_like(f)
+    nz, ny, nx = f.shape
+    _lib().oracle_convolve_axis_f32(_ptr(f), _ptr(k), _ptr(out), nz, ny, nx, int(dim), k.shape[0] // 2)
+    return out
+
+
+def bitpack_encode(mask: np.ndarray) -> np.ndarray:
+    """uint8 mask -> uint32 words, MSB first (reference cpu_seq/bitpacking.cc:9-24)."""
+    m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+    assert m.size % 32 == 0
+    out = np.empty(m.size // 32, np.uint32)
+    _lib().oracle_bitpack_encode_u32(_ptr(m), m.size, _ptr(out))
+    return out
+
+
+def bitpack_decode(packed: np.ndarray, n: int) -> np.ndarray:
+    p = np.ascontiguousarray(packed, dtype=np.uint32)
+    out = np.empty(n, np.uint8)
+    _lib().oracle_bitpack_decode_u32(_ptr(p), n, _ptr(out))
+    return out
+
+
+def scipy_chain(mask: np.ndarray, kernel: np.ndarray, repititions: int) -> np.ndarray:
+    """The reference unit test's oracle (src/test/test_diffusion.py:49-59), uint16 result."""
+    import scipy.ndimage as ndi
+    a = np.asarray(mask).astype(bool)
+    k = np.asarray(kernel, dtype=np.float32)
+    buf0 = a.astype(np.float32)
+    buf1 = np.zeros_like(buf0)
+    for _ in range(repititions):
+        buf1[:] = ndi.convolve1d(buf0, k, axis=0, mode="constant")
+        buf0[:] = ndi.convolve1d(buf1, k, axis=1, mode="constant")
+        buf1[:] = ndi.convolve1d(buf0, k, axis=2, mode="constant")
+        buf1[a] = 1
+        buf0, buf1 = buf1, buf0
+    return np.floor(buf0 * 65535).astype(np.uint16)
+
+
+def reference_module(name: str = "diffusion"):
+    """Import the reference's own CPU pybind module built into oracle/_ref, or None."""
+    ref_dir = os.path.join(HERE, "_ref")
+    if not os.path.isdir(ref_dir):
+        return None
+    for f in os.listdir(ref_dir):
+        if f.startswith(name + ".") and f.endswith(".so"):
+            spec = importlib.util.spec_from_file_location(name, os.path.join(ref_dir, f))
+            mod = importlib.util.module_from_spec(spec)
+            try:
+                spec.loader.exec_module(mod)
+            except ImportError:
+                return None
+            return mod
+    return None

@@ -1,0 +1,185 @@
+"""Parity of the CUDA library against the oracle (run with -m gpu on a B200).
+
+Criteria (from the reference's test, src/test/test_diffusion.py:90-98, and
+the path's FP32 contract):
+  * FP32 field: max |GPU - oracle| <= 1e-5 (summation order and FMA only);
+  * uint16 output: within 1 LSB of the oracle;
+  * mask voxels: exactly 65535 (re-illumination is bit-exact);
+  * reference-rounding mode: bit-identical to the oracle (and so to the
+    reference module) in both the field and the uint16 output;
+  * FP64 form: within 1e-12 of the CPU FP64 oracle;
+  * BF16 / FP16 field forms: max abs error vs FP64 within the stated bounds.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from conftest import DIFFUSION_CASES, load_golden
+from maxibone_b200 import device, diffusion, gauss_kernel
+from maxibone_b200.synthetic import random_mask, spheres_mask
+
+pytestmark = pytest.mark.gpu
+
+F32_TOL = 1e-5
+# Max abs error vs the FP64 form, per storage type (field values lie in [0, 1]).
+LOWP_TOL = {"bf16": 4e-3, "f16": 5e-4}
+
+
+def run_gpu(mask, kernel, reps, field="f32", mask_format="u8", reference_rounding=False):
+    m = torch.from_numpy(np.ascontiguousarray(mask, np.uint8)).cuda()
+    shape = tuple(mask.shape)
+    out = torch.empty(shape, dtype=torch.uint16, device="cuda")
+    fo = torch.empty(shape, dtype=torch.float64 if field == "f64" else torch.float32, device="cuda")
+    if mask_format == "bitpacked":
+        m = device.bitpack(m)
+    device.diffuse(m, kernel, reps, output=out, field=field, field_out=fo, shape=shape,
+                   reference_rounding=reference_rounding)
+    torch.cuda.synchronize()
+    return out.cpu().numpy(), fo.cpu().numpy()
+
+
+def assert_parity(mask, kernel, reps, got_u16, got_field, want_u16, want_field):
+    np.testing.assert_array_less(np.abs(got_field.astype(np.float64) - want_field), F32_TOL + 1e-30)
+    assert np.abs(got_u16.astype(np.int32) - want_u16.astype(np.int32)).max(initial=0) <= 1
+    if reps > 0:
+        assert np.all(got_u16[np.asarray(mask) > 0] == 65535)
+
+
+@pytest.mark.parametrize("name", DIFFUSION_CASES)
+def test_golden_cases_fp32(name):
+    mask, kernel, reps, golden, entry = load_golden(name)
+    want_u16, want_field = oracle.diffusion_in_memory(mask, kernel, reps)
+    got_u16, got_field = run_gpu(mask, kernel, reps)
+    assert_parity(mask, kernel, reps, got_u16, got_field, want_u16, want_field)
+    if golden is not None:
+        assert np.abs(got_u16.astype(np.int32) - golden.astype(np.int32)).max(initial=0) <= 1
+
+
+@pytest.mark.parametrize("name", DIFFUSION_CASES)
+def test_golden_cases_reference_rounding_bit_exact(name):
+    mask, kernel, reps, golden, entry = load_golden(name)
+    want_u16, want_field = oracle.diffusion_in_memory(mask, kernel, reps)
+    got_u16, got_field = run_gpu(mask, kernel, reps, reference_rounding=True)
+    np.testing.assert_array_equal(got_u16, want_u16)
+    np.testing.assert_array_equal(got_field, want_field)
+    if golden is not None:
+        np.testing.assert_array_equal(got_u16, golden)
+
+
+# Every unrolled radius bucket, radii between buckets (zero-padded taps), and
+# radii above the unrolled set (generic pass).
+@pytest.mark.parametrize("radius", [1, 2, 3, 4, 5, 6, 7, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 96, 128, 140])
+def test_radius_coverage(radius):
+    shape = (19, 37, 300) if radius > 40 else (23, 45, 77)
+    mask = random_mask(shape, 0.03, seed=radius)
+    kernel = gauss_kernel(radius / 4.0).astype(np.float32)
+    assert kernel.shape[0] == 2 * radius + 1
+    want_u16, want_field = oracle.diffusion_in_memory(mask, kernel, 2)
+    got_u16, got_field = run_gpu(mask, kernel, 2)
+    assert_parity(mask, kernel, 2, got_u16, got_field, want_u16, want_field)
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (1, 1, 40), (1, 40, 1), (40, 1, 1), (2, 3, 5), (33, 17, 70),
+                                   (130, 7, 9), (5, 129, 260), (3, 2, 513)])
+def test_edge_shapes(shape):
+    mask = random_mask(shape, 0.1, seed=sum(shape))
+    kernel = gauss_kernel(3).astype(np.float32)  # radius 12: larger than several axes
+    want_u16, want_field = oracle.diffusion_in_memory(mask, kernel, 3)
+    got_u16, got_field = run_gpu(mask, kernel, 3)
+    assert_parity(mask, kernel, 3, got_u16, got_field, want_u16, want_field)
+
+
+@pytest.mark.parametrize("fill", [0, 1])
+def test_empty_and_full_masks(fill):
+    mask = np.full((20, 21, 22), fill, np.uint8)
+    kernel = gauss_kernel(2).astype(np.float32)
+    got_u16, got_field = run_gpu(mask, kernel, 4)
+    want_u16, want_field = oracle.diffusion_in_memory(mask, kernel, 4)
+    assert_parity(mask, kernel, 4, got_u16, got_field, want_u16, want_field)
+    if fill == 0:
+        assert not got_u16.any()
+    else:
+        assert np.all(got_u16 == 65535)
+
+
+def test_non_binary_mask_values_count_as_set():
+    mask = random_mask((16, 16, 16), 0.2, seed=3) * np.uint8(7)
+    mask[0, 0, :8] = 255
+    kernel = gauss_kernel(1.5).astype(np.float32)
+    want_u16, want_field = oracle.diffusion_in_memory(mask, kernel, 3)
+    got_u16, got_field = run_gpu(mask, kernel, 3)
+    assert_parity(mask, kernel, 3, got_u16, got_field, want_u16, want_field)
+
+
+def test_bitpacked_mask_equals_u8_mask():
+    mask = spheres_mask((40, 44, 50), 10, (3, 8), seed=4)  # 88000 voxels: words straddle rows
+    kernel = gauss_kernel(2).astype(np.float32)
+    a_u16, a_field = run_gpu(mask, kernel, 5)
+    b_u16, b_field = run_gpu(mask, kernel, 5, mask_format="bitpacked")
+    np.testing.assert_array_equal(a_u16, b_u16)
+    np.testing.assert_array_equal(a_field, b_field)
+
+
+def test_device_bitpack_matches_reference_layout():
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "bitpack_u32.npz"))
+    packed = device.bitpack(torch.from_numpy(z["mask"]).cuda())
+    np.testing.assert_array_equal(packed.cpu().numpy().view(np.uint32), z["packed"])
+    decoded = device.bitunpack(torch.from_numpy(z["packed"].view(np.int32)).cuda(), z["mask"].size)
+    np.testing.assert_array_equal(decoded.cpu().numpy(), z["decoded"])
+
+
+def test_fp64_form_matches_cpu_fp64_oracle():
+    mask = spheres_mask((24, 28, 36), 8, (2, 6), seed=8)
+    k64 = gauss_kernel(2.0)
+    want = oracle.diffusion_f64(mask, k64.astype(np.float32).astype(np.float64), 6)
+    _, got = run_gpu(mask, k64.astype(np.float32), 6, field="f64")
+    assert np.abs(got - want).max() < 1e-12
+
+
+@pytest.mark.parametrize("field", ["bf16", "f16"])
+def test_low_precision_fields_vs_fp64(field):
+    mask = spheres_mask((48, 48, 48), 12, (3, 8), seed=9)
+    kernel = gauss_kernel(2.0).astype(np.float32)
+    _, want = run_gpu(mask, kernel, 20, field="f64")
+    got_u16, got = run_gpu(mask, kernel, 20, field=field)
+    err = np.abs(got.astype(np.float64) - want)
+    assert err.max() <= LOWP_TOL[field], err.max()
+    assert np.all(got_u16[mask > 0] == 65535)
+    assert np.all(got[mask > 0] == 1.0)
+
+
+def test_dropin_host_call_matches_oracle():
+    mask, kernel, reps, golden, entry = load_golden("spheres_32x40x48_s2_r5")
+    out = np.zeros(mask.shape, np.uint16)
+    diffusion(mask.astype(bool), kernel.astype(np.float64), out, reps)
+    assert np.abs(out.astype(np.int32) - golden.astype(np.int32)).max() <= 1
+
+
+def test_dropin_zero_repetitions():
+    mask = random_mask((5, 6, 7), 0.5, seed=1)
+    out = np.zeros(mask.shape, np.uint16)
+    diffusion(mask, gauss_kernel(1), out, 0)
+    np.testing.assert_array_equal(out, mask.astype(np.uint16) * 65535)
+
+
+def test_workspace_reuse_and_stream():
+    mask = random_mask((30, 31, 32), 0.05, seed=12)
+    kernel = gauss_kernel(2).astype(np.float32)
+    m = torch.from_numpy(mask).cuda()
+    ws = torch.empty(device.workspace_bytes(mask.shape, "f32"), dtype=torch.uint8, device="cuda")
+    s = torch.cuda.Stream()
+    outs = []
+    for _ in range(2):
+        out = torch.empty(mask.shape, dtype=torch.uint16, device="cuda")
+        with torch.cuda.stream(s):
+            device.diffuse(m, kernel, 3, output=out, workspace=ws)
+        s.synchronize()
+        outs.append(out.cpu().numpy())
+    np.testing.assert_array_equal(outs[0], outs[1])
+    want, _ = oracle.diffusion_in_memory(mask, kernel, 3)
+    assert np.abs(outs[0].astype(np.int32) - want.astype(np.int32)).max() <= 1
+    with pytest.raises(ValueError):
+        device.diffuse(m, kernel, 3, output=out, workspace=ws[:100])

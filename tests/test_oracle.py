@@ -1,0 +1,76 @@
+"""Pins the CPU oracle (the parity checker) against the reference.
+
+* golden vectors made by the reference's own OpenMP module (tests/golden);
+* the reference module itself where it has been built into oracle/_ref;
+* the scipy chain of the reference's unit test (src/test/test_diffusion.py:49-98),
+  with its 1-LSB criterion, at the test's own configuration.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import DIFFUSION_CASES, load_golden
+from maxibone_b200.kernels import gauss_kernel
+
+
+@pytest.mark.parametrize("name", DIFFUSION_CASES)
+def test_oracle_matches_reference_golden_bit_for_bit(name):
+    mask, kernel, reps, out, entry = load_golden(name)
+    got, _ = oracle.diffusion_in_memory(mask, kernel, reps)
+    assert hashlib.sha256(got.tobytes()).hexdigest() == entry["sha256"]
+    if out is not None:
+        np.testing.assert_array_equal(got, out)
+
+
+def test_oracle_bitpack_matches_reference_golden():
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "bitpack_u32.npz"))
+    np.testing.assert_array_equal(oracle.bitpack_encode(z["mask"]), z["packed"])
+    np.testing.assert_array_equal(oracle.bitpack_decode(z["packed"], z["mask"].size), z["decoded"])
+
+
+def test_oracle_matches_reference_module_if_built():
+    ref = oracle.reference_module()
+    if ref is None:
+        pytest.skip("reference module not built in oracle/_ref")
+    rng = np.random.default_rng(11)
+    for shape, sigma, reps in [((20, 31, 44), 2.0, 3), ((3, 64, 5), 3.0, 2), ((40, 1, 40), 1.0, 6)]:
+        mask = (rng.random(shape) > 0.85).astype(np.uint8)
+        k = gauss_kernel(sigma).astype(np.float32)
+        want = np.empty(shape, np.uint16)
+        ref.diffusion(mask, k, want, reps)
+        got, _ = oracle.diffusion_in_memory(mask, k, reps)
+        np.testing.assert_array_equal(got, want)
+
+
+def test_reference_unit_test_configuration_scipy_within_1_lsb():
+    # src/test/test_diffusion.py:19-43: n=128, sigma=3, reps=100, seed 42, rand > 0.99.
+    np.random.seed(42)
+    a = np.random.rand(128, 128, 128) > 0.99
+    kernel = gauss_kernel(3).astype(np.float32)
+    want = oracle.scipy_chain(a, kernel, 100)
+    got, _ = oracle.diffusion_in_memory(a.astype(np.uint8), kernel, 100)
+    assert np.abs(want.astype(np.int32) - got.astype(np.int32)).max() <= 1
+
+
+def test_f64_oracle_close_to_f32_oracle():
+    rng = np.random.default_rng(5)
+    mask = (rng.random((24, 30, 36)) > 0.9).astype(np.uint8)
+    k = gauss_kernel(2.0)
+    f64 = oracle.diffusion_f64(mask, k, 8)
+    _, f32 = oracle.diffusion_in_memory(mask, k.astype(np.float32), 8)
+    assert np.abs(f64 - f32).max() < 2e-6
+
+
+def test_on_disk_semantics_equal_in_memory_for_binary_field():
+    # The on-disk variant rebuilds the mask as field == 1.0f; with no non-mask voxel
+    # reaching exactly 1.0 the two agree.
+    rng = np.random.default_rng(6)
+    mask = (rng.random((16, 18, 20)) > 0.95).astype(np.uint8)
+    k = gauss_kernel(1.0).astype(np.float32)
+    a = oracle.diffusion_on_disk_semantics(mask, k, 4)
+    b, _ = oracle.diffusion_in_memory(mask, k, 4)
+    np.testing.assert_array_equal(a, b)

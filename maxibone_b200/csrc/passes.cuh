@@ -157,7 +157,7 @@ contig_pass(const S *__restrict__ in, S *__restrict__ out, const void *__restric
         float v = s_tile[r * STRIDE + c];
         if (MaskIO<MASK_FMT>::get(mask, idx)) v = 1.0f;  // re-illumination
         if (FINAL) {
-            out_u16[idx] = quantise_u16(v);
+            if (out_u16) out_u16[idx] = quantise_u16(v);
             if (field_out) field_out[idx] = v;
         } else {
             out[idx] = FieldIO<S>::narrow(v);
@@ -199,7 +199,7 @@ generic_pass(const S *__restrict__ in, S *__restrict__ out, const void *__restri
     if (X_PASS) {
         if (MaskIO<MASK_FMT>::get(mask, idx)) sum = Acc(1);
         if (FINAL) {
-            out_u16[idx] = quantise_u16(sum);
+            if (out_u16) out_u16[idx] = quantise_u16(sum);
             if (field_out) static_cast<Acc *>(field_out)[idx] = sum;
             return;
         }

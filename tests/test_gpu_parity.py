@@ -183,3 +183,14 @@ def test_workspace_reuse_and_stream():
     assert np.abs(outs[0].astype(np.int32) - want.astype(np.int32)).max() <= 1
     with pytest.raises(ValueError):
         device.diffuse(m, kernel, 3, output=out, workspace=ws[:100])
+
+
+@pytest.mark.parametrize("field", ["f32", "f64"])
+def test_field_out_without_uint16_output(field):
+    mask = random_mask((12, 20, 300), 0.05, seed=21)
+    kernel = gauss_kernel(2).astype(np.float32)
+    m = torch.from_numpy(mask).cuda()
+    fo = torch.empty(mask.shape, dtype=torch.float64 if field == "f64" else torch.float32, device="cuda")
+    device.diffuse(m, kernel, 3, output=None, field=field, field_out=fo)
+    _, want = oracle.diffusion_in_memory(mask, kernel, 3)
+    assert np.abs(fo.cpu().numpy() - want).max() < 1e-5

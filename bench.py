@@ -259,9 +259,11 @@ def main():
                 "per_kind_ms": {k: v[0] / v[1] for k, v in prof.items()},
                 "fp32_tflops_dominant": 2 * (2 * radius + 1) * vox / (dom_ms / 1e3) / 1e12,
                 "fp32_tflops_whole_step": 2 * 3 * (2 * radius + 1) * vox * reps * args.steps / (ms / 1e3) / 1e12,
-                "note": "direct FP32 stencil at radius 32 is CUDA-core bound (2*65 flop per 8 B); "
-                        "FFMA peak measured 73 TFLOP/s (profiles/fp32_peak.md)"}
+                "note": "the direct FP32 stencil at radius 32 is bound by the FP32 pipe (2*65 flop per 8 B "
+                        "of field traffic); fp32_peak_tflops = 148 SMs x 128 FMA/clk x 2 x median SM clock"}
 
+    if clocks:
+        roofline["fp32_peak_tflops"] = 148 * 128 * 2 * clocks["sm_mhz"] * 1e6 / 1e12
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",

@@ -115,6 +115,29 @@ int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int
                           void *workspace, int64_t workspace_bytes, void *stream);
 
 /*
+ * Allocation-free variant of maxi_diffusion_device() for the FP32 field.  It
+ * has no counterpart in the reference.  It serves callers that may not
+ * allocate device memory while they run (a host that owns the whole device
+ * heap through its own sub-allocator, a fixed memory budget set at start-up,
+ * code that cannot accept an allocation's synchronisation or failure in the
+ * middle of its work): the two field buffers come from a fixed 64 MiB array
+ * inside the library, so no cudaMalloc or other allocation happens.
+ *   - at most 8,388,608 voxels (2^23) per call, radius <= 128, repititions >= 1;
+ *     anything larger is rejected with MAXI_ERR_INVALID_ARGUMENT (radius:
+ *     MAXI_ERR_UNSUPPORTED) before GPU work starts;
+ *   - the array is reserved on each GPU that uses this call until the process
+ *     exits; the first call on a device looks up its address (cudaGetSymbolAddress),
+ *     so make that first call before any stream capture;
+ *   - all calls share the array: calls whose GPU work overlaps (different
+ *     streams or threads without ordering) race and give wrong results.
+ * mask, output (uint16, or NULL) and field_out (float, or NULL) are device
+ * buffers supplied by the caller; work is enqueued on `stream`.
+ */
+int maxi_diffusion_device_noalloc(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,
+                                  const float *kernel, int64_t kernel_size, int64_t repititions,
+                                  uint16_t *output, float *field_out, void *stream);
+
+/*
  * Bit-packing of a device mask to uint32 words, MSB first.  Replaces the
  * reference `bitpacking.encode` / `decode` (src/pybind/bitpacking-pybind.cc:17-48,
  * src/lib/cpp/cpu_seq/bitpacking.cc:9-42); n must be a multiple of 32.

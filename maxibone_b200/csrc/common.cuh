@@ -48,6 +48,67 @@ template <> struct FieldIO<double> {
 };
 
 // ---------------------------------------------------------------------------
+// 16-byte vector staging: global (aligned) -> shared floats (aligned).
+// Float fields use cp.async (no register round trip); 2-byte fields are
+// widened in registers (8 values per 16 bytes).
+// ---------------------------------------------------------------------------
+template <typename S> struct Vec16 { static constexpr int N = 16 / sizeof(S); };
+
+__device__ __forceinline__ void cp_async16(float *smem, const void *gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <typename S> __device__ __forceinline__ void stage16(float *smem, const S *gmem);
+template <> __device__ __forceinline__ void stage16<float>(float *smem, const float *gmem) { cp_async16(smem, gmem); }
+template <> __device__ __forceinline__ void stage16<__nv_bfloat16>(float *smem, const __nv_bfloat16 *gmem) {
+    const uint4 q = __ldg(reinterpret_cast<const uint4 *>(gmem));
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+    float f[8];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        f[2 * i] = __uint_as_float(w[i] << 16);
+        f[2 * i + 1] = __uint_as_float(w[i] & 0xffff0000u);
+    }
+    reinterpret_cast<float4 *>(smem)[0] = make_float4(f[0], f[1], f[2], f[3]);
+    reinterpret_cast<float4 *>(smem)[1] = make_float4(f[4], f[5], f[6], f[7]);
+}
+template <> __device__ __forceinline__ void stage16<__half>(float *smem, const __half *gmem) {
+    const uint4 q = __ldg(reinterpret_cast<const uint4 *>(gmem));
+    const __half2 *h = reinterpret_cast<const __half2 *>(&q);
+    float f[8];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float2 t = __half22float2(h[i]);
+        f[2 * i] = t.x;
+        f[2 * i + 1] = t.y;
+    }
+    reinterpret_cast<float4 *>(smem)[0] = make_float4(f[0], f[1], f[2], f[3]);
+    reinterpret_cast<float4 *>(smem)[1] = make_float4(f[4], f[5], f[6], f[7]);
+}
+
+// Stores 4 consecutive values (destination aligned to 4 elements).
+template <typename S> __device__ __forceinline__ void store4(S *dst, float a, float b, float c, float d);
+template <> __device__ __forceinline__ void store4<float>(float *dst, float a, float b, float c, float d) {
+    *reinterpret_cast<float4 *>(dst) = make_float4(a, b, c, d);
+}
+template <> __device__ __forceinline__ void store4<__nv_bfloat16>(__nv_bfloat16 *dst, float a, float b, float c, float d) {
+    const __nv_bfloat162 lo = __floats2bfloat162_rn(a, b), hi = __floats2bfloat162_rn(c, d);
+    uint2 u;
+    u.x = *reinterpret_cast<const uint32_t *>(&lo);
+    u.y = *reinterpret_cast<const uint32_t *>(&hi);
+    *reinterpret_cast<uint2 *>(dst) = u;
+}
+template <> __device__ __forceinline__ void store4<__half>(__half *dst, float a, float b, float c, float d) {
+    const __half2 lo = __floats2half2_rn(a, b), hi = __floats2half2_rn(c, d);
+    uint2 u;
+    u.x = *reinterpret_cast<const uint32_t *>(&lo);
+    u.y = *reinterpret_cast<const uint32_t *>(&hi);
+    *reinterpret_cast<uint2 *>(dst) = u;
+}
+
+// ---------------------------------------------------------------------------
 // Mask access.  U8: set when the byte is > 0 (the reference's `mask > 0`).
 // Bit-packed: flat voxel order, uint32 words, most significant bit first.
 // ---------------------------------------------------------------------------
@@ -63,6 +124,22 @@ template <> struct MaskIO<MAXI_MASK_BITPACKED> {
         return (w >> (31 - (int) (i & 31))) & 1u;
     }
 };
+
+// Four consecutive mask flags starting at a voxel index that is a multiple of 4
+// (bit q of the result = voxel i + q).
+template <int FMT> __device__ __forceinline__ uint32_t mask4(const void *m, int64_t i);
+template <> __device__ __forceinline__ uint32_t mask4<MAXI_MASK_U8>(const void *m, int64_t i) {
+    const uint32_t w = __ldg(reinterpret_cast<const uint32_t *>(static_cast<const uint8_t *>(m) + i));
+    uint32_t r = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) r |= (((w >> (8 * q)) & 0xffu) != 0u) << q;
+    return r;
+}
+template <> __device__ __forceinline__ uint32_t mask4<MAXI_MASK_BITPACKED>(const void *m, int64_t i) {
+    const uint32_t w = __ldg(static_cast<const uint32_t *>(m) + (i >> 5));
+    const uint32_t nib = (w >> (28 - (int) (i & 31))) & 0xfu;  // bits for voxels i..i+3, MSB first
+    return __brev(nib) >> 28;                                   // reorder: bit q = voxel i + q
+}
 
 // Quantisation of the reference (src/lib/cpp/cpu/diffusion.cc:191-195):
 // floor(v * 65535.0f) in FP32, clamped to the uint16 range.

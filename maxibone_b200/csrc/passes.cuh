@@ -50,13 +50,41 @@ strided_pass(const S *__restrict__ in, S *__restrict__ out, int64_t A, int64_t I
     const int col = threadIdx.x % kStrTI;
     const int seg = threadIdx.x / kStrTI;
     const bool col_ok = i0 + col < I;
-    const S *src = in + o * A * I + i0 + col;
-
-    for (int r = seg; r < ROWS; r += kStrThreads / kStrTI) {
-        const int64_t a = a0 - R + r;
-        float v = 0.0f;
-        if (col_ok && a >= 0 && a < A) v = FieldIO<S>::load(src + a * I);
-        s_tile[r * kStrTI + col] = v;
+    constexpr int VEC = Vec16<S>::N;            // elements per 16-byte chunk
+    constexpr int CH = kStrTI / VEC;            // chunks per staged row
+    constexpr int RPI = kStrThreads / CH;       // rows staged per iteration
+    // Vector path: all columns of the tile inside the volume and 16-byte aligned
+    // rows.  Rows outside [0, A) are zero-filled a chunk at a time.
+    const bool vec = i0 + kStrTI <= I && I % VEC == 0;
+    if (vec) {
+        const int chunk = threadIdx.x % CH;
+        const int row0 = threadIdx.x / CH;
+        const bool rows_inside = a0 >= R && a0 + kStrTA + R <= A;
+        const S *src = in + (o * A + a0 - R + row0) * I + i0 + chunk * VEC;
+        float *dst = s_tile + row0 * kStrTI + chunk * VEC;
+#pragma unroll
+        for (int r = row0, k = 0; k < (ROWS + RPI - 1) / RPI; k++, r += RPI) {
+            if (ROWS % RPI == 0 || r < ROWS) {
+                const int64_t a = a0 - R + r;
+                if (rows_inside || (a >= 0 && a < A)) {
+                    stage16<S>(dst, src);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < VEC; q += 4) *reinterpret_cast<float4 *>(dst + q) = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            }
+            src += RPI * I;
+            dst += RPI * kStrTI;
+        }
+        cp_async_wait_all();
+    } else {
+        const S *src = in + o * A * I + i0 + col;
+        for (int r = seg; r < ROWS; r += kStrThreads / kStrTI) {
+            const int64_t a = a0 - R + r;
+            float v = 0.0f;
+            if (col_ok && a >= 0 && a < A) v = FieldIO<S>::load(src + a * I);
+            s_tile[r * kStrTI + col] = v;
+        }
     }
     __syncthreads();
 
@@ -75,11 +103,14 @@ strided_pass(const S *__restrict__ in, S *__restrict__ out, int64_t A, int64_t I
     }
 
     if (!col_ok) return;
-    S *dst = out + o * A * I + i0 + col;
+    S *dst = out + (o * A + a0 + seg * kStrM) * I + i0 + col;
+    if (a0 + kStrTA <= A) {
 #pragma unroll
-    for (int i = 0; i < kStrM; i++) {
-        const int64_t a = a0 + seg * kStrM + i;
-        if (a < A) dst[a * I] = FieldIO<S>::narrow(acc[i]);
+        for (int i = 0; i < kStrM; i++, dst += I) *dst = FieldIO<S>::narrow(acc[i]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < kStrM; i++, dst += I)
+            if (a0 + seg * kStrM + i < A) *dst = FieldIO<S>::narrow(acc[i]);
     }
 }
 
@@ -113,17 +144,45 @@ contig_pass(const S *__restrict__ in, S *__restrict__ out, const void *__restric
     const int64_t r0 = (blockIdx.x / n_x_tiles) * kConTR;
     const int64_t x0 = xt * kConTX;
     const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    constexpr int VEC = Vec16<S>::N;
+    // Vector path: full row block, rows and halo start on 16-byte boundaries, and
+    // every output pointer aligned for 4-voxel vector access.  Chunks outside
+    // [0, nx) are zero-filled (chunks never straddle the row ends).
+    const bool vec = r0 + kConTR <= rows && nx % VEC == 0 && R % VEC == 0 &&
+                     ((reinterpret_cast<uintptr_t>(out_u16) & 7) | (reinterpret_cast<uintptr_t>(field_out) & 15) |
+                      (reinterpret_cast<uintptr_t>(mask) & 3)) == 0;
 
-    for (int e = tid; e < kConTR * W; e += kConThreads) {
-        const int r = e / W, c = e % W;
-        const int64_t row = r0 + r, x = x0 - R + c;
-        float v = 0.0f;
-        if (row < rows && x >= 0 && x < nx) v = FieldIO<S>::load(in + row * nx + x);
-        s_tile[r * STRIDE + c] = v;
+    if (vec) {
+        constexpr int CPR = (kConTX + 2 * R) / VEC;  // chunks per row (exact: R % VEC == 0)
+#pragma unroll
+        for (int rr = 0; rr < kConTR / kConWarps; rr++) {
+            const int r = warp + rr * kConWarps;
+            const S *src = in + (r0 + r) * nx + x0 - R;
+#pragma unroll
+            for (int c = lane; c < CPR; c += 32) {
+                const int64_t x = x0 - R + c * VEC;
+                float *d = s_tile + r * STRIDE + c * VEC;
+                if (x >= 0 && x < nx) {
+                    stage16<S>(d, src + c * VEC);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < VEC; q += 4) *reinterpret_cast<float4 *>(d + q) = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            }
+        }
+        cp_async_wait_all();
+    } else {
+        for (int e = tid; e < kConTR * W; e += kConThreads) {
+            const int r = e / W, c = e % W;
+            const int64_t row = r0 + r, x = x0 - R + c;
+            float v = 0.0f;
+            if (row < rows && x >= 0 && x < nx) v = FieldIO<S>::load(in + row * nx + x);
+            s_tile[r * STRIDE + c] = v;
+        }
     }
     __syncthreads();
 
-    const int lane = tid & 31, warp = tid >> 5;
     float acc[kConM];
 #pragma unroll
     for (int i = 0; i < kConM; i++) acc[i] = 0.0f;
@@ -149,6 +208,36 @@ contig_pass(const S *__restrict__ in, S *__restrict__ out, const void *__restric
         *reinterpret_cast<float4 *>(so + i) = make_float4(acc[i], acc[i + 1], acc[i + 2], acc[i + 3]);
     __syncthreads();
 
+    if (vec) {
+        // Vector epilogue: 4 voxels per lane-chunk (nx % 4 == 0, so a chunk is
+        // either inside the row or past its end).
+#pragma unroll
+        for (int rr = 0; rr < kConTR / kConWarps; rr++) {
+            const int r = warp + rr * kConWarps;
+            const int64_t rowbase = (r0 + r) * nx + x0;
+#pragma unroll
+            for (int c = lane * 4; c < kConTX; c += 128) {
+                if (x0 + c >= nx) continue;
+                const float4 q = *reinterpret_cast<const float4 *>(s_tile + r * STRIDE + c);
+                const int64_t idx = rowbase + c;
+                const uint32_t m = mask4<MASK_FMT>(mask, idx);
+                const float v0 = (m & 1u) ? 1.0f : q.x, v1 = (m & 2u) ? 1.0f : q.y;
+                const float v2 = (m & 4u) ? 1.0f : q.z, v3 = (m & 8u) ? 1.0f : q.w;
+                if (FINAL) {
+                    if (out_u16) {
+                        ushort4 u;
+                        u.x = quantise_u16(v0); u.y = quantise_u16(v1);
+                        u.z = quantise_u16(v2); u.w = quantise_u16(v3);
+                        *reinterpret_cast<ushort4 *>(out_u16 + idx) = u;
+                    }
+                    if (field_out) *reinterpret_cast<float4 *>(field_out + idx) = make_float4(v0, v1, v2, v3);
+                } else {
+                    store4<S>(out + idx, v0, v1, v2, v3);
+                }
+            }
+        }
+        return;
+    }
     for (int e = tid; e < kConTR * kConTX; e += kConThreads) {
         const int r = e / kConTX, c = e % kConTX;
         const int64_t row = r0 + r, x = x0 + c;

@@ -52,9 +52,21 @@ typedef enum maxi_mask_format {
 #define MAXI_FLAG_REFERENCE_ROUNDING 0x1 /* FP32 only: separate multiply and add in the
                                             reference's tap order, bit-identical to the
                                             reference OpenMP backend */
+#define MAXI_FLAG_NO_TENSOR_CORES 0x2    /* BF16/FP16: CUDA-core passes only */
+#define MAXI_FLAG_NEAREST_ROUNDING 0x4   /* BF16/FP16: plain round-to-nearest stores instead of
+                                            error-feedback rounding along x (the default, which
+                                            keeps the stored rounding noise out of the result) */
 
 const char *maxi_last_error(void);
 const char *maxi_version(void);
+
+/*
+ * Status of the tensor-core passes since the last call: their waits are
+ * bounded (about one second); a pass that gave up records a code here instead
+ * of hanging.  Synchronises with the device; returns MAXI_OK or MAXI_ERR_CUDA
+ * (message from maxi_last_error()) and clears the recorded code.
+ */
+int maxi_tensor_core_status(void);
 
 /* Kernel kinds reported by maxi_profile_read(). */
 typedef enum maxi_kernel_kind {

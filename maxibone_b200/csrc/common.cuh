@@ -141,6 +141,27 @@ template <> __device__ __forceinline__ uint32_t mask4<MAXI_MASK_BITPACKED>(const
     return __brev(nib) >> 28;                                   // reorder: bit q = voxel i + q
 }
 
+// Mask flags of up to 32 consecutive voxels [i, i + count) of a row (bit q =
+// voxel i + q; bits at or above `count` are zero).  `n` is the volume size,
+// bounding the bit-packed words read.
+template <int FMT> __device__ __forceinline__ uint32_t mask32(const void *m, int64_t i, int count, int64_t n);
+template <> __device__ __forceinline__ uint32_t mask32<MAXI_MASK_U8>(const void *m, int64_t i, int count, int64_t n) {
+    const uint8_t *p = static_cast<const uint8_t *>(m) + i;
+    uint32_t r = 0;
+    for (int q = 0; q < count; q++) r |= (uint32_t) (__ldg(p + q) != 0) << q;
+    return r;
+}
+template <> __device__ __forceinline__ uint32_t mask32<MAXI_MASK_BITPACKED>(const void *m, int64_t i, int count, int64_t n) {
+    const uint32_t *w = static_cast<const uint32_t *>(m);
+    const int64_t w0 = i >> 5;
+    const int b = (int) (i & 31);
+    const uint64_t hi = __ldg(w + w0);
+    const uint64_t lo = (b > 0 && (w0 + 1) * 32 < n) ? __ldg(w + w0 + 1) : 0u;
+    const uint32_t msb_first = (uint32_t) ((((hi << 32) | lo) << b) >> 32);  // voxel i at bit 31
+    const uint32_t r = __brev(msb_first);                                      // voxel i at bit 0
+    return count >= 32 ? r : (r & ((1u << count) - 1u));
+}
+
 // Quantisation of the reference (src/lib/cpp/cpu/diffusion.cc:191-195):
 // floor(v * 65535.0f) in FP32, clamped to the uint16 range.
 __device__ __forceinline__ uint16_t quantise_u16(float v) {

@@ -15,6 +15,7 @@
 #include "host_util.h"
 #include "unrolled.h"
 #include "profiler.h"
+#include "tc_pass.h"
 
 namespace maxi {
 
@@ -105,7 +106,7 @@ static cudaError_t run_typed(const Volume &v, const void *mask, int mask_fmt, co
     }
     if constexpr (!is_f64)
         return dispatch_unrolled<S>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16,
-                                    static_cast<float *>(field_out), st);
+                                    static_cast<float *>(field_out), flags, st);
     return cudaErrorInvalidValue;
 }
 
@@ -118,6 +119,14 @@ extern "C" {
 const char *maxi_version(void) { return "maxibone_b200 diffusion 0.1 (sm_100a)"; }
 
 const char *maxi_last_error(void) { return last_error_cstr(); }
+
+int maxi_tensor_core_status(void) {
+    clear_error();
+    const int v = tc::tc_read_and_clear_error();
+    if (v < 0) return set_error(MAXI_ERR_CUDA, "could not read the tensor-core error word");
+    if (v > 0) return set_error(MAXI_ERR_CUDA, "a tensor-core pass timed out waiting (code %d)", v);
+    return MAXI_OK;
+}
 
 int64_t maxi_diffusion_workspace_size(int64_t nz, int64_t ny, int64_t nx, int32_t field_type) {
     if (nz <= 0 || ny <= 0 || nx <= 0 || field_bytes(field_type) == 0) return -1;

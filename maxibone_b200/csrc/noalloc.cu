@@ -89,7 +89,7 @@ extern "C" int maxi_diffusion_device_noalloc(const void *mask, int32_t mask_form
     if ((rc = noalloc_scratch(&scratch))) return rc;
     const Volume v{nz, ny, nx};
     cudaError_t e = dispatch_unrolled<float>(v, mask, mask_format, kernel, (int) (kernel_size / 2), repititions,
-                                             scratch, scratch + kNoAllocMaxVoxels, output, field_out,
+                                             scratch, scratch + kNoAllocMaxVoxels, output, field_out, 0,
                                              static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return set_cuda_error(e, "no-alloc diffusion launch");
     return MAXI_OK;

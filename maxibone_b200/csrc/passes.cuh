@@ -33,9 +33,15 @@ constexpr int kStrTA = 128;   // axis outputs per CTA
 constexpr int kStrM = 16;     // axis outputs per thread
 constexpr int kStrThreads = kStrTI * (kStrTA / kStrM);  // 256
 
-template <int R> constexpr int strided_smem_bytes() { return (kStrTA + 2 * R) * kStrTI * 4; }
+// The staged tile, or (error-feedback epilogue) the outputs on a 33-word row stride.
+template <int R> constexpr int strided_smem_bytes() {
+    return ((kStrTA + 2 * R) * kStrTI > kStrTA * (kStrTI + 1) ? (kStrTA + 2 * R) * kStrTI : kStrTA * (kStrTI + 1)) * 4;
+}
 
-template <int R, typename S>
+// EF: error-feedback rounding to the 16-bit storage type along x (the inner
+// columns), chains of 16 voxels: the stored rounding noise is high-pass along
+// x and the following x pass filters it out.
+template <int R, typename S, bool EF = false>
 __global__ void __launch_bounds__(kStrThreads)
 strided_pass(const S *__restrict__ in, S *__restrict__ out, int64_t A, int64_t I,
              int64_t n_axis_tiles, int64_t n_inner_tiles, const Taps<R> taps) {
@@ -102,6 +108,26 @@ strided_pass(const S *__restrict__ in, S *__restrict__ out, int64_t A, int64_t I
         }
     }
 
+    if (EF) {
+        // Transpose through shared memory: thread -> (axis row, 16 consecutive columns).
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kStrM; i++) s_tile[(seg * kStrM + i) * (kStrTI + 1) + col] = acc[i];
+        __syncthreads();
+        const int row = threadIdx.x >> 1, c0 = (threadIdx.x & 1) * 16;
+        const int64_t a = a0 + row;
+        if (a >= A) return;
+        S *dst = out + (o * A + a) * I + i0 + c0;
+        float carry = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 16; c++) {
+            const float w = s_tile[row * (kStrTI + 1) + c0 + c] + carry;
+            const S q = FieldIO<S>::narrow(w);
+            carry = w - FieldIO<S>::widen(q);
+            if (i0 + c0 + c < I) dst[c] = q;
+        }
+        return;
+    }
     if (!col_ok) return;
     S *dst = out + (o * A + a0 + seg * kStrM) * I + i0 + col;
     if (a0 + kStrTA <= A) {
@@ -130,7 +156,10 @@ template <int R> constexpr int contig_smem_bytes() { return kConTR * contig_stri
 
 // FINAL: last repetition -- write the uint16 output (and optionally the FP32
 // field) instead of the storage-type field.
-template <int R, typename S, int MASK_FMT, bool FINAL>
+// EF (16-bit storage, not FINAL): the thread's 32 consecutive outputs are
+// re-illuminated and rounded with error feedback along x in registers (the
+// carry restarts after every mask voxel, which is stored as exactly 1.0).
+template <int R, typename S, int MASK_FMT, bool FINAL, bool EF = false>
 __global__ void __launch_bounds__(kConThreads)
 contig_pass(const S *__restrict__ in, S *__restrict__ out, const void *__restrict__ mask,
             uint16_t *__restrict__ out_u16, float *__restrict__ field_out,
@@ -198,6 +227,26 @@ contig_pass(const S *__restrict__ in, S *__restrict__ out, const void *__restric
             for (int i = 0; i < kConM; i++) {
                 const int t = j - i;
                 if (t >= 0 && t <= 2 * R) acc[i] = fmaf(taps.k[t], vv[u], acc[i]);
+            }
+        }
+    }
+    if (EF && !FINAL) {
+        const int64_t row = r0 + lane, xs = x0 + warp * kConM;
+        if (row < rows && xs < nx) {
+            const int count = nx - xs < kConM ? (int) (nx - xs) : kConM;
+            const uint32_t m = mask32<MASK_FMT>(mask, row * nx + xs, count, rows * nx);
+            float carry = 0.0f;
+#pragma unroll
+            for (int i = 0; i < kConM; i++) {
+                if ((m >> i) & 1u) {
+                    acc[i] = 1.0f;
+                    carry = 0.0f;
+                } else {
+                    const float w = acc[i] + carry;
+                    const float q = FieldIO<S>::widen(FieldIO<S>::narrow(w));
+                    carry = w - q;
+                    acc[i] = q;
+                }
             }
         }
     }

@@ -4,6 +4,7 @@
 namespace maxi {
 
 template cudaError_t dispatch_unrolled<__nv_bfloat16>(const Volume &, const void *, int, const float *, int, int64_t,
-                                           __nv_bfloat16 *, __nv_bfloat16 *, uint16_t *, float *, cudaStream_t);
+                                           __nv_bfloat16 *, __nv_bfloat16 *, uint16_t *, float *, int32_t,
+                                           cudaStream_t);
 
 }  // namespace maxi

@@ -4,6 +4,7 @@
 namespace maxi {
 
 template cudaError_t dispatch_unrolled<__half>(const Volume &, const void *, int, const float *, int, int64_t,
-                                           __half *, __half *, uint16_t *, float *, cudaStream_t);
+                                           __half *, __half *, uint16_t *, float *, int32_t,
+                                           cudaStream_t);
 
 }  // namespace maxi

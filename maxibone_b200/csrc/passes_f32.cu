@@ -6,6 +6,7 @@ namespace maxi {
 int radius_bucket(int r) { return radius_bucket_impl(r); }
 
 template cudaError_t dispatch_unrolled<float>(const Volume &, const void *, int, const float *, int, int64_t,
-                                           float *, float *, uint16_t *, float *, cudaStream_t);
+                                           float *, float *, uint16_t *, float *, int32_t,
+                                           cudaStream_t);
 
 }  // namespace maxi

@@ -1,0 +1,28 @@
+// Host interface of the tensor-core (tcgen05) passes for 16-bit field storage.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace maxi {
+namespace tc {
+
+// Largest kernel radius the tensor-core passes serve (the K extent 128 + 2R
+// must fit one TMA box of at most 256 rows, and both Toeplitz halves plus a
+// 2-stage tile ring must fit shared memory).
+constexpr int kTcMaxRadius = 32;
+
+// True when the device is sm_100 and the shape fits the TMA constraints.
+bool tc_supported(int radius, int64_t nz, int64_t ny, int64_t nx);
+
+// One z (axis_z) or y pass: out = conv(in) along the axis with a zero boundary.
+template <typename S>
+cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, bool axis_z, const float *kernel,
+                       int radius, bool error_feedback, cudaStream_t st);
+
+// Reads (and clears) the device error word of the tensor-core kernels:
+// 0 = fine, 1..3 = a bounded wait timed out, -1 = could not be read.
+int tc_read_and_clear_error();
+
+}  // namespace tc
+}  // namespace maxi

@@ -18,8 +18,11 @@ int radius_bucket(int r);
 // Runs `reps` repetitions (reps >= 1) of the unrolled passes: buf0 receives
 // the initial field, buf0/buf1 ping-pong, the last x pass writes out_u16 and
 // field_out (either may be NULL).
+// flags: MAXI_FLAG_* bits (NO_TENSOR_CORES and NEAREST_ROUNDING apply to the
+// 16-bit storage types).
 template <typename S>
 cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
-                              int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, cudaStream_t st);
+                              int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, int32_t flags,
+                              cudaStream_t st);
 
 }  // namespace maxi

@@ -5,6 +5,7 @@
 #include "passes.cuh"
 #include "unrolled.h"
 #include "profiler.h"
+#include "tc_pass.h"
 
 namespace maxi {
 
@@ -35,21 +36,23 @@ static cudaError_t set_smem(F *f, int bytes) {
     return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-// One repetition loop on the unrolled CUDA-core passes for bucket radius R.
-template <int R, typename S>
+// One repetition loop for bucket radius R.  EF: error-feedback rounding of the
+// 16-bit storage type (see passes.cuh); use_tc: z and y passes on the tensor
+// cores (16-bit storage only, tc_pass.cu).
+template <int R, typename S, bool EF>
 static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel,
                                 int radius, int64_t reps, S *buf0, S *buf1, uint16_t *out_u16,
-                                float *field_out, cudaStream_t st) {
+                                float *field_out, bool use_tc, cudaStream_t st) {
     const Taps<R> taps = make_taps<R>(kernel, radius);
     const int str_smem = strided_smem_bytes<R>();
     const int con_smem = contig_smem_bytes<R>();
-    auto *zy = strided_pass<R, S>;
+    auto *zy = strided_pass<R, S, EF>;
     cudaError_t e = set_smem(zy, str_smem);
     if (e != cudaSuccess) return e;
-    auto *xu8 = contig_pass<R, S, MAXI_MASK_U8, false>;
-    auto *xu8f = contig_pass<R, S, MAXI_MASK_U8, true>;
-    auto *xbp = contig_pass<R, S, MAXI_MASK_BITPACKED, false>;
-    auto *xbpf = contig_pass<R, S, MAXI_MASK_BITPACKED, true>;
+    auto *xu8 = contig_pass<R, S, MAXI_MASK_U8, false, EF>;
+    auto *xu8f = contig_pass<R, S, MAXI_MASK_U8, true, EF>;
+    auto *xbp = contig_pass<R, S, MAXI_MASK_BITPACKED, false, EF>;
+    auto *xbpf = contig_pass<R, S, MAXI_MASK_BITPACKED, true, EF>;
     for (auto *f : {xu8, xu8f, xbp, xbpf})
         if ((e = set_smem(f, con_smem)) != cudaSuccess) return e;
     auto *xpass = mask_fmt == MAXI_MASK_U8 ? xu8 : xbp;
@@ -72,12 +75,24 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
     for (int64_t rep = 0; rep < reps; rep++) {
         {
             ProfScope ps(MAXI_KERNEL_Z, st);
-            zy<<<zat * zit, kStrThreads, str_smem, st>>>(buf0, buf1, zA, zI, zat, zit, taps);
+            if constexpr (sizeof(S) == 2) {
+                if (use_tc) e = tc::tc_strided<S>(buf0, buf1, v.nz, v.ny, v.nx, true, kernel, radius, EF, st);
+                else zy<<<zat * zit, kStrThreads, str_smem, st>>>(buf0, buf1, zA, zI, zat, zit, taps);
+            } else {
+                zy<<<zat * zit, kStrThreads, str_smem, st>>>(buf0, buf1, zA, zI, zat, zit, taps);
+            }
         }
+        if (e != cudaSuccess) return e;
         {
             ProfScope ps(MAXI_KERNEL_Y, st);
-            zy<<<yat * yit * yO, kStrThreads, str_smem, st>>>(buf1, buf0, yA, yI, yat, yit, taps);
+            if constexpr (sizeof(S) == 2) {
+                if (use_tc) e = tc::tc_strided<S>(buf1, buf0, v.nz, v.ny, v.nx, false, kernel, radius, EF, st);
+                else zy<<<yat * yit * yO, kStrThreads, str_smem, st>>>(buf1, buf0, yA, yI, yat, yit, taps);
+            } else {
+                zy<<<yat * yit * yO, kStrThreads, str_smem, st>>>(buf1, buf0, yA, yI, yat, yit, taps);
+            }
         }
+        if (e != cudaSuccess) return e;
         if (rep + 1 < reps) {
             ProfScope ps(MAXI_KERNEL_X, st);
             xpass<<<xt * xrb, kConThreads, con_smem, st>>>(buf0, buf1, mask, nullptr, nullptr, rows, v.nx, xt, taps);
@@ -90,13 +105,13 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
     return cudaGetLastError();
 }
 
-template <typename S>
-cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel,
-                                     int radius, int64_t reps, S *b0, S *b1, uint16_t *out_u16,
-                                     float *field_out, cudaStream_t st) {
+template <typename S, bool EF>
+static cudaError_t dispatch_radius(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
+                                   int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, bool use_tc,
+                                   cudaStream_t st) {
     switch (radius_bucket_impl(radius)) {
 #define MAXI_CASE(RB) \
-    case RB: return run_unrolled<RB, S>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, st);
+    case RB: return run_unrolled<RB, S, EF>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, st);
         MAXI_CASE(1) MAXI_CASE(2) MAXI_CASE(3) MAXI_CASE(4) MAXI_CASE(6) MAXI_CASE(8) MAXI_CASE(12)
         MAXI_CASE(16) MAXI_CASE(24) MAXI_CASE(32) MAXI_CASE(48) MAXI_CASE(64) MAXI_CASE(96) MAXI_CASE(128)
 #undef MAXI_CASE
@@ -104,5 +119,18 @@ cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, c
     }
 }
 
+template <typename S>
+cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
+                              int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, int32_t flags,
+                              cudaStream_t st) {
+    if constexpr (sizeof(S) == 2) {
+        const bool ef = (flags & MAXI_FLAG_NEAREST_ROUNDING) == 0;
+        const bool use_tc = (flags & MAXI_FLAG_NO_TENSOR_CORES) == 0 && tc::tc_supported(radius, v.nz, v.ny, v.nx);
+        if (ef) return dispatch_radius<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, st);
+        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, st);
+    } else {
+        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, false, st);
+    }
+}
 
 }  // namespace maxi

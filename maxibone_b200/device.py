@@ -23,7 +23,8 @@ def workspace_bytes(shape, field: str = "f32") -> int:
 def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor | None = None,
             field: str = "f32", field_out: torch.Tensor | None = None, shape=None,
             reference_rounding: bool = False, workspace: torch.Tensor | None = None,
-            stream: torch.cuda.Stream | None = None) -> None:
+            stream: torch.cuda.Stream | None = None, tensor_cores: bool = True,
+            error_feedback: bool = True) -> None:
     """Run the diffusion on device buffers.
 
     mask: uint8 [nz, ny, nx] CUDA tensor (set when > 0), or a bit-packed int32/uint32
@@ -33,6 +34,8 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
     field: storage type between passes: "f32", "bf16", "f16" or "f64".
     field_out: final field before quantisation (float32; float64 for "f64"), or None.
     workspace: uint8 CUDA tensor of at least workspace_bytes(shape, field), or None.
+    tensor_cores: 16-bit fields: z and y passes on tcgen05 tensor cores where supported.
+    error_feedback: 16-bit fields: error-feedback rounding along x (else round to nearest).
     """
     if not mask.is_cuda:
         raise ValueError("mask must be a CUDA tensor")
@@ -67,6 +70,10 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
         ws_ptr, ws_bytes = workspace.data_ptr(), workspace.numel() * workspace.element_size()
     st = stream if stream is not None else torch.cuda.current_stream(mask.device)
     flags = _lib.FLAG_REFERENCE_ROUNDING if reference_rounding else 0
+    if not tensor_cores:
+        flags |= _lib.FLAG_NO_TENSOR_CORES
+    if not error_feedback:
+        flags |= _lib.FLAG_NEAREST_ROUNDING
     with torch.cuda.device(mask.device):
         _lib.check(_lib.lib().maxi_diffusion_device(
             mask.data_ptr(), fmt, nz, ny, nx, k.ctypes.data, k.shape[0], int(repititions),
@@ -113,3 +120,8 @@ def profile_read() -> dict:
     cnt = (ctypes.c_int64 * n)()
     _lib.check(_lib.lib().maxi_profile_read(ctypes.addressof(ms), ctypes.addressof(cnt), n))
     return {k: (ms[i], cnt[i]) for i, k in enumerate(_lib.KERNEL_KINDS) if cnt[i]}
+
+
+def tensor_core_status() -> None:
+    """Raise if a tensor-core pass gave up on a bounded wait since the last check."""
+    _lib.check(_lib.lib().maxi_tensor_core_status())

@@ -1,0 +1,69 @@
+"""tcgen05 tensor-core z/y passes for the 16-bit field forms (run with -m gpu).
+
+The tensor-core passes compute each z/y pass as a banded Toeplitz product with
+FP32 accumulation; they must agree with the CUDA-core passes of the same form
+(both store the field in the same 16-bit type) and stay within the stated
+error of the FP64 form.  Shapes cover partial x chunks (nx not a multiple of
+128), axes shorter than and not multiple of the 128-output tile, and the
+radius range the tensor-core path serves (1..32).
+"""
+import numpy as np
+import pytest
+import torch
+
+from maxibone_b200 import device, gauss_kernel
+from maxibone_b200.synthetic import random_mask, spheres_mask
+
+pytestmark = pytest.mark.gpu
+
+# Max abs difference between the tensor-core and CUDA-core forms (same storage type).
+TC_VS_CC = {"bf16": 8e-3, "f16": 1e-3}
+VS_F64 = {"bf16": 8e-3, "f16": 1e-3}
+
+
+def run(mask, kernel, reps, field, tensor_cores=True, error_feedback=True):
+    m = torch.from_numpy(np.ascontiguousarray(mask, np.uint8)).cuda()
+    fo = torch.empty(mask.shape, dtype=torch.float64 if field == "f64" else torch.float32, device="cuda")
+    out = torch.empty(mask.shape, dtype=torch.uint16, device="cuda")
+    device.diffuse(m, kernel, reps, output=out, field=field, field_out=fo, tensor_cores=tensor_cores,
+                   error_feedback=error_feedback)
+    torch.cuda.synchronize()
+    device.tensor_core_status()
+    return out.cpu().numpy(), fo.cpu().numpy()
+
+
+@pytest.mark.parametrize("field", ["bf16", "f16"])
+@pytest.mark.parametrize("shape,sigma", [((40, 70, 136), 1.0), ((130, 64, 128), 3.0), ((33, 129, 200), 8.0),
+                                         ((8, 300, 64), 2.0), ((200, 24, 72), 8.0)])
+@pytest.mark.parametrize("ef", [False, True])
+def test_tensor_core_matches_cuda_core_and_fp64(field, shape, sigma, ef):
+    mask = random_mask(shape, 0.02, seed=sum(shape))
+    kernel = gauss_kernel(sigma).astype(np.float32)
+    reps = 3
+    _, want = run(mask, kernel, reps, "f64")
+    tc_u16, tc = run(mask, kernel, reps, field, True, ef)
+    _, cc = run(mask, kernel, reps, field, False, ef)
+    assert np.abs(tc - cc).max() <= TC_VS_CC[field]
+    assert np.abs(tc.astype(np.float64) - want).max() <= VS_F64[field]
+    assert np.all(tc_u16[mask > 0] == 65535)
+    assert np.all(tc[mask > 0] == 1.0)
+
+
+@pytest.mark.parametrize("radius", [1, 5, 12, 16, 31, 32])
+def test_tensor_core_radius_range(radius):
+    mask = spheres_mask((64, 96, 128), 10, (3, 9), seed=radius)
+    kernel = gauss_kernel(radius / 4.0).astype(np.float32)
+    _, want = run(mask, kernel, 4, "f64")
+    _, got = run(mask, kernel, 4, "f16", True, True)
+    assert np.abs(got.astype(np.float64) - want).max() <= VS_F64["f16"]
+
+
+def test_error_feedback_reduces_bf16_error():
+    mask = spheres_mask((96, 96, 128), 30, (4, 14), seed=5)
+    kernel = gauss_kernel(4.0).astype(np.float32)
+    _, want = run(mask, kernel, 30, "f64")
+    _, rn = run(mask, kernel, 30, "bf16", True, False)
+    _, ef = run(mask, kernel, 30, "bf16", True, True)
+    e_rn = np.abs(rn.astype(np.float64) - want).max()
+    e_ef = np.abs(ef.astype(np.float64) - want).max()
+    assert e_ef < e_rn

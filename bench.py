@@ -303,24 +303,34 @@ def main():
         f64 = torch.empty(shape, dtype=torch.float64, device="cuda")
         device.diffuse(mask, kernel, reps, field="f64", field_out=f64)
         forms = {}
-        for form in ("f32", "bf16", "f16"):
+        variants = [("f32", "f32", {}), ("bf16", "bf16", {}), ("f16", "f16", {}),
+                    ("bf16_nearest", "bf16", {"error_feedback": False}),
+                    ("bf16_cuda_cores", "bf16", {"tensor_cores": False}),
+                    ("f16_cuda_cores", "f16", {"tensor_cores": False})]
+        for name, form, opts in variants:
             fo = torch.empty(shape, dtype=torch.float32, device="cuda")
             w = torch.empty(device.workspace_bytes(shape, form), dtype=torch.uint8, device="cuda")
-            device.diffuse(mask, kernel, reps, output=out, field=form, field_out=fo, workspace=w)
+            device.diffuse(mask, kernel, reps, output=out, field=form, field_out=fo, workspace=w, **opts)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             n_t = 2
+            device.profile_enable(True)
+            device.profile_read()
             e0.record(stream)
             for _ in range(n_t):
-                device.diffuse(mask, kernel, reps, output=out, field=form, workspace=w)
+                device.diffuse(mask, kernel, reps, output=out, field=form, workspace=w, **opts)
             e1.record(stream)
             torch.cuda.synchronize()
+            fprof = device.profile_read()
+            device.profile_enable(False)
+            device.tensor_core_status()
             t_ms = e0.elapsed_time(e1)
             err = (fo.double() - f64).abs_()
-            forms[form] = {"value": vox * reps * n_t / (t_ms / 1e3) / 1e9, "unit": UNIT,
+            forms[name] = {"value": vox * reps * n_t / (t_ms / 1e3) / 1e9, "unit": UNIT, "field": form, **opts,
                            "max_abs_err_vs_f64": float(err.max().item()),
                            "mean_abs_err_vs_f64": float(err.mean().item()),
-                           "mask_voxels_exact": bool((out.view(torch.int16)[mask > 0] == -1).all().item())}
+                           "mask_voxels_exact": bool((out.view(torch.int16)[mask > 0] == -1).all().item()),
+                           "per_kind_ms": {k: v[0] / v[1] for k, v in fprof.items()}}
             del err, fo, w
             torch.cuda.empty_cache()
         line["precision"] = forms

@@ -54,8 +54,9 @@ typedef enum maxi_mask_format {
                                             reference OpenMP backend */
 #define MAXI_FLAG_NO_TENSOR_CORES 0x2    /* BF16/FP16: CUDA-core passes only */
 #define MAXI_FLAG_NEAREST_ROUNDING 0x4   /* BF16/FP16: plain round-to-nearest stores instead of
-                                            error-feedback rounding along x (the default, which
-                                            keeps the stored rounding noise out of the result) */
+                                            error-feedback rounding along x (the default for
+                                            radius >= 4, which keeps the stored rounding noise
+                                            out of the result) */
 
 const char *maxi_last_error(void);
 const char *maxi_version(void);

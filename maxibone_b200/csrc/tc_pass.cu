@@ -37,7 +37,8 @@ namespace tc {
 constexpr int kTM = 128;      // outputs along the axis per tile
 constexpr int kTN = 128;      // x columns per tile
 constexpr int kStages = 2;    // TMA ring depth
-constexpr int kThreads = 192; // 6 warps
+constexpr int kEpiWarps = 8;  // two warps per TMEM lane quadrant, each drains half the columns
+constexpr int kThreads = 64 + 32 * kEpiWarps;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
 
 struct StridedParams {
     void *out;
@@ -47,7 +48,7 @@ struct StridedParams {
     int64_t stride_a;   // element stride along the axis in `out`
     int64_t stride_o;   // element stride of the third coordinate
     int n_at, n_xc;     // axis tiles, x chunks
-    int64_t n_tiles;
+    int64_t n_cols;     // columns = x chunks x third coordinate; a CTA marches a column's axis tiles
     int radius, kp, kpa; // radius, K (multiple of 16), K rounded to 64
     int axis_is_z;
     float inv_scale;
@@ -107,7 +108,7 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
     }
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-        for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], 4); }
+        for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], kEpiWarps); }
         fence_barrier_init();
         prefetch_tmap(&tmap);
     }
@@ -125,14 +126,14 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
     if (warp == 0 && lane == 0) {
         // TMA producer.
         int64_t tl = 0;
-        for (int64_t tile = blockIdx.x; tile < p.n_tiles; tile += gridDim.x, tl++) {
+        bool ok = true;
+        for (int64_t col = blockIdx.x; ok && col < p.n_cols; col += gridDim.x)
+        for (int at = 0; at < p.n_at; at++, tl++) {
             const int s = (int) (tl % kStages);
             const uint32_t ph = (uint32_t) ((tl / kStages) & 1);
-            if (!mbar_wait(&empty[s], ph ^ 1, 1)) break;
-            const int at = (int) (tile % p.n_at);
-            const int64_t rest = tile / p.n_at;
-            const int xc = (int) (rest % p.n_xc);
-            const int oth = (int) (rest / p.n_xc);
+            if (!mbar_wait(&empty[s], ph ^ 1, 1)) { ok = false; break; }
+            const int xc = (int) (col % p.n_xc);
+            const int oth = (int) (col / p.n_xc);
             const int a_in = at * kTM - p.radius;
             const int x0 = xc * kTN;
             mbar_arrive_expect_tx(&full[s], stage_bytes);
@@ -148,13 +149,14 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
         const uint32_t idesc = idesc_f16(fmt, 0 /*A K-major*/, 1 /*B MN-major*/, kTM, kTN);
         const uint32_t a_hi = smem_u32(t_hi), a_lo = smem_u32(t_lo), b0 = smem_u32(ring);
         int64_t tl = 0;
-        for (int64_t tile = blockIdx.x; tile < p.n_tiles; tile += gridDim.x, tl++) {
+        bool ok = true;
+        for (int64_t col = blockIdx.x; ok && col < p.n_cols; col += gridDim.x)
+        for (int at = 0; at < p.n_at; at++, tl++) {
             const int s = (int) (tl % kStages);
             const uint32_t ph = (uint32_t) ((tl / kStages) & 1);
             const int d = (int) (tl & 1);
             const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
-            if (!mbar_wait(&full[s], ph, 1)) break;
-            if (!mbar_wait(&tempty[d], dph ^ 1, 3)) break;
+            if (!mbar_wait(&full[s], ph, 1) || !mbar_wait(&tempty[d], dph ^ 1, 3)) { ok = false; break; }
             tc_fence_after();
             const uint32_t dt = tmem + d * kTN;
             for (int ks = 0; ks < p.kp / 16; ks++) {
@@ -169,23 +171,24 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
     } else if (warp >= 2) {
         // Epilogue: TMEM -> registers -> storage type -> global.
         const int quad = warp & 3;           // TMEM lane quadrant this warp may access
+        const int half = (warp - 2) >> 2;    // which half of the columns it drains
         const int o = quad * 32 + lane;      // output row within the tile
         S *out = static_cast<S *>(p.out);
         int64_t tl = 0;
-        for (int64_t tile = blockIdx.x; tile < p.n_tiles; tile += gridDim.x, tl++) {
+        bool ok = true;
+        for (int64_t col = blockIdx.x; ok && col < p.n_cols; col += gridDim.x)
+        for (int at = 0; at < p.n_at; at++, tl++) {
             const int d = (int) (tl & 1);
             const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
-            if (!mbar_wait(&tfull[d], dph, 2)) break;
+            if (!mbar_wait(&tfull[d], dph, 2)) { ok = false; break; }
             tc_fence_after();
-            const int at = (int) (tile % p.n_at);
-            const int64_t rest = tile / p.n_at;
-            const int xc = (int) (rest % p.n_xc);
-            const int64_t oth = rest / p.n_xc;
+            const int xc = (int) (col % p.n_xc);
+            const int64_t oth = col / p.n_xc;
             const int64_t a = (int64_t) at * kTM + o;
             const int64_t x0 = (int64_t) xc * kTN;
             float carry = 0.0f;
 #pragma unroll 1
-            for (int c = 0; c < kTN / 32; c++) {
+            for (int c = half * (kTN / 64); c < (half + 1) * (kTN / 64); c++) {
                 float v[32];
                 __syncwarp();
                 tmem_ld32(tmem + ((uint32_t) (quad * 32) << 16) + d * kTN + c * 32, v);
@@ -206,7 +209,9 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
                         *reinterpret_cast<uint4 *>(dst + i) = u;
                     }
                 } else {
-                    for (int i = 0; i < 32 && xb + i < p.nx; i++) reinterpret_cast<uint16_t *>(dst)[i] = q[i];
+#pragma unroll
+                    for (int i = 0; i < 32; i++)
+                        if (xb + i < p.nx) reinterpret_cast<uint16_t *>(dst)[i] = q[i];
                 }
             }
             tc_fence_before();
@@ -218,6 +223,241 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
     if (warp == 0) {
         tc_fence_after();
         tmem_dealloc(tmem, 2 * kTN);
+    }
+}
+
+// ---- x pass -----------------------------------------------------------------------
+//
+// The x pass with the field as the A operand: 128 volume rows (M, TMEM lanes)
+// x 128 x-outputs, so each epilogue thread owns 32 consecutive voxels of one
+// row -- the layout re-illumination, error feedback along x and vector stores
+// want.  D[r, o] = sum_j F[r, x0 - RA + j] * Tt[j, o] with RA = R rounded up to
+// 8 (TMA x coordinates must be 16-byte aligned); Tt[j, o] = k[j - o - RA + R].
+// The high and low coefficient halves are concatenated along N (N = 256:
+// columns 0..127 hold F*Tt_hi, 128..255 F*Tt_lo) so one MMA reads the A tile
+// once; the epilogue adds the halves.
+constexpr int kXTN = 128;            // x outputs per tile
+constexpr int kXThreads = kThreads;
+
+struct ContigParams {
+    void *out;             // storage-type field (not FINAL)
+    const void *mask;
+    uint16_t *out_u16;     // FINAL
+    float *field_out;      // FINAL, optional
+    int64_t rows, nx;
+    int n_xt;              // x tiles
+    int64_t n_tiles;
+    int radius, ra, kp, kpa;
+    int mask_fmt, final_pass, error_feedback;
+    float inv_scale;
+    uint16_t hi[2 * kTcMaxRadius + 1];
+    uint16_t lo[2 * kTcMaxRadius + 1];
+};
+
+__host__ __device__ constexpr int contig_smem_bytes_tc(int kp, int kpa) {
+    return 1024 + kpa * 2 * kXTN * 2 /*Tt_hi|Tt_lo, 256 rows*/ + kStages * (kpa / 64) * kTM * 128 /*A ring*/ + 256;
+}
+
+template <int FMT>
+__device__ __forceinline__ uint32_t row_mask32(const void *m, int64_t idx, int count, int64_t n) {
+    if (FMT == MAXI_MASK_U8 && count == 32 && ((reinterpret_cast<uintptr_t>(m) + idx) & 15) == 0) {
+        const uint4 *p = reinterpret_cast<const uint4 *>(static_cast<const uint8_t *>(m) + idx);
+        const uint4 a = __ldg(p), b = __ldg(p + 1);
+        const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        uint32_t r = 0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+#pragma unroll
+            for (int by = 0; by < 4; by++) r |= (uint32_t) (((w[q] >> (8 * by)) & 0xffu) != 0u) << (q * 4 + by);
+        }
+        return r;
+    }
+    return mask32<FMT>(m, idx, count, n);
+}
+
+template <typename S, int FMT>
+__global__ void __launch_bounds__(kXThreads, 1)
+tc_contig_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ ContigParams p) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    uint8_t *smem = smem_raw + (((raw + 1023) & ~1023u) - raw);
+    uint8_t *tt = smem;                                  // K-major, 256 rows (hi 0..127, lo 128..255)
+    uint8_t *ring = tt + p.kpa * 2 * kXTN * 2;
+    const int nkb = p.kpa / 64;                          // 64-wide x boxes per stage
+    const int stage_bytes = nkb * kTM * 128;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kStages * stage_bytes);
+    uint64_t *full = bars, *empty = bars + kStages, *tfull = bars + 2 * kStages, *tempty = bars + 2 * kStages + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 4);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    for (int e = threadIdx.x; e < 2 * kXTN * p.kpa; e += kXThreads) {
+        const int n = e / p.kpa, j = e - n * p.kpa;
+        const int o = n & (kXTN - 1);
+        const int t = j - o - p.ra + p.radius;  // tap index 0..2R
+        uint16_t v = 0;
+        if (t >= 0 && t <= 2 * p.radius && j < p.kp) v = n < kXTN ? p.hi[t] : p.lo[t];
+        *reinterpret_cast<uint16_t *>(tt + sw128_kmajor_offset(n, j, 2 * kXTN)) = v;
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], kEpiWarps); }
+        fence_barrier_init();
+        prefetch_tmap(&tmap);
+    }
+    __syncwarp();
+    if (warp == 0) {
+        tmem_alloc(tmem_slot, 4 * kXTN);
+        tmem_relinquish();
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        int64_t tl = 0;
+        for (int64_t tile = blockIdx.x; tile < p.n_tiles; tile += gridDim.x, tl++) {
+            const int s = (int) (tl % kStages);
+            const uint32_t ph = (uint32_t) ((tl / kStages) & 1);
+            if (!mbar_wait(&empty[s], ph ^ 1, 1)) break;
+            const int xt = (int) (tile % p.n_xt);
+            const int r0 = (int) (tile / p.n_xt) * kTM;
+            const int xs = xt * kXTN - p.ra;
+            mbar_arrive_expect_tx(&full[s], stage_bytes);
+            for (int kb = 0; kb < nkb; kb++)
+                tma_load_3d(ring + s * stage_bytes + kb * kTM * 128, &tmap, xs + 64 * kb, r0, 0, &full[s]);
+        }
+    } else if (warp == 1 && lane == 0) {
+        const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
+        const uint32_t idesc = idesc_f16(fmt, 0 /*A K-major*/, 0 /*B K-major*/, kTM, 2 * kXTN);
+        const uint32_t a0 = smem_u32(ring), b0 = smem_u32(tt);
+        int64_t tl = 0;
+        for (int64_t tile = blockIdx.x; tile < p.n_tiles; tile += gridDim.x, tl++) {
+            const int s = (int) (tl % kStages);
+            const uint32_t ph = (uint32_t) ((tl / kStages) & 1);
+            const int d = (int) (tl & 1);
+            const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
+            if (!mbar_wait(&full[s], ph, 1) || !mbar_wait(&tempty[d], dph ^ 1, 3)) break;
+            tc_fence_after();
+            const uint32_t dt = tmem + d * 2 * kXTN;
+            for (int ks = 0; ks < p.kp / 16; ks++) {
+                const uint32_t kin = (ks & 3) * 32;
+                const uint64_t ad = smem_desc_sw128(a0 + s * stage_bytes + (ks >> 2) * (kTM * 128) + kin, 16, 1024);
+                const uint64_t bd = smem_desc_sw128(b0 + (ks >> 2) * (2 * kXTN * 128) + kin, 16, 1024);
+                umma_f16(dt, ad, bd, idesc, ks > 0 ? 1u : 0u);
+            }
+            umma_commit(&empty[s]);
+            umma_commit(&tfull[d]);
+        }
+    } else if (warp >= 2) {
+        const int quad = warp & 3;
+        const int half = (warp - 2) >> 2;
+        const int r = quad * 32 + lane;
+        int64_t tl = 0;
+        for (int64_t tile = blockIdx.x; tile < p.n_tiles; tile += gridDim.x, tl++) {
+            const int d = (int) (tl & 1);
+            const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
+            if (!mbar_wait(&tfull[d], dph, 2)) break;
+            tc_fence_after();
+            const int64_t row = (tile / p.n_xt) * kTM + r;
+            const int64_t x0 = (tile % p.n_xt) * kXTN;
+            float carry = 0.0f;
+            // Mask flags of this thread's 64 voxels, fetched before the TMEM loads.
+            uint32_t mw[kXTN / 64];
+#pragma unroll
+            for (int c2 = 0; c2 < kXTN / 64; c2++) {
+                const int64_t xb = x0 + (half * (kXTN / 64) + c2) * 32;
+                mw[c2] = 0;
+                if (row < p.rows && xb < p.nx)
+                    mw[c2] = row_mask32<FMT>(p.mask, row * p.nx + xb, p.nx - xb < 32 ? (int) (p.nx - xb) : 32,
+                                             p.rows * p.nx);
+            }
+#pragma unroll
+            for (int c2 = 0; c2 < kXTN / 64; c2++) {
+                const int c = half * (kXTN / 64) + c2;
+                float h[32], l[32];
+                __syncwarp();
+                const uint32_t ta = tmem + ((uint32_t) (quad * 32) << 16) + d * 2 * kXTN + c * 32;
+                tmem_ld32(ta, h);
+                tmem_ld32(ta + kXTN, l);
+                const int64_t xb = x0 + c * 32;
+                if (row >= p.rows || xb >= p.nx) continue;
+                const int count = p.nx - xb < 32 ? (int) (p.nx - xb) : 32;
+                const int64_t idx = row * p.nx + xb;
+                const uint32_t m = mw[c2];
+                if (p.final_pass) {
+                    float v[32];
+                    uint16_t q[32];
+#pragma unroll
+                    for (int i = 0; i < 32; i++) {
+                        v[i] = ((m >> i) & 1u) ? 1.0f : (h[i] + l[i]) * p.inv_scale;
+                        q[i] = quantise_u16(v[i]);
+                    }
+                    if (count == 32) {
+                        if (p.out_u16) {
+#pragma unroll
+                            for (int i = 0; i < 32; i += 8) {
+                                uint4 u;
+                                u.x = q[i] | ((uint32_t) q[i + 1] << 16);
+                                u.y = q[i + 2] | ((uint32_t) q[i + 3] << 16);
+                                u.z = q[i + 4] | ((uint32_t) q[i + 5] << 16);
+                                u.w = q[i + 6] | ((uint32_t) q[i + 7] << 16);
+                                *reinterpret_cast<uint4 *>(p.out_u16 + idx + i) = u;
+                            }
+                        }
+                        if (p.field_out) {
+#pragma unroll
+                            for (int i = 0; i < 32; i += 4)
+                                *reinterpret_cast<float4 *>(p.field_out + idx + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 32; i++) {
+                            if (i < count) {
+                                if (p.out_u16) p.out_u16[idx + i] = q[i];
+                                if (p.field_out) p.field_out[idx + i] = v[i];
+                            }
+                        }
+                    }
+                } else {
+                    uint16_t q[32];
+#pragma unroll
+                    for (int i = 0; i < 32; i++) {
+                        if ((m >> i) & 1u) {
+                            q[i] = Narrow16<S>::bits(1.0f, carry, false);
+                            carry = 0.0f;
+                        } else {
+                            q[i] = Narrow16<S>::bits((h[i] + l[i]) * p.inv_scale, carry, p.error_feedback);
+                        }
+                    }
+                    uint16_t *dst = static_cast<uint16_t *>(p.out) + idx;
+                    if (count == 32) {
+#pragma unroll
+                        for (int i = 0; i < 32; i += 8) {
+                            uint4 u;
+                            u.x = q[i] | ((uint32_t) q[i + 1] << 16);
+                            u.y = q[i + 2] | ((uint32_t) q[i + 3] << 16);
+                            u.z = q[i + 4] | ((uint32_t) q[i + 5] << 16);
+                            u.w = q[i + 6] | ((uint32_t) q[i + 7] << 16);
+                            *reinterpret_cast<uint4 *>(dst + i) = u;
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 32; i++)
+                            if (i < count) dst[i] = q[i];
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[d]);
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 4 * kXTN);
     }
 }
 
@@ -243,6 +483,8 @@ static uint16_t bits_bf16(float v) { return __bfloat16_as_ushort(__float2bfloat1
 static float from_bf16(uint16_t b) { return __bfloat162float(__ushort_as_bfloat16(b)); }
 static uint16_t bits_f16(float v) { return __half_as_ushort(__float2half_rn(v)); }
 static float from_f16(uint16_t b) { return __half2float(__ushort_as_half(b)); }
+
+static void split_taps(const float *kernel, int radius, bool is_bf16, float scale, uint16_t *hi, uint16_t *lo);
 
 bool tc_supported(int radius, int64_t nz, int64_t ny, int64_t nx) {
     if (radius < 1 || radius > kTcMaxRadius) return false;
@@ -270,21 +512,12 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
     p.error_feedback = error_feedback ? 1 : 0;
     const float scale = is_bf16 ? 1.0f : 1024.0f;
     p.inv_scale = 1.0f / scale;
-    for (int i = 0; i < 2 * radius + 1; i++) {
-        const float k = kernel[i] * scale;
-        if (is_bf16) {
-            p.hi[i] = bits_bf16(k);
-            p.lo[i] = bits_bf16(k - from_bf16(p.hi[i]));
-        } else {
-            p.hi[i] = bits_f16(k);
-            p.lo[i] = bits_f16(k - from_f16(p.hi[i]));
-        }
-    }
+    split_taps(kernel, radius, is_bf16, scale, p.hi, p.lo);
     if (axis_z) { p.A = nz; p.n_other = ny; p.stride_a = ny * nx; p.stride_o = nx; }
     else { p.A = ny; p.n_other = nz; p.stride_a = nx; p.stride_o = ny * nx; }
     p.n_at = (int) ceil_div(p.A, kTM);
     p.n_xc = (int) ceil_div(nx, kTN);
-    p.n_tiles = (int64_t) p.n_at * p.n_xc * p.n_other;
+    p.n_cols = (int64_t) p.n_xc * p.n_other;
 
     CUtensorMap map;
     const cuuint64_t dims[3] = {(cuuint64_t) nx, (cuuint64_t) ny, (cuuint64_t) nz};
@@ -303,7 +536,7 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t grid = std::min<int64_t>(p.n_tiles, sms);
+    const int64_t grid = std::min<int64_t>(p.n_cols, sms);
     tc_strided_pass<S><<<(unsigned) grid, kThreads, smem, st>>>(map, p);
     return cudaGetLastError();
 }
@@ -312,6 +545,72 @@ template cudaError_t tc_strided<__nv_bfloat16>(const __nv_bfloat16 *, __nv_bfloa
                                                bool, const float *, int, bool, cudaStream_t);
 template cudaError_t tc_strided<__half>(const __half *, __half *, int64_t, int64_t, int64_t, bool, const float *, int,
                                         bool, cudaStream_t);
+
+static void split_taps(const float *kernel, int radius, bool is_bf16, float scale, uint16_t *hi, uint16_t *lo) {
+    for (int i = 0; i < 2 * radius + 1; i++) {
+        const float k = kernel[i] * scale;
+        if (is_bf16) {
+            hi[i] = bits_bf16(k);
+            lo[i] = bits_bf16(k - from_bf16(hi[i]));
+        } else {
+            hi[i] = bits_f16(k);
+            lo[i] = bits_f16(k - from_f16(hi[i]));
+        }
+    }
+}
+
+template <typename S>
+cudaError_t tc_contig(const S *in, S *out, const void *mask, int mask_fmt, bool final_pass, uint16_t *out_u16,
+                      float *field_out, int64_t nz, int64_t ny, int64_t nx, const float *kernel, int radius,
+                      bool error_feedback, cudaStream_t st) {
+    const bool is_bf16 = std::is_same<S, __nv_bfloat16>::value;
+    ContigParams p{};
+    p.out = out;
+    p.mask = mask;
+    p.out_u16 = out_u16;
+    p.field_out = field_out;
+    p.rows = nz * ny;
+    p.nx = nx;
+    p.radius = radius;
+    p.ra = (int) round_up(radius, 8);
+    p.kp = (int) round_up(kXTN + p.ra + radius, 16);
+    p.kpa = (int) round_up(p.kp, 64);
+    p.mask_fmt = mask_fmt;
+    p.final_pass = final_pass ? 1 : 0;
+    p.error_feedback = error_feedback ? 1 : 0;
+    const float scale = is_bf16 ? 1.0f : 1024.0f;
+    p.inv_scale = 1.0f / scale;
+    split_taps(kernel, radius, is_bf16, scale, p.hi, p.lo);
+    p.n_xt = (int) ceil_div(nx, kXTN);
+    p.n_tiles = (int64_t) p.n_xt * ceil_div(p.rows, kTM);
+
+    CUtensorMap map;
+    const cuuint64_t dims[3] = {(cuuint64_t) nx, (cuuint64_t) p.rows, 1};
+    const cuuint64_t strides[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (nx * p.rows * 2)};
+    const cuuint32_t box[3] = {64u, (cuuint32_t) kTM, 1u};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult cr = encode_fn()(&map, is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
+                              const_cast<S *>(in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    const int smem = contig_smem_bytes_tc(p.kp, p.kpa);
+    auto *kern = mask_fmt == MAXI_MASK_U8 ? tc_contig_pass<S, MAXI_MASK_U8> : tc_contig_pass<S, MAXI_MASK_BITPACKED>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t grid = std::min<int64_t>(p.n_tiles, sms);
+    kern<<<(unsigned) grid, kXThreads, smem, st>>>(map, p);
+    return cudaGetLastError();
+}
+
+template cudaError_t tc_contig<__nv_bfloat16>(const __nv_bfloat16 *, __nv_bfloat16 *, const void *, int, bool,
+                                              uint16_t *, float *, int64_t, int64_t, int64_t, const float *, int,
+                                              bool, cudaStream_t);
+template cudaError_t tc_contig<__half>(const __half *, __half *, const void *, int, bool, uint16_t *, float *,
+                                       int64_t, int64_t, int64_t, const float *, int, bool, cudaStream_t);
 
 int tc_read_and_clear_error() {
     int v = 0;

@@ -20,6 +20,14 @@ template <typename S>
 cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, bool axis_z, const float *kernel,
                        int radius, bool error_feedback, cudaStream_t st);
 
+// The x pass fused with re-illumination; on the last repetition (final_pass)
+// it writes the uint16 output and/or the FP32 field (either may be NULL)
+// instead of `out`.
+template <typename S>
+cudaError_t tc_contig(const S *in, S *out, const void *mask, int mask_fmt, bool final_pass, uint16_t *out_u16,
+                      float *field_out, int64_t nz, int64_t ny, int64_t nx, const float *kernel, int radius,
+                      bool error_feedback, cudaStream_t st);
+
 // Reads (and clears) the device error word of the tensor-core kernels:
 // 0 = fine, 1..3 = a bounded wait timed out, -1 = could not be read.
 int tc_read_and_clear_error();

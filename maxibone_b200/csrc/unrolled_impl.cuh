@@ -72,6 +72,10 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
     const int64_t zI = v.ny * v.nx, zA = v.nz, zat = ceil_div(zA, kStrTA), zit = ceil_div(zI, kStrTI);
     const int64_t yI = v.nx, yA = v.ny, yO = v.nz, yat = ceil_div(yA, kStrTA), yit = ceil_div(yI, kStrTI);
     const int64_t rows = v.nz * v.ny, xt = ceil_div(v.nx, kConTX), xrb = ceil_div(rows, kConTR);
+    // Tensor-core x pass: vector epilogue needs 16-byte aligned mask (u8), output and field.
+    const bool tc_x = use_tc &&
+                      ((reinterpret_cast<uintptr_t>(out_u16) | reinterpret_cast<uintptr_t>(field_out) |
+                        (mask_fmt == MAXI_MASK_U8 ? reinterpret_cast<uintptr_t>(mask) : 0)) & 15) == 0;
     for (int64_t rep = 0; rep < reps; rep++) {
         {
             ProfScope ps(MAXI_KERNEL_Z, st);
@@ -93,14 +97,21 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
             }
         }
         if (e != cudaSuccess) return e;
-        if (rep + 1 < reps) {
-            ProfScope ps(MAXI_KERNEL_X, st);
-            xpass<<<xt * xrb, kConThreads, con_smem, st>>>(buf0, buf1, mask, nullptr, nullptr, rows, v.nx, xt, taps);
-            std::swap(buf0, buf1);
-        } else {
-            ProfScope ps(MAXI_KERNEL_X_FINAL, st);
-            xfinal<<<xt * xrb, kConThreads, con_smem, st>>>(buf0, buf1, mask, out_u16, field_out, rows, v.nx, xt, taps);
+        const bool last = rep + 1 == reps;
+        {
+            ProfScope ps(last ? MAXI_KERNEL_X_FINAL : MAXI_KERNEL_X, st);
+            if (tc_x) {
+                if constexpr (sizeof(S) == 2)
+                    e = tc::tc_contig<S>(buf0, buf1, mask, mask_fmt, last, last ? out_u16 : nullptr,
+                                         last ? field_out : nullptr, v.nz, v.ny, v.nx, kernel, radius, EF, st);
+            } else if (!last) {
+                xpass<<<xt * xrb, kConThreads, con_smem, st>>>(buf0, buf1, mask, nullptr, nullptr, rows, v.nx, xt, taps);
+            } else {
+                xfinal<<<xt * xrb, kConThreads, con_smem, st>>>(buf0, buf1, mask, out_u16, field_out, rows, v.nx, xt, taps);
+            }
         }
+        if (e != cudaSuccess) return e;
+        if (!last) std::swap(buf0, buf1);
     }
     return cudaGetLastError();
 }
@@ -124,7 +135,9 @@ cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, c
                               int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, int32_t flags,
                               cudaStream_t st) {
     if constexpr (sizeof(S) == 2) {
-        const bool ef = (flags & MAXI_FLAG_NEAREST_ROUNDING) == 0;
+        // Error feedback relies on the following x pass to remove high-pass noise;
+        // kernels narrower than radius 4 (sigma < 1) pass too much of it.
+        const bool ef = (flags & MAXI_FLAG_NEAREST_ROUNDING) == 0 && radius >= 4;
         const bool use_tc = (flags & MAXI_FLAG_NO_TENSOR_CORES) == 0 && tc::tc_supported(radius, v.nz, v.ny, v.nx);
         if (ef) return dispatch_radius<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, st);
         return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, st);

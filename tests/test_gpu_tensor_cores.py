@@ -54,8 +54,11 @@ def test_tensor_core_radius_range(radius):
     mask = spheres_mask((64, 96, 128), 10, (3, 9), seed=radius)
     kernel = gauss_kernel(radius / 4.0).astype(np.float32)
     _, want = run(mask, kernel, 4, "f64")
-    _, got = run(mask, kernel, 4, "f16", True, True)
-    assert np.abs(got.astype(np.float64) - want).max() <= VS_F64["f16"]
+    for field in ("f16", "bf16"):
+        _, got = run(mask, kernel, 4, field, True, True)
+        _, cc = run(mask, kernel, 4, field, False, True)
+        assert np.abs(got - cc).max() <= TC_VS_CC[field]
+        assert np.abs(got.astype(np.float64) - want).max() <= VS_F64[field]
 
 
 def test_error_feedback_reduces_bf16_error():
@@ -67,3 +70,31 @@ def test_error_feedback_reduces_bf16_error():
     e_rn = np.abs(rn.astype(np.float64) - want).max()
     e_ef = np.abs(ef.astype(np.float64) - want).max()
     assert e_ef < e_rn
+
+
+@pytest.mark.parametrize("field", ["bf16", "f16"])
+def test_tensor_core_final_pass_outputs_optional(field):
+    mask = random_mask((20, 40, 128), 0.03, seed=3)
+    kernel = gauss_kernel(2.0).astype(np.float32)
+    m = torch.from_numpy(mask).cuda()
+    u16_only = torch.empty(mask.shape, dtype=torch.uint16, device="cuda")
+    device.diffuse(m, kernel, 3, output=u16_only, field=field)
+    fo_only = torch.empty(mask.shape, dtype=torch.float32, device="cuda")
+    device.diffuse(m, kernel, 3, output=None, field_out=fo_only, field=field)
+    both_u16, both_fo = run(mask, kernel, 3, field)
+    np.testing.assert_array_equal(u16_only.cpu().numpy(), both_u16)
+    np.testing.assert_array_equal(fo_only.cpu().numpy(), both_fo)
+
+
+@pytest.mark.parametrize("field", ["bf16", "f16"])
+def test_tensor_core_bitpacked_mask(field):
+    mask = spheres_mask((24, 50, 136), 8, (3, 8), seed=6)
+    kernel = gauss_kernel(3.0).astype(np.float32)
+    m = torch.from_numpy(mask).cuda()
+    packed = device.bitpack(m)
+    out_p = torch.empty(mask.shape, dtype=torch.uint16, device="cuda")
+    fo_p = torch.empty(mask.shape, dtype=torch.float32, device="cuda")
+    device.diffuse(packed, kernel, 3, output=out_p, field_out=fo_p, field=field, shape=mask.shape)
+    u, f = run(mask, kernel, 3, field)
+    np.testing.assert_array_equal(out_p.cpu().numpy(), u)
+    np.testing.assert_array_equal(fo_p.cpu().numpy(), f)

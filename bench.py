@@ -60,6 +60,8 @@ def parse_args():
     p.add_argument("--workload", choices=sorted(WORKLOADS), default="bone1024_s8_r100")
     p.add_argument("--field", choices=["f32", "bf16", "f16"], default="f32")
     p.add_argument("--quick", action="store_true", help="skip e2e, precision forms and CPU baseline")
+    p.add_argument("--shape", type=str, default=None,
+                   help="override the workload's volume shape, e.g. 256x1024x1024 (profiling of smaller cases)")
     return p.parse_args()
 
 
@@ -194,6 +196,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
     shape, sigma, reps = WORKLOADS[args.workload]
+    if args.shape:
+        shape = tuple(int(v) for v in args.shape.lower().split("x"))
     nz, ny, nx = shape
     vox = nz * ny * nx
     kernel = gauss_kernel(sigma).astype(np.float32)
@@ -268,7 +272,8 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": args.field, "data": "synthetic (seeded bone+implant mask, random-init)",
-        "config": {"workload": args.workload, "shape": list(shape), "sigma": sigma, "kernel_size": int(2 * radius + 1),
+        "config": {"workload": args.workload + (f" (shape override {args.shape})" if args.shape else ""),
+                   "shape": list(shape), "sigma": sigma, "kernel_size": int(2 * radius + 1),
                    "reps": reps, "field": args.field, "mask": "u8", "foreground": round(fg, 4),
                    "parallelism": f"{world} independent volumes (one per rank)",
                    "l2": "inputs larger than L2 (field %d MiB per buffer)" % (s * vox >> 20)},

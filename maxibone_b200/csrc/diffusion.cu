@@ -87,8 +87,10 @@ static size_t field_bytes(int32_t ft) {
     }
 }
 
+// Two field buffers plus the bit-packed copy of a uint8 mask (the passes read
+// the mask as 1 bit per voxel).
 static int64_t workspace_bytes_for(int64_t n, int32_t ft) {
-    return 2 * round_up((int64_t) field_bytes(ft) * n, 256);
+    return 2 * round_up((int64_t) field_bytes(ft) * n, 256) + round_up(ceil_div(n, 32) * 4, 256);
 }
 
 template <typename S>
@@ -104,9 +106,18 @@ static cudaError_t run_typed(const Volume &v, const void *mask, int mask_fmt, co
         if (exact) return run_generic<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, st);
         return run_generic<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, st);
     }
-    if constexpr (!is_f64)
+    if constexpr (!is_f64) {
+        if (mask_fmt == MAXI_MASK_U8) {
+            // Read the mask as 1 bit per voxel in every x pass: pack it once.
+            uint32_t *packed = reinterpret_cast<uint32_t *>(ws + 2 * round_up((int64_t) sizeof(S) * v.n(), 256));
+            cudaError_t e = launch_bitpack_encode(static_cast<const uint8_t *>(mask), v.n(), packed, false, st);
+            if (e != cudaSuccess) return e;
+            mask = packed;
+            mask_fmt = MAXI_MASK_BITPACKED;
+        }
         return dispatch_unrolled<S>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16,
                                     static_cast<float *>(field_out), flags, st);
+    }
     return cudaErrorInvalidValue;
 }
 

@@ -233,9 +233,9 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
 // row -- the layout re-illumination, error feedback along x and vector stores
 // want.  D[r, o] = sum_j F[r, x0 - RA + j] * Tt[j, o] with RA = R rounded up to
 // 8 (TMA x coordinates must be 16-byte aligned); Tt[j, o] = k[j - o - RA + R].
-// The high and low coefficient halves are concatenated along N (N = 256:
-// columns 0..127 hold F*Tt_hi, 128..255 F*Tt_lo) so one MMA reads the A tile
-// once; the epilogue adds the halves.
+// The high and low coefficient halves sit in one K-major operand (rows
+// 0..127 Tt_hi, 128..255 Tt_lo); two N = 128 MMAs accumulate both into the
+// same FP32 accumulator, so the epilogue reads one value per voxel.
 constexpr int kXTN = 128;            // x outputs per tile
 constexpr int kXThreads = kThreads;
 
@@ -306,7 +306,7 @@ tc_contig_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__
     }
     __syncwarp();
     if (warp == 0) {
-        tmem_alloc(tmem_slot, 4 * kXTN);
+        tmem_alloc(tmem_slot, 2 * kXTN);
         tmem_relinquish();
     }
     fence_proxy_async_smem();
@@ -330,7 +330,7 @@ tc_contig_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__
         }
     } else if (warp == 1 && lane == 0) {
         const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
-        const uint32_t idesc = idesc_f16(fmt, 0 /*A K-major*/, 0 /*B K-major*/, kTM, 2 * kXTN);
+        const uint32_t idesc = idesc_f16(fmt, 0 /*A K-major*/, 0 /*B K-major*/, kTM, kXTN);
         const uint32_t a0 = smem_u32(ring), b0 = smem_u32(tt);
         int64_t tl = 0;
         for (int64_t tile = blockIdx.x; tile < p.n_tiles; tile += gridDim.x, tl++) {
@@ -340,12 +340,13 @@ tc_contig_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__
             const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
             if (!mbar_wait(&full[s], ph, 1) || !mbar_wait(&tempty[d], dph ^ 1, 3)) break;
             tc_fence_after();
-            const uint32_t dt = tmem + d * 2 * kXTN;
+            const uint32_t dt = tmem + d * kXTN;
             for (int ks = 0; ks < p.kp / 16; ks++) {
                 const uint32_t kin = (ks & 3) * 32;
                 const uint64_t ad = smem_desc_sw128(a0 + s * stage_bytes + (ks >> 2) * (kTM * 128) + kin, 16, 1024);
-                const uint64_t bd = smem_desc_sw128(b0 + (ks >> 2) * (2 * kXTN * 128) + kin, 16, 1024);
-                umma_f16(dt, ad, bd, idesc, ks > 0 ? 1u : 0u);
+                const uint32_t bhi = b0 + (ks >> 2) * (2 * kXTN * 128) + kin;  // rows 0..127: Tt_hi
+                umma_f16(dt, ad, smem_desc_sw128(bhi, 16, 1024), idesc, ks > 0 ? 1u : 0u);
+                umma_f16(dt, ad, smem_desc_sw128(bhi + kXTN * 128, 16, 1024), idesc, 1u);  // rows 128..255: Tt_lo
             }
             umma_commit(&empty[s]);
             umma_commit(&tfull[d]);
@@ -376,11 +377,10 @@ tc_contig_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__
 #pragma unroll
             for (int c2 = 0; c2 < kXTN / 64; c2++) {
                 const int c = half * (kXTN / 64) + c2;
-                float h[32], l[32];
+                float h[32];
                 __syncwarp();
-                const uint32_t ta = tmem + ((uint32_t) (quad * 32) << 16) + d * 2 * kXTN + c * 32;
+                const uint32_t ta = tmem + ((uint32_t) (quad * 32) << 16) + d * kXTN + c * 32;
                 tmem_ld32(ta, h);
-                tmem_ld32(ta + kXTN, l);
                 const int64_t xb = x0 + c * 32;
                 if (row >= p.rows || xb >= p.nx) continue;
                 const int count = p.nx - xb < 32 ? (int) (p.nx - xb) : 32;
@@ -391,7 +391,7 @@ tc_contig_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__
                     uint16_t q[32];
 #pragma unroll
                     for (int i = 0; i < 32; i++) {
-                        v[i] = ((m >> i) & 1u) ? 1.0f : (h[i] + l[i]) * p.inv_scale;
+                        v[i] = ((m >> i) & 1u) ? 1.0f : h[i] * p.inv_scale;
                         q[i] = quantise_u16(v[i]);
                     }
                     if (count == 32) {
@@ -428,7 +428,7 @@ tc_contig_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__
                             q[i] = Narrow16<S>::bits(1.0f, carry, false);
                             carry = 0.0f;
                         } else {
-                            q[i] = Narrow16<S>::bits((h[i] + l[i]) * p.inv_scale, carry, p.error_feedback);
+                            q[i] = Narrow16<S>::bits(h[i] * p.inv_scale, carry, p.error_feedback);
                         }
                     }
                     uint16_t *dst = static_cast<uint16_t *>(p.out) + idx;
@@ -457,7 +457,7 @@ tc_contig_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        tmem_dealloc(tmem, 4 * kXTN);
+        tmem_dealloc(tmem, 2 * kXTN);
     }
 }
 

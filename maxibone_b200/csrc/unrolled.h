@@ -12,6 +12,10 @@ struct Volume {
     int64_t n() const { return nz * ny * nx; }
 };
 
+// Packs a uint8 mask into uint32 words, MSB first (bitpack.cu).  keep_bit0:
+// the reference encode's `mask & 1`; otherwise the diffusion's `mask > 0`.
+cudaError_t launch_bitpack_encode(const uint8_t *mask, int64_t n, uint32_t *packed, bool keep_bit0, cudaStream_t st);
+
 // Smallest radius with an unrolled instantiation that is >= r, or -1.
 int radius_bucket(int r);
 

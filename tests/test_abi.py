@@ -73,8 +73,9 @@ def test_device_entry_rejects_bad_enums():
 
 def test_workspace_size():
     lib = _lib.lib()
-    assert lib.maxi_diffusion_workspace_size(10, 10, 10, 0) == 2 * 4096
-    assert lib.maxi_diffusion_workspace_size(10, 10, 10, 1) == 2 * 2048
+    # two field buffers (256-byte rounded) + the bit-packed mask (32 words -> 256 bytes)
+    assert lib.maxi_diffusion_workspace_size(10, 10, 10, 0) == 2 * 4096 + 256
+    assert lib.maxi_diffusion_workspace_size(10, 10, 10, 1) == 2 * 2048 + 256
     assert lib.maxi_diffusion_workspace_size(0, 10, 10, 0) == -1
     assert lib.maxi_diffusion_workspace_size(10, 10, 10, 42) == -1
 

@@ -37,6 +37,7 @@ namespace tc {
 constexpr int kTM = 128;      // outputs along the axis per tile
 constexpr int kTN = 128;      // x columns per tile
 constexpr int kStages = 2;    // TMA ring depth
+constexpr int kPrefetch = 3;  // tiles prefetched into L2 ahead of the ring
 constexpr int kEpiWarps = 8;  // two warps per TMEM lane quadrant, each drains half the columns
 constexpr int kThreads = 64 + 32 * kEpiWarps;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
 
@@ -57,9 +58,14 @@ struct StridedParams {
     uint16_t lo[2 * kTcMaxRadius + 1];
 };
 
+// Per-epilogue-warp staging of a 32-row x 32-column output chunk: row stride
+// 80 bytes (16-byte stores of 32 lanes on 32 rows hit 8 distinct bank groups).
+constexpr int kStageRowBytes = 80;
+constexpr int kStageWarpBytes = 32 * kStageRowBytes;
+
 __host__ __device__ constexpr int strided_smem_bytes(int kp, int kpa) {
     return 1024 /*alignment slack*/ + 2 * kpa * kTM * 2 /*T_hi, T_lo*/ + kStages * (kTN / 64) * kp * 128 /*B ring*/ +
-           256 /*barriers, TMEM slot*/;
+           256 /*barriers, TMEM slot*/ + kEpiWarps * kStageWarpBytes;
 }
 
 template <typename S> struct Narrow16;
@@ -93,6 +99,7 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
     uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kStages * stage_bytes);
     uint64_t *full = bars, *empty = bars + kStages, *tfull = bars + 2 * kStages, *tempty = bars + 2 * kStages + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 4);
+    uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 256;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -132,6 +139,19 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
             const int s = (int) (tl % kStages);
             const uint32_t ph = (uint32_t) ((tl / kStages) & 1);
             if (!mbar_wait(&empty[s], ph ^ 1, 1)) { ok = false; break; }
+            {
+                // L2 prefetch of the tile kPrefetch tiles ahead in this CTA's order.
+                const int64_t tp = tl + kPrefetch;
+                const int64_t colp = blockIdx.x + (tp / p.n_at) * gridDim.x;
+                if (colp < p.n_cols) {
+                    const int atp = (int) (tp % p.n_at);
+                    const int xcp = (int) (colp % p.n_xc), othp = (int) (colp / p.n_xc);
+                    for (int c = 0; c < kTN / 64; c++) {
+                        if (p.axis_is_z) tma_prefetch_3d(&tmap, xcp * kTN + 64 * c, othp, atp * kTM - p.radius);
+                        else tma_prefetch_3d(&tmap, xcp * kTN + 64 * c, atp * kTM - p.radius, othp);
+                    }
+                }
+            }
             const int xc = (int) (col % p.n_xc);
             const int oth = (int) (col / p.n_xc);
             const int a_in = at * kTM - p.radius;
@@ -174,6 +194,7 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
         const int half = (warp - 2) >> 2;    // which half of the columns it drains
         const int o = quad * 32 + lane;      // output row within the tile
         S *out = static_cast<S *>(p.out);
+        uint8_t *stg = stage_out + (warp - 2) * kStageWarpBytes;
         int64_t tl = 0;
         bool ok = true;
         for (int64_t col = blockIdx.x; ok && col < p.n_cols; col += gridDim.x)
@@ -192,27 +213,44 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
                 float v[32];
                 __syncwarp();
                 tmem_ld32(tmem + ((uint32_t) (quad * 32) << 16) + d * kTN + c * 32, v);
-                if (a >= p.A) continue;
                 const int64_t xb = x0 + c * 32;
-                S *dst = out + a * p.stride_a + oth * p.stride_o + xb;
                 uint16_t q[32];
 #pragma unroll
                 for (int i = 0; i < 32; i++) q[i] = Narrow16<S>::bits(v[i] * p.inv_scale, carry, p.error_feedback);
-                if (xb + 32 <= p.nx) {
+                uint4 u[4];
 #pragma unroll
-                    for (int i = 0; i < 32; i += 8) {
-                        uint4 u;
-                        u.x = q[i] | ((uint32_t) q[i + 1] << 16);
-                        u.y = q[i + 2] | ((uint32_t) q[i + 3] << 16);
-                        u.z = q[i + 4] | ((uint32_t) q[i + 5] << 16);
-                        u.w = q[i + 6] | ((uint32_t) q[i + 7] << 16);
-                        *reinterpret_cast<uint4 *>(dst + i) = u;
-                    }
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 32; i++)
-                        if (xb + i < p.nx) reinterpret_cast<uint16_t *>(dst)[i] = q[i];
+                for (int i = 0; i < 32; i += 8) {
+                    u[i / 8].x = q[i] | ((uint32_t) q[i + 1] << 16);
+                    u[i / 8].y = q[i + 2] | ((uint32_t) q[i + 3] << 16);
+                    u[i / 8].z = q[i + 4] | ((uint32_t) q[i + 5] << 16);
+                    u[i / 8].w = q[i + 6] | ((uint32_t) q[i + 7] << 16);
                 }
+                if (!p.axis_is_z) {
+                    // y pass: a lane's row is 2 KB from its neighbour's, one page per warp.
+                    if (a < p.A) {
+                        S *dst = out + a * p.stride_a + oth * p.stride_o + xb;
+#pragma unroll
+                        for (int i = 0; i < 4; i++)  // nx % 8 == 0: each 8-voxel group is wholly in or out
+                            if (xb + 8 * i < p.nx) reinterpret_cast<uint4 *>(dst)[i] = u[i];
+                    }
+                    continue;
+                }
+                // z pass: lanes' rows lie on different planes (2 MB apart at 1024^2), so
+                // stage the warp's 32 x 32 chunk and store 8 rows (8 x 64 bytes) per
+                // instruction instead of 32 distant rows.
+#pragma unroll
+                for (int i = 0; i < 4; i++) *reinterpret_cast<uint4 *>(stg + lane * kStageRowBytes + i * 16) = u[i];
+                __syncwarp();
+                const int sub = lane & 3, rsub = lane >> 2;
+#pragma unroll
+                for (int r4 = 0; r4 < 4; r4++) {
+                    const int rr = r4 * 8 + rsub;
+                    const int64_t ar = (int64_t) at * kTM + quad * 32 + rr;
+                    const uint4 w = *reinterpret_cast<const uint4 *>(stg + rr * kStageRowBytes + sub * 16);
+                    if (ar < p.A && xb + sub * 8 < p.nx)
+                        *reinterpret_cast<uint4 *>(out + ar * p.stride_a + oth * p.stride_o + xb + sub * 8) = w;
+                }
+                __syncwarp();
             }
             tc_fence_before();
             __syncwarp();
@@ -321,6 +359,11 @@ tc_contig_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__
             const int s = (int) (tl % kStages);
             const uint32_t ph = (uint32_t) ((tl / kStages) & 1);
             if (!mbar_wait(&empty[s], ph ^ 1, 1)) break;
+            const int64_t tp = tile + kPrefetch * (int64_t) gridDim.x;
+            if (tp < p.n_tiles) {
+                const int xsp = (int) (tp % p.n_xt) * kXTN - p.ra, r0p = (int) (tp / p.n_xt) * kTM;
+                for (int kb = 0; kb < nkb; kb++) tma_prefetch_3d(&tmap, xsp + 64 * kb, r0p, 0);
+            }
             const int xt = (int) (tile % p.n_xt);
             const int r0 = (int) (tile / p.n_xt) * kTM;
             const int xs = xt * kXTN - p.ra;

@@ -53,6 +53,9 @@ typedef enum maxi_mask_format {
                                             reference's tap order, bit-identical to the
                                             reference OpenMP backend */
 #define MAXI_FLAG_NO_TENSOR_CORES 0x2    /* BF16/FP16: CUDA-core passes only */
+#define MAXI_FLAG_MASK_FROM_FIELD 0x8    /* FP32 only: before every repetition after the first,
+                                            the mask is rebuilt as `field == 1.0f` -- the
+                                            semantics of the reference's on-disk variant */
 #define MAXI_FLAG_NEAREST_ROUNDING 0x4   /* BF16/FP16: plain round-to-nearest stores instead of
                                             error-feedback rounding along x (the default for
                                             radius >= 4, which keeps the stored rounding noise
@@ -149,6 +152,36 @@ int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int
 int maxi_diffusion_device_noalloc(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,
                                   const float *kernel, int64_t kernel_size, int64_t repititions,
                                   uint16_t *output, float *field_out, void *stream);
+
+/*
+ * Out-of-core diffusion of a HOST volume that need not fit the device.
+ * Replaces NS::diffusion_out_of_core, src/lib/cpp/include/diffusion.hh:74
+ * (GPU body src/lib/cpp/gpu/diffusion.cc:947-1129).  The volume is processed as
+ * z-slabs of global_z planes, each loaded with repititions x radius halo planes
+ * per side so all repetitions run on the device without exchanges; slabs span
+ * the full y and x extent (global_y / global_x only have to be positive).
+ * FP32 field; results equal maxi_diffusion_in_memory().
+ */
+int maxi_diffusion_out_of_core(const uint8_t *voxels, int64_t total_z, int64_t total_y, int64_t total_x,
+                               int64_t global_z, int64_t global_y, int64_t global_x, const float *kernel,
+                               int64_t kernel_size, int64_t repititions, uint16_t *output, int verbose);
+
+/* The same with the field storage type and MAXI_FLAG_* options. */
+int maxi_diffusion_out_of_core_ex(const uint8_t *voxels, int64_t nz, int64_t ny, int64_t nx, int64_t slab_z,
+                                  const float *kernel, int64_t kernel_size, int64_t repititions, uint16_t *output,
+                                  int32_t field_type, int32_t flags, int verbose);
+
+/*
+ * On-disk diffusion: raw uint8 volume file in, raw uint16 file out.  Replaces
+ * NS::diffusion_on_disk, src/lib/cpp/include/diffusion.hh:55, as bound by
+ * python_api::diffusion_on_disk, src/pybind/diffusion-pybind.cc:67-77 (GPU
+ * semantics: uint16 output, src/lib/cpp/gpu/diffusion.cc:937; the mask of each
+ * repetition is rebuilt as field == 1.0f).  Streams z-slabs of global_z planes;
+ * writes no temporary files.
+ */
+int maxi_diffusion_on_disk(const char *input_file, const float *kernel, int64_t kernel_size, const char *output_file,
+                           int64_t total_z, int64_t total_y, int64_t total_x, int64_t global_z, int64_t global_y,
+                           int64_t global_x, int64_t repititions, int verbose);
 
 /*
  * Bit-packing of a device mask to uint32 words, MSB first.  Replaces the

@@ -21,6 +21,7 @@ MASK_FORMATS = {"u8": 0, "bitpacked": 1}
 FLAG_REFERENCE_ROUNDING = 0x1
 FLAG_NO_TENSOR_CORES = 0x2
 FLAG_NEAREST_ROUNDING = 0x4
+FLAG_MASK_FROM_FIELD = 0x8
 
 # Every symbol include/maxibone_diffusion.h declares, with (restype, argtypes).
 _i64, _i32, _p, _int = ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int
@@ -34,6 +35,10 @@ SIGNATURES = {
     "maxi_bitpack_decode": (_int, [_p, _i64, _p, _p]),
     "maxi_diffusion_device_noalloc": (_int, [_p, _i32, _i64, _i64, _i64, _p, _i64, _i64, _p, _p, _p]),
     "maxi_tensor_core_status": (_int, []),
+    "maxi_diffusion_out_of_core": (_int, [_p, _i64, _i64, _i64, _i64, _i64, _i64, _p, _i64, _i64, _p, _int]),
+    "maxi_diffusion_out_of_core_ex": (_int, [_p, _i64, _i64, _i64, _i64, _p, _i64, _i64, _p, _i32, _i32, _int]),
+    "maxi_diffusion_on_disk": (_int, [ctypes.c_char_p, _p, _i64, ctypes.c_char_p, _i64, _i64, _i64, _i64, _i64,
+                                      _i64, _i64, _int]),
     "maxi_profile_enable": (_int, [_int]),
     "maxi_profile_read": (_int, [_p, _p, _i32]),
 }

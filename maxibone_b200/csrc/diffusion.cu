@@ -107,13 +107,18 @@ static cudaError_t run_typed(const Volume &v, const void *mask, int mask_fmt, co
         return run_generic<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, st);
     }
     if constexpr (!is_f64) {
+        uint32_t *packed = reinterpret_cast<uint32_t *>(ws + 2 * round_up((int64_t) sizeof(S) * v.n(), 256));
         if (mask_fmt == MAXI_MASK_U8) {
             // Read the mask as 1 bit per voxel in every x pass: pack it once.
-            uint32_t *packed = reinterpret_cast<uint32_t *>(ws + 2 * round_up((int64_t) sizeof(S) * v.n(), 256));
             cudaError_t e = launch_bitpack_encode(static_cast<const uint8_t *>(mask), v.n(), packed, false, st);
             if (e != cudaSuccess) return e;
             mask = packed;
             mask_fmt = MAXI_MASK_BITPACKED;
+        } else if (flags & MAXI_FLAG_MASK_FROM_FIELD) {
+            // The mask is rewritten every repetition: work on a copy, never the caller's.
+            cudaError_t e = cudaMemcpyAsync(packed, mask, ceil_div(v.n(), 32) * 4, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return e;
+            mask = packed;
         }
         return dispatch_unrolled<S>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16,
                                     static_cast<float *>(field_out), flags, st);
@@ -157,6 +162,10 @@ int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int
         return set_error(MAXI_ERR_INVALID_ARGUMENT, "unknown field_type %d", field_type);
     if ((flags & MAXI_FLAG_REFERENCE_ROUNDING) && field_type != MAXI_FIELD_F32)
         return set_error(MAXI_ERR_INVALID_ARGUMENT, "reference rounding is defined for the FP32 field only");
+    if ((flags & MAXI_FLAG_MASK_FROM_FIELD) &&
+        (field_type != MAXI_FIELD_F32 || (flags & MAXI_FLAG_REFERENCE_ROUNDING) || kernel_size / 2 > 128))
+        return set_error(MAXI_ERR_UNSUPPORTED,
+                         "the rebuilt-mask semantics are served for the FP32 field with the fast passes (radius <= 128)");
     if (!output && !field_out)
         return set_error(MAXI_ERR_INVALID_ARGUMENT, "neither output nor field_out given");
     if ((rc = require_device())) return rc;

@@ -345,6 +345,21 @@ generic_pass(const S *__restrict__ in, S *__restrict__ out, const void *__restri
     out[idx] = FieldIO<S>::narrow(sum);
 }
 
+// Rebuilds the bit-packed mask as `field == 1` (the reference's store_mask,
+// src/lib/cpp/cpu/diffusion.cc:304-312, used by its on-disk variant).
+template <typename S>
+__global__ void mask_from_field(const S *__restrict__ field, uint32_t *__restrict__ packed, int64_t n) {
+    const int64_t words = (n + 31) / 32;
+    for (int64_t w = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (int64_t) gridDim.x * blockDim.x) {
+        uint32_t bits = 0;
+        for (int j = 0; j < 32; j++) {
+            const int64_t i = w * 32 + j;
+            if (i < n && FieldIO<S>::widen(field[i]) == 1.0f) bits |= 1u << (31 - j);
+        }
+        packed[w] = bits;
+    }
+}
+
 // mask -> {0, 1} field (src/lib/cpp/cpu/diffusion.cc:243-247); with FINAL set
 // (zero repetitions) the quantised output and field are written directly.
 template <typename S, int MASK_FMT, bool FINAL>

@@ -42,7 +42,7 @@ static cudaError_t set_smem(F *f, int bytes) {
 template <int R, typename S, bool EF>
 static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel,
                                 int radius, int64_t reps, S *buf0, S *buf1, uint16_t *out_u16,
-                                float *field_out, bool use_tc, cudaStream_t st) {
+                                float *field_out, bool use_tc, uint32_t *rebuild_mask, cudaStream_t st) {
     const Taps<R> taps = make_taps<R>(kernel, radius);
     const int str_smem = strided_smem_bytes<R>();
     const int con_smem = contig_smem_bytes<R>();
@@ -77,6 +77,11 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
                       ((reinterpret_cast<uintptr_t>(out_u16) | reinterpret_cast<uintptr_t>(field_out) |
                         (mask_fmt == MAXI_MASK_U8 ? reinterpret_cast<uintptr_t>(mask) : 0)) & 15) == 0;
     for (int64_t rep = 0; rep < reps; rep++) {
+        if (rebuild_mask && rep > 0) {
+            ProfScope ps(MAXI_KERNEL_OTHER, st);
+            const int64_t blocks = std::min<int64_t>(ceil_div(ceil_div(n, 32), 256), 148 * 16);
+            mask_from_field<S><<<blocks, 256, 0, st>>>(buf0, rebuild_mask, n);
+        }
         {
             ProfScope ps(MAXI_KERNEL_Z, st);
             if constexpr (sizeof(S) == 2) {
@@ -119,10 +124,10 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
 template <typename S, bool EF>
 static cudaError_t dispatch_radius(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
                                    int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, bool use_tc,
-                                   cudaStream_t st) {
+                                   uint32_t *rebuild, cudaStream_t st) {
     switch (radius_bucket_impl(radius)) {
 #define MAXI_CASE(RB) \
-    case RB: return run_unrolled<RB, S, EF>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, st);
+    case RB: return run_unrolled<RB, S, EF>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, rebuild, st);
         MAXI_CASE(1) MAXI_CASE(2) MAXI_CASE(3) MAXI_CASE(4) MAXI_CASE(6) MAXI_CASE(8) MAXI_CASE(12)
         MAXI_CASE(16) MAXI_CASE(24) MAXI_CASE(32) MAXI_CASE(48) MAXI_CASE(64) MAXI_CASE(96) MAXI_CASE(128)
 #undef MAXI_CASE
@@ -134,15 +139,20 @@ template <typename S>
 cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
                               int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, int32_t flags,
                               cudaStream_t st) {
+    // Mask rebuilt from the field each repetition: the caller passes a writable
+    // bit-packed copy (the workspace's).
+    uint32_t *rebuild = (flags & MAXI_FLAG_MASK_FROM_FIELD) && mask_fmt == MAXI_MASK_BITPACKED
+                            ? const_cast<uint32_t *>(static_cast<const uint32_t *>(mask))
+                            : nullptr;
     if constexpr (sizeof(S) == 2) {
         // Error feedback relies on the following x pass to remove high-pass noise;
         // kernels narrower than radius 4 (sigma < 1) pass too much of it.
         const bool ef = (flags & MAXI_FLAG_NEAREST_ROUNDING) == 0 && radius >= 4;
         const bool use_tc = (flags & MAXI_FLAG_NO_TENSOR_CORES) == 0 && tc::tc_supported(radius, v.nz, v.ny, v.nx);
-        if (ef) return dispatch_radius<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, st);
-        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, st);
+        if (ef) return dispatch_radius<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, rebuild, st);
+        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, rebuild, st);
     } else {
-        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, false, st);
+        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, false, rebuild, st);
     }
 }
 

@@ -73,6 +73,23 @@ def _on_disk(input_file, np_kernel, output_file, total_shape, global_shape, repi
         _as_int(repititions, "repititions"), _as_int(verbose, "verbose")))
 
 
+def diffusion_out_of_core(np_voxels, np_kernel, np_output, global_shape, repititions=1, verbose=0, field="f32"):
+    """Out-of-core form for host volumes larger than the device (the reference's
+    NS::diffusion_out_of_core, src/lib/cpp/include/diffusion.hh:74): z-slabs of
+    global_shape[0] planes with deep halos, streamed through the GPU."""
+    if not isinstance(np_output, np.ndarray) or np_output.dtype != np.uint16 or not np_output.flags.c_contiguous:
+        raise TypeError("np_output must be a C-contiguous numpy.ndarray of dtype uint16")
+    voxels = np.ascontiguousarray(np_voxels, dtype=np.uint8)
+    kernel = np.ascontiguousarray(np_kernel, dtype=np.float32)
+    if voxels.ndim != 3 or np_output.shape != voxels.shape:
+        raise ValueError("np_voxels must be 3-D and np_output of the same shape")
+    gz = _as_int(global_shape[0], "global_shape")
+    nz, ny, nx = voxels.shape
+    _lib.check(_lib.lib().maxi_diffusion_out_of_core_ex(
+        voxels.ctypes.data, nz, ny, nx, gz, kernel.ctypes.data, kernel.shape[0], _as_int(repititions, "repititions"),
+        np_output.ctypes.data, _lib.FIELD_TYPES[field], 0, _as_int(verbose, "verbose")))
+
+
 def diffusion(*args, **kwargs):
     """Repeated separable 3-D Gaussian with re-illumination, quantised to uint16.
 

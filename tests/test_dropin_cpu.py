@@ -49,3 +49,16 @@ def test_gauss_kernel_matches_reference_construction():
     np.testing.assert_array_equal(gauss_kernel(sigma), phi / phi.sum())
     assert gauss_kernel(8).shape == (65,)
     assert gauss_kernel(32).shape == (257,)
+
+
+def test_on_disk_overload_io_errors_without_gpu(tmp_path):
+    from maxibone_b200._lib import MaxiError
+    with pytest.raises(MaxiError, match="IO"):
+        diffusion(str(tmp_path / "missing.uint8"), gauss_kernel(1), str(tmp_path / "out.uint16"),
+                  (4, 4, 4), (2, 4, 4), 1)
+    short = tmp_path / "short.uint8"
+    np.zeros(10, np.uint8).tofile(short)
+    with pytest.raises(MaxiError, match="fewer than"):
+        diffusion(str(short), gauss_kernel(1), str(tmp_path / "out.uint16"), (4, 4, 4), (2, 4, 4), 1)
+    with pytest.raises(ValueError):
+        diffusion(str(short), gauss_kernel(1), str(tmp_path / "out.uint16"), (4, 4), (2, 4, 4), 1)

@@ -56,6 +56,8 @@ typedef enum maxi_mask_format {
 #define MAXI_FLAG_MASK_FROM_FIELD 0x8    /* FP32 only: before every repetition after the first,
                                             the mask is rebuilt as `field == 1.0f` -- the
                                             semantics of the reference's on-disk variant */
+#define MAXI_FLAG_AUTOTUNE 0x10          /* batch plans: time tensor-core vs CUDA-core passes per
+                                            group and keep the faster (cached per process) */
 #define MAXI_FLAG_NEAREST_ROUNDING 0x4   /* BF16/FP16: plain round-to-nearest stores instead of
                                             error-feedback rounding along x (the default for
                                             radius >= 4, which keeps the stored rounding noise
@@ -152,6 +154,40 @@ int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int
 int maxi_diffusion_device_noalloc(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,
                                   const float *kernel, int64_t kernel_size, int64_t repititions,
                                   uint16_t *output, float *field_out, void *stream);
+
+/*
+ * Batched form (no reference counterpart: the reference diffuses one volume
+ * per call).  Many independent DEVICE volumes of uneven sizes, each with its
+ * own kernel and repetition count, run as one CUDA graph; on the tensor-core
+ * path every pass of every repetition is one persistent launch over the tiles
+ * of all volumes that share a kernel and a repetition count.
+ */
+typedef struct maxi_volume {
+    const void *mask;      /* device uint8 [nz][ny][nx], set when > 0 */
+    uint16_t *output;      /* device uint16 [nz][ny][nx], or NULL */
+    float *field_out;      /* device float [nz][ny][nx] final field, or NULL */
+    int64_t nz, ny, nx;
+    const float *kernel;   /* host float[kernel_size], odd length, radius <= 128 (copied) */
+    int64_t kernel_size;
+    int64_t repititions;   /* >= 1 */
+} maxi_volume;
+
+typedef struct maxi_batch_plan maxi_batch_plan; /* opaque */
+
+/* Allocates the workspace of all volumes, groups them, optionally autotunes
+ * (MAXI_FLAG_AUTOTUNE, timing on `stream`) and captures the repetition loop
+ * into a CUDA graph.  Field types F32, BF16, F16. */
+int maxi_batch_plan_create(const maxi_volume *volumes, int64_t n_volumes, int32_t field_type, int32_t flags,
+                           void *stream, maxi_batch_plan **plan);
+/* Launches the plan's graph on `stream` (asynchronous; may be replayed). */
+int maxi_batch_plan_run(maxi_batch_plan *plan, void *stream);
+/* Text summary of the plan's groups and tuning decisions. */
+int maxi_batch_plan_describe(const maxi_batch_plan *plan, char *buffer, int64_t buffer_bytes);
+/* Waits for the device and frees the plan. */
+int maxi_batch_plan_destroy(maxi_batch_plan *plan);
+/* create + run + synchronise + destroy. */
+int maxi_diffusion_batched(const maxi_volume *volumes, int64_t n_volumes, int32_t field_type, int32_t flags,
+                           void *stream);
 
 /*
  * Out-of-core diffusion of a HOST volume that need not fit the device.

@@ -22,6 +22,14 @@ FLAG_REFERENCE_ROUNDING = 0x1
 FLAG_NO_TENSOR_CORES = 0x2
 FLAG_NEAREST_ROUNDING = 0x4
 FLAG_MASK_FROM_FIELD = 0x8
+FLAG_AUTOTUNE = 0x10
+
+
+class MaxiVolume(ctypes.Structure):
+    """The C struct maxi_volume."""
+    _fields_ = [("mask", ctypes.c_void_p), ("output", ctypes.c_void_p), ("field_out", ctypes.c_void_p),
+                ("nz", ctypes.c_int64), ("ny", ctypes.c_int64), ("nx", ctypes.c_int64),
+                ("kernel", ctypes.c_void_p), ("kernel_size", ctypes.c_int64), ("repititions", ctypes.c_int64)]
 
 # Every symbol include/maxibone_diffusion.h declares, with (restype, argtypes).
 _i64, _i32, _p, _int = ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int
@@ -35,6 +43,11 @@ SIGNATURES = {
     "maxi_bitpack_decode": (_int, [_p, _i64, _p, _p]),
     "maxi_diffusion_device_noalloc": (_int, [_p, _i32, _i64, _i64, _i64, _p, _i64, _i64, _p, _p, _p]),
     "maxi_tensor_core_status": (_int, []),
+    "maxi_batch_plan_create": (_int, [_p, _i64, _i32, _i32, _p, ctypes.POINTER(ctypes.c_void_p)]),
+    "maxi_batch_plan_run": (_int, [_p, _p]),
+    "maxi_batch_plan_describe": (_int, [_p, ctypes.c_char_p, _i64]),
+    "maxi_batch_plan_destroy": (_int, [_p]),
+    "maxi_diffusion_batched": (_int, [_p, _i64, _i32, _i32, _p]),
     "maxi_diffusion_out_of_core": (_int, [_p, _i64, _i64, _i64, _i64, _i64, _i64, _p, _i64, _i64, _p, _int]),
     "maxi_diffusion_out_of_core_ex": (_int, [_p, _i64, _i64, _i64, _i64, _p, _i64, _i64, _p, _i32, _i32, _int]),
     "maxi_diffusion_on_disk": (_int, [ctypes.c_char_p, _p, _i64, ctypes.c_char_p, _i64, _i64, _i64, _i64, _i64,

@@ -1,0 +1,398 @@
+// Batched form: many independent volumes of uneven sizes, each with its own
+// kernel and repetition count, run as one CUDA graph.
+//
+// Plan creation sorts the volumes into groups that share a kernel and a
+// repetition count.  A group on the tensor-core path (16-bit field, radius
+// <= 32, x extent a multiple of 8 and >= 64) runs each pass of each repetition
+// as ONE persistent launch over the tiles of all its volumes (tc_batch.cu);
+// the other volumes run their own passes.  The whole repetition loop is
+// captured once into a CUDA graph and replayed by maxi_batch_plan_run(): a
+// 64-volume, 50-repetition batch is a single graph launch.
+//
+// Autotuning (MAXI_FLAG_AUTOTUNE): for each tensor-core group the plan times
+// one repetition of the group's batched tensor-core passes against the
+// per-volume CUDA-core passes and keeps the faster; decisions are cached per
+// process, keyed by the group's kernel length, field type and volume shapes,
+// and reported by maxi_batch_plan_describe().
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "host_util.h"
+#include "tc_batch.h"
+#include "unrolled.h"
+
+extern "C" int64_t maxi_diffusion_workspace_size(int64_t nz, int64_t ny, int64_t nx, int32_t field_type);
+
+namespace maxi {
+
+struct BatchVolume {
+    maxi_volume v;
+    std::vector<float> kernel;
+    int64_t ws_offset = 0;
+    int group = -1;  // tensor-core group index, or -1 for the per-volume path
+};
+
+struct TcGroup {
+    std::vector<int> members;
+    std::vector<float> kernel;
+    int64_t reps = 0;
+    tc::TcGeometry geo{};
+    tc::TcVol *d_vols = nullptr;
+    int64_t *d_prefix = nullptr;  // [3][n + 1]: z columns, y columns, x tiles
+    int64_t totals[3] = {0, 0, 0};
+    bool use_tc = true;
+    std::string note;
+};
+
+static std::mutex g_tune_mu;
+static std::map<std::string, bool> g_tune_cache;  // group signature -> tensor cores faster
+
+}  // namespace maxi
+
+struct maxi_batch_plan {
+    int device = 0;
+    int32_t field_type = 0, flags = 0;
+    std::vector<maxi::BatchVolume> vols;
+    std::vector<maxi::TcGroup> groups;
+    char *d_ws = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::string description;
+};
+
+namespace maxi {
+
+static size_t field_size(int32_t ft) { return ft == MAXI_FIELD_F32 ? 4 : 2; }
+
+template <typename S>
+static S *vol_buf(maxi_batch_plan *p, const BatchVolume &bv, int b) {
+    const int64_t n = bv.v.nz * bv.v.ny * bv.v.nx;
+    return reinterpret_cast<S *>(p->d_ws + bv.ws_offset + b * round_up((int64_t) sizeof(S) * n, 256));
+}
+static uint32_t *vol_packed(maxi_batch_plan *p, const BatchVolume &bv) {
+    const int64_t n = bv.v.nz * bv.v.ny * bv.v.nx;
+    return reinterpret_cast<uint32_t *>(p->d_ws + bv.ws_offset + 2 * round_up((int64_t) field_size(p->field_type) * n, 256));
+}
+
+// Enqueues mask packing and the rep-0 field of every member volume.
+template <typename S>
+static cudaError_t enqueue_init(maxi_batch_plan *p, const std::vector<int> &idx, cudaStream_t st) {
+    for (int i : idx) {
+        BatchVolume &bv = p->vols[i];
+        const int64_t n = bv.v.nz * bv.v.ny * bv.v.nx;
+        cudaError_t e = launch_bitpack_encode(static_cast<const uint8_t *>(bv.v.mask), n, vol_packed(p, bv), false, st);
+        if (e == cudaSuccess) e = launch_init_field<S>(vol_packed(p, bv), MAXI_MASK_BITPACKED, vol_buf<S>(p, bv, 0), n, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// The per-volume path of one volume (all repetitions).
+template <typename S>
+static cudaError_t enqueue_single(maxi_batch_plan *p, BatchVolume &bv, int32_t extra_flags, cudaStream_t st) {
+    const int64_t n = bv.v.nz * bv.v.ny * bv.v.nx;
+    cudaError_t e = launch_bitpack_encode(static_cast<const uint8_t *>(bv.v.mask), n, vol_packed(p, bv), false, st);
+    if (e != cudaSuccess) return e;
+    const Volume vol{bv.v.nz, bv.v.ny, bv.v.nx};
+    return dispatch_unrolled<S>(vol, vol_packed(p, bv), MAXI_MASK_BITPACKED, bv.kernel.data(),
+                                (int) (bv.v.kernel_size / 2), bv.v.repititions, vol_buf<S>(p, bv, 0),
+                                vol_buf<S>(p, bv, 1), bv.v.output, bv.v.field_out, p->flags | extra_flags, st);
+}
+
+// All repetitions of a tensor-core group as batched launches.
+template <typename S>
+static cudaError_t enqueue_group_tc(maxi_batch_plan *p, TcGroup &g, cudaStream_t st) {
+    cudaError_t e = enqueue_init<S>(p, g.members, st);
+    if (e != cudaSuccess) return e;
+    const bool bf16 = std::is_same<S, __nv_bfloat16>::value;
+    const bool ef = (p->flags & MAXI_FLAG_NEAREST_ROUNDING) == 0 && g.geo.radius >= 4;
+    const int n = (int) g.members.size();
+    int in = 0;
+    for (int64_t rep = 0; rep < g.reps; rep++) {
+        const bool last = rep + 1 == g.reps;
+        if ((e = tc::tc_batch_pass(g.d_vols, g.d_prefix, g.totals[0], n, 0, in, false, g.kernel.data(), g.geo, bf16, ef, st)) != cudaSuccess ||
+            (e = tc::tc_batch_pass(g.d_vols, g.d_prefix + (n + 1), g.totals[1], n, 1, in ^ 1, false, g.kernel.data(), g.geo, bf16, ef, st)) != cudaSuccess ||
+            (e = tc::tc_batch_pass(g.d_vols, g.d_prefix + 2 * (n + 1), g.totals[2], n, 2, in, last, g.kernel.data(), g.geo, bf16, ef, st)) != cudaSuccess)
+            return e;
+        in ^= 1;
+    }
+    return cudaSuccess;
+}
+
+template <typename S>
+static cudaError_t enqueue_all(maxi_batch_plan *p, cudaStream_t st) {
+    cudaError_t e = cudaSuccess;
+    for (TcGroup &g : p->groups) {
+        if (g.use_tc) e = enqueue_group_tc<S>(p, g, st);
+        else
+            for (int i : g.members)
+                if ((e = enqueue_single<S>(p, p->vols[i], MAXI_FLAG_NO_TENSOR_CORES, st)) != cudaSuccess) break;
+        if (e != cudaSuccess) return e;
+    }
+    for (BatchVolume &bv : p->vols)
+        if (bv.group < 0 && (e = enqueue_single<S>(p, bv, 0, st)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+template <typename S>
+static cudaError_t time_group(maxi_batch_plan *p, TcGroup &g, bool use_tc, cudaStream_t st, float *ms) {
+    const int64_t saved = g.reps;
+    std::vector<int64_t> saved_reps;
+    g.reps = 1;
+    for (int i : g.members) {
+        saved_reps.push_back(p->vols[i].v.repititions);
+        p->vols[i].v.repititions = 1;
+    }
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaError_t e = cudaSuccess;
+    for (int it = 0; it < 2 && e == cudaSuccess; it++) {  // first run warms up
+        cudaEventRecord(a, st);
+        if (use_tc) e = enqueue_group_tc<S>(p, g, st);
+        else
+            for (int i : g.members)
+                if ((e = enqueue_single<S>(p, p->vols[i], MAXI_FLAG_NO_TENSOR_CORES, st)) != cudaSuccess) break;
+        cudaEventRecord(b, st);
+    }
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    g.reps = saved;
+    for (size_t k = 0; k < g.members.size(); k++) p->vols[g.members[k]].v.repititions = saved_reps[k];
+    return e;
+}
+
+static std::string group_signature(const maxi_batch_plan *p, const TcGroup &g) {
+    std::string s = "f" + std::to_string(p->field_type) + ":k" + std::to_string(g.kernel.size()) + ":";
+    for (int i : g.members) {
+        const maxi_volume &v = p->vols[i].v;
+        s += std::to_string(v.nz) + "x" + std::to_string(v.ny) + "x" + std::to_string(v.nx) + ",";
+    }
+    return s;
+}
+
+template <typename S>
+static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
+    const bool tc_type = sizeof(S) == 2 && (p->flags & MAXI_FLAG_NO_TENSOR_CORES) == 0;
+    // Group tensor-core-eligible volumes by (kernel, repetitions).
+    for (size_t i = 0; i < p->vols.size(); i++) {
+        BatchVolume &bv = p->vols[i];
+        const int radius = (int) (bv.v.kernel_size / 2);
+        const bool eligible = tc_type && bv.v.repititions > 0 && tc::tc_supported(radius, bv.v.nz, bv.v.ny, bv.v.nx) &&
+                              ((reinterpret_cast<uintptr_t>(bv.v.output) | reinterpret_cast<uintptr_t>(bv.v.field_out)) & 15) == 0;
+        if (!eligible) continue;
+        int gi = -1;
+        for (size_t k = 0; k < p->groups.size(); k++)
+            if (p->groups[k].reps == bv.v.repititions && p->groups[k].kernel == bv.kernel) gi = (int) k;
+        if (gi < 0) {
+            TcGroup g;
+            g.kernel = bv.kernel;
+            g.reps = bv.v.repititions;
+            g.geo = tc::tc_geometry(radius);
+            p->groups.push_back(g);
+            gi = (int) p->groups.size() - 1;
+        }
+        p->groups[gi].members.push_back((int) i);
+        bv.group = gi;
+    }
+    // Device tables of each group.
+    for (TcGroup &g : p->groups) {
+        const int n = (int) g.members.size();
+        std::vector<tc::TcVol> vols(n);
+        std::vector<int64_t> prefix(3 * (n + 1), 0);
+        for (int k = 0; k < n; k++) {
+            BatchVolume &bv = p->vols[g.members[k]];
+            if (tc::tc_fill_volume(vols[k], vol_buf<S>(p, bv, 0), vol_buf<S>(p, bv, 1), vol_packed(p, bv), bv.v.output,
+                                   bv.v.field_out, bv.v.nz, bv.v.ny, bv.v.nx, std::is_same<S, __nv_bfloat16>::value,
+                                   g.geo) != 0)
+                return set_error(MAXI_ERR_CUDA, "could not encode the tensor maps of a batch volume");
+            prefix[k + 1] = prefix[k] + vols[k].cols_z;
+            prefix[(n + 1) + k + 1] = prefix[(n + 1) + k] + vols[k].cols_y;
+            prefix[2 * (n + 1) + k + 1] = prefix[2 * (n + 1) + k] + vols[k].tiles_x;
+        }
+        for (int q = 0; q < 3; q++) g.totals[q] = prefix[q * (n + 1) + n];
+        if (cudaMalloc(&g.d_vols, sizeof(tc::TcVol) * n) != cudaSuccess ||
+            cudaMalloc(&g.d_prefix, sizeof(int64_t) * prefix.size()) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(MAXI_ERR_OUT_OF_MEMORY, "could not allocate the batch tables");
+        }
+        if (cudaMemcpy(g.d_vols, vols.data(), sizeof(tc::TcVol) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(g.d_prefix, prefix.data(), sizeof(int64_t) * prefix.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            return set_cuda_error(cudaGetLastError(), "batch table upload");
+    }
+    // Autotune: tensor-core batch vs per-volume CUDA-core passes, per group.
+    if (p->flags & MAXI_FLAG_AUTOTUNE) {
+        for (TcGroup &g : p->groups) {
+            const std::string sig = group_signature(p, g);
+            bool known = false, tc_wins = true;
+            {
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                auto it = g_tune_cache.find(sig);
+                if (it != g_tune_cache.end()) known = true, tc_wins = it->second;
+            }
+            float t_tc = 0, t_cc = 0;
+            if (!known) {
+                cudaError_t e = time_group<S>(p, g, true, user_st, &t_tc);
+                if (e == cudaSuccess) e = time_group<S>(p, g, false, user_st, &t_cc);
+                if (e != cudaSuccess) return set_cuda_error(e, "batch autotuning");
+                tc_wins = t_tc <= t_cc;
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                g_tune_cache[sig] = tc_wins;
+            }
+            g.use_tc = tc_wins;
+            char buf[160];
+            if (known) snprintf(buf, sizeof(buf), "cached choice: %s", tc_wins ? "tensor cores" : "CUDA cores");
+            else snprintf(buf, sizeof(buf), "tuned: tensor cores %.3f ms vs CUDA cores %.3f ms per repetition -> %s",
+                          t_tc, t_cc, tc_wins ? "tensor cores" : "CUDA cores");
+            g.note = buf;
+        }
+    }
+    // Capture the whole repetition loop.
+    cudaStream_t cap;
+    if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess)
+        return set_cuda_error(cudaGetLastError(), "capture stream");
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        cudaError_t ee = enqueue_all<S>(p, cap);
+        e = cudaStreamEndCapture(cap, &p->graph);
+        if (ee != cudaSuccess) e = ee;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+    cudaStreamDestroy(cap);
+    if (e != cudaSuccess) return set_cuda_error(e, "batch graph capture");
+    // Description.
+    char line[256];
+    snprintf(line, sizeof(line), "%zu volumes, field type %d, %zu tensor-core groups\n", p->vols.size(),
+             p->field_type, p->groups.size());
+    p->description = line;
+    for (size_t k = 0; k < p->groups.size(); k++) {
+        const TcGroup &g = p->groups[k];
+        snprintf(line, sizeof(line), "group %zu: %zu volumes, kernel length %zu, %lld repetitions, %s%s%s\n", k,
+                 g.members.size(), g.kernel.size(), (long long) g.reps,
+                 g.use_tc ? "one tensor-core launch per pass" : "per-volume CUDA-core passes",
+                 g.note.empty() ? "" : "; ", g.note.c_str());
+        p->description += line;
+    }
+    size_t singles = 0;
+    for (const BatchVolume &bv : p->vols) singles += bv.group < 0;
+    snprintf(line, sizeof(line), "%zu volumes on the per-volume path\n", singles);
+    p->description += line;
+    return MAXI_OK;
+}
+
+static void destroy_plan(maxi_batch_plan *p) {
+    if (!p) return;
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    for (TcGroup &g : p->groups) {
+        cudaFree(g.d_vols);
+        cudaFree(g.d_prefix);
+    }
+    cudaFree(p->d_ws);
+    delete p;
+}
+
+}  // namespace maxi
+
+using namespace maxi;
+
+extern "C" {
+
+int maxi_batch_plan_create(const maxi_volume *volumes, int64_t n_volumes, int32_t field_type, int32_t flags,
+                           void *stream, maxi_batch_plan **plan) {
+    clear_error();
+    if (!plan) return set_error(MAXI_ERR_INVALID_ARGUMENT, "plan is NULL");
+    *plan = nullptr;
+    if (!volumes || n_volumes <= 0) return set_error(MAXI_ERR_INVALID_ARGUMENT, "no volumes");
+    if (field_type != MAXI_FIELD_F32 && field_type != MAXI_FIELD_BF16 && field_type != MAXI_FIELD_F16)
+        return set_error(MAXI_ERR_UNSUPPORTED, "batched form serves the F32, BF16 and F16 fields");
+    if (flags & (MAXI_FLAG_REFERENCE_ROUNDING | MAXI_FLAG_MASK_FROM_FIELD))
+        return set_error(MAXI_ERR_UNSUPPORTED, "reference rounding and rebuilt masks are not served in batches");
+    int rc;
+    for (int64_t i = 0; i < n_volumes; i++) {
+        const maxi_volume &v = volumes[i];
+        if ((rc = validate_common(v.mask, v.nz, v.ny, v.nx, v.kernel, v.kernel_size, v.repititions, 128))) {
+            std::string m = last_error_ref();
+            return set_error(rc, "volume %lld: %s", (long long) i, m.c_str());
+        }
+        if (!v.output && !v.field_out) return set_error(MAXI_ERR_INVALID_ARGUMENT, "volume %lld has no output", (long long) i);
+        if (v.repititions == 0) return set_error(MAXI_ERR_INVALID_ARGUMENT, "volume %lld has zero repetitions", (long long) i);
+    }
+    if ((rc = require_device())) return rc;
+    auto *p = new maxi_batch_plan();
+    cudaGetDevice(&p->device);
+    p->field_type = field_type;
+    p->flags = flags;
+    int64_t total = 0;
+    for (int64_t i = 0; i < n_volumes; i++) {
+        BatchVolume bv;
+        bv.v = volumes[i];
+        bv.kernel.assign(volumes[i].kernel, volumes[i].kernel + volumes[i].kernel_size);
+        bv.v.kernel = nullptr;  // the plan keeps its own copy
+        bv.ws_offset = total;
+        total += round_up(maxi_diffusion_workspace_size(bv.v.nz, bv.v.ny, bv.v.nx, field_type), 1024);
+        p->vols.push_back(bv);
+    }
+    if (cudaMalloc(&p->d_ws, total) != cudaSuccess) {
+        cudaGetLastError();
+        destroy_plan(p);
+        return set_error(MAXI_ERR_OUT_OF_MEMORY, "could not allocate %lld bytes of batch workspace", (long long) total);
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    switch (field_type) {
+    case MAXI_FIELD_F32: rc = build_plan<float>(p, st); break;
+    case MAXI_FIELD_BF16: rc = build_plan<__nv_bfloat16>(p, st); break;
+    default: rc = build_plan<__half>(p, st); break;
+    }
+    if (rc) {
+        destroy_plan(p);
+        return rc;
+    }
+    *plan = p;
+    return MAXI_OK;
+}
+
+int maxi_batch_plan_run(maxi_batch_plan *plan, void *stream) {
+    clear_error();
+    if (!plan || !plan->exec) return set_error(MAXI_ERR_INVALID_ARGUMENT, "plan is NULL");
+    cudaError_t e = cudaGraphLaunch(plan->exec, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? MAXI_OK : set_cuda_error(e, "batch graph launch");
+}
+
+int maxi_batch_plan_describe(const maxi_batch_plan *plan, char *buffer, int64_t buffer_bytes) {
+    clear_error();
+    if (!plan || !buffer || buffer_bytes <= 0) return set_error(MAXI_ERR_INVALID_ARGUMENT, "NULL argument");
+    snprintf(buffer, (size_t) buffer_bytes, "%s", plan->description.c_str());
+    return MAXI_OK;
+}
+
+int maxi_batch_plan_destroy(maxi_batch_plan *plan) {
+    clear_error();
+    if (plan) {
+        cudaDeviceSynchronize();
+        destroy_plan(plan);
+    }
+    return MAXI_OK;
+}
+
+int maxi_diffusion_batched(const maxi_volume *volumes, int64_t n_volumes, int32_t field_type, int32_t flags,
+                           void *stream) {
+    maxi_batch_plan *plan = nullptr;
+    int rc = maxi_batch_plan_create(volumes, n_volumes, field_type, flags, stream, &plan);
+    if (rc) return rc;
+    rc = maxi_batch_plan_run(plan, stream);
+    if (rc == MAXI_OK) {
+        cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+        if (e != cudaSuccess) rc = set_cuda_error(e, "batched diffusion");
+    }
+    maxi_batch_plan_destroy(plan);
+    return rc;
+}
+
+}  // extern "C"

@@ -16,6 +16,7 @@
 #include "unrolled.h"
 #include "profiler.h"
 #include "tc_pass.h"
+#include "tc_batch.h"
 
 namespace maxi {
 
@@ -138,7 +139,8 @@ const char *maxi_last_error(void) { return last_error_cstr(); }
 
 int maxi_tensor_core_status(void) {
     clear_error();
-    const int v = tc::tc_read_and_clear_error();
+    const int a = tc::tc_read_and_clear_error(), b = tc::tc_batch_read_and_clear_error();
+    const int v = (a < 0 || b < 0) ? -1 : (a ? a : b);
     if (v < 0) return set_error(MAXI_ERR_CUDA, "could not read the tensor-core error word");
     if (v > 0) return set_error(MAXI_ERR_CUDA, "a tensor-core pass timed out waiting (code %d)", v);
     return MAXI_OK;

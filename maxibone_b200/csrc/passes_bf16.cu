@@ -7,4 +7,6 @@ template cudaError_t dispatch_unrolled<__nv_bfloat16>(const Volume &, const void
                                            __nv_bfloat16 *, __nv_bfloat16 *, uint16_t *, float *, int32_t,
                                            cudaStream_t);
 
+template cudaError_t launch_init_field<__nv_bfloat16>(const void *, int, __nv_bfloat16 *, int64_t, cudaStream_t);
+
 }  // namespace maxi

@@ -7,4 +7,6 @@ template cudaError_t dispatch_unrolled<__half>(const Volume &, const void *, int
                                            __half *, __half *, uint16_t *, float *, int32_t,
                                            cudaStream_t);
 
+template cudaError_t launch_init_field<__half>(const void *, int, __half *, int64_t, cudaStream_t);
+
 }  // namespace maxi

@@ -9,4 +9,6 @@ template cudaError_t dispatch_unrolled<float>(const Volume &, const void *, int,
                                            float *, float *, uint16_t *, float *, int32_t,
                                            cudaStream_t);
 
+template cudaError_t launch_init_field<float>(const void *, int, float *, int64_t, cudaStream_t);
+
 }  // namespace maxi

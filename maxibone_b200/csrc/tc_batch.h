@@ -1,0 +1,50 @@
+// Host interface of the multi-volume tensor-core passes (tc_batch.cu).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <stdint.h>
+
+#include "tc_pass.h"
+
+namespace maxi {
+namespace tc {
+
+// Device-table entry of one volume: tensor maps of the pass inputs
+// ([pass z/y/x][buffer]), the two ping-pong field buffers, the bit-packed
+// mask, the final outputs and the tile counts.
+struct alignas(64) TcVol {
+    CUtensorMap map[3][2];
+    void *buf[2];
+    const uint32_t *mask;
+    uint16_t *out_u16;
+    float *field_out;
+    int64_t nz, ny, nx;
+    int n_at_z, n_at_y, n_xc, n_xt;
+    int64_t cols_z, cols_y, tiles_x;
+};
+
+// K extents of the strided (z/y) and contiguous (x) tensor-core passes.
+struct TcGeometry {
+    int radius, kp_strided, kpa_strided, ra, kp_contig, kpa_contig;
+};
+
+TcGeometry tc_geometry(int radius);
+PFN_cuTensorMapEncodeTiled_v12000 tc_encode_fn();
+// Splits float taps (times `scale`) into high and low 16-bit halves.
+void tc_split_taps(const float *kernel, int radius, bool is_bf16, float scale, uint16_t *hi, uint16_t *lo);
+
+int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_mask, uint16_t *out_u16,
+                   float *field_out, int64_t nz, int64_t ny, int64_t nx, bool is_bf16, const TcGeometry &g);
+
+// One pass (0 z, 1 y, 2 x) over all volumes of a device table; d_prefix holds
+// n_vol + 1 prefix sums of the volumes' columns (z: cols_z, y: cols_y) or x tiles.
+cudaError_t tc_batch_pass(const TcVol *d_vols, const int64_t *d_prefix, int64_t total, int n_vol, int pass, int in_buf,
+                          bool final_pass, const float *kernel, const TcGeometry &g, bool is_bf16, bool error_feedback,
+                          cudaStream_t st);
+
+int tc_batch_read_and_clear_error();
+
+}  // namespace tc
+}  // namespace maxi

@@ -160,5 +160,44 @@ __device__ __forceinline__ uint32_t sw128_kmajor_offset(int row, int k, int rows
     return kb * rows * 128 + (row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4) + within;
 }
 
+// Rounds to the 16-bit storage type; with `ef` the rounding error is carried
+// into the next value of the chain (error feedback).
+template <typename S> struct Narrow16;
+template <> struct Narrow16<__nv_bfloat16> {
+    static __device__ __forceinline__ uint16_t bits(float v, float &carry, bool ef) {
+        const float w = ef ? v + carry : v;
+        const __nv_bfloat16 q = __float2bfloat16_rn(w);
+        if (ef) carry = w - __bfloat162float(q);
+        return __bfloat16_as_ushort(q);
+    }
+};
+template <> struct Narrow16<__half> {
+    static __device__ __forceinline__ uint16_t bits(float v, float &carry, bool ef) {
+        const float w = ef ? v + carry : v;
+        const __half q = __float2half_rn(w);
+        if (ef) carry = w - __half2float(q);
+        return __half_as_ushort(q);
+    }
+};
+
+// Mask flags of up to 32 voxels of a row (bit q = voxel idx + q), with a
+// 2 x 16-byte vector read for aligned full uint8 chunks.
+template <int FMT>
+__device__ __forceinline__ uint32_t row_mask32(const void *m, int64_t idx, int count, int64_t n) {
+    if (FMT == MAXI_MASK_U8 && count == 32 && ((reinterpret_cast<uintptr_t>(m) + idx) & 15) == 0) {
+        const uint4 *p = reinterpret_cast<const uint4 *>(static_cast<const uint8_t *>(m) + idx);
+        const uint4 a = __ldg(p), b = __ldg(p + 1);
+        const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        uint32_t r = 0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+#pragma unroll
+            for (int by = 0; by < 4; by++) r |= (uint32_t) (((w[q] >> (8 * by)) & 0xffu) != 0u) << (q * 4 + by);
+        }
+        return r;
+    }
+    return mask32<FMT>(m, idx, count, n);
+}
+
 }  // namespace tc
 }  // namespace maxi

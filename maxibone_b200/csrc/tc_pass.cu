@@ -30,6 +30,7 @@
 #include "profiler.h"
 #include "tc_common.cuh"
 #include "tc_pass.h"
+#include "tc_batch.h"
 
 namespace maxi {
 namespace tc {
@@ -67,24 +68,6 @@ __host__ __device__ constexpr int strided_smem_bytes(int kp, int kpa) {
     return 1024 /*alignment slack*/ + 2 * kpa * kTM * 2 /*T_hi, T_lo*/ + kStages * (kTN / 64) * kp * 128 /*B ring*/ +
            256 /*barriers, TMEM slot*/ + kEpiWarps * kStageWarpBytes;
 }
-
-template <typename S> struct Narrow16;
-template <> struct Narrow16<__nv_bfloat16> {
-    static __device__ __forceinline__ uint16_t bits(float v, float &carry, bool ef) {
-        const float w = ef ? v + carry : v;
-        const __nv_bfloat16 q = __float2bfloat16_rn(w);
-        if (ef) carry = w - __bfloat162float(q);
-        return __bfloat16_as_ushort(q);
-    }
-};
-template <> struct Narrow16<__half> {
-    static __device__ __forceinline__ uint16_t bits(float v, float &carry, bool ef) {
-        const float w = ef ? v + carry : v;
-        const __half q = __float2half_rn(w);
-        if (ef) carry = w - __half2float(q);
-        return __half_as_ushort(q);
-    }
-};
 
 template <typename S>
 __global__ void __launch_bounds__(kThreads, 1)
@@ -296,23 +279,6 @@ __host__ __device__ constexpr int contig_smem_bytes_tc(int kp, int kpa) {
     return 1024 + kpa * 2 * kXTN * 2 /*Tt_hi|Tt_lo, 256 rows*/ + kStages * (kpa / 64) * kTM * 128 /*A ring*/ + 256;
 }
 
-template <int FMT>
-__device__ __forceinline__ uint32_t row_mask32(const void *m, int64_t idx, int count, int64_t n) {
-    if (FMT == MAXI_MASK_U8 && count == 32 && ((reinterpret_cast<uintptr_t>(m) + idx) & 15) == 0) {
-        const uint4 *p = reinterpret_cast<const uint4 *>(static_cast<const uint8_t *>(m) + idx);
-        const uint4 a = __ldg(p), b = __ldg(p + 1);
-        const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-        uint32_t r = 0;
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-#pragma unroll
-            for (int by = 0; by < 4; by++) r |= (uint32_t) (((w[q] >> (8 * by)) & 0xffu) != 0u) << (q * 4 + by);
-        }
-        return r;
-    }
-    return mask32<FMT>(m, idx, count, n);
-}
-
 template <typename S, int FMT>
 __global__ void __launch_bounds__(kXThreads, 1)
 tc_contig_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ ContigParams p) {
@@ -506,7 +472,7 @@ tc_contig_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__
 
 // ---- host side -----------------------------------------------------------------
 
-static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+PFN_cuTensorMapEncodeTiled_v12000 tc_encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;
     std::call_once(once, [] {
@@ -527,7 +493,6 @@ static float from_bf16(uint16_t b) { return __bfloat162float(__ushort_as_bfloat1
 static uint16_t bits_f16(float v) { return __half_as_ushort(__float2half_rn(v)); }
 static float from_f16(uint16_t b) { return __half2float(__ushort_as_half(b)); }
 
-static void split_taps(const float *kernel, int radius, bool is_bf16, float scale, uint16_t *hi, uint16_t *lo);
 
 bool tc_supported(int radius, int64_t nz, int64_t ny, int64_t nx) {
     if (radius < 1 || radius > kTcMaxRadius) return false;
@@ -538,7 +503,7 @@ bool tc_supported(int radius, int64_t nz, int64_t ny, int64_t nx) {
         cudaGetLastError();
         return false;
     }
-    return major == 10 && encode_fn() != nullptr;
+    return major == 10 && tc_encode_fn() != nullptr;
 }
 
 template <typename S>
@@ -555,7 +520,7 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
     p.error_feedback = error_feedback ? 1 : 0;
     const float scale = is_bf16 ? 1.0f : 1024.0f;
     p.inv_scale = 1.0f / scale;
-    split_taps(kernel, radius, is_bf16, scale, p.hi, p.lo);
+    tc_split_taps(kernel, radius, is_bf16, scale, p.hi, p.lo);
     if (axis_z) { p.A = nz; p.n_other = ny; p.stride_a = ny * nx; p.stride_o = nx; }
     else { p.A = ny; p.n_other = nz; p.stride_a = nx; p.stride_o = ny * nx; }
     p.n_at = (int) ceil_div(p.A, kTM);
@@ -567,7 +532,7 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
     const cuuint64_t strides[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (nx * ny * 2)};
     const cuuint32_t box[3] = {64u, axis_z ? 1u : (cuuint32_t) p.kp, axis_z ? (cuuint32_t) p.kp : 1u};
     const cuuint32_t estr[3] = {1, 1, 1};
-    CUresult cr = encode_fn()(&map, is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
+    CUresult cr = tc_encode_fn()(&map, is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
                               const_cast<S *>(in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -589,7 +554,7 @@ template cudaError_t tc_strided<__nv_bfloat16>(const __nv_bfloat16 *, __nv_bfloa
 template cudaError_t tc_strided<__half>(const __half *, __half *, int64_t, int64_t, int64_t, bool, const float *, int,
                                         bool, cudaStream_t);
 
-static void split_taps(const float *kernel, int radius, bool is_bf16, float scale, uint16_t *hi, uint16_t *lo) {
+void tc_split_taps(const float *kernel, int radius, bool is_bf16, float scale, uint16_t *hi, uint16_t *lo) {
     for (int i = 0; i < 2 * radius + 1; i++) {
         const float k = kernel[i] * scale;
         if (is_bf16) {
@@ -623,7 +588,7 @@ cudaError_t tc_contig(const S *in, S *out, const void *mask, int mask_fmt, bool 
     p.error_feedback = error_feedback ? 1 : 0;
     const float scale = is_bf16 ? 1.0f : 1024.0f;
     p.inv_scale = 1.0f / scale;
-    split_taps(kernel, radius, is_bf16, scale, p.hi, p.lo);
+    tc_split_taps(kernel, radius, is_bf16, scale, p.hi, p.lo);
     p.n_xt = (int) ceil_div(nx, kXTN);
     p.n_tiles = (int64_t) p.n_xt * ceil_div(p.rows, kTM);
 
@@ -632,7 +597,7 @@ cudaError_t tc_contig(const S *in, S *out, const void *mask, int mask_fmt, bool 
     const cuuint64_t strides[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (nx * p.rows * 2)};
     const cuuint32_t box[3] = {64u, (cuuint32_t) kTM, 1u};
     const cuuint32_t estr[3] = {1, 1, 1};
-    CUresult cr = encode_fn()(&map, is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
+    CUresult cr = tc_encode_fn()(&map, is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
                               const_cast<S *>(in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);

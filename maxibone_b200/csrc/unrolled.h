@@ -16,6 +16,10 @@ struct Volume {
 // the reference encode's `mask & 1`; otherwise the diffusion's `mask > 0`.
 cudaError_t launch_bitpack_encode(const uint8_t *mask, int64_t n, uint32_t *packed, bool keep_bit0, cudaStream_t st);
 
+// field <- mask > 0 ? 1 : 0 in the storage type (rep-0 input).
+template <typename S>
+cudaError_t launch_init_field(const void *mask, int mask_fmt, S *field, int64_t n, cudaStream_t st);
+
 // Smallest radius with an unrolled instantiation that is >= r, or -1.
 int radius_bucket(int r);
 

@@ -121,6 +121,16 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
     return cudaGetLastError();
 }
 
+template <typename S>
+cudaError_t launch_init_field(const void *mask, int mask_fmt, S *field, int64_t n, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148 * 64);
+    if (mask_fmt == MAXI_MASK_U8)
+        mask_to_field<S, MAXI_MASK_U8, false><<<blocks, 256, 0, st>>>(mask, field, nullptr, nullptr, n);
+    else
+        mask_to_field<S, MAXI_MASK_BITPACKED, false><<<blocks, 256, 0, st>>>(mask, field, nullptr, nullptr, n);
+    return cudaGetLastError();
+}
+
 template <typename S, bool EF>
 static cudaError_t dispatch_radius(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
                                    int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, bool use_tc,

@@ -125,3 +125,62 @@ def profile_read() -> dict:
 def tensor_core_status() -> None:
     """Raise if a tensor-core pass gave up on a bounded wait since the last check."""
     _lib.check(_lib.lib().maxi_tensor_core_status())
+
+
+class BatchPlan:
+    """Many device volumes, each with its own kernel and repetition count, run
+    as one CUDA graph (see maxi_batch_plan_create).  Build once, run many times.
+
+    masks / outputs: lists of uint8 / uint16 CUDA tensors; field_outs: optional
+    list of float32 tensors (or None entries); kernels: one 1-D array per volume
+    (or one for all); reps: an int or one per volume."""
+
+    def __init__(self, masks, kernels, reps, outputs=None, field="bf16", field_outs=None, autotune=False,
+                 tensor_cores=True, error_feedback=True, stream=None):
+        import ctypes
+        n = len(masks)
+        if not isinstance(kernels, (list, tuple)):
+            kernels = [kernels] * n
+        if isinstance(reps, int):
+            reps = [reps] * n
+        outputs = outputs if outputs is not None else [None] * n
+        field_outs = field_outs if field_outs is not None else [None] * n
+        self._keep = [np.ascontiguousarray(k, dtype=np.float32) for k in kernels]
+        self._tensors = (list(masks), list(outputs), list(field_outs))
+        arr = (_lib.MaxiVolume * n)()
+        for i in range(n):
+            m, o, f = masks[i], outputs[i], field_outs[i]
+            if m.dtype != torch.uint8 or not m.is_cuda or not m.is_contiguous() or m.dim() != 3:
+                raise ValueError("masks must be contiguous 3-D uint8 CUDA tensors")
+            for t, dt in ((o, torch.uint16), (f, torch.float32)):
+                if t is not None and (t.dtype != dt or not t.is_cuda or not t.is_contiguous() or t.shape != m.shape):
+                    raise ValueError(f"outputs must be contiguous {dt} CUDA tensors shaped like their masks")
+            nz, ny, nx = m.shape
+            k = self._keep[i]
+            arr[i] = _lib.MaxiVolume(m.data_ptr(), o.data_ptr() if o is not None else None,
+                                     f.data_ptr() if f is not None else None, nz, ny, nx, k.ctypes.data, k.shape[0],
+                                     int(reps[i]))
+        flags = (_lib.FLAG_AUTOTUNE if autotune else 0) | (0 if tensor_cores else _lib.FLAG_NO_TENSOR_CORES) | \
+            (0 if error_feedback else _lib.FLAG_NEAREST_ROUNDING)
+        st = stream if stream is not None else torch.cuda.current_stream()
+        self._plan = ctypes.c_void_p()
+        _lib.check(_lib.lib().maxi_batch_plan_create(ctypes.addressof(arr), n, _lib.FIELD_TYPES[field], flags,
+                                                     st.cuda_stream, ctypes.byref(self._plan)))
+
+    def run(self, stream=None):
+        st = stream if stream is not None else torch.cuda.current_stream()
+        _lib.check(_lib.lib().maxi_batch_plan_run(self._plan, st.cuda_stream))
+
+    def describe(self) -> str:
+        import ctypes
+        buf = ctypes.create_string_buffer(1 << 14)
+        _lib.check(_lib.lib().maxi_batch_plan_describe(self._plan, buf, len(buf)))
+        return buf.value.decode()
+
+    def close(self):
+        if getattr(self, "_plan", None) and self._plan.value:
+            _lib.lib().maxi_batch_plan_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        self.close()

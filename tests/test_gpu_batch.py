@@ -1,0 +1,90 @@
+"""Batched form: many uneven device volumes in one CUDA graph (run with -m gpu).
+
+The batched tensor-core launches do the same arithmetic per tile as the
+single-volume passes, so every volume must equal its own single-volume run
+exactly; FP32 batches take the per-volume CUDA-core path and must match too."""
+import numpy as np
+import pytest
+import torch
+
+from maxibone_b200 import device, gauss_kernel
+from maxibone_b200.synthetic import spheres_mask
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(96, 128, 192), (128, 96, 128), (64, 64, 64), (40, 72, 136), (33, 50, 60), (20, 30, 44), (130, 64, 256)]
+SIGMAS = [2.0, 4.0, 2.0, 8.0, 2.0, 4.0, 8.0]
+REPS = [3, 3, 3, 2, 3, 3, 2]
+
+
+def make_batch(field):
+    masks, outs, fouts, kernels = [], [], [], []
+    for i, shape in enumerate(SHAPES):
+        m = spheres_mask(shape, 8, (3, 9), seed=100 + i)
+        masks.append(torch.from_numpy(m).cuda())
+        outs.append(torch.empty(shape, dtype=torch.uint16, device="cuda"))
+        fouts.append(torch.empty(shape, dtype=torch.float32, device="cuda"))
+        kernels.append(gauss_kernel(SIGMAS[i]).astype(np.float32))
+    return masks, outs, fouts, kernels
+
+
+def single(mask, kernel, reps, field):
+    out = torch.empty(mask.shape, dtype=torch.uint16, device="cuda")
+    fo = torch.empty(mask.shape, dtype=torch.float32, device="cuda")
+    device.diffuse(mask, kernel, reps, output=out, field=field, field_out=fo)
+    return out, fo
+
+
+@pytest.mark.parametrize("field", ["bf16", "f16", "f32"])
+def test_batch_equals_single_volume_runs(field):
+    masks, outs, fouts, kernels = make_batch(field)
+    plan = device.BatchPlan(masks, kernels, REPS, outputs=outs, field=field, field_outs=fouts)
+    text = plan.describe()
+    plan.run()
+    torch.cuda.synchronize()
+    device.tensor_core_status()
+    for i in range(len(SHAPES)):
+        o, f = single(masks[i], kernels[i], REPS[i], field)
+        torch.cuda.synchronize()
+        assert torch.equal(outs[i], o), (i, text)
+        assert torch.equal(fouts[i], f), (i, text)
+    if field != "f32":
+        assert "one tensor-core launch per pass" in text
+    plan.close()
+
+
+def test_batch_plan_replays():
+    masks, outs, fouts, kernels = make_batch("bf16")
+    plan = device.BatchPlan(masks, kernels, REPS, outputs=outs, field="bf16", field_outs=fouts)
+    plan.run()
+    torch.cuda.synchronize()
+    first = [f.clone() for f in fouts]
+    for f in fouts:
+        f.zero_()
+    plan.run()
+    torch.cuda.synchronize()
+    for a, b in zip(first, fouts):
+        assert torch.equal(a, b)
+    plan.close()
+
+
+def test_batch_autotune_reports_and_stays_accurate():
+    masks, outs, fouts, kernels = make_batch("f16")
+    plan = device.BatchPlan(masks, kernels, REPS, outputs=outs, field="f16", field_outs=fouts, autotune=True)
+    text = plan.describe()
+    assert "tuned" in text or "cached" in text
+    plan.run()
+    torch.cuda.synchronize()
+    for i in range(len(SHAPES)):
+        want = torch.empty(SHAPES[i], dtype=torch.float64, device="cuda")
+        device.diffuse(masks[i], kernels[i], REPS[i], field="f64", field_out=want)
+        assert (fouts[i].double() - want).abs().max().item() < 1e-3
+    plan.close()
+
+
+def test_batch_rejects_bad_volumes():
+    m = torch.zeros((4, 4, 4), dtype=torch.uint8, device="cuda")
+    with pytest.raises(ValueError):
+        device.BatchPlan([m], [np.ones(4, np.float32)], 1, outputs=[torch.empty((4, 4, 4), dtype=torch.uint16, device="cuda")])
+    with pytest.raises(ValueError):
+        device.BatchPlan([m], [gauss_kernel(1)], 1, outputs=None)

@@ -60,6 +60,8 @@ def parse_args():
     p.add_argument("--workload", choices=sorted(WORKLOADS), default="bone1024_s8_r100")
     p.add_argument("--field", choices=["f32", "bf16", "f16"], default="f32")
     p.add_argument("--quick", action="store_true", help="skip e2e, precision forms and CPU baseline")
+    p.add_argument("--extended", action="store_true",
+                   help="also run the out-of-core workload, R=500 errors and the sigma=32 case")
     p.add_argument("--shape", type=str, default=None,
                    help="override the workload's volume shape, e.g. 256x1024x1024 (profiling of smaller cases)")
     return p.parse_args()
@@ -170,6 +172,133 @@ def run_reference_arm(args, rank):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def batched_section(device, torch, np, stream, reps=50):
+    """64 uneven volumes, sigma in {2, 4, 8}, R = 50: one BF16 batch plan (one CUDA
+    graph, one tensor-core launch per pass per group) vs per-volume FP32 launches."""
+    from maxibone_b200.kernels import gauss_kernel
+    from maxibone_b200.synthetic import batch_shapes, spheres_mask_torch
+
+    specs = batch_shapes(64, seed=0)
+    masks = [spheres_mask_torch(sh, fg, seed=i) for i, (sh, _, fg) in enumerate(specs)]
+    kernels = [gauss_kernel(sig).astype(np.float32) for _, sig, _ in specs]
+    outs = [torch.empty(sh, dtype=torch.uint16, device="cuda") for sh, _, _ in specs]
+    fouts = [torch.empty(sh, dtype=torch.float32, device="cuda") for sh, _, _ in specs]
+    vox = sum(int(np.prod(sh)) for sh, _, _ in specs)
+    res = {"workload": "64 volumes, dims per axis from {96,128,192,256,384,512}, sigma from {2,4,8}, "
+                       f"5-30% foreground spheres, R={reps}", "voxels": vox}
+    plan = device.BatchPlan(masks, kernels, reps, outputs=outs, field="bf16", field_outs=fouts, autotune=True)
+    res["plan"] = plan.describe()
+    plan.run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_t = 3
+    e0.record(stream)
+    for _ in range(n_t):
+        plan.run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    device.tensor_core_status()
+    t_bf16 = e0.elapsed_time(e1) / n_t
+    res["bf16_batch"] = {"value": vox * reps / (t_bf16 / 1e3) / 1e9, "unit": UNIT, "ms": t_bf16}
+    # Accuracy of a few volumes against the FP64 form.
+    errs = []
+    for i in range(0, 64, 16):
+        want = torch.empty(specs[i][0], dtype=torch.float64, device="cuda")
+        device.diffuse(masks[i], kernels[i], reps, field="f64", field_out=want)
+        errs.append(float((fouts[i].double() - want).abs().max().item()))
+        del want
+    res["bf16_batch"]["max_abs_err_vs_f64_sampled"] = max(errs)
+    plan.close()
+    # Per-volume FP32 launches (the plain form, one call per volume).
+    ws = torch.empty(max(device.workspace_bytes(sh, "f32") for sh, _, _ in specs), dtype=torch.uint8, device="cuda")
+    for i in range(2):
+        device.diffuse(masks[i], kernels[i], reps, output=outs[i], field="f32", workspace=ws)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(64):
+        device.diffuse(masks[i], kernels[i], reps, output=outs[i], field="f32", workspace=ws)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_f32 = e0.elapsed_time(e1)
+    res["f32_per_volume"] = {"value": vox * reps / (t_f32 / 1e3) / 1e9, "unit": UNIT, "ms": t_f32}
+    res["speedup_bf16_batch_vs_f32_per_volume"] = t_f32 / t_bf16
+    del masks, outs, fouts, ws
+    torch.cuda.empty_cache()
+    return res
+
+
+def out_of_core_section(torch, np, reps=20, shape=(4096, 1728, 2048), slab=256):
+    """Out-of-core z-slabs streamed from pinned host memory: sigma 8, R = 20, BF16
+    field, slabs of 256 planes with 640-plane halos.  The plane is a quarter of the
+    3456 x 4096 plane of the full-size case so host and device memory stay bounded."""
+    from maxibone_b200.diffusion import diffusion_out_of_core
+    from maxibone_b200.kernels import gauss_kernel
+    from maxibone_b200.synthetic import bone_implant_mask
+
+    kernel = gauss_kernel(8.0).astype(np.float32)
+    host_m = torch.empty(shape, dtype=torch.uint8, pin_memory=True)
+    for z0 in range(0, shape[0], 512):  # generate on the GPU in chunks
+        z1 = min(shape[0], z0 + 512)
+        host_m[z0:z1].copy_(bone_implant_mask((z1 - z0, shape[1], shape[2]), seed=z0, implant_radius=60.0,
+                                              device="cuda"))
+    host_o = torch.empty(shape, dtype=torch.int16, pin_memory=True)
+    vox = int(np.prod(shape))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    diffusion_out_of_core(host_m.numpy(), kernel, host_o.numpy().view(np.uint16), (slab, shape[1], shape[2]), reps,
+                          field="bf16")
+    dt = time.perf_counter() - t0
+    halo = reps * (kernel.shape[0] // 2)
+    res = {"workload": f"{shape[0]}x{shape[1]}x{shape[2]} bone-implant mask in pinned host memory, sigma 8, R={reps}, "
+                       f"BF16 field, slabs of {slab} planes + {halo}-plane halos", "voxels": vox,
+           "value": vox * reps / dt / 1e9, "unit": UNIT, "seconds": dt,
+           "h2d_bytes": None, "d2h_bytes": 2 * vox,
+           "timing": "host clock around the synchronous out-of-core call (uploads, compute, downloads)"}
+    n_slabs = -(-shape[0] // slab)
+    ext = sum(min(shape[0], (s + 1) * slab + halo) - max(0, s * slab - halo) for s in range(n_slabs))
+    res["h2d_bytes"] = ext * shape[1] * shape[2]
+    res["redundancy"] = ext / shape[0]
+    del host_m, host_o
+    return res
+
+
+def long_section(device, torch, np, mask, shape, stream):
+    """R = 500 error growth of the 16-bit forms and the sigma = 32 (257 taps) case."""
+    from maxibone_b200.kernels import gauss_kernel
+
+    res = {}
+    k8 = gauss_kernel(8.0).astype(np.float32)
+    f64 = torch.empty(shape, dtype=torch.float64, device="cuda")
+    device.diffuse(mask, k8, 500, field="f64", field_out=f64)
+    for form in ("bf16", "f16"):
+        fo = torch.empty(shape, dtype=torch.float32, device="cuda")
+        t0 = time.perf_counter()
+        device.diffuse(mask, k8, 500, field=form, field_out=fo)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        err = (fo.double() - f64).abs_()
+        res[f"{form}_r500"] = {"value": int(np.prod(shape)) * 500 / dt / 1e9, "unit": UNIT,
+                               "max_abs_err_vs_f64": float(err.max().item()),
+                               "mean_abs_err_vs_f64": float(err.mean().item())}
+        del fo, err
+    del f64
+    torch.cuda.empty_cache()
+    k32 = gauss_kernel(32.0).astype(np.float32)
+    for form in ("f32", "bf16"):
+        fo = torch.empty(shape, dtype=torch.float32, device="cuda")
+        device.diffuse(mask, k32, 2, field=form, field_out=fo)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        device.diffuse(mask, k32, 10, field=form, field_out=fo)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        res[f"sigma32_{form}"] = {"value": int(np.prod(shape)) * 10 / dt / 1e9, "unit": UNIT, "reps": 10,
+                                  "note": "radius 128: CUDA-core passes (the tensor-core passes serve radius <= 32)"}
+        del fo
+    torch.cuda.empty_cache()
+    return res
 
 
 def main():
@@ -340,6 +469,12 @@ def main():
             torch.cuda.empty_cache()
         line["precision"] = forms
         del f64
+
+        line["batched"] = batched_section(device, torch, np, stream)
+
+        if args.extended:
+            line["out_of_core"] = out_of_core_section(torch, np)
+            line["long"] = long_section(device, torch, np, mask, shape, stream)
 
         if rank == 0 and world == 1:
             cshape, csig, creps = CPU_SAMPLE

@@ -10,7 +10,7 @@
 // 64-volume, 50-repetition batch is a single graph launch.
 //
 // Autotuning (MAXI_FLAG_AUTOTUNE): for each tensor-core group the plan times
-// one repetition of the group's batched tensor-core passes against the
+// three repetitions of the group's batched tensor-core passes against the
 // per-volume CUDA-core passes and keeps the faster; decisions are cached per
 // process, keyed by the group's kernel length, field type and volume shapes,
 // and reported by maxi_batch_plan_describe().
@@ -140,12 +140,14 @@ static cudaError_t enqueue_all(maxi_batch_plan *p, cudaStream_t st) {
 
 template <typename S>
 static cudaError_t time_group(maxi_batch_plan *p, TcGroup &g, bool use_tc, cudaStream_t st, float *ms) {
+    // Three repetitions so the one-off mask packing and field set-up of both
+    // candidates do not dominate the comparison.
     const int64_t saved = g.reps;
     std::vector<int64_t> saved_reps;
-    g.reps = 1;
+    g.reps = 3;
     for (int i : g.members) {
         saved_reps.push_back(p->vols[i].v.repititions);
-        p->vols[i].v.repititions = 1;
+        p->vols[i].v.repititions = 3;
     }
     cudaEvent_t a, b;
     cudaEventCreate(&a);
@@ -248,7 +250,7 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
             g.use_tc = tc_wins;
             char buf[160];
             if (known) snprintf(buf, sizeof(buf), "cached choice: %s", tc_wins ? "tensor cores" : "CUDA cores");
-            else snprintf(buf, sizeof(buf), "tuned: tensor cores %.3f ms vs CUDA cores %.3f ms per repetition -> %s",
+            else snprintf(buf, sizeof(buf), "tuned: tensor cores %.3f ms vs CUDA cores %.3f ms for 3 repetitions -> %s",
                           t_tc, t_cc, tc_wins ? "tensor cores" : "CUDA cores");
             g.note = buf;
         }

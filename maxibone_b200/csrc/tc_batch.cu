@@ -340,11 +340,30 @@ __global__ void __launch_bounds__(kThreads, 1) tc_batch_contig(const __grid_cons
                         fv[i] = ((m >> i) & 1u) ? 1.0f : h[i] * p.inv_scale;
                         q[i] = quantise_u16(fv[i]);
                     }
+                    if (count == 32) {  // idx % 32 == 0 and 16-byte aligned outputs: vector stores
+                        if (vol.out_u16) {
 #pragma unroll
-                    for (int i = 0; i < 32; i++) {
-                        if (i < count) {
-                            if (vol.out_u16) vol.out_u16[idx + i] = q[i];
-                            if (vol.field_out) vol.field_out[idx + i] = fv[i];
+                            for (int i = 0; i < 32; i += 8) {
+                                uint4 u;
+                                u.x = q[i] | ((uint32_t) q[i + 1] << 16);
+                                u.y = q[i + 2] | ((uint32_t) q[i + 3] << 16);
+                                u.z = q[i + 4] | ((uint32_t) q[i + 5] << 16);
+                                u.w = q[i + 6] | ((uint32_t) q[i + 7] << 16);
+                                *reinterpret_cast<uint4 *>(vol.out_u16 + idx + i) = u;
+                            }
+                        }
+                        if (vol.field_out) {
+#pragma unroll
+                            for (int i = 0; i < 32; i += 4)
+                                *reinterpret_cast<float4 *>(vol.field_out + idx + i) = make_float4(fv[i], fv[i + 1], fv[i + 2], fv[i + 3]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 32; i++) {
+                            if (i < count) {
+                                if (vol.out_u16) vol.out_u16[idx + i] = q[i];
+                                if (vol.field_out) vol.field_out[idx + i] = fv[i];
+                            }
                         }
                     }
                 } else {

@@ -178,9 +178,10 @@ class BatchPlan:
         return buf.value.decode()
 
     def close(self):
-        if getattr(self, "_plan", None) and self._plan.value:
-            _lib.lib().maxi_batch_plan_destroy(self._plan)
-            self._plan = None
+        plan = getattr(self, "_plan", None)
+        if plan is not None and plan.value and _lib is not None:
+            _lib.lib().maxi_batch_plan_destroy(plan)
+        self._plan = None
 
     def __del__(self):
         self.close()

@@ -72,3 +72,49 @@ def bone_implant_mask(shape, seed: int = 0, foreground: float = 0.25, implant_ra
     del dist
     mask |= cyl[None, :, :]
     return mask.to(torch.uint8)
+
+
+def spheres_mask_torch(shape, foreground: float, seed: int = 0, device="cuda", r_frac=(0.04, 0.12)):
+    """uint8 torch tensor: random spheres (radius r_frac x the smallest extent)
+    placed until the expected covered fraction reaches `foreground`."""
+    import math
+
+    import torch
+
+    nz, ny, nx = shape
+    g = np.random.default_rng(seed)
+    vol = nz * ny * nx
+    rmin, rmax = (f * min(shape) for f in r_frac)
+    mean_v = 4.0 / 3.0 * math.pi * ((rmin + rmax) / 2) ** 3
+    count = max(1, int(-math.log(max(1e-6, 1.0 - foreground)) * vol / mean_v))
+    if count > 200:  # fewer, larger spheres with the same expected coverage
+        scale = (count / 200) ** (1.0 / 3.0)
+        rmin, rmax, count = rmin * scale, rmax * scale, 200
+    mask = torch.zeros(shape, dtype=torch.bool, device=device)
+    zz = torch.arange(nz, device=device, dtype=torch.float32)
+    yy = torch.arange(ny, device=device, dtype=torch.float32)
+    xx = torch.arange(nx, device=device, dtype=torch.float32)
+    for _ in range(count):
+        cz, cy, cx = g.uniform(0, nz), g.uniform(0, ny), g.uniform(0, nx)
+        r = g.uniform(rmin, rmax)
+        z0, z1 = max(0, int(cz - r)), min(nz, int(cz + r) + 1)
+        y0, y1 = max(0, int(cy - r)), min(ny, int(cy + r) + 1)
+        x0, x1 = max(0, int(cx - r)), min(nx, int(cx + r) + 1)
+        if z0 >= z1 or y0 >= y1 or x0 >= x1:
+            continue
+        d = ((zz[z0:z1, None, None] - cz) ** 2 + (yy[None, y0:y1, None] - cy) ** 2 +
+             (xx[None, None, x0:x1] - cx) ** 2)
+        mask[z0:z1, y0:y1, x0:x1] |= d <= r * r
+    return mask.to(torch.uint8)
+
+
+def batch_shapes(n: int = 64, seed: int = 0):
+    """Per-axis dims drawn from {96, 128, 192, 256, 384, 512}, sigma from {2, 4, 8},
+    foreground from U(5%, 30%): the batched workload's volumes."""
+    g = np.random.default_rng(seed)
+    dims = [96, 128, 192, 256, 384, 512]
+    out = []
+    for _ in range(n):
+        shape = tuple(int(v) for v in g.choice(dims, size=3))
+        out.append((shape, float(g.choice([2.0, 4.0, 8.0])), float(g.uniform(0.05, 0.30))))
+    return out

@@ -165,24 +165,17 @@ __global__ void __launch_bounds__(kThreads, 1) tc_batch_strided(const __grid_con
                 tc_fence_after();
                 const int64_t a = (int64_t) at * kTM + o;
                 const int64_t x0 = (int64_t) xc * kTN;
-                float carry = 0.0f;
-#pragma unroll 1
-                for (int c = half * (kTN / 64); c < (half + 1) * (kTN / 64); c++) {
-                    float vv[32];
+                const int c0 = half * 2;
+                const uint32_t tbase = tmem + ((uint32_t) (quad * 32) << 16) + d * kTN;
+#pragma unroll
+                for (int cc = 0; cc < 2; cc++) {
+                    float va[32];
                     __syncwarp();
-                    tmem_ld32(tmem + ((uint32_t) (quad * 32) << 16) + d * kTN + c * 32, vv);
-                    const int64_t xb = x0 + c * 32;
+                    tmem_ld32(tbase + (c0 + cc) * 32, va);
                     uint16_t q[32];
-#pragma unroll
-                    for (int i = 0; i < 32; i++) q[i] = Narrow16<S>::bits(vv[i] * p.inv_scale, carry, p.error_feedback);
-                    uint4 u[4];
-#pragma unroll
-                    for (int i = 0; i < 32; i += 8) {
-                        u[i / 8].x = q[i] | ((uint32_t) q[i + 1] << 16);
-                        u[i / 8].y = q[i + 2] | ((uint32_t) q[i + 3] << 16);
-                        u[i / 8].z = q[i + 4] | ((uint32_t) q[i + 5] << 16);
-                        u[i / 8].w = q[i + 6] | ((uint32_t) q[i + 7] << 16);
-                    }
+                    narrow32<S>(va, p.inv_scale, p.error_feedback, q);
+                    const int64_t xb = x0 + (c0 + cc) * 32;
+                    const uint4 u[4] = {pack8(q), pack8(q + 8), pack8(q + 16), pack8(q + 24)};
                     if (!is_z) {
                         if (a < A) {
                             S *dst = out + a * stride_a + oth * stride_o + xb;
@@ -192,6 +185,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_batch_strided(const __grid_con
                         }
                         continue;
                     }
+                    __syncwarp();
 #pragma unroll
                     for (int i = 0; i < 4; i++) *reinterpret_cast<uint4 *>(stg + lane * kStageRowBytes + i * 16) = u[i];
                     __syncwarp();
@@ -204,7 +198,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_batch_strided(const __grid_con
                         if (ar < A && xb + sub * 8 < vol.nx)
                             *reinterpret_cast<uint4 *>(out + ar * stride_a + oth * stride_o + xb + sub * 8) = w;
                     }
-                    __syncwarp();
                 }
                 tc_fence_before();
                 __syncwarp();
@@ -310,91 +303,23 @@ __global__ void __launch_bounds__(kThreads, 1) tc_batch_contig(const __grid_cons
             tc_fence_after();
             const int64_t rows = vol.nz * vol.ny, nx = vol.nx;
             const int64_t row = (tile / vol.n_xt) * kTM + r;
-            const int64_t x0 = (tile % vol.n_xt) * kXTN;
-            uint32_t mw[kXTN / 64];
+            const int64_t xa = (tile % vol.n_xt) * kXTN + half * 64;
+            uint32_t mw[2];
 #pragma unroll
-            for (int c2 = 0; c2 < kXTN / 64; c2++) {
-                const int64_t xb = x0 + (half * (kXTN / 64) + c2) * 32;
-                mw[c2] = 0;
-                if (row < rows && xb < nx)
-                    mw[c2] = row_mask32<MAXI_MASK_BITPACKED>(vol.mask, row * nx + xb, nx - xb < 32 ? (int) (nx - xb) : 32,
-                                                             rows * nx);
+            for (int cc = 0; cc < 2; cc++) {
+                const int64_t xb = xa + cc * 32;
+                mw[cc] = (row < rows && xb < nx)
+                             ? row_mask32<MAXI_MASK_BITPACKED>(vol.mask, row * nx + xb, nx - xb < 32 ? (int) (nx - xb) : 32,
+                                                               rows * nx)
+                             : 0u;
             }
-            float carry = 0.0f;
-#pragma unroll
-            for (int c2 = 0; c2 < kXTN / 64; c2++) {
-                const int c = half * (kXTN / 64) + c2;
-                float h[32];
-                __syncwarp();
-                tmem_ld32(tmem + ((uint32_t) (quad * 32) << 16) + d * kXTN + c * 32, h);
-                const int64_t xb = x0 + c * 32;
-                if (row >= rows || xb >= nx) continue;
-                const int count = nx - xb < 32 ? (int) (nx - xb) : 32;
-                const int64_t idx = row * nx + xb;
-                const uint32_t m = mw[c2];
-                if (p.final_pass) {
-                    float fv[32];
-                    uint16_t q[32];
-#pragma unroll
-                    for (int i = 0; i < 32; i++) {
-                        fv[i] = ((m >> i) & 1u) ? 1.0f : h[i] * p.inv_scale;
-                        q[i] = quantise_u16(fv[i]);
-                    }
-                    if (count == 32) {  // idx % 32 == 0 and 16-byte aligned outputs: vector stores
-                        if (vol.out_u16) {
-#pragma unroll
-                            for (int i = 0; i < 32; i += 8) {
-                                uint4 u;
-                                u.x = q[i] | ((uint32_t) q[i + 1] << 16);
-                                u.y = q[i + 2] | ((uint32_t) q[i + 3] << 16);
-                                u.z = q[i + 4] | ((uint32_t) q[i + 5] << 16);
-                                u.w = q[i + 6] | ((uint32_t) q[i + 7] << 16);
-                                *reinterpret_cast<uint4 *>(vol.out_u16 + idx + i) = u;
-                            }
-                        }
-                        if (vol.field_out) {
-#pragma unroll
-                            for (int i = 0; i < 32; i += 4)
-                                *reinterpret_cast<float4 *>(vol.field_out + idx + i) = make_float4(fv[i], fv[i + 1], fv[i + 2], fv[i + 3]);
-                        }
-                    } else {
-#pragma unroll
-                        for (int i = 0; i < 32; i++) {
-                            if (i < count) {
-                                if (vol.out_u16) vol.out_u16[idx + i] = q[i];
-                                if (vol.field_out) vol.field_out[idx + i] = fv[i];
-                            }
-                        }
-                    }
-                } else {
-                    uint16_t q[32];
-#pragma unroll
-                    for (int i = 0; i < 32; i++) {
-                        if ((m >> i) & 1u) {
-                            q[i] = Narrow16<S>::bits(1.0f, carry, false);
-                            carry = 0.0f;
-                        } else {
-                            q[i] = Narrow16<S>::bits(h[i] * p.inv_scale, carry, p.error_feedback);
-                        }
-                    }
-                    uint16_t *dst = static_cast<uint16_t *>(vol.buf[p.in_buf ^ 1]) + idx;
-                    if (count == 32) {
-#pragma unroll
-                        for (int i = 0; i < 32; i += 8) {
-                            uint4 u;
-                            u.x = q[i] | ((uint32_t) q[i + 1] << 16);
-                            u.y = q[i + 2] | ((uint32_t) q[i + 3] << 16);
-                            u.z = q[i + 4] | ((uint32_t) q[i + 5] << 16);
-                            u.w = q[i + 6] | ((uint32_t) q[i + 7] << 16);
-                            *reinterpret_cast<uint4 *>(dst + i) = u;
-                        }
-                    } else {
-#pragma unroll
-                        for (int i = 0; i < 32; i++)
-                            if (i < count) dst[i] = q[i];
-                    }
-                }
-            }
+            float ha[32], hb[32];
+            __syncwarp();
+            const uint32_t ta = tmem + ((uint32_t) (quad * 32) << 16) + d * kXTN + half * 64;
+            tmem_ld32(ta, ha);
+            tmem_ld32(ta + 32, hb);
+            contig_epilogue64<S>(ha, hb, mw[0], mw[1], row, rows, nx, xa, p.inv_scale, p.error_feedback, p.final_pass,
+                                 static_cast<uint16_t *>(vol.buf[p.in_buf ^ 1]), vol.out_u16, vol.field_out);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[d]);

@@ -190,24 +190,17 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
             const int64_t oth = col / p.n_xc;
             const int64_t a = (int64_t) at * kTM + o;
             const int64_t x0 = (int64_t) xc * kTN;
-            float carry = 0.0f;
-#pragma unroll 1
-            for (int c = half * (kTN / 64); c < (half + 1) * (kTN / 64); c++) {
-                float v[32];
+            const int c0 = half * 2;  // this warp's two 32-column chunks
+            const uint32_t tbase = tmem + ((uint32_t) (quad * 32) << 16) + d * kTN;
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                float va[32];
                 __syncwarp();
-                tmem_ld32(tmem + ((uint32_t) (quad * 32) << 16) + d * kTN + c * 32, v);
-                const int64_t xb = x0 + c * 32;
+                tmem_ld32(tbase + (c0 + cc) * 32, va);
                 uint16_t q[32];
-#pragma unroll
-                for (int i = 0; i < 32; i++) q[i] = Narrow16<S>::bits(v[i] * p.inv_scale, carry, p.error_feedback);
-                uint4 u[4];
-#pragma unroll
-                for (int i = 0; i < 32; i += 8) {
-                    u[i / 8].x = q[i] | ((uint32_t) q[i + 1] << 16);
-                    u[i / 8].y = q[i + 2] | ((uint32_t) q[i + 3] << 16);
-                    u[i / 8].z = q[i + 4] | ((uint32_t) q[i + 5] << 16);
-                    u[i / 8].w = q[i + 6] | ((uint32_t) q[i + 7] << 16);
-                }
+                narrow32<S>(va, p.inv_scale, p.error_feedback, q);
+                const int64_t xb = x0 + (c0 + cc) * 32;
+                const uint4 u[4] = {pack8(q), pack8(q + 8), pack8(q + 16), pack8(q + 24)};
                 if (!p.axis_is_z) {
                     // y pass: a lane's row is 2 KB from its neighbour's, one page per warp.
                     if (a < p.A) {
@@ -221,6 +214,7 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
                 // z pass: lanes' rows lie on different planes (2 MB apart at 1024^2), so
                 // stage the warp's 32 x 32 chunk and store 8 rows (8 x 64 bytes) per
                 // instruction instead of 32 distant rows.
+                __syncwarp();
 #pragma unroll
                 for (int i = 0; i < 4; i++) *reinterpret_cast<uint4 *>(stg + lane * kStageRowBytes + i * 16) = u[i];
                 __syncwarp();
@@ -233,7 +227,6 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
                     if (ar < p.A && xb + sub * 8 < p.nx)
                         *reinterpret_cast<uint4 *>(out + ar * p.stride_a + oth * p.stride_o + xb + sub * 8) = w;
                 }
-                __syncwarp();
             }
             tc_fence_before();
             __syncwarp();
@@ -371,93 +364,24 @@ tc_contig_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__
             if (!mbar_wait(&tfull[d], dph, 2)) break;
             tc_fence_after();
             const int64_t row = (tile / p.n_xt) * kTM + r;
-            const int64_t x0 = (tile % p.n_xt) * kXTN;
-            float carry = 0.0f;
-            // Mask flags of this thread's 64 voxels, fetched before the TMEM loads.
-            uint32_t mw[kXTN / 64];
+            const int64_t xa = (tile % p.n_xt) * kXTN + half * 64;  // this warp's 64 voxels of the row
+            // Mask flags fetched before the TMEM loads.
+            uint32_t mw[2];
 #pragma unroll
-            for (int c2 = 0; c2 < kXTN / 64; c2++) {
-                const int64_t xb = x0 + (half * (kXTN / 64) + c2) * 32;
-                mw[c2] = 0;
-                if (row < p.rows && xb < p.nx)
-                    mw[c2] = row_mask32<FMT>(p.mask, row * p.nx + xb, p.nx - xb < 32 ? (int) (p.nx - xb) : 32,
-                                             p.rows * p.nx);
+            for (int cc = 0; cc < 2; cc++) {
+                const int64_t xb = xa + cc * 32;
+                mw[cc] = (row < p.rows && xb < p.nx)
+                             ? row_mask32<FMT>(p.mask, row * p.nx + xb, p.nx - xb < 32 ? (int) (p.nx - xb) : 32,
+                                               p.rows * p.nx)
+                             : 0u;
             }
-#pragma unroll
-            for (int c2 = 0; c2 < kXTN / 64; c2++) {
-                const int c = half * (kXTN / 64) + c2;
-                float h[32];
-                __syncwarp();
-                const uint32_t ta = tmem + ((uint32_t) (quad * 32) << 16) + d * kXTN + c * 32;
-                tmem_ld32(ta, h);
-                const int64_t xb = x0 + c * 32;
-                if (row >= p.rows || xb >= p.nx) continue;
-                const int count = p.nx - xb < 32 ? (int) (p.nx - xb) : 32;
-                const int64_t idx = row * p.nx + xb;
-                const uint32_t m = mw[c2];
-                if (p.final_pass) {
-                    float v[32];
-                    uint16_t q[32];
-#pragma unroll
-                    for (int i = 0; i < 32; i++) {
-                        v[i] = ((m >> i) & 1u) ? 1.0f : h[i] * p.inv_scale;
-                        q[i] = quantise_u16(v[i]);
-                    }
-                    if (count == 32) {
-                        if (p.out_u16) {
-#pragma unroll
-                            for (int i = 0; i < 32; i += 8) {
-                                uint4 u;
-                                u.x = q[i] | ((uint32_t) q[i + 1] << 16);
-                                u.y = q[i + 2] | ((uint32_t) q[i + 3] << 16);
-                                u.z = q[i + 4] | ((uint32_t) q[i + 5] << 16);
-                                u.w = q[i + 6] | ((uint32_t) q[i + 7] << 16);
-                                *reinterpret_cast<uint4 *>(p.out_u16 + idx + i) = u;
-                            }
-                        }
-                        if (p.field_out) {
-#pragma unroll
-                            for (int i = 0; i < 32; i += 4)
-                                *reinterpret_cast<float4 *>(p.field_out + idx + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
-                        }
-                    } else {
-#pragma unroll
-                        for (int i = 0; i < 32; i++) {
-                            if (i < count) {
-                                if (p.out_u16) p.out_u16[idx + i] = q[i];
-                                if (p.field_out) p.field_out[idx + i] = v[i];
-                            }
-                        }
-                    }
-                } else {
-                    uint16_t q[32];
-#pragma unroll
-                    for (int i = 0; i < 32; i++) {
-                        if ((m >> i) & 1u) {
-                            q[i] = Narrow16<S>::bits(1.0f, carry, false);
-                            carry = 0.0f;
-                        } else {
-                            q[i] = Narrow16<S>::bits(h[i] * p.inv_scale, carry, p.error_feedback);
-                        }
-                    }
-                    uint16_t *dst = static_cast<uint16_t *>(p.out) + idx;
-                    if (count == 32) {
-#pragma unroll
-                        for (int i = 0; i < 32; i += 8) {
-                            uint4 u;
-                            u.x = q[i] | ((uint32_t) q[i + 1] << 16);
-                            u.y = q[i + 2] | ((uint32_t) q[i + 3] << 16);
-                            u.z = q[i + 4] | ((uint32_t) q[i + 5] << 16);
-                            u.w = q[i + 6] | ((uint32_t) q[i + 7] << 16);
-                            *reinterpret_cast<uint4 *>(dst + i) = u;
-                        }
-                    } else {
-#pragma unroll
-                        for (int i = 0; i < 32; i++)
-                            if (i < count) dst[i] = q[i];
-                    }
-                }
-            }
+            float ha[32], hb[32];
+            __syncwarp();
+            const uint32_t ta = tmem + ((uint32_t) (quad * 32) << 16) + d * kXTN + half * 64;
+            tmem_ld32(ta, ha);
+            tmem_ld32(ta + 32, hb);
+            contig_epilogue64<S>(ha, hb, mw[0], mw[1], row, p.rows, p.nx, xa, p.inv_scale, p.error_feedback,
+                                 p.final_pass, static_cast<uint16_t *>(p.out), p.out_u16, p.field_out);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[d]);

@@ -29,8 +29,8 @@ template <int R> struct Taps { float k[2 * R + 1]; };
 
 // ---- strided (z / y) pass -------------------------------------------------
 constexpr int kStrTI = 32;    // inner columns per CTA (one warp wide)
-constexpr int kStrTA = 128;   // axis outputs per CTA
-constexpr int kStrM = 16;     // axis outputs per thread
+constexpr int kStrTA = 256;   // axis outputs per CTA
+constexpr int kStrM = 32;     // axis outputs per thread
 constexpr int kStrThreads = kStrTI * (kStrTA / kStrM);  // 256
 
 // The staged tile, or (error-feedback epilogue) the outputs on a 33-word row stride.
@@ -114,17 +114,19 @@ strided_pass(const S *__restrict__ in, S *__restrict__ out, int64_t A, int64_t I
 #pragma unroll
         for (int i = 0; i < kStrM; i++) s_tile[(seg * kStrM + i) * (kStrTI + 1) + col] = acc[i];
         __syncthreads();
-        const int row = threadIdx.x >> 1, c0 = (threadIdx.x & 1) * 16;
-        const int64_t a = a0 + row;
-        if (a >= A) return;
-        S *dst = out + (o * A + a) * I + i0 + c0;
-        float carry = 0.0f;
+        const int c0 = (threadIdx.x & 1) * 16;
+        for (int row = threadIdx.x >> 1; row < kStrTA; row += kStrThreads / 2) {
+            const int64_t a = a0 + row;
+            if (a >= A) break;
+            S *dst = out + (o * A + a) * I + i0 + c0;
+            float carry = 0.0f;
 #pragma unroll
-        for (int c = 0; c < 16; c++) {
-            const float w = s_tile[row * (kStrTI + 1) + c0 + c] + carry;
-            const S q = FieldIO<S>::narrow(w);
-            carry = w - FieldIO<S>::widen(q);
-            if (i0 + c0 + c < I) dst[c] = q;
+            for (int c = 0; c < 16; c++) {
+                const float w = s_tile[row * (kStrTI + 1) + c0 + c] + carry;
+                const S q = FieldIO<S>::narrow(w);
+                carry = w - FieldIO<S>::widen(q);
+                if (i0 + c0 + c < I) dst[c] = q;
+            }
         }
         return;
     }

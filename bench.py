@@ -460,7 +460,19 @@ def main():
             device.tensor_core_status()
             t_ms = e0.elapsed_time(e1)
             err = (fo.double() - f64).abs_()
+            fb = FIELD_BYTES[form]
+            f_bytes = {"z": 2 * fb * vox, "y": 2 * fb * vox, "x": (2 * fb + 0.125) * vox}
+            fdom = max(("z", "y", "x"), key=lambda k: fprof.get(k, (0, 1))[0])
+            fms = fprof[fdom][0] / fprof[fdom][1]
+            f_traffic = None
+            if os.path.exists(tpath):
+                with open(tpath) as f:
+                    f_traffic = json.load(f).get(args.workload, {}).get(form, {}).get(fdom)
+            froof = {"bound": "hbm", "kernel": fdom, "achieved": f_bytes[fdom] / (fms / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": f_bytes[fdom] / (fms / 1e3) / 1e9 / peak, "traffic": f_traffic,
+                     "whole_rep_frac": (2 * fb + 0.125) * vox * reps * n_t / (t_ms / 1e3) / 1e9 / peak}
             forms[name] = {"value": vox * reps * n_t / (t_ms / 1e3) / 1e9, "unit": UNIT, "field": form, **opts,
+                           "roofline": froof,
                            "max_abs_err_vs_f64": float(err.max().item()),
                            "mean_abs_err_vs_f64": float(err.mean().item()),
                            "mask_voxels_exact": bool((out.view(torch.int16)[mask > 0] == -1).all().item()),

@@ -37,7 +37,8 @@ namespace tc {
 
 constexpr int kTM = 128;      // outputs along the axis per tile
 constexpr int kTN = 128;      // x columns per tile
-constexpr int kStages = 2;    // TMA ring depth
+constexpr int kStages = 2;    // TMA ring depth (x pass)
+
 constexpr int kPrefetch = 3;  // tiles prefetched into L2 ahead of the ring
 constexpr int kEpiWarps = 8;  // two warps per TMEM lane quadrant, each drains half the columns
 constexpr int kThreads = 64 + 32 * kEpiWarps;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
@@ -61,28 +62,33 @@ struct StridedParams {
 
 // Per-epilogue-warp staging of a 32-row x 32-column output chunk: row stride
 // 80 bytes (16-byte stores of 32 lanes on 32 rows hit 8 distinct bank groups).
-constexpr int kStageRowBytes = 80;
-constexpr int kStageWarpBytes = 32 * kStageRowBytes;
+constexpr int kStageWarpBytes = 2 * 32 * 64;  // two 32 x 32 16-bit buffers per epilogue warp
 
-__host__ __device__ constexpr int strided_smem_bytes(int kp, int kpa) {
-    return 1024 /*alignment slack*/ + 2 * kpa * kTM * 2 /*T_hi, T_lo*/ + kStages * (kTN / 64) * kp * 128 /*B ring*/ +
-           256 /*barriers, TMEM slot*/ + kEpiWarps * kStageWarpBytes;
+__host__ __device__ constexpr int strided_smem_bytes(int kp, int kpa, int tn, int stages) {
+    return 1024 /*alignment slack*/ + 2 * kpa * kTM * 2 /*T_hi, T_lo*/ + stages * (tn / 64) * kp * 128 /*B ring*/ +
+           1024 /*barriers, TMEM slot*/ + kEpiWarps * kStageWarpBytes;
 }
 
-template <typename S>
+// TN x-columns per tile, STAGES-deep TMA ring.  The z pass uses 128-column tiles
+// (256 contiguous bytes per plane row per tile) and stages its stores so one
+// instruction writes 8 rows; the y pass uses 64-column tiles with a 4-deep ring
+// and TMA bulk stores of each warp's 32 x 32 chunk.
+template <typename S, int TN, int STAGES>
 __global__ void __launch_bounds__(kThreads, 1)
-tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ StridedParams p) {
+tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmap_out,
+                const __grid_constant__ StridedParams p) {
+    constexpr int kStrTN = TN, kStrStages = STAGES, kStrChunks = TN / 64;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     uint8_t *smem = smem_raw + (((raw + 1023) & ~1023u) - raw);
     uint8_t *t_hi = smem;
     uint8_t *t_lo = t_hi + p.kpa * kTM * 2;
     uint8_t *ring = t_lo + p.kpa * kTM * 2;
-    const int stage_bytes = (kTN / 64) * p.kp * 128;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kStages * stage_bytes);
-    uint64_t *full = bars, *empty = bars + kStages, *tfull = bars + 2 * kStages, *tempty = bars + 2 * kStages + 2;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 4);
-    uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 256;
+    const int stage_bytes = (kStrTN / 64) * p.kp * 128;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kStrStages * stage_bytes);
+    uint64_t *full = bars, *empty = bars + kStrStages, *tfull = bars + 2 * kStrStages, *tempty = bars + 2 * kStrStages + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kStrStages + 4);
+    uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 1024;  // 1024-byte aligned
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -97,14 +103,14 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
         *reinterpret_cast<uint16_t *>(t_lo + off) = l;
     }
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        for (int s = 0; s < kStrStages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], kEpiWarps); }
         fence_barrier_init();
         prefetch_tmap(&tmap);
     }
     __syncwarp();
     if (warp == 0) {
-        tmem_alloc(tmem_slot, 2 * kTN);
+        tmem_alloc(tmem_slot, 2 * kStrTN);
         tmem_relinquish();
     }
     fence_proxy_async_smem();
@@ -119,8 +125,8 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
         bool ok = true;
         for (int64_t col = blockIdx.x; ok && col < p.n_cols; col += gridDim.x)
         for (int at = 0; at < p.n_at; at++, tl++) {
-            const int s = (int) (tl % kStages);
-            const uint32_t ph = (uint32_t) ((tl / kStages) & 1);
+            const int s = (int) (tl % kStrStages);
+            const uint32_t ph = (uint32_t) ((tl / kStrStages) & 1);
             if (!mbar_wait(&empty[s], ph ^ 1, 1)) { ok = false; break; }
             {
                 // L2 prefetch of the tile kPrefetch tiles ahead in this CTA's order.
@@ -129,18 +135,18 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
                 if (colp < p.n_cols) {
                     const int atp = (int) (tp % p.n_at);
                     const int xcp = (int) (colp % p.n_xc), othp = (int) (colp / p.n_xc);
-                    for (int c = 0; c < kTN / 64; c++) {
-                        if (p.axis_is_z) tma_prefetch_3d(&tmap, xcp * kTN + 64 * c, othp, atp * kTM - p.radius);
-                        else tma_prefetch_3d(&tmap, xcp * kTN + 64 * c, atp * kTM - p.radius, othp);
+                    for (int c = 0; c < kStrTN / 64; c++) {
+                        if (p.axis_is_z) tma_prefetch_3d(&tmap, xcp * kStrTN + 64 * c, othp, atp * kTM - p.radius);
+                        else tma_prefetch_3d(&tmap, xcp * kStrTN + 64 * c, atp * kTM - p.radius, othp);
                     }
                 }
             }
             const int xc = (int) (col % p.n_xc);
             const int oth = (int) (col / p.n_xc);
             const int a_in = at * kTM - p.radius;
-            const int x0 = xc * kTN;
+            const int x0 = xc * kStrTN;
             mbar_arrive_expect_tx(&full[s], stage_bytes);
-            for (int c = 0; c < kTN / 64; c++) {
+            for (int c = 0; c < kStrTN / 64; c++) {
                 uint8_t *dst = ring + s * stage_bytes + c * p.kp * 128;
                 if (p.axis_is_z) tma_load_3d(dst, &tmap, x0 + 64 * c, oth, a_in, &full[s]);
                 else tma_load_3d(dst, &tmap, x0 + 64 * c, a_in, oth, &full[s]);
@@ -149,19 +155,19 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
     } else if (warp == 1 && lane == 0) {
         // MMA issuer.
         const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
-        const uint32_t idesc = idesc_f16(fmt, 0 /*A K-major*/, 1 /*B MN-major*/, kTM, kTN);
+        const uint32_t idesc = idesc_f16(fmt, 0 /*A K-major*/, 1 /*B MN-major*/, kTM, kStrTN);
         const uint32_t a_hi = smem_u32(t_hi), a_lo = smem_u32(t_lo), b0 = smem_u32(ring);
         int64_t tl = 0;
         bool ok = true;
         for (int64_t col = blockIdx.x; ok && col < p.n_cols; col += gridDim.x)
         for (int at = 0; at < p.n_at; at++, tl++) {
-            const int s = (int) (tl % kStages);
-            const uint32_t ph = (uint32_t) ((tl / kStages) & 1);
+            const int s = (int) (tl % kStrStages);
+            const uint32_t ph = (uint32_t) ((tl / kStrStages) & 1);
             const int d = (int) (tl & 1);
             const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
             if (!mbar_wait(&full[s], ph, 1) || !mbar_wait(&tempty[d], dph ^ 1, 3)) { ok = false; break; }
             tc_fence_after();
-            const uint32_t dt = tmem + d * kTN;
+            const uint32_t dt = tmem + d * kStrTN;
             for (int ks = 0; ks < p.kp / 16; ks++) {
                 const uint32_t koff = (ks >> 2) * (kTM * 128) + (ks & 3) * 32;
                 const uint64_t bd = smem_desc_sw128(b0 + s * stage_bytes + ks * 2048, p.kp * 128, 1024);
@@ -177,7 +183,8 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
         const int half = (warp - 2) >> 2;    // which half of the columns it drains
         const int o = quad * 32 + lane;      // output row within the tile
         S *out = static_cast<S *>(p.out);
-        uint8_t *stg = stage_out + (warp - 2) * kStageWarpBytes;
+        uint8_t *stg = stage_out + (warp - 2) * kStageWarpBytes;  // two 32 x 32 staging buffers
+        int sbuf = 0;
         int64_t tl = 0;
         bool ok = true;
         for (int64_t col = blockIdx.x; ok && col < p.n_cols; col += gridDim.x)
@@ -188,55 +195,61 @@ tc_strided_pass(const __grid_constant__ CUtensorMap tmap, const __grid_constant_
             tc_fence_after();
             const int xc = (int) (col % p.n_xc);
             const int64_t oth = col / p.n_xc;
-            const int64_t a = (int64_t) at * kTM + o;
-            const int64_t x0 = (int64_t) xc * kTN;
-            const int c0 = half * 2;  // this warp's two 32-column chunks
-            const uint32_t tbase = tmem + ((uint32_t) (quad * 32) << 16) + d * kTN;
+            const int64_t x0 = (int64_t) xc * kStrTN;
+            const int c0 = half * kStrChunks;  // this warp's 32-column chunks
+            const uint32_t tbase = tmem + ((uint32_t) (quad * 32) << 16) + d * kStrTN;
 #pragma unroll
-            for (int cc = 0; cc < 2; cc++) {
+            for (int cc = 0; cc < kStrChunks; cc++) {
                 float va[32];
                 __syncwarp();
                 tmem_ld32(tbase + (c0 + cc) * 32, va);
                 uint16_t q[32];
                 narrow32<S>(va, p.inv_scale, p.error_feedback, q);
                 const int64_t xb = x0 + (c0 + cc) * 32;
-                const uint4 u[4] = {pack8(q), pack8(q + 8), pack8(q + 16), pack8(q + 24)};
-                if (!p.axis_is_z) {
-                    // y pass: a lane's row is 2 KB from its neighbour's, one page per warp.
-                    if (a < p.A) {
-                        S *dst = out + a * p.stride_a + oth * p.stride_o + xb;
+                if (p.axis_is_z) {
+                    // z pass: lanes' rows lie on different planes (2 MB apart at 1024^2);
+                    // stage the 32 x 32 chunk and write 8 rows (8 x 64 bytes) per instruction.
+                    __syncwarp();
 #pragma unroll
-                        for (int i = 0; i < 4; i++)  // nx % 8 == 0: each 8-voxel group is wholly in or out
-                            if (xb + 8 * i < p.nx) reinterpret_cast<uint4 *>(dst)[i] = u[i];
+                    for (int i = 0; i < 4; i++) *reinterpret_cast<uint4 *>(stg + lane * 80 + i * 16) = pack8(q + 8 * i);
+                    __syncwarp();
+                    const int sub = lane & 3, rsub = lane >> 2;
+#pragma unroll
+                    for (int r4 = 0; r4 < 4; r4++) {
+                        const int rr = r4 * 8 + rsub;
+                        const int64_t ar = (int64_t) at * kTM + quad * 32 + rr;
+                        const uint4 w = *reinterpret_cast<const uint4 *>(stg + rr * 80 + sub * 16);
+                        if (ar < p.A && xb + sub * 8 < p.nx)
+                            *reinterpret_cast<uint4 *>(out + ar * p.stride_a + oth * p.stride_o + xb + sub * 8) = w;
                     }
                     continue;
                 }
-                // z pass: lanes' rows lie on different planes (2 MB apart at 1024^2), so
-                // stage the warp's 32 x 32 chunk and store 8 rows (8 x 64 bytes) per
-                // instruction instead of 32 distant rows.
+                // y pass: TMA store of the warp's 32 rows x 32 columns (64-byte swizzle of
+                // the store tensor map) instead of 32 per-lane row stores.
+                if (lane == 0) bulk_wait_read<1>();  // the store issued two chunks ago has read this buffer
                 __syncwarp();
+                uint8_t *sb = stg + sbuf * 2048;
 #pragma unroll
-                for (int i = 0; i < 4; i++) *reinterpret_cast<uint4 *>(stg + lane * kStageRowBytes + i * 16) = u[i];
+                for (int i = 0; i < 4; i++)
+                    *reinterpret_cast<uint4 *>(sb + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) = pack8(q + 8 * i);
+                fence_proxy_async_smem();
                 __syncwarp();
-                const int sub = lane & 3, rsub = lane >> 2;
-#pragma unroll
-                for (int r4 = 0; r4 < 4; r4++) {
-                    const int rr = r4 * 8 + rsub;
-                    const int64_t ar = (int64_t) at * kTM + quad * 32 + rr;
-                    const uint4 w = *reinterpret_cast<const uint4 *>(stg + rr * kStageRowBytes + sub * 16);
-                    if (ar < p.A && xb + sub * 8 < p.nx)
-                        *reinterpret_cast<uint4 *>(out + ar * p.stride_a + oth * p.stride_o + xb + sub * 8) = w;
+                if (lane == 0) {
+                    tma_store_3d(&tmap_out, sb, (int) xb, at * kTM + quad * 32, (int) oth);
+                    bulk_commit();
                 }
+                sbuf ^= 1;
             }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[d]);
         }
     }
+    if (warp >= 2 && lane == 0) bulk_wait_all();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        tmem_dealloc(tmem, 2 * kTN);
+        tmem_dealloc(tmem, 2 * kStrTN);
     }
 }
 
@@ -448,7 +461,7 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
     if (axis_z) { p.A = nz; p.n_other = ny; p.stride_a = ny * nx; p.stride_o = nx; }
     else { p.A = ny; p.n_other = nz; p.stride_a = nx; p.stride_o = ny * nx; }
     p.n_at = (int) ceil_div(p.A, kTM);
-    p.n_xc = (int) ceil_div(nx, kTN);
+    p.n_xc = (int) ceil_div(nx, axis_z ? 128 : 64);
     p.n_cols = (int64_t) p.n_xc * p.n_other;
 
     CUtensorMap map;
@@ -462,14 +475,23 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
 
-    const int smem = strided_smem_bytes(p.kp, p.kpa);
-    cudaError_t e = cudaFuncSetAttribute(tc_strided_pass<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    CUtensorMap map_out;
+    const cuuint64_t odims[3] = {(cuuint64_t) nx, (cuuint64_t) ny, (cuuint64_t) nz};
+    const cuuint32_t obox[3] = {32u, axis_z ? 1u : 32u, axis_z ? 32u : 1u};
+    cr = tc_encode_fn()(&map_out, is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, out,
+                        odims, strides, obox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                        CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    const int tn = axis_z ? 128 : 64, stages = axis_z ? 2 : 4;
+    const int smem = strided_smem_bytes(p.kp, p.kpa, tn, stages);
+    auto *kern = axis_z ? tc_strided_pass<S, 128, 2> : tc_strided_pass<S, 64, 4>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int64_t grid = std::min<int64_t>(p.n_cols, sms);
-    tc_strided_pass<S><<<(unsigned) grid, kThreads, smem, st>>>(map, p);
+    kern<<<(unsigned) grid, kThreads, smem, st>>>(map, map_out, p);
     return cudaGetLastError();
 }
 

@@ -109,6 +109,15 @@ int maxi_diffusion_in_memory(const uint8_t *voxels, int64_t nz, int64_t ny, int6
                              uint16_t *output, int verbose);
 
 /*
+ * maxi_diffusion_in_memory() keeps its device buffers between calls (one
+ * grow-only allocation per device) so repeated calls do not map gigabytes each
+ * time; volumes larger than the device go to the out-of-core form, as the
+ * reference's pybind module does (src/pybind/diffusion-pybind.cc:40-45).
+ * maxi_release_cached_memory() frees those buffers.
+ */
+int maxi_release_cached_memory(void);
+
+/*
  * Working memory (bytes) that maxi_diffusion_device() needs for one volume:
  * two field buffers of the storage type plus the bit-packed mask.
  */

@@ -43,6 +43,7 @@ SIGNATURES = {
     "maxi_bitpack_decode": (_int, [_p, _i64, _p, _p]),
     "maxi_diffusion_device_noalloc": (_int, [_p, _i32, _i64, _i64, _i64, _p, _i64, _i64, _p, _p, _p]),
     "maxi_tensor_core_status": (_int, []),
+    "maxi_release_cached_memory": (_int, []),
     "maxi_batch_plan_create": (_int, [_p, _i64, _i32, _i32, _p, ctypes.POINTER(ctypes.c_void_p)]),
     "maxi_batch_plan_run": (_int, [_p, _p]),
     "maxi_batch_plan_describe": (_int, [_p, ctypes.c_char_p, _i64]),

@@ -9,6 +9,8 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <map>
+#include <mutex>
 
 #include "common.cuh"
 #include "passes.cuh"
@@ -127,9 +129,70 @@ static cudaError_t run_typed(const Volume &v, const void *mask, int mask_fmt, co
     return cudaErrorInvalidValue;
 }
 
+// Device buffers of the host entry point, kept between calls (one per device,
+// grow-only) so repeated calls do not map and unmap gigabytes each time.
+struct DeviceCache {
+    std::mutex mu;
+    void *buf = nullptr;
+    int64_t bytes = 0;
+    cudaStream_t stream = nullptr;
+};
+static std::mutex g_cache_mu;
+static std::map<int, DeviceCache *> g_caches;
+
+static int device_cache(DeviceCache **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaGetDevice");
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    DeviceCache *&c = g_caches[dev];
+    if (!c) {
+        c = new DeviceCache();
+        if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess)
+            return set_cuda_error(e, "stream creation");
+    }
+    *out = c;
+    return MAXI_OK;
+}
+
+static int cache_reserve(DeviceCache *c, int64_t bytes) {
+    if (c->bytes >= bytes) return MAXI_OK;
+    if (c->buf) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(c->buf);
+        c->buf = nullptr;
+        c->bytes = 0;
+    }
+    if (cudaMalloc(&c->buf, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        c->buf = nullptr;
+        return set_error(MAXI_ERR_OUT_OF_MEMORY, "could not allocate %lld bytes on the device", (long long) bytes);
+    }
+    c->bytes = bytes;
+    return MAXI_OK;
+}
+
+static void release_device_caches() {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (auto &kv : g_caches) {
+        std::lock_guard<std::mutex> lk2(kv.second->mu);
+        if (kv.second->buf) {
+            cudaStreamSynchronize(kv.second->stream);
+            cudaFree(kv.second->buf);
+            kv.second->buf = nullptr;
+            kv.second->bytes = 0;
+        }
+    }
+}
+
 }  // namespace maxi
 
 using namespace maxi;
+
+extern "C" int maxi_diffusion_out_of_core_ex(const uint8_t *voxels, int64_t nz, int64_t ny, int64_t nx,
+                                             int64_t slab_z, const float *kernel, int64_t kernel_size,
+                                             int64_t repititions, uint16_t *output, int32_t field_type,
+                                             int32_t flags, int verbose);
 
 extern "C" {
 
@@ -213,39 +276,48 @@ int maxi_diffusion_in_memory(const uint8_t *voxels, int64_t nz, int64_t ny, int6
     if ((rc = require_device())) return rc;
     const int64_t n = nz * ny * nx;
     const int64_t need = workspace_bytes_for(n, MAXI_FIELD_F32);
+    const int64_t mask_off = 0, out_off = round_up(n, 256), ws_off = out_off + round_up(2 * n, 256);
+    const int64_t total = ws_off + need;
     if (verbose >= 1)
         printf("Diffusion: shape (%lld, %lld, %lld), kernel size %lld, %lld repetitions, FP32 field on the GPU\n",
                (long long) nz, (long long) ny, (long long) nx, (long long) kernel_size, (long long) repititions);
-    cudaStream_t st;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
-        return set_cuda_error(cudaGetLastError(), "stream creation");
-    uint8_t *d_mask = nullptr;
-    uint16_t *d_out = nullptr;
-    char *ws = nullptr;
-    cudaError_t e = cudaSuccess;
-    do {
-        if ((e = cudaMallocAsync(reinterpret_cast<void **>(&d_mask), n, st)) != cudaSuccess) break;
-        if ((e = cudaMallocAsync(reinterpret_cast<void **>(&d_out), 2 * n, st)) != cudaSuccess) break;
-        if (repititions > 0 && (e = cudaMallocAsync(reinterpret_cast<void **>(&ws), need, st)) != cudaSuccess) break;
-        if ((e = cudaMemcpyAsync(d_mask, voxels, n, cudaMemcpyHostToDevice, st)) != cudaSuccess) break;
-        rc = maxi_diffusion_device(d_mask, MAXI_MASK_U8, nz, ny, nx, kernel, kernel_size, repititions, d_out,
-                                   nullptr, MAXI_FIELD_F32, 0, ws, need, st);
-        if (rc) break;
-        if ((e = cudaMemcpyAsync(output, d_out, 2 * n, cudaMemcpyDeviceToHost, st)) != cudaSuccess) break;
-        e = cudaStreamSynchronize(st);
-    } while (0);
-    if (d_mask) cudaFreeAsync(d_mask, st);
-    if (d_out) cudaFreeAsync(d_out, st);
-    if (ws) cudaFreeAsync(ws, st);
-    cudaStreamSynchronize(st);
-    cudaStreamDestroy(st);
-    if (rc) return rc;
-    if (e == cudaErrorMemoryAllocation) {
-        cudaGetLastError();
-        return set_error(MAXI_ERR_OUT_OF_MEMORY, "device allocation failed for a %lld-voxel volume", (long long) n);
+    DeviceCache *cache = nullptr;
+    if ((rc = device_cache(&cache))) return rc;
+    std::lock_guard<std::mutex> lk(cache->mu);
+    if ((rc = cache_reserve(cache, total))) {
+        // Larger than the device: the reference's pybind module sends such volumes to
+        // its out-of-core form (src/pybind/diffusion-pybind.cc:40-45); do the same.
+        const int64_t plane = ny * nx;
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const int64_t halo = std::min(nz, repititions * (kernel_size / 2));
+        int64_t slab = (int64_t) (free_b / 2) / std::max<int64_t>(1, plane * 15) - 2 * halo;
+        if (slab < 1) slab = 1;
+        if (verbose >= 1) printf("Volume exceeds device memory: out-of-core slabs of %lld planes\n", (long long) slab);
+        clear_error();
+        return maxi_diffusion_out_of_core_ex(voxels, nz, ny, nx, slab, kernel, kernel_size, repititions, output,
+                                             MAXI_FIELD_F32, 0, verbose);
     }
+    char *base = static_cast<char *>(cache->buf);
+    uint8_t *d_mask = reinterpret_cast<uint8_t *>(base + mask_off);
+    uint16_t *d_out = reinterpret_cast<uint16_t *>(base + out_off);
+    cudaStream_t st = cache->stream;
+    cudaError_t e = cudaMemcpyAsync(d_mask, voxels, n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        rc = maxi_diffusion_device(d_mask, MAXI_MASK_U8, nz, ny, nx, kernel, kernel_size, repititions, d_out, nullptr,
+                                   MAXI_FIELD_F32, 0, base + ws_off, need, st);
+        if (rc) return rc;
+        e = cudaMemcpyAsync(output, d_out, 2 * n, cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return set_cuda_error(e, "in-memory diffusion");
     if (verbose >= 1) printf("Diffusion is complete!\n");
+    return MAXI_OK;
+}
+
+int maxi_release_cached_memory(void) {
+    clear_error();
+    release_device_caches();
     return MAXI_OK;
 }
 

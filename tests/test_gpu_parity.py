@@ -194,3 +194,17 @@ def test_field_out_without_uint16_output(field):
     device.diffuse(m, kernel, 3, output=None, field=field, field_out=fo)
     _, want = oracle.diffusion_in_memory(mask, kernel, 3)
     assert np.abs(fo.cpu().numpy() - want).max() < 1e-5
+
+
+def test_dropin_repeated_calls_reuse_and_grow_cached_buffers():
+    from maxibone_b200 import _lib
+    k = gauss_kernel(2).astype(np.float32)
+    for shape in [(20, 30, 40), (10, 10, 10), (40, 50, 60), (20, 30, 40)]:
+        mask = random_mask(shape, 0.05, seed=sum(shape))
+        out = np.zeros(shape, np.uint16)
+        diffusion(mask, k, out, 3)
+        want, _ = oracle.diffusion_in_memory(mask, k, 3)
+        assert np.abs(out.astype(np.int32) - want.astype(np.int32)).max() <= 1
+    assert _lib.lib().maxi_release_cached_memory() == 0
+    out = np.zeros((8, 8, 8), np.uint16)
+    diffusion(random_mask((8, 8, 8), 0.2, seed=1), k, out, 2)  # allocates again after the release

@@ -229,9 +229,10 @@ def batched_section(device, torch, np, stream, reps=50):
     return res
 
 
-def out_of_core_section(torch, np, reps=20, shape=(4096, 1728, 2048), slab=256):
+def out_of_core_section(torch, np, reps=20, shape=(4096, 1728, 2048), slab=1024):
     """Out-of-core z-slabs streamed from pinned host memory: sigma 8, R = 20, BF16
-    field, slabs of 256 planes with 640-plane halos.  The plane is a quarter of the
+    field, slabs of 1024 planes with 640-plane halos (repetition k computes the
+    planes at least 32k from a cut side).  The plane is a quarter of the
     3456 x 4096 plane of the full-size case so host and device memory stay bounded."""
     from maxibone_b200.diffusion import diffusion_out_of_core
     from maxibone_b200.kernels import gauss_kernel
@@ -257,9 +258,15 @@ def out_of_core_section(torch, np, reps=20, shape=(4096, 1728, 2048), slab=256):
            "h2d_bytes": None, "d2h_bytes": 2 * vox,
            "timing": "host clock around the synchronous out-of-core call (uploads, compute, downloads)"}
     n_slabs = -(-shape[0] // slab)
-    ext = sum(min(shape[0], (s + 1) * slab + halo) - max(0, s * slab - halo) for s in range(n_slabs))
+    r = kernel.shape[0] // 2
+    ext = computed = 0
+    for s in range(n_slabs):
+        e0, e1 = max(0, s * slab - halo), min(shape[0], (s + 1) * slab + halo)
+        ext += e1 - e0
+        computed += sum(e1 - e0 - k * r * ((e0 > 0) + (e1 < shape[0])) for k in range(reps))
     res["h2d_bytes"] = ext * shape[1] * shape[2]
     res["redundancy"] = ext / shape[0]
+    res["compute_redundancy"] = computed / (shape[0] * reps)
     del host_m, host_o
     return res
 

@@ -99,7 +99,7 @@ static int64_t workspace_bytes_for(int64_t n, int32_t ft) {
 template <typename S>
 static cudaError_t run_typed(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
                              int64_t reps, uint16_t *out_u16, void *field_out, int32_t flags, char *ws,
-                             cudaStream_t st) {
+                             cudaStream_t st, int64_t shrink_lo, int64_t shrink_hi) {
     if (reps == 0) return zero_reps<S>(v, mask, mask_fmt, out_u16, field_out, st);
     S *b0 = reinterpret_cast<S *>(ws);
     S *b1 = reinterpret_cast<S *>(ws + round_up((int64_t) sizeof(S) * v.n(), 256));
@@ -124,7 +124,7 @@ static cudaError_t run_typed(const Volume &v, const void *mask, int mask_fmt, co
             mask = packed;
         }
         return dispatch_unrolled<S>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16,
-                                    static_cast<float *>(field_out), flags, st);
+                                    static_cast<float *>(field_out), flags, st, shrink_lo, shrink_hi);
     }
     return cudaErrorInvalidValue;
 }
@@ -218,6 +218,17 @@ int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int
                           const float *kernel, int64_t kernel_size, int64_t repititions,
                           uint16_t *output, void *field_out, int32_t field_type, int32_t flags,
                           void *workspace, int64_t workspace_bytes, void *stream) {
+    return diffusion_device_shrinking(mask, mask_format, nz, ny, nx, kernel, kernel_size, repititions, output,
+                                      field_out, field_type, flags, workspace, workspace_bytes, stream, 0, 0);
+}
+
+}  // extern "C"
+
+int maxi::diffusion_device_shrinking(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,
+                                     const float *kernel, int64_t kernel_size, int64_t repititions,
+                                     uint16_t *output, void *field_out, int32_t field_type, int32_t flags,
+                                     void *workspace, int64_t workspace_bytes, void *stream, int64_t shrink_lo,
+                                     int64_t shrink_hi) {
     clear_error();
     int rc = validate_common(mask, nz, ny, nx, kernel, kernel_size, repititions);
     if (rc) return rc;
@@ -254,17 +265,23 @@ int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int
             owned = true;
         }
     }
+    // Plane windows start at multiples of ny*nx voxels: keep them on whole
+    // 32-bit words of the bit-packed mask (and 16-byte aligned for TMA).
+    if ((ny * nx) % 32 != 0 || shrink_lo < 0 || shrink_hi < 0) shrink_lo = shrink_hi = 0;
+    const int64_t slo = shrink_lo, shi = shrink_hi;
     cudaError_t e;
     switch (field_type) {
-    case MAXI_FIELD_F32: e = run_typed<float>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st); break;
-    case MAXI_FIELD_BF16: e = run_typed<__nv_bfloat16>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st); break;
-    case MAXI_FIELD_F16: e = run_typed<__half>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st); break;
-    default: e = run_typed<double>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st); break;
+    case MAXI_FIELD_F32: e = run_typed<float>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st, slo, shi); break;
+    case MAXI_FIELD_BF16: e = run_typed<__nv_bfloat16>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st, slo, shi); break;
+    case MAXI_FIELD_F16: e = run_typed<__half>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st, slo, shi); break;
+    default: e = run_typed<double>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st, 0, 0); break;
     }
     if (owned) cudaFreeAsync(ws, st);
     if (e != cudaSuccess) return set_cuda_error(e, "diffusion launch");
     return MAXI_OK;
 }
+
+extern "C" {
 
 int maxi_diffusion_in_memory(const uint8_t *voxels, int64_t nz, int64_t ny, int64_t nx,
                              const float *kernel, int64_t kernel_size, int64_t repititions,

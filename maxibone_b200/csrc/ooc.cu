@@ -8,7 +8,10 @@
 // repetitions run on the device, and only the slab's own S planes are written
 // back: a voxel's value after R repetitions depends only on input planes
 // within R x radius of it (one z pass per repetition), so the core planes are
-// exact and no exchange between slabs is needed.  Two slab contexts on
+// exact and no exchange between slabs is needed.  The halo's width is only
+// needed at the first repetition: repetition k runs on the planes that are at
+// least k x radius from a cut side, which brings the computed planes per slab
+// from R x (S + 2H) down to about R x (S + H).  Two slab contexts on
 // separate streams overlap one slab's host<->device copies with the other's
 // compute; pageable host buffers are staged through pinned memory by the host
 // thread while the device works.
@@ -18,6 +21,7 @@
 #include <functional>
 
 #include "host_util.h"
+#include "unrolled.h"
 
 namespace maxi {
 
@@ -58,10 +62,6 @@ static void free_ctx(OocContext &c) {
 
 using namespace maxi;
 
-extern "C" int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,
-                                     const float *kernel, int64_t kernel_size, int64_t repititions,
-                                     uint16_t *output, void *field_out, int32_t field_type, int32_t flags,
-                                     void *workspace, int64_t workspace_bytes, void *stream);
 extern "C" int64_t maxi_diffusion_workspace_size(int64_t nz, int64_t ny, int64_t nx, int32_t field_type);
 
 namespace maxi {
@@ -137,8 +137,13 @@ static int run_slabs(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, const f
         if (!direct_in && (rc = read(e0, ez, x.h_in))) return fail(rc);
         cudaError_t e = cudaMemcpyAsync(x.d_mask, src, ez * plane, cudaMemcpyHostToDevice, x.stream);
         if (e != cudaSuccess) return fail(set_cuda_error(e, "slab upload"));
-        rc = maxi_diffusion_device(x.d_mask, MAXI_MASK_U8, ez, ny, nx, kernel, kernel_size, repititions, x.d_out,
-                                   nullptr, field_type, flags, x.ws, x.ws_bytes, x.stream);
+        // A cut side (one that is not the volume's edge) carries a halo of
+        // repititions*radius planes, and after repetition k only the planes at
+        // least (k+1)*radius away from the cut still hold the whole-volume
+        // values: repetition k is computed on those planes alone.
+        rc = diffusion_device_shrinking(x.d_mask, MAXI_MASK_U8, ez, ny, nx, kernel, kernel_size, repititions,
+                                        x.d_out, nullptr, field_type, flags, x.ws, x.ws_bytes, x.stream,
+                                        e0 > 0 ? radius : 0, e1 < nz ? radius : 0);
         if (rc) return fail(rc);
         uint16_t *dst = direct_out ? direct_out + z0 * plane : x.h_out;
         e = cudaMemcpyAsync(dst, x.d_out + (z0 - e0) * plane, (z1 - z0) * plane * 2, cudaMemcpyDeviceToHost, x.stream);

@@ -28,9 +28,18 @@ int radius_bucket(int r);
 // field_out (either may be NULL).
 // flags: MAXI_FLAG_* bits (NO_TENSOR_CORES and NEAREST_ROUNDING apply to the
 // 16-bit storage types).
+// shrink_lo / shrink_hi (out-of-core slabs): repetition k works on planes
+// [k*shrink_lo, nz - k*shrink_hi) only -- the planes that can still reach the
+// slab's core; the bit-packed mask must then have (ny*nx) % 32 == 0.
 template <typename S>
 cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
                               int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, int32_t flags,
-                              cudaStream_t st);
+                              cudaStream_t st, int64_t shrink_lo = 0, int64_t shrink_hi = 0);
+
+// maxi_diffusion_device() with a shrinking plane window (see dispatch_unrolled).
+int diffusion_device_shrinking(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,
+                               const float *kernel, int64_t kernel_size, int64_t repititions, uint16_t *output,
+                               void *field_out, int32_t field_type, int32_t flags, void *workspace,
+                               int64_t workspace_bytes, void *stream, int64_t shrink_lo, int64_t shrink_hi);
 
 }  // namespace maxi

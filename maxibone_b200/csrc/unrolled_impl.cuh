@@ -42,7 +42,8 @@ static cudaError_t set_smem(F *f, int bytes) {
 template <int R, typename S, bool EF>
 static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel,
                                 int radius, int64_t reps, S *buf0, S *buf1, uint16_t *out_u16,
-                                float *field_out, bool use_tc, uint32_t *rebuild_mask, cudaStream_t st) {
+                                float *field_out, bool use_tc, uint32_t *rebuild_mask, int64_t shrink_lo,
+                                int64_t shrink_hi, cudaStream_t st) {
     const Taps<R> taps = make_taps<R>(kernel, radius);
     const int str_smem = strided_smem_bytes<R>();
     const int con_smem = contig_smem_bytes<R>();
@@ -68,37 +69,47 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
         else
             mask_to_field<S, MAXI_MASK_BITPACKED, false><<<blocks, threads, 0, st>>>(mask, buf0, nullptr, nullptr, n);
     }
-    // z pass: [1][nz][ny*nx]; y pass: [nz][ny][nx]
-    const int64_t zI = v.ny * v.nx, zA = v.nz, zat = ceil_div(zA, kStrTA), zit = ceil_div(zI, kStrTI);
-    const int64_t yI = v.nx, yA = v.ny, yO = v.nz, yat = ceil_div(yA, kStrTA), yit = ceil_div(yI, kStrTI);
-    const int64_t rows = v.nz * v.ny, xt = ceil_div(v.nx, kConTX), xrb = ceil_div(rows, kConTR);
+    const int64_t plane = v.ny * v.nx;
     // Tensor-core x pass: vector epilogue needs 16-byte aligned mask (u8), output and field.
     const bool tc_x = use_tc &&
                       ((reinterpret_cast<uintptr_t>(out_u16) | reinterpret_cast<uintptr_t>(field_out) |
                         (mask_fmt == MAXI_MASK_U8 ? reinterpret_cast<uintptr_t>(mask) : 0)) & 15) == 0;
     for (int64_t rep = 0; rep < reps; rep++) {
+        // Plane window of this repetition (the whole volume unless shrinking).
+        const int64_t lo = std::min(v.nz - 1, shrink_lo * rep);
+        const int64_t hi = std::max(lo + 1, v.nz - shrink_hi * rep);
+        const int64_t nzv = hi - lo, off = lo * plane;
+        S *b0 = buf0 + off, *b1 = buf1 + off;
+        const void *mv = mask_fmt == MAXI_MASK_U8 ? static_cast<const void *>(static_cast<const uint8_t *>(mask) + off)
+                                                  : static_cast<const void *>(static_cast<const uint32_t *>(mask) + off / 32);
+        uint16_t *ou = out_u16 ? out_u16 + off : nullptr;
+        float *fo = field_out ? field_out + off : nullptr;
+        // z pass: [1][nzv][ny*nx]; y pass: [nzv][ny][nx]
+        const int64_t zI = plane, zA = nzv, zat = ceil_div(zA, kStrTA), zit = ceil_div(zI, kStrTI);
+        const int64_t yI = v.nx, yA = v.ny, yO = nzv, yat = ceil_div(yA, kStrTA), yit = ceil_div(yI, kStrTI);
+        const int64_t rows = nzv * v.ny, xt = ceil_div(v.nx, kConTX), xrb = ceil_div(rows, kConTR);
         if (rebuild_mask && rep > 0) {
             ProfScope ps(MAXI_KERNEL_OTHER, st);
-            const int64_t blocks = std::min<int64_t>(ceil_div(ceil_div(n, 32), 256), 148 * 16);
-            mask_from_field<S><<<blocks, 256, 0, st>>>(buf0, rebuild_mask, n);
+            const int64_t blocks = std::min<int64_t>(ceil_div(ceil_div(nzv * plane, 32), 256), 148 * 16);
+            mask_from_field<S><<<blocks, 256, 0, st>>>(b0, rebuild_mask + off / 32, nzv * plane);
         }
         {
             ProfScope ps(MAXI_KERNEL_Z, st);
             if constexpr (sizeof(S) == 2) {
-                if (use_tc) e = tc::tc_strided<S>(buf0, buf1, v.nz, v.ny, v.nx, true, kernel, radius, EF, st);
-                else zy<<<zat * zit, kStrThreads, str_smem, st>>>(buf0, buf1, zA, zI, zat, zit, taps);
+                if (use_tc) e = tc::tc_strided<S>(b0, b1, nzv, v.ny, v.nx, true, kernel, radius, EF, st);
+                else zy<<<zat * zit, kStrThreads, str_smem, st>>>(b0, b1, zA, zI, zat, zit, taps);
             } else {
-                zy<<<zat * zit, kStrThreads, str_smem, st>>>(buf0, buf1, zA, zI, zat, zit, taps);
+                zy<<<zat * zit, kStrThreads, str_smem, st>>>(b0, b1, zA, zI, zat, zit, taps);
             }
         }
         if (e != cudaSuccess) return e;
         {
             ProfScope ps(MAXI_KERNEL_Y, st);
             if constexpr (sizeof(S) == 2) {
-                if (use_tc) e = tc::tc_strided<S>(buf1, buf0, v.nz, v.ny, v.nx, false, kernel, radius, EF, st);
-                else zy<<<yat * yit * yO, kStrThreads, str_smem, st>>>(buf1, buf0, yA, yI, yat, yit, taps);
+                if (use_tc) e = tc::tc_strided<S>(b1, b0, nzv, v.ny, v.nx, false, kernel, radius, EF, st);
+                else zy<<<yat * yit * yO, kStrThreads, str_smem, st>>>(b1, b0, yA, yI, yat, yit, taps);
             } else {
-                zy<<<yat * yit * yO, kStrThreads, str_smem, st>>>(buf1, buf0, yA, yI, yat, yit, taps);
+                zy<<<yat * yit * yO, kStrThreads, str_smem, st>>>(b1, b0, yA, yI, yat, yit, taps);
             }
         }
         if (e != cudaSuccess) return e;
@@ -107,12 +118,12 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
             ProfScope ps(last ? MAXI_KERNEL_X_FINAL : MAXI_KERNEL_X, st);
             if (tc_x) {
                 if constexpr (sizeof(S) == 2)
-                    e = tc::tc_contig<S>(buf0, buf1, mask, mask_fmt, last, last ? out_u16 : nullptr,
-                                         last ? field_out : nullptr, v.nz, v.ny, v.nx, kernel, radius, EF, st);
+                    e = tc::tc_contig<S>(b0, b1, mv, mask_fmt, last, last ? ou : nullptr, last ? fo : nullptr, nzv,
+                                         v.ny, v.nx, kernel, radius, EF, st);
             } else if (!last) {
-                xpass<<<xt * xrb, kConThreads, con_smem, st>>>(buf0, buf1, mask, nullptr, nullptr, rows, v.nx, xt, taps);
+                xpass<<<xt * xrb, kConThreads, con_smem, st>>>(b0, b1, mv, nullptr, nullptr, rows, v.nx, xt, taps);
             } else {
-                xfinal<<<xt * xrb, kConThreads, con_smem, st>>>(buf0, buf1, mask, out_u16, field_out, rows, v.nx, xt, taps);
+                xfinal<<<xt * xrb, kConThreads, con_smem, st>>>(b0, b1, mv, ou, fo, rows, v.nx, xt, taps);
             }
         }
         if (e != cudaSuccess) return e;
@@ -134,10 +145,10 @@ cudaError_t launch_init_field(const void *mask, int mask_fmt, S *field, int64_t 
 template <typename S, bool EF>
 static cudaError_t dispatch_radius(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
                                    int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, bool use_tc,
-                                   uint32_t *rebuild, cudaStream_t st) {
+                                   uint32_t *rebuild, int64_t shrink_lo, int64_t shrink_hi, cudaStream_t st) {
     switch (radius_bucket_impl(radius)) {
 #define MAXI_CASE(RB) \
-    case RB: return run_unrolled<RB, S, EF>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, rebuild, st);
+    case RB: return run_unrolled<RB, S, EF>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, rebuild, shrink_lo, shrink_hi, st);
         MAXI_CASE(1) MAXI_CASE(2) MAXI_CASE(3) MAXI_CASE(4) MAXI_CASE(6) MAXI_CASE(8) MAXI_CASE(12)
         MAXI_CASE(16) MAXI_CASE(24) MAXI_CASE(32) MAXI_CASE(48) MAXI_CASE(64) MAXI_CASE(96) MAXI_CASE(128)
 #undef MAXI_CASE
@@ -148,7 +159,7 @@ static cudaError_t dispatch_radius(const Volume &v, const void *mask, int mask_f
 template <typename S>
 cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
                               int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, int32_t flags,
-                              cudaStream_t st) {
+                              cudaStream_t st, int64_t shrink_lo, int64_t shrink_hi) {
     // Mask rebuilt from the field each repetition: the caller passes a writable
     // bit-packed copy (the workspace's).
     uint32_t *rebuild = (flags & MAXI_FLAG_MASK_FROM_FIELD) && mask_fmt == MAXI_MASK_BITPACKED
@@ -159,10 +170,10 @@ cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, c
         // kernels narrower than radius 4 (sigma < 1) pass too much of it.
         const bool ef = (flags & MAXI_FLAG_NEAREST_ROUNDING) == 0 && radius >= 4;
         const bool use_tc = (flags & MAXI_FLAG_NO_TENSOR_CORES) == 0 && tc::tc_supported(radius, v.nz, v.ny, v.nx);
-        if (ef) return dispatch_radius<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, rebuild, st);
-        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, rebuild, st);
+        if (ef) return dispatch_radius<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, rebuild, shrink_lo, shrink_hi, st);
+        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, rebuild, shrink_lo, shrink_hi, st);
     } else {
-        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, false, rebuild, st);
+        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, false, rebuild, shrink_lo, shrink_hi, st);
     }
 }
 

@@ -16,8 +16,11 @@ from maxibone_b200.synthetic import random_mask, spheres_mask
 pytestmark = pytest.mark.gpu
 
 
+# Planes of a multiple of 32 voxels take the shrinking plane windows; the others
+# run every repetition over the whole slab.
 @pytest.mark.parametrize("shape,slab,sigma,reps", [((70, 33, 48), 16, 1.5, 3), ((40, 20, 64), 7, 1.0, 5),
-                                                    ((128, 64, 128), 40, 2.0, 2), ((9, 9, 9), 2, 1.0, 1)])
+                                                    ((128, 64, 128), 40, 2.0, 2), ((9, 9, 9), 2, 1.0, 1),
+                                                    ((200, 32, 64), 30, 2.0, 6), ((61, 16, 96), 5, 1.0, 9)])
 def test_out_of_core_equals_in_memory_fp32(shape, slab, sigma, reps):
     mask = random_mask(shape, 0.05, seed=sum(shape))
     kernel = gauss_kernel(sigma).astype(np.float32)
@@ -53,6 +56,32 @@ def test_on_disk_matches_reference_semantics(tmp_path):
     diffusion(str(fin), kernel, str(fout), shape, (10, shape[1], shape[2]), 4)
     got = np.fromfile(fout, dtype=np.uint16).reshape(shape)
     want = oracle.diffusion_on_disk_semantics(mask, kernel, 4)
+    assert np.abs(got.astype(np.int32) - want.astype(np.int32)).max() <= 1
+
+
+@pytest.mark.parametrize("field", ["bf16", "f16"])
+def test_out_of_core_16bit_fields_match_in_memory_field(field):
+    # Shrinking windows (plane of 8192 voxels) on the tensor-core path.
+    shape = (160, 64, 128)
+    mask = spheres_mask(shape, 14, (3, 9), seed=5)
+    kernel = gauss_kernel(2.0).astype(np.float32)
+    got = np.zeros(shape, np.uint16)
+    diffusion_out_of_core(mask, kernel, got, (24, 64, 128), 4, field=field)
+    whole = np.zeros(shape, np.uint16)
+    diffusion_out_of_core(mask, kernel, whole, (160, 64, 128), 4, field=field)
+    assert np.abs(got.astype(np.int32) - whole.astype(np.int32)).max() <= 64
+    assert np.all(got[mask > 0] == 65535)
+
+
+def test_on_disk_shrinking_windows_match_reference_semantics(tmp_path):
+    shape = (64, 32, 48)
+    mask = spheres_mask(shape, 8, (2, 7), seed=4)
+    kernel = gauss_kernel(1.0).astype(np.float32)
+    fin, fout = tmp_path / "mask.uint8", tmp_path / "field.uint16"
+    mask.tofile(fin)
+    diffusion(str(fin), kernel, str(fout), shape, (9, shape[1], shape[2]), 5)
+    got = np.fromfile(fout, dtype=np.uint16).reshape(shape)
+    want = oracle.diffusion_on_disk_semantics(mask, kernel, 5)
     assert np.abs(got.astype(np.int32) - want.astype(np.int32)).max() <= 1
 
 

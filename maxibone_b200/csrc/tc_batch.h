@@ -12,16 +12,18 @@ namespace maxi {
 namespace tc {
 
 // Device-table entry of one volume: tensor maps of the pass inputs
-// ([pass z/y/x][buffer]), the two ping-pong field buffers, the bit-packed
-// mask, the final outputs and the tile counts.
+// ([pass z/y/x][buffer]) and of the y pass's stores ([buffer]), the two
+// ping-pong field buffers, the bit-packed mask, the final outputs and the tile
+// counts (z columns are 128 x-columns wide, y columns 64).
 struct alignas(64) TcVol {
     CUtensorMap map[3][2];
+    CUtensorMap ystore[2];
     void *buf[2];
     const uint32_t *mask;
     uint16_t *out_u16;
     float *field_out;
     int64_t nz, ny, nx;
-    int n_at_z, n_at_y, n_xc, n_xt;
+    int n_at_z, n_at_y, n_xc_z, n_xc_y, n_xt;
     int64_t cols_z, cols_y, tiles_x;
 };
 

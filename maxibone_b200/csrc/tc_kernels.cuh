@@ -1,0 +1,560 @@
+// Tensor-core (tcgen05) pass kernels for 16-bit field storage (BF16 / FP16),
+// shared by the single-volume passes (tc_pass.cu) and the multi-volume
+// persistent passes (tc_batch.cu).  A kernel is written once against a
+// "schedule" that maps the launch's global work index to one volume's column
+// (z / y passes) or tile (x pass): OneVolume* for a single volume whose tensor
+// maps are kernel parameters, ManyVolumes* for a device table of volumes
+// searched through prefix sums.  Both forms run the same instructions on a
+// given tile, so a batch reproduces the single-volume results bit for bit.
+//
+// z / y passes.  A 1-D convolution along an axis is a banded Toeplitz matrix
+// product.  For a tile of 128 consecutive outputs along the axis and TN
+// x-columns:
+//
+//     D[o, x] = sum_j T[o, j] * F[a0 - R + j, x],   T[o, j] = k[j - o] for 0 <= j - o <= 2R
+//
+// M = 128 outputs (TMEM lanes), N = TN x-columns (TMEM columns), K = KP >=
+// 128 + 2R input rows.  T is built once per CTA in shared memory (K-major,
+// 128-byte swizzle); the field tile F arrives by TMA (x contiguous: MN-major,
+// 128-byte swizzle; rows outside the volume are zero-filled by TMA, which is
+// exactly the reference's zero boundary).  Coefficients are split into a high
+// and a low 16-bit part (T = T_hi + T_lo, two MMAs into one FP32 accumulator)
+// so the effective kernel keeps ~16 significant bits and its sum stays 1 to
+// ~1e-6: with single-rounded 16-bit coefficients the kernel's gain error
+// compounds over 3 x R passes.  FP16 coefficients are scaled by 2^10 to stay in
+// the normal range; the epilogue undoes the scale exactly.
+//
+// x pass.  The field is the A operand: 128 volume rows (M, TMEM lanes) x 128
+// x-outputs, so each epilogue thread owns 32 consecutive voxels of one row --
+// the layout re-illumination, error feedback along x and vector stores want.
+// D[r, o] = sum_j F[r, x0 - RA + j] * Tt[j, o] with RA = R rounded up to 8 (TMA
+// x coordinates must be 16-byte aligned); Tt[j, o] = k[j - o - RA + R].  The
+// high and low coefficient halves sit in one K-major operand (rows 0..127
+// Tt_hi, 128..255 Tt_lo); two N = 128 MMAs accumulate both into the same FP32
+// accumulator, so the epilogue reads one value per voxel.
+//
+// Warp roles in a persistent CTA (one per SM): warp 0 issues TMA loads into a
+// tile ring (and L2 prefetches a few tiles ahead), warp 1 issues the MMAs (one
+// thread) into a double-buffered TMEM accumulator, warps 2-9 drain TMEM
+// (tcgen05.ld), narrow to the storage type and store.  With error feedback on,
+// the rounding error of each stored value is carried to its x-neighbour
+// (32-voxel chains along x): the stored field's rounding noise becomes
+// high-pass along x and the next x pass removes it.  Every wait is bounded:
+// on a timeout the kernel records a code in g_tc_error and winds down.
+#pragma once
+
+#include <cudaTypedefs.h>
+
+#include "host_util.h"
+#include "tc_batch.h"
+#include "tc_common.cuh"
+#include "tc_pass.h"
+
+namespace maxi {
+namespace tc {
+
+constexpr int kTM = 128;      // outputs along the axis (z / y) or rows (x) per tile
+constexpr int kXTN = 128;     // x outputs per x-pass tile
+constexpr int kXStages = 2;   // TMA ring depth of the x pass
+constexpr int kPrefetch = 3;  // tiles prefetched into L2 ahead of the ring
+constexpr int kEpiWarps = 8;  // two warps per TMEM lane quadrant, each drains half the columns
+constexpr int kThreads = 64 + 32 * kEpiWarps;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
+
+// z pass: 128-column tiles (256 contiguous bytes per plane row) in a 2-deep
+// ring, stores staged so one instruction writes 8 rows.  y pass: 64-column
+// tiles in a 4-deep ring, TMA bulk stores of each warp's 32 x 32 chunk.
+template <bool AXIS_Z> struct StridedShape {
+    static constexpr int kTN = AXIS_Z ? 128 : 64;
+    static constexpr int kStages = AXIS_Z ? 2 : 4;
+};
+
+// Per-epilogue-warp staging: two 32-row x 32-column 16-bit buffers (z pass:
+// row stride 80 bytes; y pass: the store map's 64-byte swizzle).
+constexpr int kStageWarpBytes = 2 * 32 * 64;
+
+__host__ __device__ constexpr int strided_smem_bytes(int kp, int kpa, int tn, int stages) {
+    return 1024 /*alignment slack*/ + 2 * kpa * kTM * 2 /*T_hi, T_lo*/ + stages * (tn / 64) * kp * 128 /*B ring*/ +
+           1024 /*barriers, TMEM slot*/ + kEpiWarps * kStageWarpBytes;
+}
+
+__host__ __device__ constexpr int contig_smem_bytes_tc(int kp, int kpa) {
+    return 1024 + kpa * 2 * kXTN * 2 /*Tt_hi|Tt_lo, 256 rows*/ + kXStages * (kpa / 64) * kTM * 128 /*A ring*/ + 256;
+}
+
+// Taps and K extents of one pass.
+struct PassTaps {
+    int radius, ra, kp, kpa;  // radius, x-pass left pad, K (multiple of 16), K rounded to 64
+    int error_feedback;
+    float inv_scale;
+    uint16_t hi[2 * kTcMaxRadius + 1];
+    uint16_t lo[2 * kTcMaxRadius + 1];
+};
+
+// One column of a z / y pass: n_at axis tiles of TN x-columns at (x0, oth).
+struct StridedCol {
+    const CUtensorMap *in;       // load map (box 64 x KP along the axis)
+    const CUtensorMap *out_map;  // y pass: store map (box 32 x 32, 64-byte swizzle)
+    void *out;
+    int64_t A, stride_a, stride_o, nx;
+    int n_at, x0, oth;
+};
+
+// One tile of the x pass: 128 rows from r0, 128 x-outputs from x0.
+struct ContigTile {
+    const CUtensorMap *in;       // load map (box 64 x 128 rows)
+    const void *mask;
+    uint16_t *out;               // storage-type field (not final)
+    uint16_t *out_u16;           // final
+    float *field_out;            // final, optional
+    int64_t rows, nx, r0;
+    int x0;
+};
+
+__device__ __forceinline__ int find_volume(const int64_t *prefix, int n_vol, int64_t g) {
+    int lo = 0, hi = n_vol - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---- schedules -------------------------------------------------------------------
+
+struct OneVolumeStrided {
+    static constexpr bool kParamMaps = true;
+    void *out;
+    int64_t A, nx, stride_a, stride_o;
+    int n_at, n_xc, tn;
+    int64_t n_cols;
+    __device__ __forceinline__ int64_t total() const { return n_cols; }
+    __device__ __forceinline__ StridedCol col(int64_t g, const CUtensorMap *in, const CUtensorMap *out_map) const {
+        StridedCol c;
+        c.in = in;
+        c.out_map = out_map;
+        c.out = out;
+        c.A = A;
+        c.stride_a = stride_a;
+        c.stride_o = stride_o;
+        c.nx = nx;
+        c.n_at = n_at;
+        c.x0 = (int) (g % n_xc) * tn;
+        c.oth = (int) (g / n_xc);
+        return c;
+    }
+};
+
+struct ManyVolumesStrided {
+    static constexpr bool kParamMaps = false;
+    const TcVol *vols;
+    const int64_t *prefix;  // n_vol + 1 prefix sums of the volumes' columns
+    int n_vol, axis_z, in_buf, tn;
+    __device__ __forceinline__ int64_t total() const { return __ldg(prefix + n_vol); }
+    __device__ __forceinline__ StridedCol col(int64_t g, const CUtensorMap *, const CUtensorMap *) const {
+        const int v = find_volume(prefix, n_vol, g);
+        const TcVol &vol = vols[v];
+        const int64_t local = g - __ldg(prefix + v);
+        const int n_xc = axis_z ? vol.n_xc_z : vol.n_xc_y;
+        StridedCol c;
+        c.in = &vol.map[axis_z ? 0 : 1][in_buf];
+        c.out_map = &vol.ystore[in_buf ^ 1];
+        c.out = vol.buf[in_buf ^ 1];
+        c.A = axis_z ? vol.nz : vol.ny;
+        c.stride_a = axis_z ? vol.ny * vol.nx : vol.nx;
+        c.stride_o = axis_z ? vol.nx : vol.ny * vol.nx;
+        c.nx = vol.nx;
+        c.n_at = axis_z ? vol.n_at_z : vol.n_at_y;
+        c.x0 = (int) (local % n_xc) * tn;
+        c.oth = (int) (local / n_xc);
+        return c;
+    }
+};
+
+struct OneVolumeContig {
+    static constexpr bool kParamMaps = true;
+    const void *mask;
+    void *out;
+    uint16_t *out_u16;
+    float *field_out;
+    int64_t rows, nx;
+    int n_xt;
+    int64_t n_tiles;
+    __device__ __forceinline__ int64_t total() const { return n_tiles; }
+    __device__ __forceinline__ ContigTile tile(int64_t g, const CUtensorMap *in) const {
+        ContigTile t;
+        t.in = in;
+        t.mask = mask;
+        t.out = static_cast<uint16_t *>(out);
+        t.out_u16 = out_u16;
+        t.field_out = field_out;
+        t.rows = rows;
+        t.nx = nx;
+        t.r0 = (g / n_xt) * kTM;
+        t.x0 = (int) (g % n_xt) * kXTN;
+        return t;
+    }
+};
+
+struct ManyVolumesContig {
+    static constexpr bool kParamMaps = false;
+    const TcVol *vols;
+    const int64_t *prefix;  // n_vol + 1 prefix sums of the volumes' x tiles
+    int n_vol, in_buf;
+    __device__ __forceinline__ int64_t total() const { return __ldg(prefix + n_vol); }
+    __device__ __forceinline__ ContigTile tile(int64_t g, const CUtensorMap *) const {
+        const int v = find_volume(prefix, n_vol, g);
+        const TcVol &vol = vols[v];
+        const int64_t local = g - __ldg(prefix + v);
+        ContigTile t;
+        t.in = &vol.map[2][in_buf];
+        t.mask = vol.mask;
+        t.out = static_cast<uint16_t *>(vol.buf[in_buf ^ 1]);
+        t.out_u16 = vol.out_u16;
+        t.field_out = vol.field_out;
+        t.rows = vol.nz * vol.ny;
+        t.nx = vol.nx;
+        t.r0 = (local / vol.n_xt) * kTM;
+        t.x0 = (int) (local % vol.n_xt) * kXTN;
+        return t;
+    }
+};
+
+template <class Sched> struct StridedLaunch {
+    Sched sched;
+    PassTaps taps;
+};
+
+template <class Sched> struct ContigLaunch {
+    Sched sched;
+    PassTaps taps;
+    int final_pass;
+};
+
+// ---- z / y passes ------------------------------------------------------------------
+
+template <typename S, bool AXIS_Z, class Sched>
+__global__ void __launch_bounds__(kThreads, 1)
+tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmap_out,
+                  const __grid_constant__ StridedLaunch<Sched> p) {
+    constexpr int TN = StridedShape<AXIS_Z>::kTN, STAGES = StridedShape<AXIS_Z>::kStages, CHUNKS = TN / 64;
+    const PassTaps &tp = p.taps;
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    uint8_t *smem = smem_raw + (((raw + 1023) & ~1023u) - raw);
+    uint8_t *t_hi = smem;
+    uint8_t *t_lo = t_hi + tp.kpa * kTM * 2;
+    uint8_t *ring = t_lo + tp.kpa * kTM * 2;
+    const int stage_bytes = CHUNKS * tp.kp * 128;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + STAGES * stage_bytes);
+    uint64_t *full = bars, *empty = bars + STAGES, *tfull = bars + 2 * STAGES, *tempty = bars + 2 * STAGES + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 4);
+    uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 1024;  // 1024-byte aligned
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t total = p.sched.total();
+
+    // Toeplitz operands, K-major with 128-byte swizzle, zero outside the band.
+    for (int e = threadIdx.x; e < kTM * tp.kpa; e += kThreads) {
+        const int o = e / tp.kpa, k = e - o * tp.kpa;
+        const int t = k - o;
+        uint16_t h = 0, l = 0;
+        if (t >= 0 && t <= 2 * tp.radius && k < tp.kp) { h = tp.hi[t]; l = tp.lo[t]; }
+        const uint32_t off = sw128_kmajor_offset(o, k, kTM);
+        *reinterpret_cast<uint16_t *>(t_hi + off) = h;
+        *reinterpret_cast<uint16_t *>(t_lo + off) = l;
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], kEpiWarps); }
+        fence_barrier_init();
+        if (Sched::kParamMaps) prefetch_tmap(&tmap);
+    }
+    __syncwarp();
+    if (warp == 0) {
+        tmem_alloc(tmem_slot, 2 * TN);
+        tmem_relinquish();
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer; L2 prefetch kPrefetch tiles ahead, into this CTA's next column.
+        int64_t tl = 0;
+        bool ok = true;
+        int64_t g = blockIdx.x;
+        StridedCol cur = p.sched.col(g < total ? g : 0, &tmap, &tmap_out), nxt = cur;
+        for (; ok && g < total; g += gridDim.x) {
+            const bool has_next = g + gridDim.x < total;
+            if (has_next) nxt = p.sched.col(g + gridDim.x, &tmap, &tmap_out);
+            for (int at = 0; at < cur.n_at; at++, tl++) {
+                const int s = (int) (tl % STAGES);
+                const uint32_t ph = (uint32_t) ((tl / STAGES) & 1);
+                if (!mbar_wait(&empty[s], ph ^ 1, 1)) { ok = false; break; }
+                {
+                    const int ap = at + kPrefetch;
+                    const CUtensorMap *pm = nullptr;
+                    int px = 0, po = 0, pa = 0;
+                    if (ap < cur.n_at) { pm = cur.in; px = cur.x0; po = cur.oth; pa = ap; }
+                    else if (has_next && ap - cur.n_at < nxt.n_at) { pm = nxt.in; px = nxt.x0; po = nxt.oth; pa = ap - cur.n_at; }
+                    if (pm) {
+                        for (int c = 0; c < CHUNKS; c++) {
+                            if (AXIS_Z) tma_prefetch_3d(pm, px + 64 * c, po, pa * kTM - tp.radius);
+                            else tma_prefetch_3d(pm, px + 64 * c, pa * kTM - tp.radius, po);
+                        }
+                    }
+                }
+                const int a_in = at * kTM - tp.radius;
+                mbar_arrive_expect_tx(&full[s], stage_bytes);
+                for (int c = 0; c < CHUNKS; c++) {
+                    uint8_t *dst = ring + s * stage_bytes + c * tp.kp * 128;
+                    if (AXIS_Z) tma_load_3d(dst, cur.in, cur.x0 + 64 * c, cur.oth, a_in, &full[s]);
+                    else tma_load_3d(dst, cur.in, cur.x0 + 64 * c, a_in, cur.oth, &full[s]);
+                }
+            }
+            cur = nxt;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer.
+        const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
+        const uint32_t idesc = idesc_f16(fmt, 0 /*A K-major*/, 1 /*B MN-major*/, kTM, TN);
+        const uint32_t a_hi = smem_u32(t_hi), a_lo = smem_u32(t_lo), b0 = smem_u32(ring);
+        int64_t tl = 0;
+        bool ok = true;
+        for (int64_t g = blockIdx.x; ok && g < total; g += gridDim.x) {
+            const int n_at = p.sched.col(g, &tmap, &tmap_out).n_at;
+            for (int at = 0; at < n_at; at++, tl++) {
+                const int s = (int) (tl % STAGES);
+                const uint32_t ph = (uint32_t) ((tl / STAGES) & 1);
+                const int d = (int) (tl & 1);
+                const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
+                if (!mbar_wait(&full[s], ph, 1) || !mbar_wait(&tempty[d], dph ^ 1, 3)) { ok = false; break; }
+                tc_fence_after();
+                const uint32_t dt = tmem + d * TN;
+                for (int ks = 0; ks < tp.kp / 16; ks++) {
+                    const uint32_t koff = (ks >> 2) * (kTM * 128) + (ks & 3) * 32;
+                    const uint64_t bd = smem_desc_sw128(b0 + s * stage_bytes + ks * 2048, tp.kp * 128, 1024);
+                    umma_f16(dt, smem_desc_sw128(a_hi + koff, 16, 1024), bd, idesc, ks > 0 ? 1u : 0u);
+                    umma_f16(dt, smem_desc_sw128(a_lo + koff, 16, 1024), bd, idesc, 1u);
+                }
+                umma_commit(&empty[s]);
+                umma_commit(&tfull[d]);
+            }
+        }
+    } else if (warp >= 2) {
+        // Epilogue: TMEM -> registers -> storage type -> global.
+        const int quad = warp & 3;           // TMEM lane quadrant this warp may access
+        const int half = (warp - 2) >> 2;    // which half of the columns it drains
+        uint8_t *stg = stage_out + (warp - 2) * kStageWarpBytes;
+        int sbuf = 0;
+        int64_t tl = 0;
+        bool ok = true;
+        for (int64_t g = blockIdx.x; ok && g < total; g += gridDim.x) {
+            const StridedCol c = p.sched.col(g, &tmap, &tmap_out);
+            S *out = static_cast<S *>(c.out);
+            for (int at = 0; at < c.n_at; at++, tl++) {
+                const int d = (int) (tl & 1);
+                const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
+                if (!mbar_wait(&tfull[d], dph, 2)) { ok = false; break; }
+                tc_fence_after();
+                const int c0 = half * CHUNKS;  // this warp's 32-column chunks
+                const uint32_t tbase = tmem + ((uint32_t) (quad * 32) << 16) + d * TN;
+#pragma unroll
+                for (int cc = 0; cc < CHUNKS; cc++) {
+                    float va[32];
+                    __syncwarp();
+                    tmem_ld32(tbase + (c0 + cc) * 32, va);
+                    uint16_t q[32];
+                    narrow32<S>(va, tp.inv_scale, tp.error_feedback, q);
+                    const int64_t xb = (int64_t) c.x0 + (c0 + cc) * 32;
+                    if (AXIS_Z) {
+                        // z pass: lanes' rows lie on different planes (2 MB apart at 1024^2);
+                        // stage the 32 x 32 chunk and write 8 rows (8 x 64 bytes) per instruction.
+                        __syncwarp();
+#pragma unroll
+                        for (int i = 0; i < 4; i++) *reinterpret_cast<uint4 *>(stg + lane * 80 + i * 16) = pack8(q + 8 * i);
+                        __syncwarp();
+                        const int sub = lane & 3, rsub = lane >> 2;
+#pragma unroll
+                        for (int r4 = 0; r4 < 4; r4++) {
+                            const int rr = r4 * 8 + rsub;
+                            const int64_t ar = (int64_t) at * kTM + quad * 32 + rr;
+                            const uint4 w = *reinterpret_cast<const uint4 *>(stg + rr * 80 + sub * 16);
+                            if (ar < c.A && xb + sub * 8 < c.nx)
+                                *reinterpret_cast<uint4 *>(out + ar * c.stride_a + (int64_t) c.oth * c.stride_o + xb +
+                                                           sub * 8) = w;
+                        }
+                    } else {
+                        // y pass: TMA store of the warp's 32 rows x 32 columns (64-byte swizzle of
+                        // the store map; the map clips rows and columns outside the volume).
+                        if (lane == 0) bulk_wait_read<1>();  // the store issued two chunks ago has read this buffer
+                        __syncwarp();
+                        uint8_t *sb = stg + sbuf * 2048;
+#pragma unroll
+                        for (int i = 0; i < 4; i++)
+                            *reinterpret_cast<uint4 *>(sb + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) = pack8(q + 8 * i);
+                        fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0) {
+                            tma_store_3d(c.out_map, sb, (int) xb, at * kTM + quad * 32, c.oth);
+                            bulk_commit();
+                        }
+                        sbuf ^= 1;
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[d]);
+            }
+        }
+    }
+    if (!AXIS_Z && warp >= 2 && lane == 0) bulk_wait_all();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 2 * TN);
+    }
+}
+
+// ---- x pass ------------------------------------------------------------------------
+
+template <typename S, int FMT, class Sched>
+__global__ void __launch_bounds__(kThreads, 1)
+tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ ContigLaunch<Sched> p) {
+    const PassTaps &tp = p.taps;
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    uint8_t *smem = smem_raw + (((raw + 1023) & ~1023u) - raw);
+    uint8_t *tt = smem;                                  // K-major, 256 rows (hi 0..127, lo 128..255)
+    uint8_t *ring = tt + tp.kpa * 2 * kXTN * 2;
+    const int nkb = tp.kpa / 64;                         // 64-wide x boxes per stage
+    const int stage_bytes = nkb * kTM * 128;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kXStages * stage_bytes);
+    uint64_t *full = bars, *empty = bars + kXStages, *tfull = bars + 2 * kXStages, *tempty = bars + 2 * kXStages + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kXStages + 4);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t total = p.sched.total();
+
+    for (int e = threadIdx.x; e < 2 * kXTN * tp.kpa; e += kThreads) {
+        const int n = e / tp.kpa, j = e - n * tp.kpa;
+        const int o = n & (kXTN - 1);
+        const int t = j - o - tp.ra + tp.radius;  // tap index 0..2R
+        uint16_t v = 0;
+        if (t >= 0 && t <= 2 * tp.radius && j < tp.kp) v = n < kXTN ? tp.hi[t] : tp.lo[t];
+        *reinterpret_cast<uint16_t *>(tt + sw128_kmajor_offset(n, j, 2 * kXTN)) = v;
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kXStages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], kEpiWarps); }
+        fence_barrier_init();
+        if (Sched::kParamMaps) prefetch_tmap(&tmap);
+    }
+    __syncwarp();
+    if (warp == 0) {
+        tmem_alloc(tmem_slot, 2 * kXTN);
+        tmem_relinquish();
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        int64_t tl = 0;
+        for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
+            const int s = (int) (tl % kXStages);
+            const uint32_t ph = (uint32_t) ((tl / kXStages) & 1);
+            if (!mbar_wait(&empty[s], ph ^ 1, 1)) break;
+            const int64_t gp = g + kPrefetch * (int64_t) gridDim.x;
+            if (gp < total) {
+                const ContigTile t = p.sched.tile(gp, &tmap);
+                for (int kb = 0; kb < nkb; kb++) tma_prefetch_3d(t.in, t.x0 - tp.ra + 64 * kb, (int) t.r0, 0);
+            }
+            const ContigTile t = p.sched.tile(g, &tmap);
+            mbar_arrive_expect_tx(&full[s], stage_bytes);
+            for (int kb = 0; kb < nkb; kb++)
+                tma_load_3d(ring + s * stage_bytes + kb * kTM * 128, t.in, t.x0 - tp.ra + 64 * kb, (int) t.r0, 0, &full[s]);
+        }
+    } else if (warp == 1 && lane == 0) {
+        const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
+        const uint32_t idesc = idesc_f16(fmt, 0 /*A K-major*/, 0 /*B K-major*/, kTM, kXTN);
+        const uint32_t a0 = smem_u32(ring), b0 = smem_u32(tt);
+        int64_t tl = 0;
+        for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
+            const int s = (int) (tl % kXStages);
+            const uint32_t ph = (uint32_t) ((tl / kXStages) & 1);
+            const int d = (int) (tl & 1);
+            const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
+            if (!mbar_wait(&full[s], ph, 1) || !mbar_wait(&tempty[d], dph ^ 1, 3)) break;
+            tc_fence_after();
+            const uint32_t dt = tmem + d * kXTN;
+            for (int ks = 0; ks < tp.kp / 16; ks++) {
+                const uint32_t kin = (ks & 3) * 32;
+                const uint64_t ad = smem_desc_sw128(a0 + s * stage_bytes + (ks >> 2) * (kTM * 128) + kin, 16, 1024);
+                const uint32_t bhi = b0 + (ks >> 2) * (2 * kXTN * 128) + kin;  // rows 0..127: Tt_hi
+                umma_f16(dt, ad, smem_desc_sw128(bhi, 16, 1024), idesc, ks > 0 ? 1u : 0u);
+                umma_f16(dt, ad, smem_desc_sw128(bhi + kXTN * 128, 16, 1024), idesc, 1u);  // rows 128..255: Tt_lo
+            }
+            umma_commit(&empty[s]);
+            umma_commit(&tfull[d]);
+        }
+    } else if (warp >= 2) {
+        const int quad = warp & 3;
+        const int half = (warp - 2) >> 2;
+        const int r = quad * 32 + lane;
+        int64_t tl = 0;
+        for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
+            const ContigTile t = p.sched.tile(g, &tmap);
+            const int d = (int) (tl & 1);
+            const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
+            if (!mbar_wait(&tfull[d], dph, 2)) break;
+            tc_fence_after();
+            const int64_t row = t.r0 + r;
+            const int64_t xa = t.x0 + half * 64;  // this warp's 64 voxels of the row
+            // Mask flags fetched before the TMEM loads.
+            uint32_t mw[2];
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                const int64_t xb = xa + cc * 32;
+                mw[cc] = (row < t.rows && xb < t.nx)
+                             ? row_mask32<FMT>(t.mask, row * t.nx + xb, t.nx - xb < 32 ? (int) (t.nx - xb) : 32,
+                                               t.rows * t.nx)
+                             : 0u;
+            }
+            float ha[32], hb[32];
+            __syncwarp();
+            const uint32_t ta = tmem + ((uint32_t) (quad * 32) << 16) + d * kXTN + half * 64;
+            tmem_ld32(ta, ha);
+            tmem_ld32(ta + 32, hb);
+            contig_epilogue64<S>(ha, hb, mw[0], mw[1], row, t.rows, t.nx, xa, tp.inv_scale, tp.error_feedback,
+                                 p.final_pass, t.out, t.out_u16, t.field_out);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[d]);
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 2 * kXTN);
+    }
+}
+
+// Fills the taps of one pass: hi/lo halves of kernel x scale (1 for BF16, 2^10 for FP16).
+inline void fill_pass_taps(PassTaps &t, const float *kernel, int radius, int ra, int kp, bool is_bf16,
+                           bool error_feedback) {
+    t.radius = radius;
+    t.ra = ra;
+    t.kp = kp;
+    t.kpa = (int) round_up(kp, 64);
+    t.error_feedback = error_feedback ? 1 : 0;
+    const float scale = is_bf16 ? 1.0f : 1024.0f;
+    t.inv_scale = 1.0f / scale;
+    tc_split_taps(kernel, radius, is_bf16, scale, t.hi, t.lo);
+}
+
+}  // namespace tc
+}  // namespace maxi

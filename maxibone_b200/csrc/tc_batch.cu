@@ -106,7 +106,7 @@ cudaError_t tc_batch_pass(const TcVol *d_vols, const int64_t *d_prefix, int64_t 
         p.sched.axis_z = axis_z ? 1 : 0;
         p.sched.in_buf = in_buf;
         p.sched.tn = axis_z ? StridedShape<true>::kTN : StridedShape<false>::kTN;
-        const int smem = strided_smem_bytes(p.taps.kp, p.taps.kpa, p.sched.tn,
+        const int smem = strided_smem_bytes(p.taps.kp, p.sched.tn,
                                             axis_z ? StridedShape<true>::kStages : StridedShape<false>::kStages);
         auto *k = axis_z ? (is_bf16 ? tc_strided_kernel<__nv_bfloat16, true, ManyVolumesStrided>
                                     : tc_strided_kernel<__half, true, ManyVolumesStrided>)

@@ -14,8 +14,11 @@
 //     D[o, x] = sum_j T[o, j] * F[a0 - R + j, x],   T[o, j] = k[j - o] for 0 <= j - o <= 2R
 //
 // M = 128 outputs (TMEM lanes), N = TN x-columns (TMEM columns), K = KP >=
-// 128 + 2R input rows.  T is built once per CTA in shared memory (K-major,
-// 128-byte swizzle); the field tile F arrives by TMA (x contiguous: MN-major,
+// 128 + 2R input rows.  T is written once per CTA into tensor memory (the A
+// operand of tcgen05.mma may live there: row o in lane o, K packed two per
+// column), so the MMAs read only the field tile from shared memory -- with
+// both operands in shared memory the MMAs' operand reads, not HBM, set the
+// pass time.  The field tile F arrives by TMA (x contiguous: MN-major,
 // 128-byte swizzle; rows outside the volume are zero-filled by TMA, which is
 // exactly the reference's zero boundary).  Coefficients are split into a high
 // and a low 16-bit part (T = T_hi + T_lo, two MMAs into one FP32 accumulator)
@@ -60,21 +63,27 @@ constexpr int kPrefetch = 3;  // tiles prefetched into L2 ahead of the ring
 constexpr int kEpiWarps = 8;  // two warps per TMEM lane quadrant, each drains half the columns
 constexpr int kThreads = 64 + 32 * kEpiWarps;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
 
-// z pass: 128-column tiles (256 contiguous bytes per plane row) in a 2-deep
-// ring, stores staged so one instruction writes 8 rows.  y pass: 64-column
-// tiles in a 4-deep ring, TMA bulk stores of each warp's 32 x 32 chunk.
+// z pass: 64-column tiles in an 8-deep ring (its loads gather one 128-byte
+// row from each of KP planes, so it wants many tiles in flight), stores
+// staged so one instruction writes 8 rows.  y pass: 128-column tiles in a
+// 3-deep ring, TMA bulk stores of each warp's 32 x 32 chunks.
 template <bool AXIS_Z> struct StridedShape {
-    static constexpr int kTN = AXIS_Z ? 128 : 64;
-    static constexpr int kStages = AXIS_Z ? 2 : 4;
+    static constexpr int kTN = AXIS_Z ? 64 : 128;
+    static constexpr int kStages = AXIS_Z ? 8 : 3;
 };
+
+// Tensor-memory columns of the strided passes: accumulators [0, 2 TN), the
+// Toeplitz halves at kTmemAHi / kTmemALo (K / 2 <= 96 columns each).
+constexpr uint32_t kTmemAHi = 256, kTmemALo = 352, kTmemColsStrided = 512;
+static_assert(kTM + 2 * kTcMaxRadius <= 2 * 96, "the Toeplitz halves hold K <= 192");
 
 // Per-epilogue-warp staging: two 32-row x 32-column 16-bit buffers (z pass:
 // row stride 80 bytes; y pass: the store map's 64-byte swizzle).
 constexpr int kStageWarpBytes = 2 * 32 * 64;
 
-__host__ __device__ constexpr int strided_smem_bytes(int kp, int kpa, int tn, int stages) {
-    return 1024 /*alignment slack*/ + 2 * kpa * kTM * 2 /*T_hi, T_lo*/ + stages * (tn / 64) * kp * 128 /*B ring*/ +
-           1024 /*barriers, TMEM slot*/ + kEpiWarps * kStageWarpBytes;
+__host__ __device__ constexpr int strided_smem_bytes(int kp, int tn, int stages) {
+    return 1024 /*alignment slack*/ + stages * (tn / 64) * kp * 128 /*B ring*/ + 1024 /*barriers, TMEM slot*/ +
+           kEpiWarps * kStageWarpBytes;
 }
 
 __host__ __device__ constexpr int contig_smem_bytes_tc(int kp, int kpa) {
@@ -241,10 +250,7 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
     const PassTaps &tp = p.taps;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
-    uint8_t *smem = smem_raw + (((raw + 1023) & ~1023u) - raw);
-    uint8_t *t_hi = smem;
-    uint8_t *t_lo = t_hi + tp.kpa * kTM * 2;
-    uint8_t *ring = t_lo + tp.kpa * kTM * 2;
+    uint8_t *ring = smem_raw + (((raw + 1023) & ~1023u) - raw);
     const int stage_bytes = CHUNKS * tp.kp * 128;
     uint64_t *bars = reinterpret_cast<uint64_t *>(ring + STAGES * stage_bytes);
     uint64_t *full = bars, *empty = bars + STAGES, *tfull = bars + 2 * STAGES, *tempty = bars + 2 * STAGES + 2;
@@ -253,16 +259,6 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t total = p.sched.total();
 
-    // Toeplitz operands, K-major with 128-byte swizzle, zero outside the band.
-    for (int e = threadIdx.x; e < kTM * tp.kpa; e += kThreads) {
-        const int o = e / tp.kpa, k = e - o * tp.kpa;
-        const int t = k - o;
-        uint16_t h = 0, l = 0;
-        if (t >= 0 && t <= 2 * tp.radius && k < tp.kp) { h = tp.hi[t]; l = tp.lo[t]; }
-        const uint32_t off = sw128_kmajor_offset(o, k, kTM);
-        *reinterpret_cast<uint16_t *>(t_hi + off) = h;
-        *reinterpret_cast<uint16_t *>(t_lo + off) = l;
-    }
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], kEpiWarps); }
@@ -271,7 +267,7 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
     }
     __syncwarp();
     if (warp == 0) {
-        tmem_alloc(tmem_slot, 2 * TN);
+        tmem_alloc(tmem_slot, kTmemColsStrided);
         tmem_relinquish();
     }
     fence_proxy_async_smem();
@@ -279,6 +275,31 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
+    if (warp >= 2) {
+        // Toeplitz halves into tensor memory, zero outside the band: the two
+        // warps of a lane quadrant write T_hi and T_lo of its 32 rows.
+        const int quad = warp & 3, lo_half = (warp - 2) >> 2;
+        const int o = quad * 32 + lane;
+        const uint16_t *taps = lo_half ? tp.lo : tp.hi;
+        for (int ch = 0; ch < 3; ch++) {
+            uint32_t r[32];
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                uint32_t v = 0;
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int k = 2 * (ch * 32 + j) + e, t = k - o;
+                    if (t >= 0 && t <= 2 * tp.radius && k < tp.kp) v |= (uint32_t) taps[t] << (16 * e);
+                }
+                r[j] = v;
+            }
+            tmem_st32(tmem + ((uint32_t) (quad * 32) << 16) + (lo_half ? kTmemALo : kTmemAHi) + ch * 32, r);
+        }
+        tmem_st_wait();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
 
     if (warp == 0 && lane == 0) {
         // TMA producer; L2 prefetch kPrefetch tiles ahead, into this CTA's next column.
@@ -320,7 +341,7 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
         // MMA issuer.
         const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
         const uint32_t idesc = idesc_f16(fmt, 0 /*A K-major*/, 1 /*B MN-major*/, kTM, TN);
-        const uint32_t a_hi = smem_u32(t_hi), a_lo = smem_u32(t_lo), b0 = smem_u32(ring);
+        const uint32_t b0 = smem_u32(ring);
         int64_t tl = 0;
         bool ok = true;
         for (int64_t g = blockIdx.x; ok && g < total; g += gridDim.x) {
@@ -333,11 +354,12 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                 if (!mbar_wait(&full[s], ph, 1) || !mbar_wait(&tempty[d], dph ^ 1, 3)) { ok = false; break; }
                 tc_fence_after();
                 const uint32_t dt = tmem + d * TN;
+                // K step ks: 16 rows of the field tile (2048 bytes on, i.e. +128 in the
+                // descriptor's address field) and 8 tensor-memory columns of T.
+                const uint64_t bd = smem_desc_sw128(b0 + s * stage_bytes, tp.kp * 128, 1024);
                 for (int ks = 0; ks < tp.kp / 16; ks++) {
-                    const uint32_t koff = (ks >> 2) * (kTM * 128) + (ks & 3) * 32;
-                    const uint64_t bd = smem_desc_sw128(b0 + s * stage_bytes + ks * 2048, tp.kp * 128, 1024);
-                    umma_f16(dt, smem_desc_sw128(a_hi + koff, 16, 1024), bd, idesc, ks > 0 ? 1u : 0u);
-                    umma_f16(dt, smem_desc_sw128(a_lo + koff, 16, 1024), bd, idesc, 1u);
+                    umma_f16_ts(dt, tmem + kTmemAHi + ks * 8, bd + (uint64_t) (ks * 128), idesc, ks > 0 ? 1u : 0u);
+                    umma_f16_ts(dt, tmem + kTmemALo + ks * 8, bd + (uint64_t) (ks * 128), idesc, 1u);
                 }
                 umma_commit(&empty[s]);
                 umma_commit(&tfull[d]);
@@ -397,7 +419,7 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                             *reinterpret_cast<uint4 *>(sb + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) = pack8(q + 8 * i);
                         fence_proxy_async_smem();
                         __syncwarp();
-                        if (lane == 0) {
+                        if (lane == 0 && xb < c.nx && at * kTM + quad * 32 < c.A) {
                             tma_store_3d(c.out_map, sb, (int) xb, at * kTM + quad * 32, c.oth);
                             bulk_commit();
                         }
@@ -414,7 +436,7 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        tmem_dealloc(tmem, 2 * TN);
+        tmem_dealloc(tmem, kTmemColsStrided);
     }
 }
 

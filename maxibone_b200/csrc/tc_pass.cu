@@ -85,7 +85,7 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
     }
-    const int smem = strided_smem_bytes(p.taps.kp, p.taps.kpa, tn, stages);
+    const int smem = strided_smem_bytes(p.taps.kp, tn, stages);
     auto *kern = axis_z ? tc_strided_kernel<S, true, OneVolumeStrided> : tc_strided_kernel<S, false, OneVolumeStrided>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;

@@ -114,9 +114,10 @@ static cudaError_t enqueue_group_tc(maxi_batch_plan *p, TcGroup &g, cudaStream_t
     int in = 0;
     for (int64_t rep = 0; rep < g.reps; rep++) {
         const bool last = rep + 1 == g.reps;
-        if ((e = tc::tc_batch_pass(g.d_vols, g.d_prefix, g.totals[0], n, 0, in, false, g.kernel.data(), g.geo, bf16, ef, st)) != cudaSuccess ||
-            (e = tc::tc_batch_pass(g.d_vols, g.d_prefix + (n + 1), g.totals[1], n, 1, in ^ 1, false, g.kernel.data(), g.geo, bf16, ef, st)) != cudaSuccess ||
-            (e = tc::tc_batch_pass(g.d_vols, g.d_prefix + 2 * (n + 1), g.totals[2], n, 2, in, last, g.kernel.data(), g.geo, bf16, ef, st)) != cudaSuccess)
+        // The x pass hands the next repetition its field in [y][z][x] row order.
+        if ((e = tc::tc_batch_pass(g.d_vols, g.d_prefix, g.totals[0], n, 0, in, false, g.kernel.data(), g.geo, bf16, ef, rep > 0, st)) != cudaSuccess ||
+            (e = tc::tc_batch_pass(g.d_vols, g.d_prefix + (n + 1), g.totals[1], n, 1, in ^ 1, false, g.kernel.data(), g.geo, bf16, ef, false, st)) != cudaSuccess ||
+            (e = tc::tc_batch_pass(g.d_vols, g.d_prefix + 2 * (n + 1), g.totals[2], n, 2, in, last, g.kernel.data(), g.geo, bf16, ef, true, st)) != cudaSuccess)
             return e;
         in ^= 1;
     }

@@ -28,7 +28,7 @@ TcGeometry tc_geometry(int radius) {
     return g;
 }
 
-// Fills the tile counts and the eight tensor maps of one volume.
+// Fills the tile counts and the ten tensor maps of one volume.
 int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_mask, uint16_t *out_u16,
                    float *field_out, int64_t nz, int64_t ny, int64_t nx, bool is_bf16, const TcGeometry &g) {
     vol = TcVol{};
@@ -60,6 +60,9 @@ int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_ma
         const cuuint64_t sx[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (nx * nz * ny * 2)};
         const cuuint32_t boxx[3] = {64u, (cuuint32_t) kTM, 1u};
         const cuuint32_t boxs[3] = {32u, 32u, 1u};
+        const cuuint64_t dr[3] = {(cuuint64_t) nx, (cuuint64_t) nz, (cuuint64_t) ny};
+        const cuuint64_t sr[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (nz * nx * 2)};
+        const cuuint32_t boxr[3] = {64u, (cuuint32_t) g.kp_strided, 1u};
         if (enc(&vol.map[0][b], dt, 3, base, d3, s3, boxz, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
             enc(&vol.map[1][b], dt, 3, base, d3, s3, boxy, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -67,7 +70,9 @@ int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_ma
             enc(&vol.map[2][b], dt, 3, base, dx, sx, boxx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
             enc(&vol.ystore[b], dt, 3, base, d3, s3, boxs, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
+            enc(&vol.zrows[b], dt, 3, base, dr, sr, boxr, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return -1;
     }
     return 0;
@@ -75,7 +80,7 @@ int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_ma
 
 cudaError_t tc_batch_pass(const TcVol *d_vols, const int64_t *d_prefix, int64_t total, int n_vol, int pass, int in_buf,
                           bool final_pass, const float *kernel, const TcGeometry &g, bool is_bf16, bool error_feedback,
-                          cudaStream_t st) {
+                          bool rows_yz, cudaStream_t st) {
     if (total == 0) return cudaSuccess;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -91,11 +96,12 @@ cudaError_t tc_batch_pass(const TcVol *d_vols, const int64_t *d_prefix, int64_t 
         p.sched.prefix = d_prefix;
         p.sched.n_vol = n_vol;
         p.sched.in_buf = in_buf;
+        p.sched.out_rows = (rows_yz && !final_pass) ? 1 : 0;
         const int smem = contig_smem_bytes_tc(p.taps.kp, p.taps.kpa);
         auto *k = is_bf16 ? tc_contig_kernel<__nv_bfloat16, MAXI_MASK_BITPACKED, ManyVolumesContig>
                           : tc_contig_kernel<__half, MAXI_MASK_BITPACKED, ManyVolumesContig>;
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-        k<<<grid, kThreads, smem, st>>>(unused, p);
+        k<<<grid, kXThreads, smem, st>>>(unused, p);
     } else {
         const bool axis_z = pass == 0;
         StridedLaunch<ManyVolumesStrided> p{};
@@ -105,6 +111,7 @@ cudaError_t tc_batch_pass(const TcVol *d_vols, const int64_t *d_prefix, int64_t 
         p.sched.n_vol = n_vol;
         p.sched.axis_z = axis_z ? 1 : 0;
         p.sched.in_buf = in_buf;
+        p.sched.z_in_rows = (axis_z && rows_yz) ? 1 : 0;
         p.sched.tn = axis_z ? StridedShape<true>::kTN : StridedShape<false>::kTN;
         const int smem = strided_smem_bytes(p.taps.kp, p.sched.tn,
                                             axis_z ? StridedShape<true>::kStages : StridedShape<false>::kStages);

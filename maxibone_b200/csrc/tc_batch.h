@@ -12,12 +12,14 @@ namespace maxi {
 namespace tc {
 
 // Device-table entry of one volume: tensor maps of the pass inputs
-// ([pass z/y/x][buffer]) and of the y pass's stores ([buffer]), the two
+// ([pass z/y/x][buffer]), of the y pass's stores and of the z pass's input in
+// [y][z][x] row order ([buffer]), the two
 // ping-pong field buffers, the bit-packed mask, the final outputs and the tile
-// counts (z columns are 128 x-columns wide, y columns 64).
+// counts.
 struct alignas(64) TcVol {
     CUtensorMap map[3][2];
     CUtensorMap ystore[2];
+    CUtensorMap zrows[2];  // z-pass input read as [y][z][x] rows ([buffer])
     void *buf[2];
     const uint32_t *mask;
     uint16_t *out_u16;
@@ -42,9 +44,11 @@ int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_ma
 
 // One pass (0 z, 1 y, 2 x) over all volumes of a device table; d_prefix holds
 // n_vol + 1 prefix sums of the volumes' columns (z: cols_z, y: cols_y) or x tiles.
+// rows_yz: the z pass reads its input as [y][z][x] rows, the x pass (not
+// final) writes its output in that order.
 cudaError_t tc_batch_pass(const TcVol *d_vols, const int64_t *d_prefix, int64_t total, int n_vol, int pass, int in_buf,
                           bool final_pass, const float *kernel, const TcGeometry &g, bool is_bf16, bool error_feedback,
-                          cudaStream_t st);
+                          bool rows_yz, cudaStream_t st);
 
 int tc_batch_read_and_clear_error();
 

@@ -218,29 +218,28 @@ template <> struct Narrow16<__half> {
     static __device__ __forceinline__ float widen(uint16_t q) { return __half2float(__ushort_as_half(q)); }
 };
 
-// Narrows two 32-voxel chunks (64 consecutive x voxels) to the 16-bit storage
-// type.  With `ef`, rounding errors are carried along x in four interleaved
-// chains of 16 voxels (independent carries give the scheduler four
-// instruction streams instead of one serial chain).  Voxels whose mask bit is
-// set are stored as exactly 1.0 and restart their chain.  `scale` undoes the
-// coefficient scaling of the MMA.
+// Narrows one 32-voxel chunk (32 consecutive x voxels) to the 16-bit storage
+// type.  With `ef`, rounding errors are carried along x in two interleaved
+// chains of 16 voxels (independent carries give the scheduler two instruction
+// streams instead of one serial chain).  Voxels whose mask bit is set are
+// stored as exactly 1.0; 1.0 is exact in both storage types, so such a voxel
+// also hands a zero carry to its neighbour.  `scale` undoes the coefficient
+// scaling of the MMA.
 template <typename S>
-__device__ __forceinline__ void narrow64(const float (&a)[32], const float (&b)[32], uint32_t ma, uint32_t mb,
-                                         float scale, bool ef, uint16_t (&qa)[32], uint16_t (&qb)[32]) {
-    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+__device__ __forceinline__ void narrow32_masked(const float (&a)[32], uint32_t ma, float scale, bool ef,
+                                                uint16_t (&qa)[32]) {
+    float c[2] = {0.0f, 0.0f};
 #pragma unroll
     for (int j = 0; j < 16; j++) {
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const int i = (k & 1) * 16 + j;
-            const float v = k < 2 ? a[i] : b[i];
-            const bool mk = ((k < 2 ? ma : mb) >> i) & 1u;
-            const float w = mk ? 1.0f : (ef ? fmaf(v, scale, c[k]) : v * scale);
+        for (int k = 0; k < 2; k++) {
+            const int i = k * 16 + j;
+            const bool mk = (ma >> i) & 1u;
+            const float w = mk ? 1.0f : (ef ? fmaf(a[i], scale, c[k]) : a[i] * scale);
             float dummy = 0.0f;
             const uint16_t q = Narrow16<S>::bits(w, dummy, false);
-            if (ef) c[k] = mk ? 0.0f : w - Narrow16<S>::widen(q);
-            if (k < 2) qa[i] = q;
-            else qb[i] = q;
+            if (ef) c[k] = w - Narrow16<S>::widen(q);
+            qa[i] = q;
         }
     }
 }
@@ -285,52 +284,32 @@ __device__ __forceinline__ void store32_u16(uint16_t *dst, const uint16_t (&q)[3
     }
 }
 
-// x-pass epilogue of one thread: 64 consecutive voxels of one row (chunks a
-// and b starting at x = xa and xa + 32) -- re-illumination, then either the
-// 16-bit field with error-feedback rounding, or (last repetition) the uint16
-// output and the FP32 field.  Requires nx % 8 == 0 and 16-byte aligned outputs.
-template <typename S>
-__device__ __forceinline__ void contig_epilogue64(const float (&ha)[32], const float (&hb)[32], uint32_t ma,
-                                                  uint32_t mb, int64_t row, int64_t rows, int64_t nx, int64_t xa,
-                                                  float scale, bool ef, bool final_pass, uint16_t *field,
-                                                  uint16_t *out_u16, float *field_out) {
-    if (row >= rows) return;
-    if (!final_pass) {
-        uint16_t qa[32], qb[32];
-        narrow64<S>(ha, hb, ma, mb, scale, ef, qa, qb);
+// Last-repetition x-pass epilogue of one thread: 32 consecutive voxels of
+// one row from x = xb -- re-illumination, then the uint16 output and the FP32
+// field (either may be NULL).  Requires nx % 8 == 0 and 16-byte aligned outputs.
+__device__ __forceinline__ void contig_final32(const float (&h)[32], uint32_t m, int64_t row, int64_t rows,
+                                               int64_t nx, int64_t xb, float scale, uint16_t *out_u16,
+                                               float *field_out) {
+    if (row >= rows || xb >= nx) return;
+    const int count = nx - xb < 32 ? (int) (nx - xb) : 32;
+    const int64_t idx = row * nx + xb;
+    float v[32];
+    uint16_t q[32];
 #pragma unroll
-        for (int cc = 0; cc < 2; cc++) {
-            const int64_t xb = xa + cc * 32;
-            if (xb >= nx) continue;
-            store32_u16(field + row * nx + xb, cc ? qb : qa, nx - xb < 32 ? (int) (nx - xb) : 32);
-        }
-        return;
+    for (int i = 0; i < 32; i++) {
+        v[i] = ((m >> i) & 1u) ? 1.0f : h[i] * scale;
+        q[i] = quantise_u16(v[i]);
     }
+    if (out_u16) store32_u16(out_u16 + idx, q, count);
+    if (field_out) {
+        if (count == 32) {
 #pragma unroll
-    for (int cc = 0; cc < 2; cc++) {
-        const int64_t xb = xa + cc * 32;
-        if (xb >= nx) continue;
-        const int count = nx - xb < 32 ? (int) (nx - xb) : 32;
-        const int64_t idx = row * nx + xb;
-        const uint32_t m = cc ? mb : ma;
-        float v[32];
-        uint16_t q[32];
+            for (int i = 0; i < 32; i += 4)
+                *reinterpret_cast<float4 *>(field_out + idx + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+        } else {
 #pragma unroll
-        for (int i = 0; i < 32; i++) {
-            v[i] = ((m >> i) & 1u) ? 1.0f : (cc ? hb[i] : ha[i]) * scale;
-            q[i] = quantise_u16(v[i]);
-        }
-        if (out_u16) store32_u16(out_u16 + idx, q, count);
-        if (field_out) {
-            if (count == 32) {
-#pragma unroll
-                for (int i = 0; i < 32; i += 4)
-                    *reinterpret_cast<float4 *>(field_out + idx + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
-            } else {
-#pragma unroll
-                for (int i = 0; i < 32; i++)
-                    if (i < count) field_out[idx + i] = v[i];
-            }
+            for (int i = 0; i < 32; i++)
+                if (i < count) field_out[idx + i] = v[i];
         }
     }
 }

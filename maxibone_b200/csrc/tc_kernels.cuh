@@ -27,6 +27,16 @@
 // compounds over 3 x R passes.  FP16 coefficients are scaled by 2^10 to stay in
 // the normal range; the epilogue undoes the scale exactly.
 //
+// Row order of the 16-bit field between repetitions.  The z pass is the only
+// pass whose tile rows lie on different planes: read from the [z][y][x] volume
+// every row of its 64 x KP box comes from another plane, and TMA delivers such
+// boxes at well under the rate of the y pass's boxes (rows one x-row apart).
+// So the x pass (which writes whole rows and can put them anywhere) stores
+// the field of every repetition but the last with its rows in [y][z][x] order,
+// and the next z pass reads its columns as rows nx apart, like the y pass.
+// The z pass writes [z][y][x] again; the first repetition's z pass reads the
+// initial [z][y][x] field.
+//
 // x pass.  The field is the A operand: 128 volume rows (M, TMEM lanes) x 128
 // x-outputs, so each epilogue thread owns 32 consecutive voxels of one row --
 // the layout re-illumination, error feedback along x and vector stores want.
@@ -38,8 +48,9 @@
 //
 // Warp roles in a persistent CTA (one per SM): warp 0 issues TMA loads into a
 // tile ring (and L2 prefetches a few tiles ahead), warp 1 issues the MMAs (one
-// thread) into a double-buffered TMEM accumulator, warps 2-9 drain TMEM
-// (tcgen05.ld), narrow to the storage type and store.  With error feedback on,
+// thread) into a double-buffered TMEM accumulator, the other warps (8 in the
+// z / y passes, 16 in the x pass) drain TMEM (tcgen05.ld), narrow to the
+// storage type and store.  With error feedback on,
 // the rounding error of each stored value is carried to its x-neighbour
 // (32-voxel chains along x): the stored field's rounding noise becomes
 // high-pass along x and the next x pass removes it.  Every wait is bounded:
@@ -60,16 +71,19 @@ constexpr int kTM = 128;      // outputs along the axis (z / y) or rows (x) per 
 constexpr int kXTN = 128;     // x outputs per x-pass tile
 constexpr int kXStages = 2;   // TMA ring depth of the x pass
 constexpr int kPrefetch = 3;  // tiles prefetched into L2 ahead of the ring
-constexpr int kEpiWarps = 8;  // two warps per TMEM lane quadrant, each drains half the columns
+constexpr int kEpiWarps = 8;  // z / y passes: two warps per TMEM lane quadrant, each drains half the columns
 constexpr int kThreads = 64 + 32 * kEpiWarps;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
+// The x pass's epilogue (mask, re-illumination, error feedback, stores) is the
+// longest: four warps per lane quadrant, each drains 32 of the 128 columns.
+constexpr int kXEpiWarps = 16;
+constexpr int kXThreads = 64 + 32 * kXEpiWarps;  // warp 0 TMA, warp 1 MMA, warps 2..17 epilogue
 
-// z pass: 64-column tiles in an 8-deep ring (its loads gather one 128-byte
-// row from each of KP planes, so it wants many tiles in flight), stores
-// staged so one instruction writes 8 rows.  y pass: 128-column tiles in a
-// 3-deep ring, TMA bulk stores of each warp's 32 x 32 chunks.
+// Both passes: 128-column tiles in a 3-deep ring.  The z pass stages its
+// stores so one instruction writes 8 rows (its output rows lie on different
+// planes); the y pass writes each warp's 32 x 32 chunks with TMA bulk stores.
 template <bool AXIS_Z> struct StridedShape {
-    static constexpr int kTN = AXIS_Z ? 64 : 128;
-    static constexpr int kStages = AXIS_Z ? 8 : 3;
+    static constexpr int kTN = 128;
+    static constexpr int kStages = 3;
 };
 
 // Tensor-memory columns of the strided passes: accumulators [0, 2 TN), the
@@ -86,8 +100,13 @@ __host__ __device__ constexpr int strided_smem_bytes(int kp, int tn, int stages)
            kEpiWarps * kStageWarpBytes;
 }
 
+// x-pass staging of one epilogue warp's 32 rows x 32 columns of 16-bit output
+// (64-byte rows, 16-byte chunks XOR-swizzled by row / 2).
+constexpr int kXStageWarpBytes = 32 * 64;
+
 __host__ __device__ constexpr int contig_smem_bytes_tc(int kp, int kpa) {
-    return 1024 + kpa * 2 * kXTN * 2 /*Tt_hi|Tt_lo, 256 rows*/ + kXStages * (kpa / 64) * kTM * 128 /*A ring*/ + 256;
+    return 1024 + kpa * 2 * kXTN * 2 /*Tt_hi|Tt_lo, 256 rows*/ + kXStages * (kpa / 64) * kTM * 128 /*A ring*/ +
+           1024 /*barriers, TMEM slot*/ + kXEpiWarps * kXStageWarpBytes;
 }
 
 // Taps and K extents of one pass.
@@ -100,15 +119,19 @@ struct PassTaps {
 };
 
 // One column of a z / y pass: n_at axis tiles of TN x-columns at (x0, oth).
+// in_rows: the load map is over (x, axis, other) -- the y pass, and the z pass
+// reading [y][z][x] rows -- instead of the z pass's (x, y, z).
 struct StridedCol {
     const CUtensorMap *in;       // load map (box 64 x KP along the axis)
     const CUtensorMap *out_map;  // y pass: store map (box 32 x 32, 64-byte swizzle)
     void *out;
     int64_t A, stride_a, stride_o, nx;
-    int n_at, x0, oth;
+    int n_at, x0, oth, in_rows;
 };
 
-// One tile of the x pass: 128 rows from r0, 128 x-outputs from x0.
+// One tile of the x pass: 128 rows from r0, 128 x-outputs from x0.  Rows are
+// numbered z * ny + y.  out_nz > 0: the storage-type output goes to [y][z][x]
+// rows of a volume of out_nz planes, at plane out_z0 + z.
 struct ContigTile {
     const CUtensorMap *in;       // load map (box 64 x 128 rows)
     const void *mask;
@@ -116,8 +139,17 @@ struct ContigTile {
     uint16_t *out_u16;           // final
     float *field_out;            // final, optional
     int64_t rows, nx, r0;
+    int64_t ny, out_nz, out_z0;
     int x0;
 };
+
+// Element index of row `row` (z * ny + y), column x in the x pass's
+// storage-type output.
+__device__ __forceinline__ int64_t contig_out_index(const ContigTile &t, int64_t row, int64_t x) {
+    if (t.out_nz == 0) return row * t.nx + x;
+    const int64_t z = row / t.ny, y = row - z * t.ny;
+    return ((y * t.out_nz + t.out_z0 + z) * t.nx) + x;
+}
 
 __device__ __forceinline__ int find_volume(const int64_t *prefix, int n_vol, int64_t g) {
     int lo = 0, hi = n_vol - 1;
@@ -135,7 +167,7 @@ struct OneVolumeStrided {
     static constexpr bool kParamMaps = true;
     void *out;
     int64_t A, nx, stride_a, stride_o;
-    int n_at, n_xc, tn;
+    int n_at, n_xc, tn, in_rows;
     int64_t n_cols;
     __device__ __forceinline__ int64_t total() const { return n_cols; }
     __device__ __forceinline__ StridedCol col(int64_t g, const CUtensorMap *in, const CUtensorMap *out_map) const {
@@ -150,6 +182,7 @@ struct OneVolumeStrided {
         c.n_at = n_at;
         c.x0 = (int) (g % n_xc) * tn;
         c.oth = (int) (g / n_xc);
+        c.in_rows = in_rows;
         return c;
     }
 };
@@ -158,7 +191,7 @@ struct ManyVolumesStrided {
     static constexpr bool kParamMaps = false;
     const TcVol *vols;
     const int64_t *prefix;  // n_vol + 1 prefix sums of the volumes' columns
-    int n_vol, axis_z, in_buf, tn;
+    int n_vol, axis_z, in_buf, tn, z_in_rows;  // z_in_rows: the z pass reads [y][z][x] rows
     __device__ __forceinline__ int64_t total() const { return __ldg(prefix + n_vol); }
     __device__ __forceinline__ StridedCol col(int64_t g, const CUtensorMap *, const CUtensorMap *) const {
         const int v = find_volume(prefix, n_vol, g);
@@ -166,7 +199,8 @@ struct ManyVolumesStrided {
         const int64_t local = g - __ldg(prefix + v);
         const int n_xc = axis_z ? vol.n_xc_z : vol.n_xc_y;
         StridedCol c;
-        c.in = &vol.map[axis_z ? 0 : 1][in_buf];
+        c.in = axis_z ? (z_in_rows ? &vol.zrows[in_buf] : &vol.map[0][in_buf]) : &vol.map[1][in_buf];
+        c.in_rows = axis_z ? z_in_rows : 1;
         c.out_map = &vol.ystore[in_buf ^ 1];
         c.out = vol.buf[in_buf ^ 1];
         c.A = axis_z ? vol.nz : vol.ny;
@@ -186,7 +220,7 @@ struct OneVolumeContig {
     void *out;
     uint16_t *out_u16;
     float *field_out;
-    int64_t rows, nx;
+    int64_t rows, nx, ny, out_nz, out_z0;
     int n_xt;
     int64_t n_tiles;
     __device__ __forceinline__ int64_t total() const { return n_tiles; }
@@ -199,6 +233,9 @@ struct OneVolumeContig {
         t.field_out = field_out;
         t.rows = rows;
         t.nx = nx;
+        t.ny = ny;
+        t.out_nz = out_nz;
+        t.out_z0 = out_z0;
         t.r0 = (g / n_xt) * kTM;
         t.x0 = (int) (g % n_xt) * kXTN;
         return t;
@@ -209,7 +246,7 @@ struct ManyVolumesContig {
     static constexpr bool kParamMaps = false;
     const TcVol *vols;
     const int64_t *prefix;  // n_vol + 1 prefix sums of the volumes' x tiles
-    int n_vol, in_buf;
+    int n_vol, in_buf, out_rows;  // out_rows: the storage output goes to [y][z][x] rows
     __device__ __forceinline__ int64_t total() const { return __ldg(prefix + n_vol); }
     __device__ __forceinline__ ContigTile tile(int64_t g, const CUtensorMap *) const {
         const int v = find_volume(prefix, n_vol, g);
@@ -223,6 +260,9 @@ struct ManyVolumesContig {
         t.field_out = vol.field_out;
         t.rows = vol.nz * vol.ny;
         t.nx = vol.nx;
+        t.ny = vol.ny;
+        t.out_nz = out_rows ? vol.nz : 0;
+        t.out_z0 = 0;
         t.r0 = (local / vol.n_xt) * kTM;
         t.x0 = (int) (local % vol.n_xt) * kXTN;
         return t;
@@ -317,13 +357,15 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                 {
                     const int ap = at + kPrefetch;
                     const CUtensorMap *pm = nullptr;
-                    int px = 0, po = 0, pa = 0;
-                    if (ap < cur.n_at) { pm = cur.in; px = cur.x0; po = cur.oth; pa = ap; }
-                    else if (has_next && ap - cur.n_at < nxt.n_at) { pm = nxt.in; px = nxt.x0; po = nxt.oth; pa = ap - cur.n_at; }
+                    int px = 0, po = 0, pa = 0, pr = 0;
+                    if (ap < cur.n_at) { pm = cur.in; px = cur.x0; po = cur.oth; pa = ap; pr = cur.in_rows; }
+                    else if (has_next && ap - cur.n_at < nxt.n_at) {
+                        pm = nxt.in; px = nxt.x0; po = nxt.oth; pa = ap - cur.n_at; pr = nxt.in_rows;
+                    }
                     if (pm) {
                         for (int c = 0; c < CHUNKS; c++) {
-                            if (AXIS_Z) tma_prefetch_3d(pm, px + 64 * c, po, pa * kTM - tp.radius);
-                            else tma_prefetch_3d(pm, px + 64 * c, pa * kTM - tp.radius, po);
+                            if (pr) tma_prefetch_3d(pm, px + 64 * c, pa * kTM - tp.radius, po);
+                            else tma_prefetch_3d(pm, px + 64 * c, po, pa * kTM - tp.radius);
                         }
                     }
                 }
@@ -331,8 +373,8 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                 mbar_arrive_expect_tx(&full[s], stage_bytes);
                 for (int c = 0; c < CHUNKS; c++) {
                     uint8_t *dst = ring + s * stage_bytes + c * tp.kp * 128;
-                    if (AXIS_Z) tma_load_3d(dst, cur.in, cur.x0 + 64 * c, cur.oth, a_in, &full[s]);
-                    else tma_load_3d(dst, cur.in, cur.x0 + 64 * c, a_in, cur.oth, &full[s]);
+                    if (cur.in_rows) tma_load_3d(dst, cur.in, cur.x0 + 64 * c, a_in, cur.oth, &full[s]);
+                    else tma_load_3d(dst, cur.in, cur.x0 + 64 * c, cur.oth, a_in, &full[s]);
                 }
             }
             cur = nxt;
@@ -443,7 +485,7 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
 // ---- x pass ------------------------------------------------------------------------
 
 template <typename S, int FMT, class Sched>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kXThreads, 1)
 tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ ContigLaunch<Sched> p) {
     const PassTaps &tp = p.taps;
     extern __shared__ uint8_t smem_raw[];
@@ -456,10 +498,11 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
     uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kXStages * stage_bytes);
     uint64_t *full = bars, *empty = bars + kXStages, *tfull = bars + 2 * kXStages, *tempty = bars + 2 * kXStages + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kXStages + 4);
+    uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 1024;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t total = p.sched.total();
 
-    for (int e = threadIdx.x; e < 2 * kXTN * tp.kpa; e += kThreads) {
+    for (int e = threadIdx.x; e < 2 * kXTN * tp.kpa; e += kXThreads) {
         const int n = e / tp.kpa, j = e - n * tp.kpa;
         const int o = n & (kXTN - 1);
         const int t = j - o - tp.ra + tp.radius;  // tap index 0..2R
@@ -469,7 +512,7 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
     }
     if (threadIdx.x == 0) {
         for (int s = 0; s < kXStages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-        for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], kEpiWarps); }
+        for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], kXEpiWarps); }
         fence_barrier_init();
         if (Sched::kParamMaps) prefetch_tmap(&tmap);
     }
@@ -524,9 +567,10 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
             umma_commit(&tfull[d]);
         }
     } else if (warp >= 2) {
-        const int quad = warp & 3;
-        const int half = (warp - 2) >> 2;
+        const int quad = warp & 3;         // TMEM lane quadrant this warp may access
+        const int part = (warp - 2) >> 2;  // which 32 of the 128 columns it drains
         const int r = quad * 32 + lane;
+        uint8_t *stg = stage_out + (warp - 2) * kXStageWarpBytes;
         int64_t tl = 0;
         for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
             const ContigTile t = p.sched.tile(g, &tmap);
@@ -535,24 +579,38 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
             if (!mbar_wait(&tfull[d], dph, 2)) break;
             tc_fence_after();
             const int64_t row = t.r0 + r;
-            const int64_t xa = t.x0 + half * 64;  // this warp's 64 voxels of the row
-            // Mask flags fetched before the TMEM loads.
-            uint32_t mw[2];
-#pragma unroll
-            for (int cc = 0; cc < 2; cc++) {
-                const int64_t xb = xa + cc * 32;
-                mw[cc] = (row < t.rows && xb < t.nx)
-                             ? row_mask32<FMT>(t.mask, row * t.nx + xb, t.nx - xb < 32 ? (int) (t.nx - xb) : 32,
-                                               t.rows * t.nx)
-                             : 0u;
-            }
-            float ha[32], hb[32];
+            const int64_t xb = t.x0 + part * 32;  // this warp's 32 voxels of the row
+            // Mask flags fetched before the TMEM load.
+            const uint32_t mw = (row < t.rows && xb < t.nx)
+                                    ? row_mask32<FMT>(t.mask, row * t.nx + xb, t.nx - xb < 32 ? (int) (t.nx - xb) : 32,
+                                                      t.rows * t.nx)
+                                    : 0u;
+            float h[32];
             __syncwarp();
-            const uint32_t ta = tmem + ((uint32_t) (quad * 32) << 16) + d * kXTN + half * 64;
-            tmem_ld32(ta, ha);
-            tmem_ld32(ta + 32, hb);
-            contig_epilogue64<S>(ha, hb, mw[0], mw[1], row, t.rows, t.nx, xa, tp.inv_scale, tp.error_feedback,
-                                 p.final_pass, t.out, t.out_u16, t.field_out);
+            tmem_ld32(tmem + ((uint32_t) (quad * 32) << 16) + d * kXTN + part * 32, h);
+            if (p.final_pass) {
+                contig_final32(h, mw, row, t.rows, t.nx, xb, tp.inv_scale, t.out_u16, t.field_out);
+            } else if (xb < t.nx) {  // warp-uniform
+                // 16-bit field: narrow with error feedback, stage the warp's 32 x 32
+                // chunk and write 8 rows (8 x 64 bytes) per instruction -- in [y][z][x]
+                // order the warp's rows lie 2 MB apart at 1024^3.
+                uint16_t q[32];
+                narrow32_masked<S>(h, mw, tp.inv_scale, tp.error_feedback, q);
+                const int64_t oi = row < t.rows ? contig_out_index(t, row, xb) : -1;
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+                    *reinterpret_cast<uint4 *>(stg + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) = pack8(q + 8 * i);
+                __syncwarp();
+                const int sub = lane & 3, rsub = lane >> 2;
+#pragma unroll
+                for (int r4 = 0; r4 < 4; r4++) {
+                    const int rr = r4 * 8 + rsub;
+                    const int64_t o = __shfl_sync(0xffffffffu, oi, rr);
+                    const uint4 w = *reinterpret_cast<const uint4 *>(stg + rr * 64 + ((sub ^ ((rr >> 1) & 3)) << 4));
+                    if (o >= 0 && xb + sub * 8 < t.nx) *reinterpret_cast<uint4 *>(t.out + o + sub * 8) = w;
+                }
+            }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[d]);

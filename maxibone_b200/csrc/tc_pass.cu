@@ -50,7 +50,8 @@ bool tc_supported(int radius, int64_t nz, int64_t ny, int64_t nx) {
 
 template <typename S>
 cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, bool axis_z, const float *kernel,
-                       int radius, bool error_feedback, cudaStream_t st) {
+                       int radius, bool error_feedback, cudaStream_t st, const YzRows *in_rows) {
+    if (!axis_z) in_rows = nullptr;
     const bool is_bf16 = std::is_same<S, __nv_bfloat16>::value;
     const int tn = axis_z ? StridedShape<true>::kTN : StridedShape<false>::kTN;
     const int stages = axis_z ? StridedShape<true>::kStages : StridedShape<false>::kStages;
@@ -66,6 +67,7 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
     sc.n_at = (int) ceil_div(sc.A, kTM);
     sc.n_xc = (int) ceil_div(nx, tn);
     sc.n_cols = (int64_t) sc.n_xc * n_other;
+    sc.in_rows = (!axis_z || in_rows) ? 1 : 0;
 
     CUtensorMap map;
     const CUtensorMapDataType dt = is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
@@ -73,8 +75,14 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
     const cuuint64_t strides[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (nx * ny * 2)};
     const cuuint32_t box[3] = {64u, axis_z ? 1u : (cuuint32_t) p.taps.kp, axis_z ? (cuuint32_t) p.taps.kp : 1u};
     const cuuint32_t estr[3] = {1, 1, 1};
-    CUresult cr = tc_encode_fn()(&map, dt, 3, const_cast<S *>(in), dims, strides, box, estr,
-                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+    // z pass over [y][z][x] rows: dims (x, z, y), rows nx apart, y slabs nz_total * nx apart.
+    const cuuint64_t rdims[3] = {(cuuint64_t) nx, (cuuint64_t) nz, (cuuint64_t) ny};
+    const cuuint64_t rstrides[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (in_rows ? in_rows->nz_total * nx * 2 : 0)};
+    const cuuint32_t rbox[3] = {64u, (cuuint32_t) p.taps.kp, 1u};
+    void *in_base = in_rows ? static_cast<void *>(static_cast<S *>(in_rows->base) + in_rows->z0 * nx)
+                            : static_cast<void *>(const_cast<S *>(in));
+    CUresult cr = tc_encode_fn()(&map, dt, 3, in_base, in_rows ? rdims : dims, in_rows ? rstrides : strides,
+                                 in_rows ? rbox : box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
     CUtensorMap map_out = map;  // the z pass stores without a map
@@ -98,9 +106,9 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
 }
 
 template cudaError_t tc_strided<__nv_bfloat16>(const __nv_bfloat16 *, __nv_bfloat16 *, int64_t, int64_t, int64_t,
-                                               bool, const float *, int, bool, cudaStream_t);
+                                               bool, const float *, int, bool, cudaStream_t, const YzRows *);
 template cudaError_t tc_strided<__half>(const __half *, __half *, int64_t, int64_t, int64_t, bool, const float *, int,
-                                        bool, cudaStream_t);
+                                        bool, cudaStream_t, const YzRows *);
 
 void tc_split_taps(const float *kernel, int radius, bool is_bf16, float scale, uint16_t *hi, uint16_t *lo) {
     for (int i = 0; i < 2 * radius + 1; i++) {
@@ -118,19 +126,23 @@ void tc_split_taps(const float *kernel, int radius, bool is_bf16, float scale, u
 template <typename S>
 cudaError_t tc_contig(const S *in, S *out, const void *mask, int mask_fmt, bool final_pass, uint16_t *out_u16,
                       float *field_out, int64_t nz, int64_t ny, int64_t nx, const float *kernel, int radius,
-                      bool error_feedback, cudaStream_t st) {
+                      bool error_feedback, cudaStream_t st, const YzRows *out_rows) {
     const bool is_bf16 = std::is_same<S, __nv_bfloat16>::value;
+    if (final_pass) out_rows = nullptr;
     ContigLaunch<OneVolumeContig> p{};
     const int ra = (int) round_up(radius, 8);
     fill_pass_taps(p.taps, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback);
     p.final_pass = final_pass ? 1 : 0;
     OneVolumeContig &sc = p.sched;
-    sc.out = out;
+    sc.out = out_rows ? out_rows->base : out;
     sc.mask = mask;
     sc.out_u16 = out_u16;
     sc.field_out = field_out;
     sc.rows = nz * ny;
     sc.nx = nx;
+    sc.ny = ny;
+    sc.out_nz = out_rows ? out_rows->nz_total : 0;
+    sc.out_z0 = out_rows ? out_rows->z0 : 0;
     sc.n_xt = (int) ceil_div(nx, kXTN);
     sc.n_tiles = (int64_t) sc.n_xt * ceil_div(sc.rows, kTM);
 
@@ -153,15 +165,16 @@ cudaError_t tc_contig(const S *in, S *out, const void *mask, int mask_fmt, bool 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int64_t grid = std::min<int64_t>(sc.n_tiles, sms);
-    kern<<<(unsigned) grid, kThreads, smem, st>>>(map, p);
+    kern<<<(unsigned) grid, kXThreads, smem, st>>>(map, p);
     return cudaGetLastError();
 }
 
 template cudaError_t tc_contig<__nv_bfloat16>(const __nv_bfloat16 *, __nv_bfloat16 *, const void *, int, bool,
                                               uint16_t *, float *, int64_t, int64_t, int64_t, const float *, int,
-                                              bool, cudaStream_t);
+                                              bool, cudaStream_t, const YzRows *);
 template cudaError_t tc_contig<__half>(const __half *, __half *, const void *, int, bool, uint16_t *, float *,
-                                       int64_t, int64_t, int64_t, const float *, int, bool, cudaStream_t);
+                                       int64_t, int64_t, int64_t, const float *, int, bool, cudaStream_t,
+                                       const YzRows *);
 
 int tc_read_and_clear_error() {
     int v = 0;

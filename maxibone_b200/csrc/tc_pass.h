@@ -15,18 +15,28 @@ constexpr int kTcMaxRadius = 32;
 // True when the device is sm_100 and the shape fits the TMA constraints.
 bool tc_supported(int radius, int64_t nz, int64_t ny, int64_t nx);
 
-// One z (axis_z) or y pass: out = conv(in) along the axis with a zero boundary.
+// A field stored with its rows in [y][z][x] order: `base` holds a volume of
+// nz_total planes, and a pass works on planes [z0, z0 + nz) of it.
+struct YzRows {
+    void *base;
+    int64_t nz_total, z0;
+};
+
+// One z (axis_z) or y pass: out = conv(in) along the axis with a zero
+// boundary.  `out` is [z][y][x]; so is `in`, unless in_rows (z pass only)
+// gives it in [y][z][x] row order.
 template <typename S>
 cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, bool axis_z, const float *kernel,
-                       int radius, bool error_feedback, cudaStream_t st);
+                       int radius, bool error_feedback, cudaStream_t st, const YzRows *in_rows = nullptr);
 
 // The x pass fused with re-illumination; on the last repetition (final_pass)
 // it writes the uint16 output and/or the FP32 field (either may be NULL)
-// instead of `out`.
+// instead of `out`.  out_rows (not final): write the 16-bit field in [y][z][x]
+// row order there instead of to `out`.
 template <typename S>
 cudaError_t tc_contig(const S *in, S *out, const void *mask, int mask_fmt, bool final_pass, uint16_t *out_u16,
                       float *field_out, int64_t nz, int64_t ny, int64_t nx, const float *kernel, int radius,
-                      bool error_feedback, cudaStream_t st);
+                      bool error_feedback, cudaStream_t st, const YzRows *out_rows = nullptr);
 
 // Reads (and clears) the device error word of the tensor-core kernels:
 // 0 = fine, 1..3 = a bounded wait timed out, -1 = could not be read.

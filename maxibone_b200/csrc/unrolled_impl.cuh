@@ -96,7 +96,11 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
         {
             ProfScope ps(MAXI_KERNEL_Z, st);
             if constexpr (sizeof(S) == 2) {
-                if (use_tc) e = tc::tc_strided<S>(b0, b1, nzv, v.ny, v.nx, true, kernel, radius, EF, st);
+                // After the first repetition the tensor-core x pass leaves the field in
+                // [y][z][x] row order (over all v.nz planes), which the z pass reads faster.
+                const tc::YzRows yz{buf0, v.nz, lo};
+                if (use_tc) e = tc::tc_strided<S>(b0, b1, nzv, v.ny, v.nx, true, kernel, radius, EF, st,
+                                                  tc_x && rep > 0 ? &yz : nullptr);
                 else zy<<<zat * zit, kStrThreads, str_smem, st>>>(b0, b1, zA, zI, zat, zit, taps);
             } else {
                 zy<<<zat * zit, kStrThreads, str_smem, st>>>(b0, b1, zA, zI, zat, zit, taps);
@@ -117,9 +121,11 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
         {
             ProfScope ps(last ? MAXI_KERNEL_X_FINAL : MAXI_KERNEL_X, st);
             if (tc_x) {
-                if constexpr (sizeof(S) == 2)
+                if constexpr (sizeof(S) == 2) {
+                    const tc::YzRows yz{buf1, v.nz, lo};
                     e = tc::tc_contig<S>(b0, b1, mv, mask_fmt, last, last ? ou : nullptr, last ? fo : nullptr, nzv,
-                                         v.ny, v.nx, kernel, radius, EF, st);
+                                         v.ny, v.nx, kernel, radius, EF, st, &yz);
+                }
             } else if (!last) {
                 xpass<<<xt * xrb, kConThreads, con_smem, st>>>(b0, b1, mv, nullptr, nullptr, rows, v.nx, xt, taps);
             } else {

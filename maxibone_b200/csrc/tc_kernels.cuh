@@ -161,6 +161,42 @@ __device__ __forceinline__ int find_volume(const int64_t *prefix, int n_vol, int
     return lo;
 }
 
+// Mask flags of up to 32 voxels of a row in two steps: load_mask_words issues
+// the loads (bit-packed: the one or two words the voxels span), mask_flags
+// turns them into bit q = voxel q.  uint8 masks are read in mask_flags.
+struct MaskWords {
+    uint32_t hi = 0, lo = 0;
+    int64_t idx = 0, n = 0;
+    int shift = 0, count = 0;  // count 0: no voxels
+};
+
+template <int FMT>
+__device__ __forceinline__ MaskWords load_mask_words(const void *m, int64_t idx, int count, int64_t n) {
+    MaskWords w;
+    w.idx = idx;
+    w.count = count;
+    w.n = n;
+    if (FMT == MAXI_MASK_BITPACKED) {
+        const uint32_t *p = static_cast<const uint32_t *>(m);
+        const int64_t w0 = idx >> 5;
+        w.shift = (int) (idx & 31);
+        w.hi = __ldg(p + w0);
+        w.lo = (w.shift > 0 && (w0 + 1) * 32 < n) ? __ldg(p + w0 + 1) : 0u;
+    }
+    return w;
+}
+
+template <int FMT>
+__device__ __forceinline__ uint32_t mask_flags(const MaskWords &w, const void *m) {
+    if (w.count == 0) return 0u;
+    if (FMT == MAXI_MASK_BITPACKED) {
+        const uint32_t msb_first = (uint32_t) (((((uint64_t) w.hi << 32) | w.lo) << w.shift) >> 32);  // voxel idx at bit 31
+        const uint32_t r = __brev(msb_first);                                                          // voxel idx at bit 0
+        return w.count >= 32 ? r : (r & ((1u << w.count) - 1u));
+    }
+    return row_mask32<FMT>(m, w.idx, w.count, w.n);
+}
+
 // ---- schedules -------------------------------------------------------------------
 
 struct OneVolumeStrided {
@@ -571,20 +607,32 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
         const int part = (warp - 2) >> 2;  // which 32 of the 128 columns it drains
         const int r = quad * 32 + lane;
         uint8_t *stg = stage_out + (warp - 2) * kXStageWarpBytes;
+        // Mask words of this thread's 32 voxels of a tile (bit-packed masks: the
+        // one or two words they span), loaded one tile ahead so that their
+        // global-memory latency overlaps the previous tile's work.
+        auto mask_words = [&](const ContigTile &t) -> MaskWords {
+            const int64_t row = t.r0 + r, xb = t.x0 + part * 32;
+            if (row >= t.rows || xb >= t.nx) return MaskWords{};
+            return load_mask_words<FMT>(t.mask, row * t.nx + xb, t.nx - xb < 32 ? (int) (t.nx - xb) : 32,
+                                        t.rows * t.nx);
+        };
+        ContigTile t_next = p.sched.tile(blockIdx.x < total ? (int64_t) blockIdx.x : 0, &tmap);
+        MaskWords mw_next = blockIdx.x < total ? mask_words(t_next) : MaskWords{};
         int64_t tl = 0;
         for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
-            const ContigTile t = p.sched.tile(g, &tmap);
+            const ContigTile t = t_next;
+            const MaskWords mwords = mw_next;
+            if (g + gridDim.x < total) {
+                t_next = p.sched.tile(g + gridDim.x, &tmap);
+                mw_next = mask_words(t_next);
+            }
             const int d = (int) (tl & 1);
             const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
             if (!mbar_wait(&tfull[d], dph, 2)) break;
             tc_fence_after();
             const int64_t row = t.r0 + r;
             const int64_t xb = t.x0 + part * 32;  // this warp's 32 voxels of the row
-            // Mask flags fetched before the TMEM load.
-            const uint32_t mw = (row < t.rows && xb < t.nx)
-                                    ? row_mask32<FMT>(t.mask, row * t.nx + xb, t.nx - xb < 32 ? (int) (t.nx - xb) : 32,
-                                                      t.rows * t.nx)
-                                    : 0u;
+            const uint32_t mw = mask_flags<FMT>(mwords, t.mask);
             float h[32];
             __syncwarp();
             tmem_ld32(tmem + ((uint32_t) (quad * 32) << 16) + d * kXTN + part * 32, h);

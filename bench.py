@@ -201,7 +201,10 @@ def batched_section(device, torch, np, stream, reps=50):
     torch.cuda.synchronize()
     device.tensor_core_status()
     t_bf16 = e0.elapsed_time(e1) / n_t
-    res["bf16_batch"] = {"value": vox * reps / (t_bf16 / 1e3) / 1e9, "unit": UNIT, "ms": t_bf16}
+    peak, _ = load_peaks()
+    gbs = (6 * 2 + 0.125) * vox * reps / (t_bf16 / 1e3) / 1e9  # three passes of a 2-byte field + the 1-bit mask
+    res["bf16_batch"] = {"value": vox * reps / (t_bf16 / 1e3) / 1e9, "unit": UNIT, "ms": t_bf16,
+                         "hbm_gbs": gbs, "hbm_frac": gbs / peak}
     # Accuracy of a few volumes against the FP64 form.
     errs = []
     for i in range(0, 64, 16):
@@ -393,17 +396,21 @@ def main():
     if os.path.exists(tpath):
         with open(tpath) as f:
             traffic = json.load(f).get(args.workload, {}).get(args.field, {}).get(dom)
+    # Whole step: three passes read and write the field once each, the x pass reads the 1-bit mask.
+    rep_bytes = (6 * s + 0.125) * vox
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": dom, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "alg_bytes_per_launch": alg_bytes.get(dom), "ms_per_launch": dom_ms,
                 "per_kind_ms": {k: v[0] / v[1] for k, v in prof.items()},
-                "fp32_tflops_dominant": 2 * (2 * radius + 1) * vox / (dom_ms / 1e3) / 1e12,
-                "fp32_tflops_whole_step": 2 * 3 * (2 * radius + 1) * vox * reps * args.steps / (ms / 1e3) / 1e12,
-                "note": "the direct FP32 stencil at radius 32 is bound by the FP32 pipe (2*65 flop per 8 B "
-                        "of field traffic); fp32_peak_tflops = 148 SMs x 128 FMA/clk x 2 x median SM clock"}
-
-    if clocks:
-        roofline["fp32_peak_tflops"] = 148 * 128 * 2 * clocks["sm_mhz"] * 1e6 / 1e12
+                "whole_step_gbs": rep_bytes * reps * args.steps / (ms / 1e3) / 1e9,
+                "whole_step_frac": rep_bytes * reps * args.steps / (ms / 1e3) / 1e9 / peak}
+    if args.field == "f32":
+        roofline["fp32_tflops_dominant"] = 2 * (2 * radius + 1) * vox / (dom_ms / 1e3) / 1e12
+        roofline["fp32_tflops_whole_step"] = 2 * 3 * (2 * radius + 1) * vox * reps * args.steps / (ms / 1e3) / 1e12
+        roofline["note"] = ("the direct FP32 stencil at radius 32 is bound by the FP32 pipe (2*65 flop per 8 B "
+                            "of field traffic); fp32_peak_tflops = 148 SMs x 128 FMA/clk x 2 x median SM clock")
+        if clocks:
+            roofline["fp32_peak_tflops"] = 148 * 128 * 2 * clocks["sm_mhz"] * 1e6 / 1e12
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -477,7 +484,7 @@ def main():
                     f_traffic = json.load(f).get(args.workload, {}).get(form, {}).get(fdom)
             froof = {"bound": "hbm", "kernel": fdom, "achieved": f_bytes[fdom] / (fms / 1e3) / 1e9, "peak": peak,
                      "unit": "GB/s", "frac": f_bytes[fdom] / (fms / 1e3) / 1e9 / peak, "traffic": f_traffic,
-                     "whole_rep_frac": (2 * fb + 0.125) * vox * reps * n_t / (t_ms / 1e3) / 1e9 / peak}
+                     "whole_rep_frac": (6 * fb + 0.125) * vox * reps * n_t / (t_ms / 1e3) / 1e9 / peak}
             forms[name] = {"value": vox * reps * n_t / (t_ms / 1e3) / 1e9, "unit": UNIT, "field": form, **opts,
                            "roofline": froof,
                            "max_abs_err_vs_f64": float(err.max().item()),
@@ -487,6 +494,10 @@ def main():
             del err, fo, w
             torch.cuda.empty_cache()
         line["precision"] = forms
+        # The BF16 form against the plain FP32 form on this workload.
+        line["bf16_vs_f32"] = {"speedup": forms["bf16"]["value"] / forms["f32"]["value"],
+                               "bf16_whole_rep_hbm_frac": forms["bf16"]["roofline"]["whole_rep_frac"],
+                               "bf16_max_abs_err_vs_f64": forms["bf16"]["max_abs_err_vs_f64"]}
         del f64
 
         line["batched"] = batched_section(device, torch, np, stream)

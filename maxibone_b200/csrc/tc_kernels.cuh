@@ -145,10 +145,12 @@ struct ContigTile {
 
 // Element index of row `row` (z * ny + y), column x in the x pass's
 // storage-type output.
+// Row and tile counts stay below 2^32 (tc_supported), so the divisions here
+// and in the schedules are 32-bit.
 __device__ __forceinline__ int64_t contig_out_index(const ContigTile &t, int64_t row, int64_t x) {
     if (t.out_nz == 0) return row * t.nx + x;
-    const int64_t z = row / t.ny, y = row - z * t.ny;
-    return ((y * t.out_nz + t.out_z0 + z) * t.nx) + x;
+    const uint32_t ny = (uint32_t) t.ny, z = (uint32_t) row / ny, y = (uint32_t) row - z * ny;
+    return (((int64_t) y * t.out_nz + t.out_z0 + z) * t.nx) + x;
 }
 
 __device__ __forceinline__ int find_volume(const int64_t *prefix, int n_vol, int64_t g) {
@@ -199,14 +201,20 @@ __device__ __forceinline__ uint32_t mask_flags(const MaskWords &w, const void *m
 
 // ---- schedules -------------------------------------------------------------------
 
+// Each role of a kernel walks the launch's work indices in increasing order
+// and keeps a Cursor (the volume it is in and that volume's index range), so
+// the binary search over the volumes runs only when the walk leaves the
+// current volume.
 struct OneVolumeStrided {
     static constexpr bool kParamMaps = true;
+    struct Cursor {};
     void *out;
     int64_t A, nx, stride_a, stride_o;
     int n_at, n_xc, tn, in_rows;
     int64_t n_cols;
     __device__ __forceinline__ int64_t total() const { return n_cols; }
-    __device__ __forceinline__ StridedCol col(int64_t g, const CUtensorMap *in, const CUtensorMap *out_map) const {
+    __device__ __forceinline__ StridedCol col(int64_t g, const CUtensorMap *in, const CUtensorMap *out_map,
+                                              Cursor &) const {
         StridedCol c;
         c.in = in;
         c.out_map = out_map;
@@ -216,8 +224,8 @@ struct OneVolumeStrided {
         c.stride_o = stride_o;
         c.nx = nx;
         c.n_at = n_at;
-        c.x0 = (int) (g % n_xc) * tn;
-        c.oth = (int) (g / n_xc);
+        c.oth = (int) ((uint32_t) g / (uint32_t) n_xc);
+        c.x0 = ((int) g - c.oth * n_xc) * tn;
         c.in_rows = in_rows;
         return c;
     }
@@ -228,11 +236,19 @@ struct ManyVolumesStrided {
     const TcVol *vols;
     const int64_t *prefix;  // n_vol + 1 prefix sums of the volumes' columns
     int n_vol, axis_z, in_buf, tn, z_in_rows;  // z_in_rows: the z pass reads [y][z][x] rows
+    struct Cursor {
+        int64_t lo = 0, hi = 0;  // the current volume's columns [lo, hi)
+        int v = 0;
+    };
     __device__ __forceinline__ int64_t total() const { return __ldg(prefix + n_vol); }
-    __device__ __forceinline__ StridedCol col(int64_t g, const CUtensorMap *, const CUtensorMap *) const {
-        const int v = find_volume(prefix, n_vol, g);
-        const TcVol &vol = vols[v];
-        const int64_t local = g - __ldg(prefix + v);
+    __device__ __forceinline__ StridedCol col(int64_t g, const CUtensorMap *, const CUtensorMap *, Cursor &cur) const {
+        if (g < cur.lo || g >= cur.hi) {
+            cur.v = find_volume(prefix, n_vol, g);
+            cur.lo = __ldg(prefix + cur.v);
+            cur.hi = __ldg(prefix + cur.v + 1);
+        }
+        const TcVol &vol = vols[cur.v];
+        const int64_t local = g - cur.lo;
         const int n_xc = axis_z ? vol.n_xc_z : vol.n_xc_y;
         StridedCol c;
         c.in = axis_z ? (z_in_rows ? &vol.zrows[in_buf] : &vol.map[0][in_buf]) : &vol.map[1][in_buf];
@@ -244,14 +260,15 @@ struct ManyVolumesStrided {
         c.stride_o = axis_z ? vol.nx : vol.ny * vol.nx;
         c.nx = vol.nx;
         c.n_at = axis_z ? vol.n_at_z : vol.n_at_y;
-        c.x0 = (int) (local % n_xc) * tn;
-        c.oth = (int) (local / n_xc);
+        c.oth = (int) ((uint32_t) local / (uint32_t) n_xc);
+        c.x0 = ((int) local - c.oth * n_xc) * tn;
         return c;
     }
 };
 
 struct OneVolumeContig {
     static constexpr bool kParamMaps = true;
+    struct Cursor {};
     const void *mask;
     void *out;
     uint16_t *out_u16;
@@ -260,7 +277,7 @@ struct OneVolumeContig {
     int n_xt;
     int64_t n_tiles;
     __device__ __forceinline__ int64_t total() const { return n_tiles; }
-    __device__ __forceinline__ ContigTile tile(int64_t g, const CUtensorMap *in) const {
+    __device__ __forceinline__ ContigTile tile(int64_t g, const CUtensorMap *in, Cursor &) const {
         ContigTile t;
         t.in = in;
         t.mask = mask;
@@ -272,8 +289,9 @@ struct OneVolumeContig {
         t.ny = ny;
         t.out_nz = out_nz;
         t.out_z0 = out_z0;
-        t.r0 = (g / n_xt) * kTM;
-        t.x0 = (int) (g % n_xt) * kXTN;
+        const uint32_t rt = (uint32_t) g / (uint32_t) n_xt;
+        t.r0 = (int64_t) rt * kTM;
+        t.x0 = ((int) g - (int) rt * n_xt) * kXTN;
         return t;
     }
 };
@@ -283,11 +301,19 @@ struct ManyVolumesContig {
     const TcVol *vols;
     const int64_t *prefix;  // n_vol + 1 prefix sums of the volumes' x tiles
     int n_vol, in_buf, out_rows;  // out_rows: the storage output goes to [y][z][x] rows
+    struct Cursor {
+        int64_t lo = 0, hi = 0;  // the current volume's tiles [lo, hi)
+        int v = 0;
+    };
     __device__ __forceinline__ int64_t total() const { return __ldg(prefix + n_vol); }
-    __device__ __forceinline__ ContigTile tile(int64_t g, const CUtensorMap *) const {
-        const int v = find_volume(prefix, n_vol, g);
-        const TcVol &vol = vols[v];
-        const int64_t local = g - __ldg(prefix + v);
+    __device__ __forceinline__ ContigTile tile(int64_t g, const CUtensorMap *, Cursor &cur) const {
+        if (g < cur.lo || g >= cur.hi) {
+            cur.v = find_volume(prefix, n_vol, g);
+            cur.lo = __ldg(prefix + cur.v);
+            cur.hi = __ldg(prefix + cur.v + 1);
+        }
+        const TcVol &vol = vols[cur.v];
+        const int64_t local = g - cur.lo;
         ContigTile t;
         t.in = &vol.map[2][in_buf];
         t.mask = vol.mask;
@@ -299,8 +325,9 @@ struct ManyVolumesContig {
         t.ny = vol.ny;
         t.out_nz = out_rows ? vol.nz : 0;
         t.out_z0 = 0;
-        t.r0 = (local / vol.n_xt) * kTM;
-        t.x0 = (int) (local % vol.n_xt) * kXTN;
+        const uint32_t rt = (uint32_t) local / (uint32_t) vol.n_xt;
+        t.r0 = (int64_t) rt * kTM;
+        t.x0 = ((int) local - (int) rt * vol.n_xt) * kXTN;
         return t;
     }
 };
@@ -382,10 +409,11 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
         int64_t tl = 0;
         bool ok = true;
         int64_t g = blockIdx.x;
-        StridedCol cur = p.sched.col(g < total ? g : 0, &tmap, &tmap_out), nxt = cur;
+        typename Sched::Cursor cc;
+        StridedCol cur = p.sched.col(g < total ? g : 0, &tmap, &tmap_out, cc), nxt = cur;
         for (; ok && g < total; g += gridDim.x) {
             const bool has_next = g + gridDim.x < total;
-            if (has_next) nxt = p.sched.col(g + gridDim.x, &tmap, &tmap_out);
+            if (has_next) nxt = p.sched.col(g + gridDim.x, &tmap, &tmap_out, cc);
             for (int at = 0; at < cur.n_at; at++, tl++) {
                 const int s = (int) (tl % STAGES);
                 const uint32_t ph = (uint32_t) ((tl / STAGES) & 1);
@@ -422,8 +450,9 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
         const uint32_t b0 = smem_u32(ring);
         int64_t tl = 0;
         bool ok = true;
+        typename Sched::Cursor cc;
         for (int64_t g = blockIdx.x; ok && g < total; g += gridDim.x) {
-            const int n_at = p.sched.col(g, &tmap, &tmap_out).n_at;
+            const int n_at = p.sched.col(g, &tmap, &tmap_out, cc).n_at;
             for (int at = 0; at < n_at; at++, tl++) {
                 const int s = (int) (tl % STAGES);
                 const uint32_t ph = (uint32_t) ((tl / STAGES) & 1);
@@ -451,8 +480,9 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
         int sbuf = 0;
         int64_t tl = 0;
         bool ok = true;
+        typename Sched::Cursor cc;
         for (int64_t g = blockIdx.x; ok && g < total; g += gridDim.x) {
-            const StridedCol c = p.sched.col(g, &tmap, &tmap_out);
+            const StridedCol c = p.sched.col(g, &tmap, &tmap_out, cc);
             S *out = static_cast<S *>(c.out);
             for (int at = 0; at < c.n_at; at++, tl++) {
                 const int d = (int) (tl & 1);
@@ -497,8 +527,12 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                             *reinterpret_cast<uint4 *>(sb + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) = pack8(q + 8 * i);
                         fence_proxy_async_smem();
                         __syncwarp();
-                        if (lane == 0 && xb < c.nx && at * kTM + quad * 32 < c.A) {
-                            tma_store_3d(c.out_map, sb, (int) xb, at * kTM + quad * 32, c.oth);
+                        // Every chunk commits exactly one bulk group (an empty one when the
+                        // chunk lies outside the volume), so that bulk_wait_read<1> above always
+                        // covers the store that last read the buffer being refilled.
+                        if (lane == 0) {
+                            if (xb < c.nx && at * kTM + quad * 32 < c.A)
+                                tma_store_3d(c.out_map, sb, (int) xb, at * kTM + quad * 32, c.oth);
                             bulk_commit();
                         }
                         sbuf ^= 1;
@@ -565,16 +599,17 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
 
     if (warp == 0 && lane == 0) {
         int64_t tl = 0;
+        typename Sched::Cursor cc, cp;  // current tile, L2-prefetched tile
         for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
             const int s = (int) (tl % kXStages);
             const uint32_t ph = (uint32_t) ((tl / kXStages) & 1);
             if (!mbar_wait(&empty[s], ph ^ 1, 1)) break;
             const int64_t gp = g + kPrefetch * (int64_t) gridDim.x;
             if (gp < total) {
-                const ContigTile t = p.sched.tile(gp, &tmap);
+                const ContigTile t = p.sched.tile(gp, &tmap, cp);
                 for (int kb = 0; kb < nkb; kb++) tma_prefetch_3d(t.in, t.x0 - tp.ra + 64 * kb, (int) t.r0, 0);
             }
-            const ContigTile t = p.sched.tile(g, &tmap);
+            const ContigTile t = p.sched.tile(g, &tmap, cc);
             mbar_arrive_expect_tx(&full[s], stage_bytes);
             for (int kb = 0; kb < nkb; kb++)
                 tma_load_3d(ring + s * stage_bytes + kb * kTM * 128, t.in, t.x0 - tp.ra + 64 * kb, (int) t.r0, 0, &full[s]);
@@ -616,16 +651,13 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
             return load_mask_words<FMT>(t.mask, row * t.nx + xb, t.nx - xb < 32 ? (int) (t.nx - xb) : 32,
                                         t.rows * t.nx);
         };
-        ContigTile t_next = p.sched.tile(blockIdx.x < total ? (int64_t) blockIdx.x : 0, &tmap);
-        MaskWords mw_next = blockIdx.x < total ? mask_words(t_next) : MaskWords{};
+        typename Sched::Cursor cc;
+        MaskWords mw_next = blockIdx.x < total ? mask_words(p.sched.tile(blockIdx.x, &tmap, cc)) : MaskWords{};
         int64_t tl = 0;
         for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
-            const ContigTile t = t_next;
+            const ContigTile t = p.sched.tile(g, &tmap, cc);
             const MaskWords mwords = mw_next;
-            if (g + gridDim.x < total) {
-                t_next = p.sched.tile(g + gridDim.x, &tmap);
-                mw_next = mask_words(t_next);
-            }
+            if (g + gridDim.x < total) mw_next = mask_words(p.sched.tile(g + gridDim.x, &tmap, cc));
             const int d = (int) (tl & 1);
             const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
             if (!mbar_wait(&tfull[d], dph, 2)) break;

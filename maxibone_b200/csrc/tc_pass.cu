@@ -40,6 +40,7 @@ bool tc_supported(int radius, int64_t nz, int64_t ny, int64_t nx) {
     if (radius < 1 || radius > kTcMaxRadius) return false;
     if (nx % 8 != 0 || nx < 64) return false;  // TMA: 16-byte row strides, at least one 64-wide box
     if (nz > INT32_MAX / 2 || ny > INT32_MAX / 2 || nx > INT32_MAX / 2) return false;
+    if (nz * ny >= (int64_t(1) << 31)) return false;  // rows and tile indices fit 32-bit arithmetic
     int dev = 0, major = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess) {
         cudaGetLastError();

@@ -53,6 +53,34 @@ def test_batch_equals_single_volume_runs(field):
     plan.close()
 
 
+# Extents that are not multiples of the 128-wide tensor-core tiles leave tiles
+# partly outside a volume.  32 volumes of the batched workload (dims from
+# {96, ..., 512}) at 30 repetitions keep the memory system busy enough that a
+# reordering of the asynchronous tile stores would show.
+@pytest.mark.parametrize("field", ["bf16"])
+def test_uneven_volumes_many_reps_batch_equals_single_and_repeats(field):
+    from maxibone_b200.synthetic import batch_shapes, spheres_mask_torch
+    reps = 30
+    specs = batch_shapes(32, seed=3)
+    masks = [spheres_mask_torch(sh, fg, seed=i) for i, (sh, _, fg) in enumerate(specs)]
+    kernels = [gauss_kernel(sig).astype(np.float32) for _, sig, _ in specs]
+    fouts = [torch.empty(sh, dtype=torch.float32, device="cuda") for sh, _, _ in specs]
+    plan = device.BatchPlan(masks, kernels, reps, field=field, field_outs=fouts)
+    plan.run()
+    torch.cuda.synchronize()
+    device.tensor_core_status()
+    plan.close()
+    for i, (sh, _, _) in enumerate(specs):
+        runs = []
+        for _ in range(2 if i < 4 else 1):
+            fo = torch.empty(sh, dtype=torch.float32, device="cuda")
+            device.diffuse(masks[i], kernels[i], reps, field=field, field_out=fo)
+            runs.append(fo)
+        torch.cuda.synchronize()
+        assert torch.equal(runs[0], runs[-1]), (i, sh)
+        assert torch.equal(fouts[i], runs[0]), (i, sh)
+
+
 def test_batch_plan_replays():
     masks, outs, fouts, kernels = make_batch("bf16")
     plan = device.BatchPlan(masks, kernels, REPS, outputs=outs, field="bf16", field_outs=fouts)

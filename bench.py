@@ -205,9 +205,9 @@ def batched_section(device, torch, np, stream, reps=50):
     gbs = (6 * 2 + 0.125) * vox * reps / (t_bf16 / 1e3) / 1e9  # three passes of a 2-byte field + the 1-bit mask
     res["bf16_batch"] = {"value": vox * reps / (t_bf16 / 1e3) / 1e9, "unit": UNIT, "ms": t_bf16,
                          "hbm_gbs": gbs, "hbm_frac": gbs / peak}
-    # Accuracy of a few volumes against the FP64 form.
+    # Accuracy of every fourth volume against the FP64 form.
     errs = []
-    for i in range(0, 64, 16):
+    for i in range(0, 64, 4):
         want = torch.empty(specs[i][0], dtype=torch.float64, device="cuda")
         device.diffuse(masks[i], kernels[i], reps, field="f64", field_out=want)
         errs.append(float((fouts[i].double() - want).abs().max().item()))

@@ -275,39 +275,43 @@ def out_of_core_section(torch, np, reps=20, shape=(4096, 1728, 2048), slab=1024)
 
 
 def long_section(device, torch, np, mask, shape, stream):
-    """R = 500 error growth of the 16-bit forms and the sigma = 32 (257 taps) case."""
+    """R = 500 error growth of the 16-bit forms, and the sigma = 32 (radius 128,
+    257 taps) case: CUDA-core FP32 and BF16 passes against the BF16 / FP16
+    banded-Toeplitz tensor-core passes, each with its error against FP64."""
     from maxibone_b200.kernels import gauss_kernel
 
+    vox = int(np.prod(shape))
+
+    def timed(kernel, reps, form, fo, **opts):
+        device.diffuse(mask, kernel, 1, field=form, field_out=fo, **opts)  # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        device.diffuse(mask, kernel, reps, field=form, field_out=fo, **opts)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        device.tensor_core_status()
+        return vox * reps / (e0.elapsed_time(e1) / 1e3) / 1e9
+
     res = {}
-    k8 = gauss_kernel(8.0).astype(np.float32)
-    f64 = torch.empty(shape, dtype=torch.float64, device="cuda")
-    device.diffuse(mask, k8, 500, field="f64", field_out=f64)
-    for form in ("bf16", "f16"):
-        fo = torch.empty(shape, dtype=torch.float32, device="cuda")
-        t0 = time.perf_counter()
-        device.diffuse(mask, k8, 500, field=form, field_out=fo)
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        err = (fo.double() - f64).abs_()
-        res[f"{form}_r500"] = {"value": int(np.prod(shape)) * 500 / dt / 1e9, "unit": UNIT,
-                               "max_abs_err_vs_f64": float(err.max().item()),
-                               "mean_abs_err_vs_f64": float(err.mean().item())}
-        del fo, err
-    del f64
-    torch.cuda.empty_cache()
-    k32 = gauss_kernel(32.0).astype(np.float32)
-    for form in ("f32", "bf16"):
-        fo = torch.empty(shape, dtype=torch.float32, device="cuda")
-        device.diffuse(mask, k32, 2, field=form, field_out=fo)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        device.diffuse(mask, k32, 10, field=form, field_out=fo)
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        res[f"sigma32_{form}"] = {"value": int(np.prod(shape)) * 10 / dt / 1e9, "unit": UNIT, "reps": 10,
-                                  "note": "radius 128: CUDA-core passes (the tensor-core passes serve radius <= 32)"}
-        del fo
-    torch.cuda.empty_cache()
+    for sigma, reps, forms in ((8.0, 500, (("bf16", {}), ("f16", {}))),
+                               (32.0, 10, (("f32", {}), ("bf16", {}), ("f16", {}),
+                                           ("bf16", {"tensor_cores": False})))):
+        kernel = gauss_kernel(sigma).astype(np.float32)
+        f64 = torch.empty(shape, dtype=torch.float64, device="cuda")
+        device.diffuse(mask, kernel, reps, field="f64", field_out=f64)
+        for form, opts in forms:
+            fo = torch.empty(shape, dtype=torch.float32, device="cuda")
+            value = timed(kernel, reps, form, fo, **opts)
+            err = (fo.double() - f64).abs_()
+            name = (f"sigma{int(sigma)}_r{reps}_{form}" + ("_cuda_cores" if opts else "")
+                    + ("_tensor_cores" if form != "f32" and not opts else ""))
+            res[name] = {"value": value, "unit": UNIT, "reps": reps, "kernel_size": int(kernel.shape[0]),
+                         "max_abs_err_vs_f64": float(err.max().item()),
+                         "mean_abs_err_vs_f64": float(err.mean().item())}
+            del fo, err
+        del f64
+        torch.cuda.empty_cache()
     return res
 
 

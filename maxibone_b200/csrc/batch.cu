@@ -187,7 +187,8 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
     for (size_t i = 0; i < p->vols.size(); i++) {
         BatchVolume &bv = p->vols[i];
         const int radius = (int) (bv.v.kernel_size / 2);
-        const bool eligible = tc_type && bv.v.repititions > 0 && tc::tc_supported(radius, bv.v.nz, bv.v.ny, bv.v.nx) &&
+        const bool eligible = tc_type && bv.v.repititions > 0 && radius <= tc::kTcMaxRadius &&
+                              tc::tc_supported(radius, bv.v.nz, bv.v.ny, bv.v.nx) &&
                               ((reinterpret_cast<uintptr_t>(bv.v.output) | reinterpret_cast<uintptr_t>(bv.v.field_out)) & 15) == 0;
         if (!eligible) continue;
         int gi = -1;

@@ -115,10 +115,10 @@ cudaError_t tc_batch_pass(const TcVol *d_vols, const int64_t *d_prefix, int64_t 
         p.sched.tn = axis_z ? StridedShape<true>::kTN : StridedShape<false>::kTN;
         const int smem = strided_smem_bytes(p.taps.kp, p.sched.tn,
                                             axis_z ? StridedShape<true>::kStages : StridedShape<false>::kStages);
-        auto *k = axis_z ? (is_bf16 ? tc_strided_kernel<__nv_bfloat16, true, ManyVolumesStrided>
-                                    : tc_strided_kernel<__half, true, ManyVolumesStrided>)
-                         : (is_bf16 ? tc_strided_kernel<__nv_bfloat16, false, ManyVolumesStrided>
-                                    : tc_strided_kernel<__half, false, ManyVolumesStrided>);
+        auto *k = axis_z ? (is_bf16 ? tc_strided_kernel<__nv_bfloat16, true, 128, ManyVolumesStrided>
+                                    : tc_strided_kernel<__half, true, 128, ManyVolumesStrided>)
+                         : (is_bf16 ? tc_strided_kernel<__nv_bfloat16, false, 128, ManyVolumesStrided>
+                                    : tc_strided_kernel<__half, false, 128, ManyVolumesStrided>);
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
         k<<<grid, kThreads, smem, st>>>(unused, unused, p);
     }

@@ -78,18 +78,22 @@ constexpr int kThreads = 64 + 32 * kEpiWarps;  // warp 0 TMA, warp 1 MMA, warps 
 constexpr int kXEpiWarps = 16;
 constexpr int kXThreads = 64 + 32 * kXEpiWarps;  // warp 0 TMA, warp 1 MMA, warps 2..17 epilogue
 
-// Both passes: 128-column tiles in a 3-deep ring.  The z pass stages its
-// stores so one instruction writes 8 rows (its output rows lie on different
-// planes); the y pass writes each warp's 32 x 32 chunks with TMA bulk stores.
+// z / y passes: 128-column tiles (64 for radius > 64) in a 3-deep ring.  The
+// z pass stages its stores so one instruction writes 8 rows (its output rows
+// lie on different planes); the y pass writes each warp's 32 x 32 chunks with
+// TMA bulk stores.  Batches (radius <= 32) always use 128-column tiles.
 template <bool AXIS_Z> struct StridedShape {
     static constexpr int kTN = 128;
     static constexpr int kStages = 3;
 };
+constexpr int kStridedStages = 3;
+__host__ __device__ constexpr int strided_tn(int radius) { return radius <= 64 ? 128 : 64; }
 
-// Tensor-memory columns of the strided passes: accumulators [0, 2 TN), the
-// Toeplitz halves at kTmemAHi / kTmemALo (K / 2 <= 96 columns each).
-constexpr uint32_t kTmemAHi = 256, kTmemALo = 352, kTmemColsStrided = 512;
-static_assert(kTM + 2 * kTcMaxRadius <= 2 * 96, "the Toeplitz halves hold K <= 192");
+// Tensor memory of the strided passes (512 columns): accumulators [0, 2 TN),
+// then the Toeplitz halves, kcols columns each (K / 2 rounded up to 32: 96 up
+// to radius 32, 128 up to 64, 192 up to 128).
+constexpr uint32_t kTmemColsStrided = 512;
+__host__ __device__ constexpr int toeplitz_cols(int kp) { return ((kp / 2) + 31) / 32 * 32; }
 
 // Per-epilogue-warp staging: two 32-row x 32-column 16-bit buffers (z pass:
 // row stride 80 bytes; y pass: the store map's 64-byte swizzle).
@@ -109,13 +113,15 @@ __host__ __device__ constexpr int contig_smem_bytes_tc(int kp, int kpa) {
            1024 /*barriers, TMEM slot*/ + kXEpiWarps * kXStageWarpBytes;
 }
 
-// Taps and K extents of one pass.
+// Taps and K extents of one pass.  K rows longer than a TMA box (256) are
+// loaded as nbox boxes of box_rows rows.
 struct PassTaps {
     int radius, ra, kp, kpa;  // radius, x-pass left pad, K (multiple of 16), K rounded to 64
+    int kcols, nbox, box_rows;
     int error_feedback;
     float inv_scale;
-    uint16_t hi[2 * kTcMaxRadius + 1];
-    uint16_t lo[2 * kTcMaxRadius + 1];
+    uint16_t hi[2 * kTcMaxRadiusWide + 1];
+    uint16_t lo[2 * kTcMaxRadiusWide + 1];
 };
 
 // One column of a z / y pass: n_at axis tiles of TN x-columns at (x0, oth).
@@ -345,11 +351,11 @@ template <class Sched> struct ContigLaunch {
 
 // ---- z / y passes ------------------------------------------------------------------
 
-template <typename S, bool AXIS_Z, class Sched>
+template <typename S, bool AXIS_Z, int TN, class Sched>
 __global__ void __launch_bounds__(kThreads, 1)
 tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmap_out,
                   const __grid_constant__ StridedLaunch<Sched> p) {
-    constexpr int TN = StridedShape<AXIS_Z>::kTN, STAGES = StridedShape<AXIS_Z>::kStages, CHUNKS = TN / 64;
+    constexpr int STAGES = kStridedStages, CHUNKS = TN / 64;
     const PassTaps &tp = p.taps;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
@@ -384,7 +390,7 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
         const int quad = warp & 3, lo_half = (warp - 2) >> 2;
         const int o = quad * 32 + lane;
         const uint16_t *taps = lo_half ? tp.lo : tp.hi;
-        for (int ch = 0; ch < 3; ch++) {
+        for (int ch = 0; ch < tp.kcols / 32; ch++) {
             uint32_t r[32];
 #pragma unroll
             for (int j = 0; j < 32; j++) {
@@ -396,7 +402,7 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                 }
                 r[j] = v;
             }
-            tmem_st32(tmem + ((uint32_t) (quad * 32) << 16) + (lo_half ? kTmemALo : kTmemAHi) + ch * 32, r);
+            tmem_st32(tmem + ((uint32_t) (quad * 32) << 16) + 2 * TN + (lo_half ? tp.kcols : 0) + ch * 32, r);
         }
         tmem_st_wait();
     }
@@ -427,19 +433,23 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                         pm = nxt.in; px = nxt.x0; po = nxt.oth; pa = ap - cur.n_at; pr = nxt.in_rows;
                     }
                     if (pm) {
-                        for (int c = 0; c < CHUNKS; c++) {
-                            if (pr) tma_prefetch_3d(pm, px + 64 * c, pa * kTM - tp.radius, po);
-                            else tma_prefetch_3d(pm, px + 64 * c, po, pa * kTM - tp.radius);
-                        }
+                        for (int c = 0; c < CHUNKS; c++)
+                            for (int b = 0; b < tp.nbox; b++) {
+                                const int a = pa * kTM - tp.radius + b * tp.box_rows;
+                                if (pr) tma_prefetch_3d(pm, px + 64 * c, a, po);
+                                else tma_prefetch_3d(pm, px + 64 * c, po, a);
+                            }
                     }
                 }
                 const int a_in = at * kTM - tp.radius;
                 mbar_arrive_expect_tx(&full[s], stage_bytes);
-                for (int c = 0; c < CHUNKS; c++) {
-                    uint8_t *dst = ring + s * stage_bytes + c * tp.kp * 128;
-                    if (cur.in_rows) tma_load_3d(dst, cur.in, cur.x0 + 64 * c, a_in, cur.oth, &full[s]);
-                    else tma_load_3d(dst, cur.in, cur.x0 + 64 * c, cur.oth, a_in, &full[s]);
-                }
+                for (int c = 0; c < CHUNKS; c++)
+                    for (int b = 0; b < tp.nbox; b++) {
+                        uint8_t *dst = ring + s * stage_bytes + c * tp.kp * 128 + b * tp.box_rows * 128;
+                        const int a = a_in + b * tp.box_rows;
+                        if (cur.in_rows) tma_load_3d(dst, cur.in, cur.x0 + 64 * c, a, cur.oth, &full[s]);
+                        else tma_load_3d(dst, cur.in, cur.x0 + 64 * c, cur.oth, a, &full[s]);
+                    }
             }
             cur = nxt;
         }
@@ -464,9 +474,10 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                 // K step ks: 16 rows of the field tile (2048 bytes on, i.e. +128 in the
                 // descriptor's address field) and 8 tensor-memory columns of T.
                 const uint64_t bd = smem_desc_sw128(b0 + s * stage_bytes, tp.kp * 128, 1024);
+                const uint32_t a_hi = tmem + 2 * TN, a_lo = a_hi + tp.kcols;
                 for (int ks = 0; ks < tp.kp / 16; ks++) {
-                    umma_f16_ts(dt, tmem + kTmemAHi + ks * 8, bd + (uint64_t) (ks * 128), idesc, ks > 0 ? 1u : 0u);
-                    umma_f16_ts(dt, tmem + kTmemALo + ks * 8, bd + (uint64_t) (ks * 128), idesc, 1u);
+                    umma_f16_ts(dt, a_hi + ks * 8, bd + (uint64_t) (ks * 128), idesc, ks > 0 ? 1u : 0u);
+                    umma_f16_ts(dt, a_lo + ks * 8, bd + (uint64_t) (ks * 128), idesc, 1u);
                 }
                 umma_commit(&empty[s]);
                 umma_commit(&tfull[d]);
@@ -703,6 +714,240 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
     }
 }
 
+// ---- x pass, transposed form (radius 33..128) --------------------------------------
+//
+// With K = 128 + RA + R up to 384 the x pass's Toeplitz no longer fits shared
+// memory beside its tile ring, so the roles swap: the Toeplitz is the A
+// operand, in tensor memory like the z / y passes' (lane o = x output, K
+// packed two per column), and 64 volume rows of the field are the B operand
+// (K-major: the rows' x runs, as TMA lands them).  D^T[o, r] = sum_j
+// Tt[j, o] F[r, x0 - RA + j], so an epilogue thread owns one x of 32
+// consecutive rows: error feedback then runs along the rows (y), and the next
+// repetition's y pass removes the high-pass noise it leaves.  The mask words
+// of the 32 rows are read one per lane and transposed across the warp.
+constexpr int kXtRows = 64;       // rows per tile (N)
+constexpr int kXtStages = 3;
+constexpr int kXtEpiWarps = 8;    // two per lane quadrant, each drains 32 of the 64 rows
+constexpr int kXtThreads = 64 + 32 * kXtEpiWarps;
+constexpr int kXtStageWarpBytes = 32 * 64;
+
+__host__ __device__ constexpr int contig_t_smem_bytes(int kpa) {
+    return 1024 + kXtStages * (kpa / 64) * kXtRows * 128 /*B ring*/ + 1024 /*barriers, TMEM slot*/ +
+           kXtEpiWarps * kXtStageWarpBytes;
+}
+
+struct OneVolumeContigT {
+    static constexpr bool kParamMaps = true;
+    const void *mask;
+    void *out;
+    uint16_t *out_u16;
+    float *field_out;
+    int64_t rows, nx, ny, out_nz, out_z0;
+    int n_xt;
+    int64_t n_tiles;
+    __device__ __forceinline__ int64_t total() const { return n_tiles; }
+    __device__ __forceinline__ ContigTile tile(int64_t g, const CUtensorMap *in) const {
+        ContigTile t;
+        t.in = in;
+        t.mask = mask;
+        t.out = static_cast<uint16_t *>(out);
+        t.out_u16 = out_u16;
+        t.field_out = field_out;
+        t.rows = rows;
+        t.nx = nx;
+        t.ny = ny;
+        t.out_nz = out_nz;
+        t.out_z0 = out_z0;
+        const uint32_t rt = (uint32_t) g / (uint32_t) n_xt;
+        t.r0 = (int64_t) rt * kXtRows;
+        t.x0 = ((int) g - (int) rt * n_xt) * kXTN;
+        return t;
+    }
+};
+
+// 32 x 32 bit transpose across a warp: lane i holds row i (bit b = column b)
+// on entry, lane b holds column b (bit i = row i) on return.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t w, int lane) {
+    const uint32_t masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const int sh = 16 >> k;
+        const uint32_t m = masks[k];
+        const uint32_t y = __shfl_xor_sync(0xffffffffu, w, sh);
+        w = (lane & sh) ? ((w & ~m) | ((y & ~m) >> sh)) : ((w & m) | ((y & m) << sh));
+    }
+    return w;
+}
+
+template <typename S, int FMT>
+__global__ void __launch_bounds__(kXtThreads, 1)
+tc_contig_t_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ ContigLaunch<OneVolumeContigT> p) {
+    const PassTaps &tp = p.taps;
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    uint8_t *ring = smem_raw + (((raw + 1023) & ~1023u) - raw);
+    const int nkb = tp.kpa / 64;                       // 64-wide x boxes per stage
+    const int stage_bytes = nkb * kXtRows * 128;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kXtStages * stage_bytes);
+    uint64_t *full = bars, *empty = bars + kXtStages, *tfull = bars + 2 * kXtStages, *tempty = bars + 2 * kXtStages + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kXtStages + 4);
+    uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 1024;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t total = p.sched.total();
+    constexpr uint32_t kAcc = 2 * kXtRows;              // accumulator columns; the Toeplitz halves follow
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kXtStages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], kXtEpiWarps); }
+        fence_barrier_init();
+        prefetch_tmap(&tmap);
+    }
+    __syncwarp();
+    if (warp == 0) {
+        tmem_alloc(tmem_slot, kTmemColsStrided);
+        tmem_relinquish();
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    if (warp >= 2) {
+        // Tt^T halves into tensor memory: lane o holds x output o, K element j
+        // the tap j - o - RA + R (zero outside the band).
+        const int quad = warp & 3, lo_half = (warp - 2) >> 2;
+        const int o = quad * 32 + lane;
+        const uint16_t *taps = lo_half ? tp.lo : tp.hi;
+        for (int ch = 0; ch < tp.kcols / 32; ch++) {
+            uint32_t r[32];
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                uint32_t v = 0;
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int k = 2 * (ch * 32 + j) + e, t = k - o - tp.ra + tp.radius;
+                    if (t >= 0 && t <= 2 * tp.radius && k < tp.kp) v |= (uint32_t) taps[t] << (16 * e);
+                }
+                r[j] = v;
+            }
+            tmem_st32(tmem + ((uint32_t) (quad * 32) << 16) + kAcc + (lo_half ? tp.kcols : 0) + ch * 32, r);
+        }
+        tmem_st_wait();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+
+    if (warp == 0 && lane == 0) {
+        int64_t tl = 0;
+        for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
+            const int s = (int) (tl % kXtStages);
+            const uint32_t ph = (uint32_t) ((tl / kXtStages) & 1);
+            if (!mbar_wait(&empty[s], ph ^ 1, 1)) break;
+            const int64_t gp = g + kPrefetch * (int64_t) gridDim.x;
+            if (gp < total) {
+                const ContigTile t = p.sched.tile(gp, &tmap);
+                for (int kb = 0; kb < nkb; kb++) tma_prefetch_3d(t.in, t.x0 - tp.ra + 64 * kb, (int) t.r0, 0);
+            }
+            const ContigTile t = p.sched.tile(g, &tmap);
+            mbar_arrive_expect_tx(&full[s], stage_bytes);
+            for (int kb = 0; kb < nkb; kb++)
+                tma_load_3d(ring + s * stage_bytes + kb * kXtRows * 128, t.in, t.x0 - tp.ra + 64 * kb, (int) t.r0, 0,
+                            &full[s]);
+        }
+    } else if (warp == 1 && lane == 0) {
+        const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
+        const uint32_t idesc = idesc_f16(fmt, 0 /*A K-major*/, 0 /*B K-major*/, kTM, kXtRows);
+        const uint32_t b0 = smem_u32(ring);
+        const uint32_t a_hi = tmem + kAcc, a_lo = a_hi + tp.kcols;
+        int64_t tl = 0;
+        for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
+            const int s = (int) (tl % kXtStages);
+            const uint32_t ph = (uint32_t) ((tl / kXtStages) & 1);
+            const int d = (int) (tl & 1);
+            const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
+            if (!mbar_wait(&full[s], ph, 1) || !mbar_wait(&tempty[d], dph ^ 1, 3)) break;
+            tc_fence_after();
+            const uint32_t dt = tmem + d * kXtRows;
+            for (int ks = 0; ks < tp.kp / 16; ks++) {
+                // K step ks: 16 x-inputs = 32 bytes inside a 64-wide box of 64 rows.
+                const uint64_t bd = smem_desc_sw128(b0 + s * stage_bytes + (ks >> 2) * (kXtRows * 128) + (ks & 3) * 32, 16,
+                                                    1024);
+                umma_f16_ts(dt, a_hi + ks * 8, bd, idesc, ks > 0 ? 1u : 0u);
+                umma_f16_ts(dt, a_lo + ks * 8, bd, idesc, 1u);
+            }
+            umma_commit(&empty[s]);
+            umma_commit(&tfull[d]);
+        }
+    } else if (warp >= 2) {
+        const int quad = warp & 3;             // TMEM lane quadrant: x outputs quad * 32 + lane
+        const int half = (warp - 2) >> 2;      // rows half * 32 .. + 32 of the tile
+        uint8_t *stg = stage_out + (warp - 2) * kXtStageWarpBytes;
+        int64_t tl = 0;
+        for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
+            const ContigTile t = p.sched.tile(g, &tmap);
+            const int64_t rbase = t.r0 + half * 32;
+            const int64_t xq = t.x0 + quad * 32;  // this warp's 32 x outputs
+            const bool live = xq < t.nx;          // warp-uniform
+            // Lane i reads the mask flags of row rbase + i over the warp's 32 x;
+            // the transpose gives lane l the flags of its x over the 32 rows.
+            uint32_t mrow = 0;
+            if (live && rbase + lane < t.rows)
+                mrow = row_mask32<FMT>(t.mask, (rbase + lane) * t.nx + xq, t.nx - xq < 32 ? (int) (t.nx - xq) : 32,
+                                       t.rows * t.nx);
+            const int d = (int) (tl & 1);
+            const uint32_t dph = (uint32_t) ((tl >> 1) & 1);
+            if (!mbar_wait(&tfull[d], dph, 2)) break;
+            tc_fence_after();
+            float h[32];
+            __syncwarp();
+            tmem_ld32(tmem + ((uint32_t) (quad * 32) << 16) + d * kXtRows + half * 32, h);
+            const uint32_t m = warp_transpose32(mrow, lane);
+            const int64_t x = xq + lane;
+            if (p.final_pass) {
+                if (live && x < t.nx) {
+#pragma unroll
+                    for (int i = 0; i < 32; i++) {
+                        const int64_t row = rbase + i;
+                        if (row < t.rows) {
+                            const float v = ((m >> i) & 1u) ? 1.0f : h[i] * tp.inv_scale;
+                            if (t.out_u16) t.out_u16[row * t.nx + x] = quantise_u16(v);
+                            if (t.field_out) t.field_out[row * t.nx + x] = v;
+                        }
+                    }
+                }
+            } else if (live) {
+                // 16-bit field, error feedback along the rows; stage the 32 rows x 32 x
+                // chunk and write 8 rows (8 x 64 bytes) per instruction.
+                uint16_t q[32];
+                narrow32_masked<S>(h, m, tp.inv_scale, tp.error_feedback, q);
+                const int64_t oi = rbase + lane < t.rows ? contig_out_index(t, rbase + lane, xq) : -1;
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 32; i++)
+                    *reinterpret_cast<uint16_t *>(stg + i * 64 + ((((lane >> 3) ^ ((i >> 1) & 3))) << 4) + (lane & 7) * 2) = q[i];
+                __syncwarp();
+                const int sub = lane & 3, rsub = lane >> 2;
+#pragma unroll
+                for (int r4 = 0; r4 < 4; r4++) {
+                    const int rr = r4 * 8 + rsub;
+                    const int64_t o = __shfl_sync(0xffffffffu, oi, rr);
+                    const uint4 w = *reinterpret_cast<const uint4 *>(stg + rr * 64 + ((sub ^ ((rr >> 1) & 3)) << 4));
+                    if (o >= 0 && xq + sub * 8 < t.nx) *reinterpret_cast<uint4 *>(t.out + o + sub * 8) = w;
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[d]);
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kTmemColsStrided);
+    }
+}
+
 // Fills the taps of one pass: hi/lo halves of kernel x scale (1 for BF16, 2^10 for FP16).
 inline void fill_pass_taps(PassTaps &t, const float *kernel, int radius, int ra, int kp, bool is_bf16,
                            bool error_feedback) {
@@ -710,6 +955,9 @@ inline void fill_pass_taps(PassTaps &t, const float *kernel, int radius, int ra,
     t.ra = ra;
     t.kp = kp;
     t.kpa = (int) round_up(kp, 64);
+    t.kcols = toeplitz_cols(kp);
+    t.nbox = kp > 256 ? 2 : 1;  // kp is a multiple of 16, so kp / 2 is a whole number of 8-row swizzle atoms
+    t.box_rows = kp / t.nbox;
     t.error_feedback = error_feedback ? 1 : 0;
     const float scale = is_bf16 ? 1.0f : 1024.0f;
     t.inv_scale = 1.0f / scale;

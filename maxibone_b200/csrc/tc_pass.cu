@@ -37,7 +37,7 @@ static float from_f16(uint16_t b) { return __half2float(__ushort_as_half(b)); }
 
 
 bool tc_supported(int radius, int64_t nz, int64_t ny, int64_t nx) {
-    if (radius < 1 || radius > kTcMaxRadius) return false;
+    if (radius < 1 || radius > kTcMaxRadiusWide) return false;
     if (nx % 8 != 0 || nx < 64) return false;  // TMA: 16-byte row strides, at least one 64-wide box
     if (nz > INT32_MAX / 2 || ny > INT32_MAX / 2 || nx > INT32_MAX / 2) return false;
     if (nz * ny >= (int64_t(1) << 31)) return false;  // rows and tile indices fit 32-bit arithmetic
@@ -54,8 +54,7 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
                        int radius, bool error_feedback, cudaStream_t st, const YzRows *in_rows) {
     if (!axis_z) in_rows = nullptr;
     const bool is_bf16 = std::is_same<S, __nv_bfloat16>::value;
-    const int tn = axis_z ? StridedShape<true>::kTN : StridedShape<false>::kTN;
-    const int stages = axis_z ? StridedShape<true>::kStages : StridedShape<false>::kStages;
+    const int tn = strided_tn(radius), stages = kStridedStages;
     StridedLaunch<OneVolumeStrided> p{};
     fill_pass_taps(p.taps, kernel, radius, 0, (int) round_up(kTM + 2 * radius, 16), is_bf16, error_feedback);
     OneVolumeStrided &sc = p.sched;
@@ -74,12 +73,13 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
     const CUtensorMapDataType dt = is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
     const cuuint64_t dims[3] = {(cuuint64_t) nx, (cuuint64_t) ny, (cuuint64_t) nz};
     const cuuint64_t strides[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (nx * ny * 2)};
-    const cuuint32_t box[3] = {64u, axis_z ? 1u : (cuuint32_t) p.taps.kp, axis_z ? (cuuint32_t) p.taps.kp : 1u};
+    const cuuint32_t brows = (cuuint32_t) p.taps.box_rows;
+    const cuuint32_t box[3] = {64u, axis_z ? 1u : brows, axis_z ? brows : 1u};
     const cuuint32_t estr[3] = {1, 1, 1};
     // z pass over [y][z][x] rows: dims (x, z, y), rows nx apart, y slabs nz_total * nx apart.
     const cuuint64_t rdims[3] = {(cuuint64_t) nx, (cuuint64_t) nz, (cuuint64_t) ny};
     const cuuint64_t rstrides[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (in_rows ? in_rows->nz_total * nx * 2 : 0)};
-    const cuuint32_t rbox[3] = {64u, (cuuint32_t) p.taps.kp, 1u};
+    const cuuint32_t rbox[3] = {64u, brows, 1u};
     void *in_base = in_rows ? static_cast<void *>(static_cast<S *>(in_rows->base) + in_rows->z0 * nx)
                             : static_cast<void *>(const_cast<S *>(in));
     CUresult cr = tc_encode_fn()(&map, dt, 3, in_base, in_rows ? rdims : dims, in_rows ? rstrides : strides,
@@ -94,8 +94,12 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
     }
+    if (2 * tn + 2 * p.taps.kcols > (int) kTmemColsStrided) return cudaErrorInvalidValue;
     const int smem = strided_smem_bytes(p.taps.kp, tn, stages);
-    auto *kern = axis_z ? tc_strided_kernel<S, true, OneVolumeStrided> : tc_strided_kernel<S, false, OneVolumeStrided>;
+    auto *kern = tn == 128 ? (axis_z ? tc_strided_kernel<S, true, 128, OneVolumeStrided>
+                                     : tc_strided_kernel<S, false, 128, OneVolumeStrided>)
+                           : (axis_z ? tc_strided_kernel<S, true, 64, OneVolumeStrided>
+                                     : tc_strided_kernel<S, false, 64, OneVolumeStrided>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
@@ -124,12 +128,62 @@ void tc_split_taps(const float *kernel, int radius, bool is_bf16, float scale, u
     }
 }
 
+// The x pass in its transposed form (radius above kTcMaxRadius).
+template <typename S>
+static cudaError_t tc_contig_t(const S *in, S *out, const void *mask, int mask_fmt, bool final_pass,
+                               uint16_t *out_u16, float *field_out, int64_t nz, int64_t ny, int64_t nx,
+                               const float *kernel, int radius, bool error_feedback, cudaStream_t st,
+                               const YzRows *out_rows) {
+    const bool is_bf16 = std::is_same<S, __nv_bfloat16>::value;
+    ContigLaunch<OneVolumeContigT> p{};
+    const int ra = (int) round_up(radius, 8);
+    fill_pass_taps(p.taps, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback);
+    if (kXtRows * 2 + 2 * p.taps.kcols > (int) kTmemColsStrided) return cudaErrorInvalidValue;
+    p.final_pass = final_pass ? 1 : 0;
+    OneVolumeContigT &sc = p.sched;
+    sc.out = out_rows ? out_rows->base : out;
+    sc.mask = mask;
+    sc.out_u16 = out_u16;
+    sc.field_out = field_out;
+    sc.rows = nz * ny;
+    sc.nx = nx;
+    sc.ny = ny;
+    sc.out_nz = out_rows ? out_rows->nz_total : 0;
+    sc.out_z0 = out_rows ? out_rows->z0 : 0;
+    sc.n_xt = (int) ceil_div(nx, kXTN);
+    sc.n_tiles = (int64_t) sc.n_xt * ceil_div(sc.rows, kXtRows);
+
+    CUtensorMap map;
+    const cuuint64_t dims[3] = {(cuuint64_t) nx, (cuuint64_t) sc.rows, 1};
+    const cuuint64_t strides[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (nx * sc.rows * 2)};
+    const cuuint32_t box[3] = {64u, (cuuint32_t) kXtRows, 1u};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult cr = tc_encode_fn()(&map, is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
+                                 const_cast<S *>(in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    const int smem = contig_t_smem_bytes(p.taps.kpa);
+    auto *kern = mask_fmt == MAXI_MASK_U8 ? tc_contig_t_kernel<S, MAXI_MASK_U8> : tc_contig_t_kernel<S, MAXI_MASK_BITPACKED>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t grid = std::min<int64_t>(sc.n_tiles, sms);
+    kern<<<(unsigned) grid, kXtThreads, smem, st>>>(map, p);
+    return cudaGetLastError();
+}
+
 template <typename S>
 cudaError_t tc_contig(const S *in, S *out, const void *mask, int mask_fmt, bool final_pass, uint16_t *out_u16,
                       float *field_out, int64_t nz, int64_t ny, int64_t nx, const float *kernel, int radius,
                       bool error_feedback, cudaStream_t st, const YzRows *out_rows) {
     const bool is_bf16 = std::is_same<S, __nv_bfloat16>::value;
     if (final_pass) out_rows = nullptr;
+    if (radius > kTcMaxRadius)
+        return tc_contig_t<S>(in, out, mask, mask_fmt, final_pass, out_u16, field_out, nz, ny, nx, kernel, radius,
+                              error_feedback, st, out_rows);
     ContigLaunch<OneVolumeContig> p{};
     const int ra = (int) round_up(radius, 8);
     fill_pass_taps(p.taps, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback);

@@ -7,12 +7,18 @@
 namespace maxi {
 namespace tc {
 
-// Largest kernel radius the tensor-core passes serve (the K extent 128 + 2R
-// must fit one TMA box of at most 256 rows, and both Toeplitz halves plus a
-// 2-stage tile ring must fit shared memory).
+// Largest kernel radius of the batched tensor-core passes and of the x pass in
+// its direct form (its shared-memory Toeplitz, K = 128 + 2 * 32 rows of both
+// halves, and a 2-stage tile ring must fit shared memory).
 constexpr int kTcMaxRadius = 32;
+// Largest radius of the single-volume tensor-core passes: the z / y passes
+// hold the Toeplitz halves in tensor memory (192 columns each at radius 128,
+// next to 64-column accumulators) and load K = 128 + 2r rows as two TMA
+// boxes; the x pass above radius 32 runs in its transposed form.
+constexpr int kTcMaxRadiusWide = 128;
 
-// True when the device is sm_100 and the shape fits the TMA constraints.
+// True when the device is sm_100 and the shape fits the TMA constraints
+// (single-volume passes, radius <= kTcMaxRadiusWide).
 bool tc_supported(int radius, int64_t nz, int64_t ny, int64_t nx);
 
 // A field stored with its rows in [y][z][x] order: `base` holds a volume of

@@ -5,7 +5,7 @@ FP32 accumulation; they must agree with the CUDA-core passes of the same form
 (both store the field in the same 16-bit type) and stay within the stated
 error of the FP64 form.  Shapes cover partial x chunks (nx not a multiple of
 128), axes shorter than and not multiple of the 128-output tile, and the
-radius range the tensor-core path serves (1..32).
+radius range the tensor-core path serves (1..128).
 """
 import numpy as np
 import pytest
@@ -59,6 +59,31 @@ def test_tensor_core_radius_range(radius):
         _, cc = run(mask, kernel, 4, field, False, True)
         assert np.abs(got - cc).max() <= TC_VS_CC[field]
         assert np.abs(got.astype(np.float64) - want).max() <= VS_F64[field]
+
+
+# Radii above 32: z / y passes with the Toeplitz halves in tensor memory (64-column
+# tiles and two TMA boxes per K run above radius 64), the x pass in its transposed
+# form with error feedback along the rows.
+@pytest.mark.parametrize("radius", [33, 40, 64, 65, 96, 128])
+@pytest.mark.parametrize("shape", [(48, 100, 264), (70, 131, 136)])
+def test_tensor_core_wide_radius(radius, shape):
+    mask = spheres_mask(shape, 10, (3, 12), seed=radius + shape[2])
+    kernel = gauss_kernel(radius / 4.0).astype(np.float32)
+    _, want = run(mask, kernel, 3, "f64")
+    for field in ("f16", "bf16"):
+        u16, got = run(mask, kernel, 3, field, True, True)
+        _, cc = run(mask, kernel, 3, field, False, True)
+        assert np.abs(got - cc).max() <= TC_VS_CC[field]
+        assert np.abs(got.astype(np.float64) - want).max() <= VS_F64[field]
+        assert np.all(u16[mask > 0] == 65535)
+
+
+def test_tensor_core_wide_radius_repeats_bit_for_bit():
+    mask = spheres_mask((64, 96, 200), 12, (3, 10), seed=11)
+    kernel = gauss_kernel(32.0).astype(np.float32)
+    a = run(mask, kernel, 4, "bf16")[1]
+    b = run(mask, kernel, 4, "bf16")[1]
+    np.testing.assert_array_equal(a, b)
 
 
 def test_error_feedback_reduces_bf16_error():

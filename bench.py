@@ -121,6 +121,25 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(value: float, world: int, device: str) -> float:
+    """The largest `value` over all ranks of the process group (every rank calls
+    this at the same point); the identity on one rank."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, vox: int, reps: int, steps: int, seconds: float) -> float:
+    """Gvox*rep/s of the whole job: every rank diffuses its own volume of `vox`
+    voxels `steps` times; `seconds` is the slowest rank's time."""
+    return world * vox * reps * steps / seconds / 1e9
+
+
 def cpu_reference_time(shape, sigma, reps, repeats):
     """Time the reference OpenMP module (or the oracle port) on a synthetic sample."""
     import numpy as np
@@ -230,6 +249,30 @@ def batched_section(device, torch, np, stream, reps=50):
     del masks, outs, fouts, ws
     torch.cuda.empty_cache()
     return res
+
+
+def batched_plan_on_volume(device, torch, np, mask, kernel, reps, stream):
+    """The BF16 batch plan (CUDA graph of persistent tensor-core launches, one per
+    pass) over the workload's single volume: the batched form on the 1024^3 mask."""
+    vox = int(mask.numel())
+    out = torch.empty(tuple(mask.shape), dtype=torch.uint16, device="cuda")
+    plan = device.BatchPlan([mask], [kernel], reps, outputs=[out], field="bf16")
+    plan.run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_t = 2
+    e0.record(stream)
+    for _ in range(n_t):
+        plan.run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    device.tensor_core_status()
+    plan.close()
+    t = e0.elapsed_time(e1) / n_t
+    peak, _ = load_peaks()
+    gbs = (6 * 2 + 0.125) * vox * reps / (t / 1e3) / 1e9
+    del out
+    return {"value": vox * reps / (t / 1e3) / 1e9, "unit": UNIT, "ms": t, "hbm_gbs": gbs, "hbm_frac": gbs / peak}
 
 
 def out_of_core_section(torch, np, reps=20, shape=(4096, 1728, 2048), slab=1024):
@@ -379,12 +422,8 @@ def main():
     prof = device.profile_read()
     device.profile_enable(False)
     barrier()
-    ms = t0.elapsed_time(t1)
-    if world > 1:
-        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-    value = world * vox * reps * args.steps / (ms / 1e3) / 1e9
+    ms = max_over_ranks(t0.elapsed_time(t1), world, "cuda")
+    value = whole_job_rate(world, vox, reps, args.steps, ms / 1e3)
     launches = sum(c for _, c in prof.values())
 
     # Roofline of the dominant kernel: algorithmic bytes per launch / event duration.
@@ -441,12 +480,8 @@ def main():
         tw = time.perf_counter()
         for _ in range(e2e_steps):
             diffusion(m_np, kernel, o_np, reps)
-        e2e_s = time.perf_counter() - tw
-        if world > 1:
-            tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
-        line["e2e"] = {"value": world * vox * reps * e2e_steps / e2e_s / 1e9, "unit": UNIT,
+        e2e_s = max_over_ranks(time.perf_counter() - tw, world, "cuda")
+        line["e2e"] = {"value": whole_job_rate(world, vox, reps, e2e_steps, e2e_s), "unit": UNIT,
                        "h2d_bytes_per_step": vox, "d2h_bytes_per_step": 2 * vox, "steps": e2e_steps,
                        "timing": "host clock around the synchronous drop-in diffusion() call (max over ranks)"}
         del host_mask, host_out
@@ -505,6 +540,9 @@ def main():
         del f64
 
         line["batched"] = batched_section(device, torch, np, stream)
+        line["batched"]["bf16_plan_on_workload_volume"] = bv = batched_plan_on_volume(
+            device, torch, np, mask, kernel, reps, stream)
+        bv["speedup_vs_f32"] = bv["value"] / forms["f32"]["value"]
 
         if args.extended:
             line["out_of_core"] = out_of_core_section(torch, np)

@@ -106,6 +106,10 @@ static cudaError_t enqueue_single(maxi_batch_plan *p, BatchVolume &bv, int32_t e
 // All repetitions of a tensor-core group as batched launches.
 template <typename S>
 static cudaError_t enqueue_group_tc(maxi_batch_plan *p, TcGroup &g, cudaStream_t st) {
+    // A group of one volume runs the single-volume tensor-core launches (tensor
+    // maps as kernel parameters instead of a device table); the arithmetic per
+    // tile is the same.
+    if (g.members.size() == 1) return enqueue_single<S>(p, p->vols[g.members[0]], 0, st);
     cudaError_t e = enqueue_init<S>(p, g.members, st);
     if (e != cudaSuccess) return e;
     const bool bf16 = std::is_same<S, __nv_bfloat16>::value;
@@ -279,7 +283,8 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
         const TcGroup &g = p->groups[k];
         snprintf(line, sizeof(line), "group %zu: %zu volumes, kernel length %zu, %lld repetitions, %s%s%s\n", k,
                  g.members.size(), g.kernel.size(), (long long) g.reps,
-                 g.use_tc ? "one tensor-core launch per pass" : "per-volume CUDA-core passes",
+                 !g.use_tc ? "per-volume CUDA-core passes"
+                 : g.members.size() == 1 ? "single-volume tensor-core launches" : "one tensor-core launch per pass",
                  g.note.empty() ? "" : "; ", g.note.c_str());
         p->description += line;
     }

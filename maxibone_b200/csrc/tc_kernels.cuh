@@ -242,32 +242,36 @@ struct ManyVolumesStrided {
     const TcVol *vols;
     const int64_t *prefix;  // n_vol + 1 prefix sums of the volumes' columns
     int n_vol, axis_z, in_buf, tn, z_in_rows;  // z_in_rows: the z pass reads [y][z][x] rows
+    // The z / y kernels have registers to spare: the cursor keeps the current
+    // volume's column data, so a column within it costs no table reads.
     struct Cursor {
         int64_t lo = 0, hi = 0;  // the current volume's columns [lo, hi)
-        int v = 0;
+        int n_xc = 1;
+        StridedCol base;
     };
     __device__ __forceinline__ int64_t total() const { return __ldg(prefix + n_vol); }
     __device__ __forceinline__ StridedCol col(int64_t g, const CUtensorMap *, const CUtensorMap *, Cursor &cur) const {
         if (g < cur.lo || g >= cur.hi) {
-            cur.v = find_volume(prefix, n_vol, g);
-            cur.lo = __ldg(prefix + cur.v);
-            cur.hi = __ldg(prefix + cur.v + 1);
+            const int v = find_volume(prefix, n_vol, g);
+            const TcVol &vol = vols[v];
+            cur.lo = __ldg(prefix + v);
+            cur.hi = __ldg(prefix + v + 1);
+            cur.n_xc = axis_z ? vol.n_xc_z : vol.n_xc_y;
+            StridedCol &c = cur.base;
+            c.in = axis_z ? (z_in_rows ? &vol.zrows[in_buf] : &vol.map[0][in_buf]) : &vol.map[1][in_buf];
+            c.in_rows = axis_z ? z_in_rows : 1;
+            c.out_map = &vol.ystore[in_buf ^ 1];
+            c.out = vol.buf[in_buf ^ 1];
+            c.A = axis_z ? vol.nz : vol.ny;
+            c.stride_a = axis_z ? vol.ny * vol.nx : vol.nx;
+            c.stride_o = axis_z ? vol.nx : vol.ny * vol.nx;
+            c.nx = vol.nx;
+            c.n_at = axis_z ? vol.n_at_z : vol.n_at_y;
         }
-        const TcVol &vol = vols[cur.v];
         const int64_t local = g - cur.lo;
-        const int n_xc = axis_z ? vol.n_xc_z : vol.n_xc_y;
-        StridedCol c;
-        c.in = axis_z ? (z_in_rows ? &vol.zrows[in_buf] : &vol.map[0][in_buf]) : &vol.map[1][in_buf];
-        c.in_rows = axis_z ? z_in_rows : 1;
-        c.out_map = &vol.ystore[in_buf ^ 1];
-        c.out = vol.buf[in_buf ^ 1];
-        c.A = axis_z ? vol.nz : vol.ny;
-        c.stride_a = axis_z ? vol.ny * vol.nx : vol.nx;
-        c.stride_o = axis_z ? vol.nx : vol.ny * vol.nx;
-        c.nx = vol.nx;
-        c.n_at = axis_z ? vol.n_at_z : vol.n_at_y;
-        c.oth = (int) ((uint32_t) local / (uint32_t) n_xc);
-        c.x0 = ((int) local - c.oth * n_xc) * tn;
+        StridedCol c = cur.base;
+        c.oth = (int) ((uint32_t) local / (uint32_t) cur.n_xc);
+        c.x0 = ((int) local - c.oth * cur.n_xc) * tn;
         return c;
     }
 };

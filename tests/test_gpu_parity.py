@@ -131,6 +131,24 @@ def test_device_bitpack_matches_reference_layout():
     np.testing.assert_array_equal(decoded.cpu().numpy(), z["decoded"])
 
 
+def test_dropin_bitpacking_module_matches_reference_golden():
+    # The pybind-style module through the reference's import path.
+    import importlib
+    import os
+    from conftest import GOLDEN
+
+    from maxibone_b200 import reference_imports
+    reference_imports.install()
+    bitpacking = importlib.import_module("lib.cpp.gpu.bitpacking")
+    z = np.load(os.path.join(GOLDEN, "bitpack_u32.npz"))
+    packed = np.zeros(z["packed"].shape, np.uint32)
+    bitpacking.encode(z["mask"], packed)
+    np.testing.assert_array_equal(packed, z["packed"])
+    decoded = np.full(z["mask"].shape, 7, np.uint8)
+    bitpacking.decode(z["packed"], decoded)
+    np.testing.assert_array_equal(decoded, z["decoded"])
+
+
 def test_fp64_form_matches_cpu_fp64_oracle():
     mask = spheres_mask((24, 28, 36), 8, (2, 6), seed=8)
     k64 = gauss_kernel(2.0)

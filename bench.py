@@ -165,14 +165,14 @@ def cpu_reference_time(shape, sigma, reps, repeats):
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     vox = shape[0] * shape[1] * shape[2]
     del torch
-    return times, kind, cores, vox
+    return times, kind, cores, vox, (mask, kernel, out if ref is not None else None)
 
 
 def run_reference_arm(args, rank):
     if rank != 0:
         return
     shape, sigma, reps = CPU_SAMPLE
-    times, kind, cores, vox = cpu_reference_time(shape, sigma, reps, args.warmup + args.steps)
+    times, kind, cores, vox, _ = cpu_reference_time(shape, sigma, reps, args.warmup + args.steps)
     timed = times[args.warmup:]
     total = sum(timed)
     value = vox * reps * len(timed) / total / 1e9
@@ -490,6 +490,7 @@ def main():
         f64 = torch.empty(shape, dtype=torch.float64, device="cuda")
         device.diffuse(mask, kernel, reps, field="f64", field_out=f64)
         forms = {}
+        f32_field = None
         variants = [("f32", "f32", {}), ("bf16", "bf16", {}), ("f16", "f16", {}),
                     ("bf16_nearest", "bf16", {"error_feedback": False}),
                     ("bf16_cuda_cores", "bf16", {"tensor_cores": False}),
@@ -530,9 +531,17 @@ def main():
                            "mean_abs_err_vs_f64": float(err.mean().item()),
                            "mask_voxels_exact": bool((out.view(torch.int16)[mask > 0] == -1).all().item()),
                            "per_kind_ms": {k: v[0] / v[1] for k, v in fprof.items()}}
+            if name == "f32":
+                f32_field = fo
+            else:
+                forms[name]["_vs_f32"] = float((fo - f32_field).abs_().max().item())
             del err, fo, w
             torch.cuda.empty_cache()
+        del f32_field
         line["precision"] = forms
+        for name in forms:
+            if name != "f32":
+                forms[name]["max_abs_err_vs_f32"] = forms[name].pop("_vs_f32", None)
         # The BF16 form against the plain FP32 form on this workload.
         line["bf16_vs_f32"] = {"speedup": forms["bf16"]["value"] / forms["f32"]["value"],
                                "bf16_whole_rep_hbm_frac": forms["bf16"]["roofline"]["whole_rep_frac"],
@@ -550,11 +559,18 @@ def main():
 
         if rank == 0 and world == 1:
             cshape, csig, creps = CPU_SAMPLE
-            times, kind, cores, cvox = cpu_reference_time(cshape, csig, creps, 2)
+            times, kind, cores, cvox, (cmask, ckernel, cref) = cpu_reference_time(cshape, csig, creps, 2)
             line["cpu_baseline"] = {"value": cvox * creps / min(times) / 1e9, "unit": UNIT, "cores": cores,
                                     "kind": kind,
                                     "sample": f"bone-implant mask {cshape[0]}^3, sigma={csig} (65 taps), R={creps}, "
                                               f"best of 2 calls"}
+            if cref is not None:
+                # The FP32 path against the reference module's own uint16 output on the sample.
+                gout = torch.empty(cshape, dtype=torch.uint16, device="cuda")
+                device.diffuse(torch.from_numpy(cmask).cuda(), ckernel, creps, output=gout, field="f32")
+                d = np.abs(gout.cpu().numpy().astype(np.int32) - cref.astype(np.int32))
+                line["cpu_baseline"]["f32_vs_reference_u16"] = {"max_lsb": int(d.max()),
+                                                                "voxels_differing": int((d > 0).sum())}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -95,8 +95,9 @@ __host__ __device__ constexpr int strided_tn(int radius) { return radius <= 64 ?
 constexpr uint32_t kTmemColsStrided = 512;
 __host__ __device__ constexpr int toeplitz_cols(int kp) { return ((kp / 2) + 31) / 32 * 32; }
 
-// Per-epilogue-warp staging: two 32-row x 32-column 16-bit buffers (z pass:
-// row stride 80 bytes; y pass: the store map's 64-byte swizzle).
+// Per-epilogue-warp staging: two 32-row x 32-column 16-bit buffers, 64-byte
+// rows with their 16-byte chunks XOR-swizzled by row / 2 (the y pass's store
+// map uses the same 64-byte swizzle; the z pass reads the rows back itself).
 constexpr int kStageWarpBytes = 2 * 32 * 64;
 
 __host__ __device__ constexpr int strided_smem_bytes(int kp, int tn, int stages) {
@@ -519,14 +520,15 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                         // stage the 32 x 32 chunk and write 8 rows (8 x 64 bytes) per instruction.
                         __syncwarp();
 #pragma unroll
-                        for (int i = 0; i < 4; i++) *reinterpret_cast<uint4 *>(stg + lane * 80 + i * 16) = pack8(q + 8 * i);
+                        for (int i = 0; i < 4; i++)
+                            *reinterpret_cast<uint4 *>(stg + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) = pack8(q + 8 * i);
                         __syncwarp();
                         const int sub = lane & 3, rsub = lane >> 2;
 #pragma unroll
                         for (int r4 = 0; r4 < 4; r4++) {
                             const int rr = r4 * 8 + rsub;
                             const int64_t ar = (int64_t) at * kTM + quad * 32 + rr;
-                            const uint4 w = *reinterpret_cast<const uint4 *>(stg + rr * 80 + sub * 16);
+                            const uint4 w = *reinterpret_cast<const uint4 *>(stg + rr * 64 + ((sub ^ ((rr >> 1) & 3)) << 4));
                             if (ar < c.A && xb + sub * 8 < c.nx)
                                 *reinterpret_cast<uint4 *>(out + ar * c.stride_a + (int64_t) c.oth * c.stride_o + xb +
                                                            sub * 8) = w;

@@ -81,6 +81,26 @@ def test_uneven_volumes_many_reps_batch_equals_single_and_repeats(field):
         assert torch.equal(fouts[i], runs[0]), (i, sh)
 
 
+def test_batch_with_wide_radius_volume_equals_single_runs():
+    # Radius 48 is above the batched tensor-core passes' 32: that volume takes the
+    # per-volume path (wide-radius tensor-core passes) inside the plan.
+    from maxibone_b200.synthetic import spheres_mask
+    shapes, sigmas = [(64, 96, 136), (48, 80, 128), (40, 64, 192)], [12.0, 2.0, 12.0]
+    masks = [torch.from_numpy(spheres_mask(sh, 6, (3, 9), seed=40 + i)).cuda() for i, sh in enumerate(shapes)]
+    kernels = [gauss_kernel(s).astype(np.float32) for s in sigmas]
+    fouts = [torch.empty(sh, dtype=torch.float32, device="cuda") for sh in shapes]
+    plan = device.BatchPlan(masks, kernels, 3, field="bf16", field_outs=fouts)
+    plan.run()
+    torch.cuda.synchronize()
+    device.tensor_core_status()
+    plan.close()
+    for i, sh in enumerate(shapes):
+        fo = torch.empty(sh, dtype=torch.float32, device="cuda")
+        device.diffuse(masks[i], kernels[i], 3, field="bf16", field_out=fo)
+        torch.cuda.synchronize()
+        assert torch.equal(fouts[i], fo), i
+
+
 def test_batch_plan_replays():
     masks, outs, fouts, kernels = make_batch("bf16")
     plan = device.BatchPlan(masks, kernels, REPS, outputs=outs, field="bf16", field_outs=fouts)

@@ -251,6 +251,70 @@ def batched_section(device, torch, np, stream, reps=50):
     return res
 
 
+def fields_section(torch, np, gauss_u16, stream):
+    """The Gaussian + EDT field combination (the pipeline step after the
+    diffusion) on the workload's uint16 output and a synthetic EDT-like field,
+    against the reference's own CPU form of the step on a 256^3 sample."""
+    import oracle
+    from maxibone_b200.fields import combine_fields
+
+    shape = tuple(gauss_u16.shape)
+    vox = int(np.prod(shape))
+    g = gauss_u16.view(torch.int16)
+    zz = torch.arange(shape[0], device="cuda", dtype=torch.float32)[:, None, None]
+    yy = torch.arange(shape[1], device="cuda", dtype=torch.float32)[None, :, None]
+    xx = torch.arange(shape[2], device="cuda", dtype=torch.float32)[None, None, :]
+    e = ((torch.sin(zz * 0.05) + torch.cos(yy * 0.03) + torch.sin(xx * 0.07) + 3.0) * 10000.0).to(torch.int32)
+    e = e.to(torch.int16)
+    out = torch.empty_like(g)
+    combine_fields(g, e, out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_t = 5
+    e0.record(stream)
+    for _ in range(n_t):
+        combine_fields(g, e, out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n_t
+    peak, _ = load_peaks()
+    alg = 14 * vox  # three passes reading both 2-byte fields, one 2-byte write
+    res = {"workload": f"{shape[0]}x{shape[1]}x{shape[2]} uint16 Gaussian field (the diffusion output) + synthetic "
+                       "uint16 EDT-like field", "value": vox / (ms / 1e3) / 1e9, "unit": "Gvox/s", "ms": ms,
+           "hbm_gbs": alg / (ms / 1e3) / 1e9, "hbm_frac": alg / (ms / 1e3) / 1e9 / peak,
+           "alg_bytes_per_voxel": 14, "timing": "CUDA events around 5 synchronous calls (two host read-backs each)"}
+    # The reference's own form of the step on a bounded sample: its numpy operations with
+    # the reference's compiled normalized_convert (oracle/_ref), else the oracle's numpy port.
+    n = 256
+    gs = gauss_u16[:n, :n, :n].cpu().numpy() if min(shape) >= n else gauss_u16.cpu().numpy()
+    es = e.view(torch.uint16)[: gs.shape[0], : gs.shape[1], : gs.shape[2]].cpu().numpy()
+    gs, es = np.ascontiguousarray(gs), np.ascontiguousarray(es)
+    gen = oracle.reference_module("general")
+    cyl = oracle.cylinder_mask(gs.shape[1], gs.shape[2])
+    t0 = time.perf_counter()
+    c = gs.astype(np.float32) / gs.max()
+    c -= es.astype(np.float32) / es.max()
+    c += np.abs(c.min())
+    c /= c.max()
+    c *= cyl
+    if gen is not None:
+        r = np.empty(c.shape, np.uint16)
+        gen.normalized_convert(np.ascontiguousarray(c), r)
+    else:
+        r = oracle.normalized_convert_u16(c)
+    r *= cyl
+    cpu_s = time.perf_counter() - t0
+    gpu_r = combine_fields(gs, es)
+    res["cpu_baseline"] = {"value": gs.size / cpu_s / 1e9, "unit": "Gvox/s",
+                           "kind": "reference" if gen is not None else "port",
+                           "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+                           "sample": f"{gs.shape[0]}x{gs.shape[1]}x{gs.shape[2]} crop, numpy steps of "
+                                     "0975_combine_fields + normalized_convert, one call",
+                           "gpu_equals_reference": bool(np.array_equal(gpu_r, r))}
+    del e, out
+    return res
+
+
 def batched_plan_on_volume(device, torch, np, mask, kernel, reps, stream):
     """The BF16 batch plan (CUDA graph of persistent tensor-core launches, one per
     pass) over the workload's single volume: the batched form on the 1024^3 mask."""
@@ -553,6 +617,7 @@ def main():
                                "bf16_max_abs_err_vs_f64": forms["bf16"]["max_abs_err_vs_f64"]}
         del f64
 
+        line["fields"] = {"combine_fields": fields_section(torch, np, out, stream)}
         line["batched"] = batched_section(device, torch, np, stream)
         line["batched"]["bf16_plan_on_workload_volume"] = bv = batched_plan_on_volume(
             device, torch, np, mask, kernel, reps, stream)

@@ -237,6 +237,20 @@ int maxi_diffusion_on_disk(const char *input_file, const float *kernel, int64_t 
 int maxi_bitpack_encode(const uint8_t *mask, int64_t n, uint32_t *packed, void *stream);
 int maxi_bitpack_decode(const uint32_t *packed, int64_t n, uint8_t *mask, void *stream);
 
+/*
+ * Combination of the Gaussian (diffusion) field and the implant EDT field into
+ * one uint16 field: the step after the diffusion in maxibone's pipeline
+ * (src/processing_steps/0975_combine_fields.py:38-62, with its to_int from
+ * src/lib/cpp/include/general.hh:78-118), bit-identical to it.  gauss, edt,
+ * output: device uint16[nz][ny][nx]; the cylinder mask spans y and x as
+ * generate_cylinder_mask(ny, nx) (the script's generate_cylinder_mask(nx) for
+ * square planes).  Three passes over both fields with two small read-backs, so
+ * the call synchronises the stream.  A field whose maximum is 0 is rejected
+ * (the reference divides by it).
+ */
+int maxi_combine_fields(const uint16_t *gauss, const uint16_t *edt, int64_t nz, int64_t ny, int64_t nx,
+                        uint16_t *output, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

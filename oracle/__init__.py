@@ -17,8 +17,14 @@ Three oracles live here:
 * ``diffusion_f64``: the same algorithm in FP64, the error reference for the
   reduced-precision field forms.
 
-``reference_module()`` imports the reference's own ``diffusion`` pybind module
-from ``oracle/_ref`` when it has been built (``make -C oracle ref``).
+* ``combine_fields``: the numpy Gaussian + EDT field combination of the
+  reference's step src/processing_steps/0975_combine_fields.py:38-62, with its
+  ``to_int`` restated as ``normalized_convert_u16`` (pinned to the reference's
+  compiled ``general.normalized_convert`` by tests/golden).
+
+``reference_module()`` imports the reference's own ``diffusion`` (and
+``bitpacking``, ``general``) pybind modules from ``oracle/_ref`` when they have
+been built (``make -C oracle ref``).
 """
 from __future__ import annotations
 
@@ -147,6 +153,45 @@ def scipy_chain(mask: np.ndarray, kernel: np.ndarray, repititions: int) -> np.nd
         buf1[a] = 1
         buf0, buf1 = buf1, buf0
     return np.floor(buf0 * 65535).astype(np.uint16)
+
+
+def cylinder_mask(ny: int, nx: int | None = None) -> np.ndarray:
+    """bool[ny, nx]: the reference's generate_cylinder_mask (src/lib/py/helpers.py:411-434)."""
+    if nx is None:
+        nx = ny
+    ys = np.linspace(-1, 1, ny)
+    xs = np.linspace(-1, 1, nx)
+    return (xs[np.newaxis, :] ** 2 + ys[:, np.newaxis] ** 2) < 1
+
+
+def normalized_convert_u16(x: np.ndarray) -> np.ndarray:
+    """normalized_convert<float, uint16_t> (src/lib/cpp/include/general.hh:78-118), the
+    3-D path of the reference's to_int (src/lib/py/helpers.py:1013-1038): FP32
+    (x - vmin) / (vmax - vmin) * 65535 with vmin, vmax the array's extremes,
+    truncated to uint16."""
+    x = np.asarray(x, dtype=np.float32)
+    vmin, vmax = x.min(), x.max()
+    r = (x - vmin) / (vmax - vmin) * np.float32(np.iinfo(np.uint16).max)
+    return r.astype(np.uint16)
+
+
+def combine_fields(gauss: np.ndarray, edt: np.ndarray) -> np.ndarray:
+    """The Gaussian + EDT field combination of src/processing_steps/0975_combine_fields.py:38-62
+    on uint16 fields [nz, ny, nx] (the cylinder mask spans y and x as
+    generate_cylinder_mask(ny, nx); the script passes nx alone, which equals it for
+    the square planes it is run on)."""
+    nz, ny, nx = edt.shape
+    cylinder = cylinder_mask(ny, nx)
+    edt_max = edt.max()
+    gauss_max = gauss.max()
+    combined = gauss.astype(np.float32) / gauss_max
+    combined -= edt.astype(np.float32) / edt_max
+    combined += np.abs(combined.min())
+    combined /= combined.max()
+    combined *= cylinder
+    combined = normalized_convert_u16(combined)
+    combined *= cylinder
+    return combined
 
 
 def reference_module(name: str = "diffusion"):

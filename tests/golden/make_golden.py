@@ -9,7 +9,8 @@ Each case runs the reference pybind ``diffusion`` (OpenMP backend,
 src/lib/cpp/cpu/diffusion.cc) on a seeded mask and kernel and stores the mask,
 the float32 kernel, the repetition count and the uint16 result (plus its
 sha256).  The bit-packing case stores the reference ``bitpacking.encode``
-words for a seeded mask.  The tests then check the oracle bit-for-bit against
+words for a seeded mask; the field-combination case stores two seeded uint16
+fields and the result of the reference's 0975_combine_fields steps on them.  The tests then check the oracle bit-for-bit against
 these files, and the CUDA library against the oracle.
 """
 from __future__ import annotations
@@ -81,6 +82,27 @@ def main():
     bits.decode(packed, decoded, 0)
     np.savez_compressed(os.path.join(HERE, "bitpack_u32.npz"), mask=m, packed=packed, decoded=decoded)
     index["bitpack_u32"] = {"file": "bitpack_u32.npz", "n": int(m.size)}
+    gen = oracle.reference_module("general")
+    if gen is None:
+        sys.exit("reference general module not built: run `make -C oracle ref`")
+    # The Gaussian + EDT combination of src/processing_steps/0975_combine_fields.py:38-62:
+    # its numpy steps, with to_int done by the reference's compiled normalized_convert.
+    rng = np.random.default_rng(11)
+    shape = (12, 48, 48)
+    gauss = (rng.random(shape) ** 3 * 65535).astype(np.uint16)
+    edt = (rng.random(shape) * 30000).astype(np.uint16)
+    cylinder = oracle.cylinder_mask(shape[2])  # the script's generate_cylinder_mask(nx)
+    combined = gauss.astype(np.float32) / gauss.max()
+    combined -= edt.astype(np.float32) / edt.max()
+    combined += np.abs(combined.min())
+    combined /= combined.max()
+    combined *= cylinder
+    result = np.empty(shape, np.uint16)
+    gen.normalized_convert(np.ascontiguousarray(combined), result)
+    result *= cylinder
+    np.savez_compressed(os.path.join(HERE, "combine_fields_u16.npz"), gauss=gauss, edt=edt, output=result)
+    index["combine_fields_u16"] = {"file": "combine_fields_u16.npz", "shape": list(shape),
+                                   "sha256": hashlib.sha256(result.tobytes()).hexdigest()}
     with open(os.path.join(HERE, "index.json"), "w") as f:
         json.dump(index, f, indent=1, sort_keys=True)
 

@@ -74,3 +74,31 @@ def test_on_disk_semantics_equal_in_memory_for_binary_field():
     a = oracle.diffusion_on_disk_semantics(mask, k, 4)
     b, _ = oracle.diffusion_in_memory(mask, k, 4)
     np.testing.assert_array_equal(a, b)
+
+
+def test_oracle_combine_fields_matches_reference_golden():
+    # src/processing_steps/0975_combine_fields.py:38-62 with the reference's compiled to_int.
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "combine_fields_u16.npz"))
+    np.testing.assert_array_equal(oracle.combine_fields(z["gauss"], z["edt"]), z["output"])
+
+
+def test_oracle_normalized_convert_matches_reference_module():
+    gen = oracle.reference_module("general")
+    if gen is None:
+        pytest.skip("reference general module not built (make -C oracle ref)")
+    rng = np.random.default_rng(3)
+    for shape in [(3, 5, 7), (8, 33, 40)]:
+        x = (rng.standard_normal(shape) * 3).astype(np.float32)
+        want = np.empty(shape, np.uint16)
+        gen.normalized_convert(x, want)
+        np.testing.assert_array_equal(oracle.normalized_convert_u16(x), want)
+
+
+def test_oracle_cylinder_mask_square_and_general():
+    m = oracle.cylinder_mask(48)
+    assert m.shape == (48, 48) and m.dtype == bool
+    assert not m[0, 0] and m[24, 24]
+    assert oracle.cylinder_mask(1, 5).sum() == 0  # linspace(-1, 1, 1) == [-1]: nothing inside
+    assert oracle.cylinder_mask(10, 20).shape == (10, 20)

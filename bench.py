@@ -315,6 +315,70 @@ def fields_section(torch, np, gauss_u16, stream):
     return res
 
 
+def histogram_section(torch, np, mask, gauss_u16, stream):
+    """The field histogram (the pipeline's consumer of the diffusion field,
+    src/processing_steps/1000_compute_histograms.py:472) of a synthetic uint16
+    tomogram made from the workload's mask against the diffusion output at half
+    resolution, with the pipeline's bins (2048 field x 4096 voxel) and ranges,
+    against the reference's own compiled module on a 256^3 crop."""
+    import oracle
+    from maxibone_b200.histograms import field_histogram
+
+    shape = tuple(mask.shape)
+    vox = int(np.prod(shape))
+    g = torch.Generator(device="cuda").manual_seed(7)
+    # Implant ~ 45000, bone-like ~ 12000-26000 with noise, background 0 in a quarter of the volume.
+    noise = torch.randn(shape, generator=g, device="cuda") * 1500.0
+    zz = torch.arange(shape[0], device="cuda", dtype=torch.float32)[:, None, None]
+    base = 19000.0 + 7000.0 * torch.sin(zz * 0.01)
+    vox_f = torch.where(mask.bool(), torch.full((), 45000.0, device="cuda"), base + noise)
+    vox_f[:, :, : shape[2] // 4] = 0.0
+    voxels = vox_f.clamp(0, 65535).to(torch.int32).to(torch.int16)
+    del noise, vox_f, base
+    field = gauss_u16.view(torch.int16)[::2, ::2, ::2].contiguous()
+    bins = torch.zeros((2048, 4096), dtype=torch.int64, device="cuda")
+    vrange, frange = (1.0, 32000.0), (1.0, 65535.0)
+    field_histogram(voxels, field, (0, 0, 0), bins, vrange, frange, 0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_t = 5
+    e0.record(stream)
+    for _ in range(n_t):
+        field_histogram(voxels, field, (0, 0, 0), bins, vrange, frange, 0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n_t
+    counted = int(bins.sum().item()) // (n_t + 1)
+    peak, _ = load_peaks()
+    alg = 2.25 * vox  # each 2-byte voxel once, each 2-byte field sample once per 8 voxels
+    res = {"workload": f"{shape[0]}x{shape[1]}x{shape[2]} synthetic uint16 tomogram vs the "
+                       f"{tuple(field.shape)} half-resolution diffusion field, bins 2048x4096, vrange {vrange}",
+           "value": vox / (ms / 1e3) / 1e9, "unit": "Gvox/s", "ms": ms, "counted_per_call": counted,
+           "hbm_gbs": alg / (ms / 1e3) / 1e9, "hbm_frac": alg / (ms / 1e3) / 1e9 / peak,
+           "alg_bytes_per_voxel": 2.25,
+           "timing": "CUDA events around 5 synchronous calls (host tables built and copied in each)"}
+    n = 256
+    vs = np.ascontiguousarray(voxels[:n, :n, :n].cpu().numpy().view(np.uint16))
+    fs = np.ascontiguousarray(field[: n // 2, : n // 2, : n // 2].cpu().numpy().view(np.uint16))
+    hist = oracle.reference_module("histograms")
+    t0 = time.perf_counter()
+    if hist is not None:
+        ref = np.zeros((2048, 4096), np.uint64)
+        hist.field_histogram(vs, fs, (0, 0, 0), ref, vrange, frange, 0)
+    else:
+        ref = oracle.field_histogram(vs, fs, (0, 0, 0), (2048, 4096), vrange, frange)
+    cpu_s = time.perf_counter() - t0
+    got = np.zeros((2048, 4096), np.uint64)
+    field_histogram(vs, fs, (0, 0, 0), got, vrange, frange, 0)
+    res["cpu_baseline"] = {"value": vs.size / cpu_s / 1e9, "unit": "Gvox/s",
+                           "kind": "reference" if hist is not None else "port",
+                           "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+                           "sample": f"{vs.shape} crop vs {fs.shape} field, one field_histogram call",
+                           "gpu_equals_reference": bool(np.array_equal(got, ref))}
+    del voxels, field, bins
+    return res
+
+
 def batched_plan_on_volume(device, torch, np, mask, kernel, reps, stream):
     """The BF16 batch plan (CUDA graph of persistent tensor-core launches, one per
     pass) over the workload's single volume: the batched form on the 1024^3 mask."""
@@ -617,7 +681,8 @@ def main():
                                "bf16_max_abs_err_vs_f64": forms["bf16"]["max_abs_err_vs_f64"]}
         del f64
 
-        line["fields"] = {"combine_fields": fields_section(torch, np, out, stream)}
+        line["fields"] = {"combine_fields": fields_section(torch, np, out, stream),
+                          "field_histogram": histogram_section(torch, np, mask, out, stream)}
         line["batched"] = batched_section(device, torch, np, stream)
         line["batched"]["bf16_plan_on_workload_volume"] = bv = batched_plan_on_volume(
             device, torch, np, mask, kernel, reps, stream)

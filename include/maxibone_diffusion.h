@@ -251,6 +251,25 @@ int maxi_bitpack_decode(const uint32_t *packed, int64_t n, uint8_t *mask, void *
 int maxi_combine_fields(const uint16_t *gauss, const uint16_t *edt, int64_t nz, int64_t ny, int64_t nx,
                         uint16_t *output, void *stream);
 
+/*
+ * 2-D histogram of (field value, voxel value) pairs, added into bins: the
+ * reference's field_histogram (src/lib/cpp/cpu/histograms.cc:231-305, bound by
+ * src/pybind/histograms-pybind.cc:81-107), the consumer of the diffusion field
+ * (src/processing_steps/1000_compute_histograms.py:80-115).  voxels: device
+ * uint16[nZ][nY][nX]; field: device uint16[nz][ny][nx], read at
+ * (min(nz-1, floor(Z*nz/nZ)), floor(Y*ny/nY), floor(X*nx/nX)); bins: device
+ * uint64[field_bins][voxel_bins], accumulated into (not cleared).  Rows start at
+ * y_start and columns at x_start (the offset's y and x; its z is unused, as in
+ * the reference).  Voxel values outside [vmin, vmax], zero voxels and zero field
+ * values are skipped; bin indices use the reference's FP64 expressions, so the
+ * counts are identical.  Field values whose bin falls outside [0, field_bins)
+ * are skipped (the reference writes out of bounds there).  Synchronises the stream.
+ */
+int maxi_field_histogram(const uint16_t *voxels, int64_t nZ, int64_t nY, int64_t nX, const uint16_t *field,
+                         int64_t nz, int64_t ny, int64_t nx, int64_t y_start, int64_t x_start, uint64_t *bins,
+                         int64_t field_bins, int64_t voxel_bins, double vmin, double vmax, double fmin, double fmax,
+                         void *stream);
+
 #ifdef __cplusplus
 }
 #endif

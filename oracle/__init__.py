@@ -4,7 +4,7 @@ Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` may import this package, and only as the checker or the timed CPU
 baseline.  The product (``maxibone_b200``) never imports it.
 
-Three oracles live here:
+The oracles:
 
 * ``diffusion_in_memory``: ctypes binding of ``diffusion_oracle.c``, a C
   restatement of the reference OpenMP backend
@@ -22,8 +22,13 @@ Three oracles live here:
   ``to_int`` restated as ``normalized_convert_u16`` (pinned to the reference's
   compiled ``general.normalized_convert`` by tests/golden).
 
+* ``field_histogram`` and ``axis_histograms``: the 2-D (field, voxel) and the
+  per-axis / radial histograms of the reference's histograms module
+  (src/lib/cpp/cpu/histograms.cc:231-305 and :14-80) in numpy, pinned to the
+  compiled module by tests/golden.
+
 ``reference_module()`` imports the reference's own ``diffusion`` (and
-``bitpacking``, ``general``) pybind modules from ``oracle/_ref`` when they have
+``bitpacking``, ``general``, ``histograms``) pybind modules from ``oracle/_ref`` when they have
 been built (``make -C oracle ref``).
 """
 from __future__ import annotations
@@ -192,6 +197,67 @@ def combine_fields(gauss: np.ndarray, edt: np.ndarray) -> np.ndarray:
     combined = normalized_convert_u16(combined)
     combined *= cylinder
     return combined
+
+
+def field_histogram(voxels: np.ndarray, field: np.ndarray, offset, bins_shape, vrange, frange) -> np.ndarray:
+    """uint64[field_bins, voxel_bins]: the reference's field_histogram
+    (src/lib/cpp/cpu/histograms.cc:231-305, via src/pybind/histograms-pybind.cc:81-107)
+    with the same FP64 expressions: each voxel value inside vrange (others count as 0)
+    is binned as floor((voxel_bins - 1) * ((v - vmin) / (vmax - vmin))), the field is
+    read at (min(nz - 1, floor(Z * nz/nZ)), floor(Y * ny/nY), floor(X * nx/nX)), zero
+    voxels and zero field values are skipped, and rows / columns start at the offset's
+    y and x.  Field bins outside [0, field_bins) (undefined in the reference) are skipped."""
+    field_bins, voxel_bins = bins_shape
+    nZ, nY, nX = voxels.shape
+    nz, ny, nx = field.shape
+    vmin, vmax = (float(v) for v in vrange)
+    fmin, fmax = (float(v) for v in frange)
+    _, y_start, x_start = (int(v) for v in offset)
+    dz, dy, dx = nz / nZ, ny / nY, nx / nX
+    v = voxels.astype(np.float64)
+    v = np.where((v >= vmin) & (v <= vmax), v, 0.0)
+    vi = np.floor(float(voxel_bins - 1) * ((v - vmin) / (vmax - vmin)))
+    z = np.minimum(nz - 1, np.floor(np.arange(nZ) * dz).astype(np.int64))
+    y = np.floor(np.arange(nY) * dy).astype(np.int64)
+    x = np.floor(np.arange(nX) * dx).astype(np.int64)
+    f = field[z[:, None, None], y[None, :, None], x[None, None, :]].astype(np.float64)
+    fi = np.floor(float(field_bins - 1) * ((f - fmin) / (fmax - fmin)))
+    keep = (v != 0) & (f > 0) & (fi >= 0) & (fi < field_bins)
+    keep[:, :y_start, :] = False
+    keep[:, :, :x_start] = False
+    bins = np.zeros((field_bins, voxel_bins), np.uint64)
+    np.add.at(bins, (fi[keep].astype(np.int64), vi[keep].astype(np.int64)), np.uint64(1))
+    return bins
+
+
+def axis_histograms(voxels: np.ndarray, offset, global_shape, voxel_bins: int, n_r: int, center, vrange):
+    """(x_bins, y_bins, z_bins, r_bins), uint64 [N, voxel_bins]: the reference's
+    axis_histogram (src/lib/cpp/cpu/histograms.cc:14-80, via
+    src/pybind/histograms-pybind.cc:30-66).  The block covers global planes
+    z_start .. min(z_start + nz_block, Nz) with the global y and x extents; voxels
+    at y >= y_start and x >= x_start whose value lies in vrange are binned as
+    floor((voxel_bins - 1) * ((v - vmin) / (vmax - vmin))) in FP64 and counted in
+    x_bins[x], y_bins[y], z_bins[z] and r_bins[floor(sqrt((x-cx)^2 + (y-cy)^2))].
+    Radii at or past n_r (undefined in the reference) are skipped."""
+    nz_g, ny_g, nx_g = global_shape
+    z_start, y_start, x_start = (int(v) for v in offset)
+    cy, cx = (int(c) for c in center)
+    vmin, vmax = (float(v) for v in vrange)
+    z_end = min(z_start + voxels.shape[0], nz_g)
+    blk = voxels[: max(0, z_end - z_start)].reshape(-1, ny_g, nx_g)
+    v = blk.astype(np.float64)
+    v = np.where((v >= vmin) & (v <= vmax), v, 0.0)
+    vi = np.floor(float(voxel_bins - 1) * ((v - vmin) / (vmax - vmin)))
+    zz, yy, xx = np.meshgrid(np.arange(z_start, z_end), np.arange(ny_g), np.arange(nx_g), indexing="ij")
+    r = np.floor(np.sqrt(((xx - cx) ** 2 + (yy - cy) ** 2).astype(np.float64))).astype(np.int64)
+    keep = (v != 0) & (vi < voxel_bins) & (yy >= y_start) & (xx >= x_start)
+    out = []
+    for coord, n in ((xx, nx_g), (yy, ny_g), (zz, nz_g), (r, n_r)):
+        k = keep & (coord < n)
+        b = np.zeros((n, voxel_bins), np.uint64)
+        np.add.at(b, (coord[k], vi[k].astype(np.int64)), np.uint64(1))
+        out.append(b)
+    return tuple(out)
 
 
 def reference_module(name: str = "diffusion"):

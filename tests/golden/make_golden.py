@@ -10,7 +10,10 @@ src/lib/cpp/cpu/diffusion.cc) on a seeded mask and kernel and stores the mask,
 the float32 kernel, the repetition count and the uint16 result (plus its
 sha256).  The bit-packing case stores the reference ``bitpacking.encode``
 words for a seeded mask; the field-combination case stores two seeded uint16
-fields and the result of the reference's 0975_combine_fields steps on them.  The tests then check the oracle bit-for-bit against
+fields and the result of the reference's 0975_combine_fields steps on them; the
+histogram cases store a voxel volume, a field and the reference's
+histograms.field_histogram bins, and a voxel block with the reference's
+histograms.axis_histograms x / y / z / radial bins.  The tests then check the oracle bit-for-bit against
 these files, and the CUDA library against the oracle.
 """
 from __future__ import annotations
@@ -103,6 +106,37 @@ def main():
     np.savez_compressed(os.path.join(HERE, "combine_fields_u16.npz"), gauss=gauss, edt=edt, output=result)
     index["combine_fields_u16"] = {"file": "combine_fields_u16.npz", "shape": list(shape),
                                    "sha256": hashlib.sha256(result.tobytes()).hexdigest()}
+    hist = oracle.reference_module("histograms")
+    if hist is None:
+        sys.exit("reference histograms module not built: run `make -C oracle ref`")
+    # field_histogram of the histograms module (src/lib/cpp/cpu/histograms.cc:231-305) on
+    # a voxel volume and a field at half its resolution, with the script's default ranges
+    # (src/processing_steps/1000_compute_histograms.py:113).
+    rng = np.random.default_rng(13)
+    voxels = (rng.random((20, 36, 44)) * 40000).astype(np.uint16)
+    field = (rng.random((10, 18, 22)) * 65535).astype(np.uint16)
+    bins = np.zeros((64, 128), np.uint64)
+    hist.field_histogram(voxels, field, (0, 0, 0), bins, (1e4, 3e4), (1, 2 ** 16 - 1), 0)
+    np.savez_compressed(os.path.join(HERE, "field_histogram_u64.npz"), voxels=voxels, field=field, bins=bins,
+                        vrange=np.array([1e4, 3e4]), frange=np.array([1.0, 2.0 ** 16 - 1]))
+    index["field_histogram_u64"] = {"file": "field_histogram_u64.npz", "bins": list(bins.shape),
+                                    "total": int(bins.sum())}
+    # axis_histograms (src/lib/cpp/cpu/histograms.cc:14-80) on a z-block of a volume, as
+    # the out-of-core loop calls it (src/processing_steps/1000_compute_histograms.py:470),
+    # with the script's centre and radial extent (:60-62).
+    gshape, z_start = (40, 36, 44), 16
+    block = rng.integers(0, 40000, (16, 36, 44), dtype=np.uint16)
+    block[rng.random(block.shape) < 0.15] = 0
+    center = (gshape[1] // 2, gshape[2] // 2)
+    n_r = int(np.sqrt((gshape[2] // 2) ** 2 + (gshape[1] // 2) ** 2)) + 1
+    xb, yb = np.zeros((gshape[2], 256), np.uint64), np.zeros((gshape[1], 256), np.uint64)
+    zb, rb = np.zeros((gshape[0], 256), np.uint64), np.zeros((n_r, 256), np.uint64)
+    hist.axis_histograms(block, (z_start, 0, 0), xb, yb, zb, rb, center, (1e4, 3e4), 0)
+    np.savez_compressed(os.path.join(HERE, "axis_histograms_u64.npz"), voxels=block, z_start=z_start,
+                        global_shape=np.array(gshape), center=np.array(center), vrange=np.array([1e4, 3e4]),
+                        x_bins=xb, y_bins=yb, z_bins=zb, r_bins=rb)
+    index["axis_histograms_u64"] = {"file": "axis_histograms_u64.npz", "voxel_bins": 256, "n_r": n_r,
+                                    "total": int(xb.sum())}
     with open(os.path.join(HERE, "index.json"), "w") as f:
         json.dump(index, f, indent=1, sort_keys=True)
 

@@ -102,3 +102,54 @@ def test_oracle_cylinder_mask_square_and_general():
     assert not m[0, 0] and m[24, 24]
     assert oracle.cylinder_mask(1, 5).sum() == 0  # linspace(-1, 1, 1) == [-1]: nothing inside
     assert oracle.cylinder_mask(10, 20).shape == (10, 20)
+
+
+def test_oracle_field_histogram_matches_reference_golden():
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "field_histogram_u64.npz"))
+    got = oracle.field_histogram(z["voxels"], z["field"], (0, 0, 0), z["bins"].shape, tuple(z["vrange"]),
+                                 tuple(z["frange"]))
+    np.testing.assert_array_equal(got, z["bins"])
+
+
+def test_oracle_field_histogram_matches_reference_module_with_offsets():
+    hist = oracle.reference_module("histograms")
+    if hist is None:
+        pytest.skip("reference histograms module not built (make -C oracle ref)")
+    rng = np.random.default_rng(5)
+    v = rng.integers(0, 65535, (9, 17, 23), dtype=np.uint16)
+    f = rng.integers(0, 65535, (5, 9, 12), dtype=np.uint16)
+    want = np.zeros((40, 70), np.uint64)
+    hist.field_histogram(v, f, (0, 3, 5), want, (0.0, 65535.0), (1.0, 65535.0), 0)
+    np.testing.assert_array_equal(oracle.field_histogram(v, f, (0, 3, 5), (40, 70), (0.0, 65535.0), (1.0, 65535.0)),
+                                  want)
+
+
+def test_oracle_axis_histograms_matches_reference_golden():
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "axis_histograms_u64.npz"))
+    got = oracle.axis_histograms(z["voxels"], (int(z["z_start"]), 0, 0), tuple(z["global_shape"]),
+                                 z["x_bins"].shape[1], z["r_bins"].shape[0], tuple(z["center"]), tuple(z["vrange"]))
+    for g, name in zip(got, ("x_bins", "y_bins", "z_bins", "r_bins")):
+        np.testing.assert_array_equal(g, z[name], err_msg=name)
+
+
+@pytest.mark.parametrize("zoff,yoff,xoff,center,nzb", [(0, 0, 0, (20, 25), 30), (10, 3, 7, (20, 25), 12),
+                                                         (25, 0, 0, (5, 44), 12)])
+def test_oracle_axis_histograms_matches_reference_module(zoff, yoff, xoff, center, nzb):
+    """Offsets in every axis, an off-centre centre and a block that runs past Nz."""
+    hist = oracle.reference_module("histograms")
+    if hist is None:
+        pytest.skip("reference histograms module not built (make -C oracle ref)")
+    gs, nb, vr = (30, 40, 50), 64, (500.5, 3e4)
+    rng = np.random.default_rng(zoff + nzb)
+    v = rng.integers(0, 40000, (nzb, gs[1], gs[2]), dtype=np.uint16)
+    n_r = int(np.ceil(np.hypot(max(center[0], gs[1] - center[0]), max(center[1], gs[2] - center[1])))) + 1
+    want = (np.zeros((gs[2], nb), np.uint64), np.zeros((gs[1], nb), np.uint64), np.zeros((gs[0], nb), np.uint64),
+            np.zeros((n_r, nb), np.uint64))
+    hist.axis_histograms(v, (zoff, yoff, xoff), *want, center, vr, 0)
+    got = oracle.axis_histograms(v, (zoff, yoff, xoff), gs, nb, n_r, center, vr)
+    for g, w in zip(got, want):
+        np.testing.assert_array_equal(g, w)

@@ -21,7 +21,11 @@ Also reported on the same line:
   precision     BF16 and FP16 field forms: throughput and max/mean abs error of
                 the final field against the FP64 form (and the FP32 form's);
   cpu_baseline  the reference's OpenMP CPU module (oracle/_ref, built from the
-                reference sources) timed on this host on a bounded sample.
+                reference sources) timed on this host on a bounded sample;
+  fields        the downstream steps on the workload's output: the Gaussian + EDT
+                field combination and the reference's field / axis histograms,
+                each beside the reference's own CPU form on a bounded sample
+                (`--downstream-only` runs just these).
 
 `--impl reference` times only the reference CPU module on the bounded sample.
 """
@@ -62,6 +66,9 @@ def parse_args():
     p.add_argument("--quick", action="store_true", help="skip e2e, precision forms and CPU baseline")
     p.add_argument("--extended", action="store_true",
                    help="also run the out-of-core workload, R=500 errors and the sigma=32 case")
+    p.add_argument("--downstream-only", action="store_true",
+                   help="run one diffusion of the workload, then only the downstream steps (field combination and "
+                        "histograms) on its output, and print their JSON object")
     p.add_argument("--shape", type=str, default=None,
                    help="override the workload's volume shape, e.g. 256x1024x1024 (profiling of smaller cases)")
     return p.parse_args()
@@ -316,13 +323,15 @@ def fields_section(torch, np, gauss_u16, stream):
 
 
 def histogram_section(torch, np, mask, gauss_u16, stream):
-    """The field histogram (the pipeline's consumer of the diffusion field,
-    src/processing_steps/1000_compute_histograms.py:472) of a synthetic uint16
-    tomogram made from the workload's mask against the diffusion output at half
-    resolution, with the pipeline's bins (2048 field x 4096 voxel) and ranges,
-    against the reference's own compiled module on a 256^3 crop."""
+    """The reference's histograms module (the pipeline's consumer of the diffusion
+    field, src/processing_steps/1000_compute_histograms.py:470-472) on a synthetic
+    uint16 tomogram made from the workload's mask: field_histogram against the
+    diffusion output at half resolution with the pipeline's bins (2048 field x
+    4096 voxel) and ranges, and axis_histograms (x, y, z, radial; 4096 bins) over
+    the whole volume as one block.  Each against the reference's own compiled
+    module on a bounded sample."""
     import oracle
-    from maxibone_b200.histograms import field_histogram
+    from maxibone_b200.histograms import axis_histograms, field_histogram
 
     shape = tuple(mask.shape)
     vox = int(np.prod(shape))
@@ -336,31 +345,39 @@ def histogram_section(torch, np, mask, gauss_u16, stream):
     voxels = vox_f.clamp(0, 65535).to(torch.int32).to(torch.int16)
     del noise, vox_f, base
     field = gauss_u16.view(torch.int16)[::2, ::2, ::2].contiguous()
-    bins = torch.zeros((2048, 4096), dtype=torch.int64, device="cuda")
     vrange, frange = (1.0, 32000.0), (1.0, 65535.0)
-    field_histogram(voxels, field, (0, 0, 0), bins, vrange, frange, 0)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    n_t = 5
-    e0.record(stream)
-    for _ in range(n_t):
-        field_histogram(voxels, field, (0, 0, 0), bins, vrange, frange, 0)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / n_t
-    counted = int(bins.sum().item()) // (n_t + 1)
+    center = (shape[1] // 2, shape[2] // 2)
+    n_r = int(np.sqrt((shape[2] // 2) ** 2 + (shape[1] // 2) ** 2)) + 1
     peak, _ = load_peaks()
+    hist = oracle.reference_module("histograms")
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    n_t = 5
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n_t):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n_t
+
+    out = {}
+    bins = torch.zeros((2048, 4096), dtype=torch.int64, device="cuda")
+    ms = timed(lambda: field_histogram(voxels, field, (0, 0, 0), bins, vrange, frange, 0))
     alg = 2.25 * vox  # each 2-byte voxel once, each 2-byte field sample once per 8 voxels
     res = {"workload": f"{shape[0]}x{shape[1]}x{shape[2]} synthetic uint16 tomogram vs the "
                        f"{tuple(field.shape)} half-resolution diffusion field, bins 2048x4096, vrange {vrange}",
-           "value": vox / (ms / 1e3) / 1e9, "unit": "Gvox/s", "ms": ms, "counted_per_call": counted,
+           "value": vox / (ms / 1e3) / 1e9, "unit": "Gvox/s", "ms": ms,
+           "counted_per_call": int(bins.sum().item()) // (n_t + 1),
            "hbm_gbs": alg / (ms / 1e3) / 1e9, "hbm_frac": alg / (ms / 1e3) / 1e9 / peak,
            "alg_bytes_per_voxel": 2.25,
            "timing": "CUDA events around 5 synchronous calls (host tables built and copied in each)"}
     n = 256
     vs = np.ascontiguousarray(voxels[:n, :n, :n].cpu().numpy().view(np.uint16))
     fs = np.ascontiguousarray(field[: n // 2, : n // 2, : n // 2].cpu().numpy().view(np.uint16))
-    hist = oracle.reference_module("histograms")
     t0 = time.perf_counter()
     if hist is not None:
         ref = np.zeros((2048, 4096), np.uint64)
@@ -371,12 +388,40 @@ def histogram_section(torch, np, mask, gauss_u16, stream):
     got = np.zeros((2048, 4096), np.uint64)
     field_histogram(vs, fs, (0, 0, 0), got, vrange, frange, 0)
     res["cpu_baseline"] = {"value": vs.size / cpu_s / 1e9, "unit": "Gvox/s",
-                           "kind": "reference" if hist is not None else "port",
-                           "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+                           "kind": "reference" if hist is not None else "port", "cores": cores,
                            "sample": f"{vs.shape} crop vs {fs.shape} field, one field_histogram call",
                            "gpu_equals_reference": bool(np.array_equal(got, ref))}
-    del voxels, field, bins
-    return res
+    out["field_histogram"] = res
+    del bins
+
+    axb = [torch.zeros((k, 4096), dtype=torch.int64, device="cuda") for k in (shape[2], shape[1], shape[0], n_r)]
+    ms = timed(lambda: axis_histograms(voxels, (0, 0, 0), *axb, center, vrange, 0))
+    res = {"workload": f"{shape[0]}x{shape[1]}x{shape[2]} synthetic uint16 tomogram as one block, x / y / z / "
+                       f"radial histograms of 4096 bins (Nr {n_r}), vrange {vrange}",
+           "value": vox / (ms / 1e3) / 1e9, "unit": "Gvox/s", "ms": ms,
+           "counted_per_call": int(axb[0].sum().item()) // (n_t + 1),
+           "hbm_gbs": 2 * vox / (ms / 1e3) / 1e9, "hbm_frac": 2 * vox / (ms / 1e3) / 1e9 / peak,
+           "alg_bytes_per_voxel": 2,
+           "timing": "CUDA events around 5 synchronous calls"}
+    nz_s = 64
+    vs = np.ascontiguousarray(voxels[:nz_s].cpu().numpy().view(np.uint16))
+    shp = (shape[2], shape[1], shape[0], n_r)
+    t0 = time.perf_counter()
+    if hist is not None:
+        ref = [np.zeros((k, 4096), np.uint64) for k in shp]
+        hist.axis_histograms(vs, (0, 0, 0), *ref, center, vrange, 0)
+    else:
+        ref = oracle.axis_histograms(vs, (0, 0, 0), (shape[0], shape[1], shape[2]), 4096, n_r, center, vrange)
+    cpu_s = time.perf_counter() - t0
+    got = [np.zeros((k, 4096), np.uint64) for k in shp]
+    axis_histograms(vs, (0, 0, 0), *got, center, vrange, 0)
+    res["cpu_baseline"] = {"value": vs.size / cpu_s / 1e9, "unit": "Gvox/s",
+                           "kind": "reference" if hist is not None else "port", "cores": cores,
+                           "sample": f"{vs.shape} block (first {nz_s} planes), one axis_histograms call",
+                           "gpu_equals_reference": all(np.array_equal(a, b) for a, b in zip(got, ref))}
+    out["axis_histograms"] = res
+    del voxels, field, axb
+    return out
 
 
 def batched_plan_on_volume(device, torch, np, mask, kernel, reps, stream):
@@ -537,6 +582,15 @@ def main():
         if world > 1:
             dist.barrier()
 
+    if args.downstream_only:
+        step()
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"workload": args.workload, "shape": list(shape), "field": args.field,
+                              "fields": {"combine_fields": fields_section(torch, np, out, stream),
+                                         **histogram_section(torch, np, mask, out, stream)}}), flush=True)
+        return
+
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -682,7 +736,7 @@ def main():
         del f64
 
         line["fields"] = {"combine_fields": fields_section(torch, np, out, stream),
-                          "field_histogram": histogram_section(torch, np, mask, out, stream)}
+                          **histogram_section(torch, np, mask, out, stream)}
         line["batched"] = batched_section(device, torch, np, stream)
         line["batched"]["bf16_plan_on_workload_volume"] = bv = batched_plan_on_volume(
             device, torch, np, mask, kernel, reps, stream)

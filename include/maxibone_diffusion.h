@@ -270,6 +270,26 @@ int maxi_field_histogram(const uint16_t *voxels, int64_t nZ, int64_t nY, int64_t
                          int64_t field_bins, int64_t voxel_bins, double vmin, double vmax, double fmin, double fmax,
                          void *stream);
 
+/*
+ * Per-axis and radial histograms of a z-block of a volume, added into the bins:
+ * the reference's axis_histograms (src/lib/cpp/cpu/histograms.cc:14-80, bound by
+ * src/pybind/histograms-pybind.cc:30-66; called per block by
+ * src/processing_steps/1000_compute_histograms.py:470).  voxels: device
+ * uint16[nz_block][Ny][Nx] holding global planes z_start .. z_start + nz_block
+ * (planes at or past Nz are ignored); x_bins [Nx][voxel_bins], y_bins
+ * [Ny][voxel_bins], z_bins [Nz][voxel_bins], r_bins [n_r][voxel_bins]: device
+ * uint64, accumulated into.  Each voxel at y >= y_start, x >= x_start whose value
+ * lies in [vmin, vmax] and is nonzero is binned as
+ * floor((voxel_bins - 1) * ((v - vmin) / (vmax - vmin))) (FP64) and counted in
+ * row x, y, z and floor(sqrt((x-cx)^2 + (y-cy)^2)) of the four histograms;
+ * radii at or past n_r (out-of-bounds writes in the reference) are skipped.
+ * Counts are identical to the reference's.  Synchronises the stream.
+ */
+int maxi_axis_histograms(const uint16_t *voxels, int64_t nz_block, int64_t Nz, int64_t Ny, int64_t Nx,
+                         int64_t z_start, int64_t y_start, int64_t x_start, uint64_t *x_bins, uint64_t *y_bins,
+                         uint64_t *z_bins, uint64_t *r_bins, int64_t voxel_bins, int64_t n_r, int64_t cy, int64_t cx,
+                         double vmin, double vmax, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

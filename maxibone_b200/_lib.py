@@ -44,6 +44,8 @@ SIGNATURES = {
     "maxi_combine_fields": (_int, [_p, _p, _i64, _i64, _i64, _p, _p]),
     "maxi_field_histogram": (_int, [_p, _i64, _i64, _i64, _p, _i64, _i64, _i64, _i64, _i64, _p, _i64, _i64,
                                     ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, _p]),
+    "maxi_axis_histograms": (_int, [_p, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _p, _p, _p, _p, _i64, _i64,
+                                    _i64, _i64, ctypes.c_double, ctypes.c_double, _p]),
     "maxi_diffusion_device_noalloc": (_int, [_p, _i32, _i64, _i64, _i64, _p, _i64, _i64, _p, _p, _p]),
     "maxi_tensor_core_status": (_int, []),
     "maxi_release_cached_memory": (_int, []),

@@ -26,10 +26,11 @@
 // Counting.  One thread takes 8 consecutive voxels of a row (one 16-byte load when
 // rows are 16-byte aligned) and adds runs of equal keys once.  field_histogram
 // issues one 64-bit reduction per run into the histogram (L2-resident at the
-// pipeline's 2048 x 4096).  axis_histograms counts each row's voxel bins in a
+// pipeline's 2048 x 4096); each of its blocks walks one contiguous range of rows.  axis_histograms counts each row's voxel bins in a
 // shared-memory histogram with a list of the bins it touched, then adds those to
 // y_bins[y] and z_bins[z]; x and radial bins take one reduction per voxel.
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -58,8 +59,9 @@ __device__ __forceinline__ int bin_of(const BinMap &m, int v) {
     return b;
 }
 
+// Voxels are read once: loaded evict-first, so the L2-resident bins stay in L2.
 __device__ __forceinline__ void load_row8(const uint16_t *p, int (&v)[kVec]) {
-    const uint4 w = __ldg(reinterpret_cast<const uint4 *>(p));
+    const uint4 w = __ldcs(reinterpret_cast<const uint4 *>(p));
     const uint32_t u[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -77,7 +79,12 @@ __global__ void field_histogram_kernel(const uint16_t *__restrict__ voxels, cons
                                        unsigned long long *__restrict__ bins, int64_t voxel_bins) {
     constexpr int V = VEC8 ? kVec : 1;
     const int x_first = x_start / V * V;
-    for (int64_t row = blockIdx.x; row < nZ * nY; row += gridDim.x) {
+    // Each block takes one contiguous range of rows, so the blocks at work at any time
+    // sit far apart in the volume: a smooth field gives neighbouring rows the same
+    // keys, and same-address reductions from many blocks at once serialise in L2.
+    const int64_t rows = nZ * nY, per = (rows + gridDim.x - 1) / gridDim.x;
+    const int64_t row_end = min(rows, (int64_t) (blockIdx.x + 1) * per);
+    for (int64_t row = (int64_t) blockIdx.x * per; row < row_end; row++) {
         const int64_t Z = row / nY, Y = row - Z * nY;
         if (Y < y_start) continue;
         const uint16_t *vrow = voxels + row * nX;
@@ -85,7 +92,7 @@ __global__ void field_histogram_kernel(const uint16_t *__restrict__ voxels, cons
         for (int X = x_first + threadIdx.x * V; X < nX; X += blockDim.x * V) {
             int v[V];
             if constexpr (VEC8) load_row8(vrow + X, v);
-            else v[0] = __ldg(vrow + X);
+            else v[0] = __ldcs(vrow + X);
             long long run_key = -1;
             unsigned run = 0;
 #pragma unroll
@@ -149,7 +156,7 @@ __global__ void axis_histograms_kernel(const uint16_t *__restrict__ voxels, int6
         for (int X = x_first + threadIdx.x * V; X < Nx; X += blockDim.x * V) {
             int v[V];
             if constexpr (VEC8) load_row8(vrow + X, v);
-            else v[0] = __ldg(vrow + X);
+            else v[0] = __ldcs(vrow + X);
             long long r_key = -1;
             unsigned r_run = 0;
             int b_key = -1;
@@ -256,16 +263,46 @@ int make_bin_map(const std::vector<int32_t> &tab, int64_t bins, double scale, do
     return MAXI_OK;
 }
 
-// Voxel bin of every uint16 value, -1 where the reference does not count it: values
-// outside [vmin, vmax] count as 0, and zero voxels are skipped.
-void voxel_table(std::vector<int32_t> &tab, double vmin, double vmax, int64_t voxel_bins) {
+// Bin of every uint16 value, -1 where the reference does not count it.  Voxels:
+// values outside [lo, hi] count as 0 and zero voxels are skipped.  Field values:
+// zero values and bins outside [0, bins) are skipped.
+void value_table(std::vector<int32_t> &tab, bool voxel, double lo, double hi, int64_t bins) {
     tab.assign(65536, -1);
     for (int v = 1; v < 65536; v++) {
         const double vv = (double) v;
-        if (!(vv >= vmin && vv <= vmax)) continue;
-        const int64_t b = ref_bin(vv, vmin, vmax, voxel_bins);
-        if (b >= 0 && b < voxel_bins) tab[v] = (int32_t) b;
+        if (voxel && !(vv >= lo && vv <= hi)) continue;
+        const int64_t b = ref_bin(vv, lo, hi, bins);
+        if (b >= 0 && b < bins) tab[v] = (int32_t) b;
     }
+}
+
+// The bin map of (kind, lo, hi, bins), built once and kept: the pipeline calls the
+// histograms block by block with the same ranges.  A few recent maps are kept.
+struct CachedMap {
+    bool voxel;
+    double lo, hi;
+    int64_t bins;
+    std::vector<uint32_t> T;
+    BinMap m;
+};
+
+int cached_bin_map(bool voxel, double lo, double hi, int64_t bins, std::vector<uint32_t> &T, BinMap &m) {
+    static std::mutex mu;
+    static std::vector<CachedMap> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    for (const CachedMap &c : cache)
+        if (c.voxel == voxel && c.lo == lo && c.hi == hi && c.bins == bins) {
+            T = c.T;
+            m = c.m;
+            return MAXI_OK;
+        }
+    std::vector<int32_t> tab;
+    value_table(tab, voxel, lo, hi, bins);
+    const int rc = make_bin_map(tab, bins, (double) (bins - 1) / (hi - lo), lo, T, m, voxel ? "voxel" : "field");
+    if (rc) return rc;
+    if (cache.size() >= 4) cache.erase(cache.begin());
+    cache.push_back({voxel, lo, hi, bins, T, m});
+    return MAXI_OK;
 }
 
 int sm_count() {
@@ -333,18 +370,10 @@ extern "C" int maxi_field_histogram(const uint16_t *voxels, int64_t nZ, int64_t 
     if (rc) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
-    std::vector<int32_t> vtab, ftab(65536, -1);
-    voxel_table(vtab, vmin, vmax, voxel_bins);
-    for (int f = 1; f < 65536; f++) {
-        const int64_t b = ref_bin((double) f, fmin, fmax, field_bins);
-        if (b >= 0 && b < field_bins) ftab[f] = (int32_t) b;
-    }
     std::vector<uint32_t> vT, fT;
     BinMap vm{}, fm{};
-    if ((rc = make_bin_map(vtab, voxel_bins, (double) (voxel_bins - 1) / (vmax - vmin), vmin, vT, vm, "voxel")))
-        return rc;
-    if ((rc = make_bin_map(ftab, field_bins, (double) (field_bins - 1) / (fmax - fmin), fmin, fT, fm, "field")))
-        return rc;
+    if ((rc = cached_bin_map(true, vmin, vmax, voxel_bins, vT, vm))) return rc;
+    if ((rc = cached_bin_map(false, fmin, fmax, field_bins, fT, fm))) return rc;
     std::vector<uint32_t> zmap(nZ), ymap(nY), xmap(nX);
     const double dz = (double) nz / (double) nZ, dy = (double) ny / (double) nY, dx = (double) nx / (double) nX;
     for (int64_t Z = 0; Z < nZ; Z++) {
@@ -406,12 +435,9 @@ extern "C" int maxi_axis_histograms(const uint16_t *voxels, int64_t nz_block, in
     if (rc) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
-    std::vector<int32_t> vtab;
-    voxel_table(vtab, vmin, vmax, voxel_bins);
     std::vector<uint32_t> vT;
     BinMap vm{};
-    if ((rc = make_bin_map(vtab, voxel_bins, (double) (voxel_bins - 1) / (vmax - vmin), vmin, vT, vm, "voxel")))
-        return rc;
+    if ((rc = cached_bin_map(true, vmin, vmax, voxel_bins, vT, vm))) return rc;
     DeviceTables t;
     const size_t o_vT = t.add(vT.data(), vT.size());
     rc = upload(t, st);

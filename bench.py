@@ -25,7 +25,10 @@ Also reported on the same line:
   fields        the downstream steps on the workload's output: the Gaussian + EDT
                 field combination and the reference's field / axis histograms,
                 each beside the reference's own CPU form on a bounded sample
-                (`--downstream-only` runs just these).
+                (`--downstream-only` runs just these and the morphology);
+  morphology    the sphere dilation that prepares masks (radius 16, uint8 and
+                bit-packed) on the workload's mask, beside the reference's CPU
+                module on a bounded sample.
 
 `--impl reference` times only the reference CPU module on the bounded sample.
 """
@@ -424,6 +427,71 @@ def histogram_section(torch, np, mask, gauss_u16, stream):
     return out
 
 
+def morphology_section(torch, np, mask, stream):
+    """The sphere morphology that prepares masks (src/lib/py/helpers.py:805-850 applies
+    radius-16 spheres repeatedly) on the workload's mask: dilation with radius 16 in the
+    uint8 form and in the bit-packed form, against the reference's compiled uint8
+    module on a bounded sample."""
+    import oracle
+    from maxibone_b200 import morphology as mo
+
+    shape = tuple(mask.shape)
+    vox = int(np.prod(shape))
+    r = 16
+    n_t = 3
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n_t):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n_t
+
+    m = (mask != 0).to(torch.uint8).contiguous()
+    out = torch.empty_like(m)
+    res = {}
+    ms = timed(lambda: mo.dilate_3d_sphere(m, r, out))
+    res["dilate_u8_r16"] = {"value": vox / (ms / 1e3) / 1e9, "unit": "Gvox/s", "ms": ms,
+                            "foreground_after": float(out.float().mean().item())}
+    words = None
+    if shape[2] % 32 == 0:
+        bits = torch.tensor([1 << (31 - b) for b in range(32)], device="cuda", dtype=torch.int64)
+        w = torch.empty((shape[0], shape[1], shape[2] // 32), dtype=torch.int32, device="cuda")
+        for z0 in range(0, shape[0], 64):  # pack in slabs to bound the int64 temporary
+            t = (m[z0:z0 + 64].view(-1, shape[1], shape[2] // 32, 32).to(torch.int64) * bits).sum(-1)
+            w[z0:z0 + 64] = (t - (t >= 2 ** 31).to(torch.int64) * 2 ** 32).to(torch.int32)
+        words = w
+        wout = torch.empty_like(words)
+        ms = timed(lambda: mo.dilate_3d_sphere_bitpacked(words, r, wout))
+        res["dilate_bitpacked_r16"] = {"value": vox / (ms / 1e3) / 1e9, "unit": "Gvox/s", "ms": ms}
+    res["workload"] = (f"{shape[0]}x{shape[1]}x{shape[2]} bone-implant mask, sphere radius 16 (the radius "
+                       "morph_3d applies repeatedly); timing: CUDA events around 3 synchronous calls")
+    morph = oracle.reference_module("morphology")
+    sample = (32, 128, 128)
+    ms_ = m[: sample[0], : sample[1], : sample[2]].contiguous()
+    sm = ms_.cpu().numpy()
+    t0 = time.perf_counter()
+    if morph is not None:
+        ref = np.zeros(sample, np.uint8)
+        morph.dilate_3d_sphere(sm, r, ref)
+    else:
+        ref = oracle.morphology_sphere(sm, r, True)
+    cpu_s = time.perf_counter() - t0
+    got = np.zeros(sample, np.uint8)
+    mo.dilate_3d_sphere(sm, r, got)
+    res["cpu_baseline"] = {"value": sm.size / cpu_s / 1e9, "unit": "Gvox/s",
+                           "kind": "reference" if morph is not None else "port",
+                           "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+                           "sample": f"{sample} crop, one dilate_3d_sphere call with radius {r}",
+                           "gpu_equals_reference": bool(np.array_equal(got, ref))}
+    del m, out, words
+    return res
+
+
 def batched_plan_on_volume(device, torch, np, mask, kernel, reps, stream):
     """The BF16 batch plan (CUDA graph of persistent tensor-core launches, one per
     pass) over the workload's single volume: the batched form on the 1024^3 mask."""
@@ -588,7 +656,8 @@ def main():
         if rank == 0:
             print(json.dumps({"workload": args.workload, "shape": list(shape), "field": args.field,
                               "fields": {"combine_fields": fields_section(torch, np, out, stream),
-                                         **histogram_section(torch, np, mask, out, stream)}}), flush=True)
+                                         **histogram_section(torch, np, mask, out, stream)},
+                              "morphology": morphology_section(torch, np, mask, stream)}), flush=True)
         return
 
     for _ in range(args.warmup):
@@ -737,6 +806,7 @@ def main():
 
         line["fields"] = {"combine_fields": fields_section(torch, np, out, stream),
                           **histogram_section(torch, np, mask, out, stream)}
+        line["morphology"] = morphology_section(torch, np, mask, stream)
         line["batched"] = batched_section(device, torch, np, stream)
         line["batched"]["bf16_plan_on_workload_volume"] = bv = batched_plan_on_volume(
             device, torch, np, mask, kernel, reps, stream)

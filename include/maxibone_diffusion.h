@@ -252,6 +252,41 @@ int maxi_combine_fields(const uint16_t *gauss, const uint16_t *edt, int64_t nz, 
                         uint16_t *output, void *stream);
 
 /*
+ * The implant cylinder mask applied to a uint16 field in place: voxels outside
+ * generate_cylinder_mask(ny, nx) (src/lib/py/helpers.py:411-434; the reference
+ * calls it with nx for its square planes) become 0, as the diffusion step's
+ * `result * cylinder_mask` before saving (src/processing_steps/
+ * 0900_generate_gauss_c.py:117,124).  Only the outside voxels are written.
+ * field: device uint16[nz][ny][nx].  Synchronises the stream.
+ */
+int maxi_mask_cylinder(uint16_t *field, int64_t nz, int64_t ny, int64_t nx, void *stream);
+
+/*
+ * 3-D sphere dilation (dilate != 0) or erosion of a mask: the reference's morphology
+ * module (src/lib/cpp/cpu_seq/morphology.cc:14-99 and gpu/morphology.cc:14-101, bound
+ * as dilate_3d_sphere / erode_3d_sphere by src/pybind/morphology-pybind.cc:24-45,
+ * 147,149).  voxels, result: device uint8[nz][ny][nx]; result[z,y,x] = 1 iff some
+ * in-volume voxel within the sphere (pz^2 + py^2 + px^2 <= radius^2) is nonzero
+ * (dilation) / every one has bit 0 set (erosion), else 0.  radius <= 32 (larger
+ * spheres: repeated calls, as the reference's morph_3d does with radius 16).
+ * Synchronises the stream.
+ */
+int maxi_morphology_sphere(const uint8_t *voxels, uint8_t *result, int64_t nz, int64_t ny, int64_t nx,
+                           int64_t radius, int dilate, void *stream);
+
+/*
+ * The same on a bit-packed mask: dilate_3d_sphere_bitpacked / erode_3d_sphere_bitpacked
+ * (src/lib/cpp/gpu/morphology.cc:103-176, src/pybind/morphology-pybind.cc:61-77,148,150).
+ * voxels, result: device uint32[nz][ny][nw], 32 voxels per word, MSB first along x.
+ * With the reference GPU build's shifts (by 32 or more, or by a negative amount: 0)
+ * its per-(pz, py) kernel rows hold x offsets -radius .. 31 - radius, so the sphere
+ * is clipped at x offset 31 - radius; this entry point computes exactly that.
+ * radius <= 31.  Synchronises the stream.
+ */
+int maxi_morphology_sphere_bitpacked(const uint32_t *voxels, uint32_t *result, int64_t nz, int64_t ny,
+                                     int64_t nw, int64_t radius, int dilate, void *stream);
+
+/*
  * 2-D histogram of (field value, voxel value) pairs, added into bins: the
  * reference's field_histogram (src/lib/cpp/cpu/histograms.cc:231-305, bound by
  * src/pybind/histograms-pybind.cc:81-107), the consumer of the diffusion field

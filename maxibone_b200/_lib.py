@@ -42,6 +42,9 @@ SIGNATURES = {
     "maxi_bitpack_encode": (_int, [_p, _i64, _p, _p]),
     "maxi_bitpack_decode": (_int, [_p, _i64, _p, _p]),
     "maxi_combine_fields": (_int, [_p, _p, _i64, _i64, _i64, _p, _p]),
+    "maxi_mask_cylinder": (_int, [_p, _i64, _i64, _i64, _p]),
+    "maxi_morphology_sphere": (_int, [_p, _p, _i64, _i64, _i64, _i64, _int, _p]),
+    "maxi_morphology_sphere_bitpacked": (_int, [_p, _p, _i64, _i64, _i64, _i64, _int, _p]),
     "maxi_field_histogram": (_int, [_p, _i64, _i64, _i64, _p, _i64, _i64, _i64, _i64, _i64, _p, _i64, _i64,
                                     ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, _p]),
     "maxi_axis_histograms": (_int, [_p, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _p, _p, _p, _p, _i64, _i64,

@@ -176,29 +176,11 @@ double linspace_pm1(int64_t i, int64_t n) {
     return t + -1.0;
 }
 
-}  // namespace
-}  // namespace maxi
-
-using namespace maxi;
-
-extern "C" int maxi_combine_fields(const uint16_t *gauss, const uint16_t *edt, int64_t nz, int64_t ny, int64_t nx,
-                                   uint16_t *output, void *stream) {
-    clear_error();
-    if (!gauss || !edt || !output) return set_error(MAXI_ERR_INVALID_ARGUMENT, "NULL pointer");
-    if (nz <= 0 || ny <= 0 || nx <= 0)
-        return set_error(MAXI_ERR_INVALID_ARGUMENT, "shape (%lld, %lld, %lld) has an empty axis", (long long) nz,
-                         (long long) ny, (long long) nx);
-    int rc = require_device();
-    if (rc) return rc;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int64_t rows = nz * ny;
-    if (rows * nx >= (int64_t(1) << 32))
-        return set_error(MAXI_ERR_UNSUPPORTED, "volumes of 2^32 voxels or more are not served by this step");
-
-    // Inside interval [x0, x1) of each row y: xs[x]^2 + ys[y]^2 < 1 in FP64.  xs^2
-    // falls then rises along x and fl(a + c) is monotone in a, so a row's inside
-    // voxels run from a first to a last index around the argmin of xs^2: two
-    // binary searches per row, exact.
+// Inside interval [x0, x1) of each row y of generate_cylinder_mask(ny, nx):
+// xs[x]^2 + ys[y]^2 < 1 in FP64.  xs^2 falls then rises along x and fl(a + c) is
+// monotone in a, so a row's inside voxels run from a first to a last index around
+// the argmin of xs^2: two binary searches per row, exact.
+void cylinder_intervals(int64_t ny, int64_t nx, std::vector<int2> &inside, bool &any_outside, bool &any_inside) {
     std::vector<double> xs2(nx);
     int64_t xm = 0;
     for (int64_t x = 0; x < nx; x++) {
@@ -207,8 +189,8 @@ extern "C" int maxi_combine_fields(const uint16_t *gauss, const uint16_t *edt, i
         xs2[x] = sq;
         if (xs2[x] < xs2[xm]) xm = x;
     }
-    std::vector<int2> inside(ny);
-    bool any_outside = false, any_inside = false;
+    inside.assign(ny, make_int2(0, 0));
+    any_outside = any_inside = false;
     for (int64_t y = 0; y < ny; y++) {
         const double v = linspace_pm1(y, ny);
         volatile double ys2 = v * v;
@@ -237,6 +219,42 @@ extern "C" int maxi_combine_fields(const uint16_t *gauss, const uint16_t *edt, i
         any_outside |= x0 > 0 || x1 < nx;
         any_inside |= x1 > x0;
     }
+}
+
+// Zeroes the voxels of each row outside its cylinder interval (one block per row
+// at a time; the inside voxels are neither read nor written).
+__global__ void cylinder_zero(uint16_t *__restrict__ f, int64_t rows, int64_t ny, int nx,
+                              const int2 *__restrict__ iv) {
+    for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int2 in = __ldg(iv + row % ny);
+        uint16_t *r = f + row * nx;
+        for (int x = threadIdx.x; x < in.x; x += blockDim.x) r[x] = 0;
+        for (int x = in.y + threadIdx.x; x < nx; x += blockDim.x) r[x] = 0;
+    }
+}
+
+}  // namespace
+}  // namespace maxi
+
+using namespace maxi;
+
+extern "C" int maxi_combine_fields(const uint16_t *gauss, const uint16_t *edt, int64_t nz, int64_t ny, int64_t nx,
+                                   uint16_t *output, void *stream) {
+    clear_error();
+    if (!gauss || !edt || !output) return set_error(MAXI_ERR_INVALID_ARGUMENT, "NULL pointer");
+    if (nz <= 0 || ny <= 0 || nx <= 0)
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "shape (%lld, %lld, %lld) has an empty axis", (long long) nz,
+                         (long long) ny, (long long) nx);
+    int rc = require_device();
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t rows = nz * ny;
+    if (rows * nx >= (int64_t(1) << 32))
+        return set_error(MAXI_ERR_UNSUPPORTED, "volumes of 2^32 voxels or more are not served by this step");
+
+    std::vector<int2> inside;
+    bool any_outside = false, any_inside = false;
+    cylinder_intervals(ny, nx, inside, any_outside, any_inside);
 
     char *scratch = nullptr;
     const size_t iv_bytes = (size_t) ny * sizeof(int2);
@@ -304,4 +322,40 @@ extern "C" int maxi_combine_fields(const uint16_t *gauss, const uint16_t *edt, i
     finish(0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     return e == cudaSuccess ? MAXI_OK : set_cuda_error(e, "combine_fields convert");
+}
+
+extern "C" int maxi_mask_cylinder(uint16_t *field, int64_t nz, int64_t ny, int64_t nx, void *stream) {
+    clear_error();
+    if (!field) return set_error(MAXI_ERR_INVALID_ARGUMENT, "NULL pointer");
+    if (nz <= 0 || ny <= 0 || nx <= 0)
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "shape (%lld, %lld, %lld) has an empty axis", (long long) nz,
+                         (long long) ny, (long long) nx);
+    if (nx >= (int64_t(1) << 31)) return set_error(MAXI_ERR_UNSUPPORTED, "rows of 2^31 voxels or more are not served");
+    int rc = require_device();
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::vector<int2> inside;
+    bool any_outside = false, any_inside = false;
+    cylinder_intervals(ny, nx, inside, any_outside, any_inside);
+    if (!any_outside) return MAXI_OK;
+    int2 *d_iv = nullptr;
+    const size_t bytes = inside.size() * sizeof(int2);
+    if (cudaMallocAsync(reinterpret_cast<void **>(&d_iv), bytes, st) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(MAXI_ERR_OUT_OF_MEMORY, "could not allocate %zu bytes of intervals", bytes);
+    }
+    cudaError_t e = cudaMemcpyAsync(d_iv, inside.data(), bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t rows = nz * ny;
+        const unsigned grid = (unsigned) std::min<int64_t>(rows, (int64_t) sms * 16);
+        cylinder_zero<<<grid, 128, 0, st>>>(field, rows, ny, (int) nx, d_iv);
+        e = cudaGetLastError();
+    }
+    cudaError_t e2 = cudaStreamSynchronize(st);  // the host intervals must outlive the copy
+    cudaFreeAsync(d_iv, st);
+    if (e == cudaSuccess) e = e2;
+    return e == cudaSuccess ? MAXI_OK : set_cuda_error(e, "cylinder mask");
 }

@@ -13,6 +13,10 @@ the second ``combined *= cylinder_mask``) with
 Both fields are uint16 [nz, ny, nx] numpy arrays (as the pipeline saves them)
 or CUDA tensors; the cylinder spans y and x as generate_cylinder_mask(ny, nx),
 which is the script's generate_cylinder_mask(nx) for its square planes.
+
+``mask_cylinder(field)`` is the diffusion step's ``result * cylinder_mask``
+before it saves the field (src/processing_steps/0900_generate_gauss_c.py:117,124):
+the voxels outside the implant cylinder become 0.
 """
 from __future__ import annotations
 
@@ -51,3 +55,26 @@ def combine_fields(gauss_field, edt_field, output=None):
     if on_device:
         return out
     return out.cpu().numpy().view(np.uint16)
+
+
+def mask_cylinder(field):
+    """field * generate_cylinder_mask(ny, nx): a new uint16 numpy array for a numpy
+    field, or the uint16/int16 CUDA tensor itself, masked in place."""
+    import torch
+
+    if isinstance(field, torch.Tensor):
+        if not field.is_cuda or field.dtype not in (torch.uint16, torch.int16) or not field.is_contiguous():
+            raise TypeError("field must be a contiguous uint16 (or int16) CUDA tensor")
+        t = field
+    else:
+        a = np.asarray(field)
+        if a.dtype != np.uint16:
+            raise TypeError("field must be a uint16 array")
+        t = torch.from_numpy(np.ascontiguousarray(a).view(np.int16)).cuda()
+    if t.dim() != 3:
+        raise ValueError(f"field must be 3-D, got {tuple(t.shape)}")
+    nz, ny, nx = t.shape
+    _lib.check(_lib.lib().maxi_mask_cylinder(t.data_ptr(), nz, ny, nx, torch.cuda.current_stream().cuda_stream))
+    if isinstance(field, torch.Tensor):
+        return field
+    return t.cpu().numpy().view(np.uint16)

@@ -5,13 +5,15 @@ maxibone's processing steps import the diffusion path as
 0900_generate_gauss_c.py:17, src/test/test_diffusion.py:17) and the mask
 packing as ``lib.cpp.gpu.bitpacking`` (src/lib/py/helpers.py); the histogram
 step imports ``axis_histograms`` and ``field_histogram`` from
-``lib.cpp.gpu.histograms`` (src/processing_steps/1000_compute_histograms.py:20).
+``lib.cpp.gpu.histograms`` (src/processing_steps/1000_compute_histograms.py:20), and
+the mask preparation reaches the sphere morphology as ``lib.cpp.gpu.morphology``
+(src/lib/py/helpers.py:19).
 ``install()``
 registers this package's drop-in modules under those dotted names, so that
 such code runs unchanged on the B200 library:
 
     import maxibone_b200.reference_imports as ri
-    ri.install()                      # lib.cpp.gpu.{diffusion, bitpacking, histograms}
+    ri.install()                      # lib.cpp.gpu.{diffusion, bitpacking, histograms, morphology}
     from lib.cpp.gpu.diffusion import diffusion
 
 ``install(cpu=True)`` also routes ``lib.cpp.cpu.*`` (the OpenMP build's import
@@ -25,7 +27,7 @@ import sys
 import types
 
 _LEAVES = {"diffusion": "maxibone_b200.diffusion", "bitpacking": "maxibone_b200.bitpacking",
-           "histograms": "maxibone_b200.histograms"}
+           "histograms": "maxibone_b200.histograms", "morphology": "maxibone_b200.morphology"}
 
 
 def _package(name: str) -> types.ModuleType:
@@ -41,7 +43,7 @@ def _package(name: str) -> types.ModuleType:
 
 
 def install(cpu: bool = False) -> list[str]:
-    """Registers lib.cpp.gpu.diffusion / .bitpacking / .histograms (and lib.cpp.cpu.* with
+    """Registers lib.cpp.gpu.diffusion / .bitpacking / .histograms / .morphology (and lib.cpp.cpu.* with
     cpu=True); returns the module names it registered."""
     done = []
     for backend in ("gpu", "cpu") if cpu else ("gpu",):

@@ -22,13 +22,18 @@ The oracles:
   ``to_int`` restated as ``normalized_convert_u16`` (pinned to the reference's
   compiled ``general.normalized_convert`` by tests/golden).
 
+* ``morphology_sphere`` and ``morphology_sphere_bitpacked``: the reference's 3-D
+  sphere dilation / erosion on uint8 and bit-packed masks
+  (src/lib/cpp/cpu_seq/morphology.cc, gpu/morphology.cc) in numpy, pinned to the
+  compiled module by tests/golden.
+
 * ``field_histogram`` and ``axis_histograms``: the 2-D (field, voxel) and the
   per-axis / radial histograms of the reference's histograms module
   (src/lib/cpp/cpu/histograms.cc:231-305 and :14-80) in numpy, pinned to the
   compiled module by tests/golden.
 
 ``reference_module()`` imports the reference's own ``diffusion`` (and
-``bitpacking``, ``general``, ``histograms``) pybind modules from ``oracle/_ref`` when they have
+``bitpacking``, ``general``, ``histograms``, ``morphology``) pybind modules from ``oracle/_ref`` when they have
 been built (``make -C oracle ref``).
 """
 from __future__ import annotations
@@ -258,6 +263,68 @@ def axis_histograms(voxels: np.ndarray, offset, global_shape, voxel_bins: int, n
         np.add.at(b, (coord[k], vi[k].astype(np.int64)), np.uint64(1))
         out.append(b)
     return tuple(out)
+
+
+def _sphere_offsets(radius: int, px_max: int | None = None):
+    r = int(radius)
+    out = []
+    for pz in range(-r, r + 1):
+        for py in range(-r, r + 1):
+            w2 = r * r - pz * pz - py * py
+            if w2 < 0:
+                continue
+            w = int(np.floor(np.sqrt(w2)))
+            while (w + 1) * (w + 1) <= w2:
+                w += 1
+            while w * w > w2:
+                w -= 1
+            hi = w if px_max is None else min(w, px_max)
+            if hi >= -w:
+                out.append((pz, py, -w, hi))
+    return out
+
+
+def morphology_sphere(mask: np.ndarray, radius: int, dilate: bool, px_max: int | None = None) -> np.ndarray:
+    """uint8 0/1 result of the reference's 3-D sphere morphology on a uint8 mask
+    (src/lib/cpp/cpu_seq/morphology.cc:14-55, as bound by
+    src/pybind/morphology-pybind.cc:24-45,147-149): every in-volume offset with
+    pz^2 + py^2 + px^2 <= radius^2 takes part (offsets outside the volume are skipped);
+    dilation ORs (v != 0), erosion ANDs (v & 1) -- std::bit_and on a bool and a byte.
+    `px_max` clips the x offsets (the bit-packed form's kernel row, below)."""
+    m = np.asarray(mask)
+    bit = (m != 0) if dilate else ((m & 1) != 0)
+    r = int(radius)
+    nz, ny, nx = bit.shape
+    pad = np.full((nz + 2 * r, ny + 2 * r, nx + 2 * r), not dilate, dtype=bool)
+    pad[r:r + nz, r:r + ny, r:r + nx] = bit
+    # x-runs: run[w_lo, w_hi][z, y, x] = op over x offsets w_lo..w_hi
+    out = np.full(bit.shape, not dilate, dtype=bool)
+    cache = {}
+    for pz, py, lo, hi in _sphere_offsets(r, px_max):
+        key = (lo, hi)
+        if key not in cache:
+            acc = np.full((nz + 2 * r, ny + 2 * r, nx), not dilate, dtype=bool)
+            for px in range(lo, hi + 1):
+                sl = pad[:, :, r + px:r + px + nx]
+                acc = (acc | sl) if dilate else (acc & sl)
+            cache[key] = acc
+        sl = cache[key][r + pz:r + pz + nz, r + py:r + py + ny, :]
+        out = (out | sl) if dilate else (out & sl)
+    return out.astype(np.uint8)
+
+
+def morphology_sphere_bitpacked(words: np.ndarray, radius: int, dilate: bool) -> np.ndarray:
+    """uint32 [nz, ny, nx/32] result of the reference's bit-packed sphere morphology
+    (src/lib/cpp/gpu/morphology.cc:103-176 and cpu_seq/morphology.cc:102-176; words
+    MSB first along x) with the GPU build's shift semantics, the module the pipeline
+    imports (src/lib/py/helpers.py:19): a shift by 32 or more, or by a negative amount,
+    gives 0.  Each (pz, py) kernel row holds x offsets -r .. 31 - r only, so the result
+    is the uint8 morphology with x offsets clipped at 31 - radius, packed again."""
+    w = np.ascontiguousarray(words, dtype=np.uint32)
+    bits = np.unpackbits(w.astype(">u4").view(np.uint8), axis=-1).reshape(w.shape[0], w.shape[1], -1)
+    res = morphology_sphere(bits, radius, dilate, px_max=31 - int(radius))
+    packed = np.packbits(res.astype(np.uint8), axis=-1).view(">u4").astype(np.uint32)
+    return packed.reshape(w.shape)
 
 
 def reference_module(name: str = "diffusion"):

@@ -13,7 +13,8 @@ words for a seeded mask; the field-combination case stores two seeded uint16
 fields and the result of the reference's 0975_combine_fields steps on them; the
 histogram cases store a voxel volume, a field and the reference's
 histograms.field_histogram bins, and a voxel block with the reference's
-histograms.axis_histograms x / y / z / radial bins.  The tests then check the oracle bit-for-bit against
+histograms.axis_histograms x / y / z / radial bins; the morphology case stores a
+uint8 mask and the reference's morphology.dilate_3d_sphere / erode_3d_sphere results.  The tests then check the oracle bit-for-bit against
 these files, and the CUDA library against the oracle.
 """
 from __future__ import annotations
@@ -137,6 +138,25 @@ def main():
                         x_bins=xb, y_bins=yb, z_bins=zb, r_bins=rb)
     index["axis_histograms_u64"] = {"file": "axis_histograms_u64.npz", "voxel_bins": 256, "n_r": n_r,
                                     "total": int(xb.sum())}
+    morph = oracle.reference_module("morphology")
+    if morph is None:
+        sys.exit("reference morphology module not built: run `make -C oracle ref`")
+    # dilate_3d_sphere / erode_3d_sphere (src/lib/cpp/cpu_seq/morphology.cc:14-99) on a
+    # seeded sphere mask with a few stray voxels, one of them a byte with bit 0 clear
+    # (erosion reads bit 0 only); radius 16 takes the reference's dedicated r16 path.
+    mshape = (24, 32, 72)
+    mmask = spheres_mask(mshape, 14, (3, 10), seed=4)
+    mmask = np.maximum(mmask, (np.random.default_rng(4).random(mshape) > 0.997).astype(np.uint8))
+    mmask[12, 16, 30] = 2
+    results = {}
+    for name, fn, r in [("dilate_r3", morph.dilate_3d_sphere, 3), ("dilate_r16", morph.dilate_3d_sphere, 16),
+                        ("erode_r2", morph.erode_3d_sphere, 2), ("erode_r5", morph.erode_3d_sphere, 5)]:
+        res = np.zeros(mshape, np.uint8)
+        fn(mmask, r, res)
+        results[name] = res
+    np.savez_compressed(os.path.join(HERE, "morphology_u8.npz"), mask=mmask, **results)
+    index["morphology_u8"] = {"file": "morphology_u8.npz", "shape": list(mshape),
+                              "counts": {k: int(v.sum()) for k, v in results.items()}}
     with open(os.path.join(HERE, "index.json"), "w") as f:
         json.dump(index, f, indent=1, sort_keys=True)
 

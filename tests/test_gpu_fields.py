@@ -12,7 +12,7 @@ import torch
 import oracle
 from conftest import GOLDEN
 from maxibone_b200 import device, gauss_kernel
-from maxibone_b200.fields import combine_fields
+from maxibone_b200.fields import combine_fields, mask_cylinder
 from maxibone_b200.synthetic import spheres_mask
 
 pytestmark = pytest.mark.gpu
@@ -66,3 +66,27 @@ def test_combine_fields_rejects_all_zero_field_and_bad_shapes():
         combine_fields(z + 1, np.ones((4, 16, 8), np.uint16))
     with pytest.raises(TypeError):
         combine_fields(z.astype(np.float32), z)
+
+
+# The diffusion step's result * generate_cylinder_mask(nx) (square planes, as the
+# script) and the (ny, nx) form for other planes; odd and even sizes, one-voxel axes.
+@pytest.mark.parametrize("shape", [(4, 64, 64), (3, 65, 65), (2, 40, 56), (2, 1, 16), (1, 7, 1), (5, 33, 100)])
+def test_mask_cylinder_matches_reference_multiply(shape):
+    rng = np.random.default_rng(sum(shape))
+    field = rng.integers(0, 65536, shape, dtype=np.uint16)
+    want = field * oracle.cylinder_mask(shape[1], shape[2])
+    assert want.dtype == np.uint16
+    np.testing.assert_array_equal(mask_cylinder(field), want)
+    t = torch.from_numpy(field.view(np.int16)).cuda()
+    assert mask_cylinder(t) is t
+    np.testing.assert_array_equal(t.cpu().numpy().view(np.uint16), want)
+
+
+def test_mask_cylinder_on_diffusion_output():
+    shape = (32, 96, 96)
+    mask = spheres_mask(shape, 10, (3, 12), seed=5)
+    out = torch.empty(shape, dtype=torch.uint16, device="cuda")
+    device.diffuse(torch.from_numpy(mask).cuda(), gauss_kernel(2.0).astype(np.float32), 4, output=out)
+    want = out.cpu().numpy() * oracle.cylinder_mask(96)
+    mask_cylinder(out)
+    np.testing.assert_array_equal(out.cpu().numpy(), want)

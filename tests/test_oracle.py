@@ -153,3 +153,46 @@ def test_oracle_axis_histograms_matches_reference_module(zoff, yoff, xoff, cente
     got = oracle.axis_histograms(v, (zoff, yoff, xoff), gs, nb, n_r, center, vr)
     for g, w in zip(got, want):
         np.testing.assert_array_equal(g, w)
+
+
+def _golden_morph():
+    import os
+    from conftest import GOLDEN
+    return np.load(os.path.join(GOLDEN, "morphology_u8.npz"))
+
+
+def test_oracle_morphology_matches_reference_golden():
+    z = _golden_morph()
+    for name in ("dilate_r3", "dilate_r16", "erode_r2", "erode_r5"):
+        op, r = name.split("_r")
+        np.testing.assert_array_equal(oracle.morphology_sphere(z["mask"], int(r), op == "dilate"), z[name],
+                                      err_msg=name)
+
+
+@pytest.mark.parametrize("r", [0, 1, 4, 7, 15])
+def test_oracle_morphology_bitpacked_equals_packed_reference_for_small_radii(r):
+    """Below radius 16 the bit-packed kernel rows hold the whole sphere, so the packed
+    form equals the reference's uint8 result packed (MSB first)."""
+    z = _golden_morph()
+    m = np.ascontiguousarray(z["mask"][:, :, :64])  # whole words
+    words = np.packbits((m != 0).astype(np.uint8), axis=-1).view(">u4").astype(np.uint32).reshape(
+        m.shape[0], m.shape[1], -1)
+    got = oracle.morphology_sphere_bitpacked(words, r, True)
+    want = np.packbits(oracle.morphology_sphere(m, r, True), axis=-1).view(">u4").astype(np.uint32).reshape(
+        words.shape)
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("shape,r", [((9, 10, 11), 0), ((12, 14, 16), 1), ((20, 22, 24), 5), ((18, 20, 37), 16),
+                                     ((8, 30, 40), 9)])
+def test_oracle_morphology_matches_reference_module(shape, r):
+    morph = oracle.reference_module("morphology")
+    if morph is None:
+        pytest.skip("reference morphology module not built (make -C oracle ref)")
+    rng = np.random.default_rng(r + shape[2])
+    m = (rng.random(shape) > 0.4).astype(np.uint8)
+    m[rng.random(shape) > 0.97] = 2
+    for dilate, fn in ((True, morph.dilate_3d_sphere), (False, morph.erode_3d_sphere)):
+        want = np.zeros(shape, np.uint8)
+        fn(m, r, want)
+        np.testing.assert_array_equal(oracle.morphology_sphere(m, r, dilate), want)

@@ -26,7 +26,8 @@ def clean_lib_modules():
 
 def test_install_serves_reference_paths(clean_lib_modules):
     names = reference_imports.install()
-    assert names == ["lib.cpp.gpu.diffusion", "lib.cpp.gpu.bitpacking", "lib.cpp.gpu.histograms"]
+    assert names == ["lib.cpp.gpu.diffusion", "lib.cpp.gpu.bitpacking", "lib.cpp.gpu.histograms",
+                     "lib.cpp.gpu.morphology"]
     from lib.cpp.gpu.diffusion import diffusion  # noqa: E402  (the production import line)
     from lib.cpp.gpu import bitpacking  # noqa: E402
     # the histogram step's import line (src/processing_steps/1000_compute_histograms.py:20)
@@ -34,6 +35,9 @@ def test_install_serves_reference_paths(clean_lib_modules):
     from lib.cpp.gpu.histograms import field_histogram as field_histogram_par_gpu  # noqa: E402
     hg = importlib.import_module("maxibone_b200.histograms")
     assert axis_histogram_par_gpu is hg.axis_histograms and field_histogram_par_gpu is hg.field_histogram
+    import lib.cpp.gpu.morphology as lib_morphology  # noqa: E402  (src/lib/py/helpers.py:19)
+    assert lib_morphology.dilate_3d_sphere_bitpacked is importlib.import_module(
+        "maxibone_b200.morphology").dilate_3d_sphere_bitpacked
     assert diffusion is dd.diffusion
     assert bitpacking.encode is bp.encode and bitpacking.decode is bp.decode
     assert importlib.import_module("lib.cpp.gpu.diffusion") is dd

@@ -335,6 +335,7 @@ int maxi_diffusion_in_memory(const uint8_t *voxels, int64_t nz, int64_t ny, int6
 int maxi_release_cached_memory(void) {
     clear_error();
     release_device_caches();
+    release_morphology_scratch();
     return MAXI_OK;
 }
 

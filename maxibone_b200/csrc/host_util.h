@@ -71,4 +71,7 @@ inline int validate_common(const void *mask, int64_t nz, int64_t ny, int64_t nx,
     return MAXI_OK;
 }
 
+// Frees the sphere-morphology scratch kept between calls (morphology.cu).
+void release_morphology_scratch();
+
 }  // namespace maxi

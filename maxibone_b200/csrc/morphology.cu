@@ -14,16 +14,21 @@
 // around each output word; with the GPU build's shifts (a shift by 32 or more, or by a
 // negative amount, gives 0) that is the sphere with x offsets clipped at 31 - r.
 //
-// Three passes over packed words, radius <= 32:
-//   1. x-runs: X_w[z][y][i] = OP over x offsets -w .. min(w, P) of the row (P = r for
-//      the uint8 form, 31 - r for the bit-packed one), w = 0 .. r, built incrementally
-//      with one funnel shift each way per step from the word and its two neighbours.
-//   2. discs: D_k[z][y][i] = OP over in-volume py of X_{isqrt(r^2 - k^2 - py^2)}[z][y+py][i]
-//      for k = 0 .. r (the sphere's cross-section at |pz| = k).
-//   3. z: out[z][y][i] = OP over in-volume pz of D_{|pz|}[z+pz][y][i].
-// OP is OR for dilation and AND for erosion; outside-volume words and the padding bits
-// of a row are the neutral element.  Each output word costs about (pi/2) r^2 + 3r reads
-// instead of the (2r+1)^2 * 32 bit steps of the direct form.
+// Two kernels over packed words, radius <= 32:
+//   1. morph_plane_discs, one block per tile of a plane (16 rows, up to 32 words):
+//      the tile's rows +- r with one halo word each side go to shared memory; there
+//      the x-runs X_w = OP over x offsets -w .. min(w, P) (P = r for the uint8 form,
+//      31 - r for the bit-packed one), w = 0 .. r, are built incrementally with one
+//      funnel shift each way per step; then each output word gets the discs
+//      D_k = OP over py of X_{isqrt(r^2 - k^2 - py^2)}[y + py], k = 0 .. r (the
+//      sphere's cross-section at |pz| = k), written to global scratch.
+//   2. morph_z: out[z][y][i] = OP over in-volume pz of D_{|pz|}[z+pz][y][i].
+// OP is OR for dilation and AND for erosion; outside-volume rows and words and the
+// padding bits of a row are the neutral element.  Each output word costs about
+// (pi/2) r^2 shared-memory reads and 3r global accesses, instead of the
+// (2r+1)^2 * 32 bit steps of the direct form.
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -46,47 +51,82 @@ __device__ __forceinline__ int isqrt_small(int n) {  // floor(sqrt(n)), 0 <= n <
     return r;
 }
 
-// Pass 1.  Word i of a row; its bits at x offset d come from the 96-bit stream
-// (left, word, right): d < 0 from funnelshift_rc(word, left, -d), d > 0 from
-// funnelshift_lc(right, word, d).
-template <bool DILATE>
-__global__ void morph_xruns(const uint32_t *__restrict__ in, uint32_t *__restrict__ xr, int64_t words, int nw,
-                            int radius, int pmax) {
-    const uint32_t neutral = DILATE ? 0u : 0xffffffffu;
-    for (int64_t idx = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; idx < words;
-         idx += (int64_t) gridDim.x * blockDim.x) {
-        const int i = (int) (idx % nw);
-        const uint32_t mid = __ldg(in + idx);
-        const uint32_t left = i > 0 ? __ldg(in + idx - 1) : neutral;
-        const uint32_t right = i < nw - 1 ? __ldg(in + idx + 1) : neutral;
-        uint32_t acc = neutral;
-        for (int w = 0; w <= radius; w++) {
-            if (-w <= pmax) acc = op<DILATE>(acc, w == 0 ? mid : __funnelshift_rc(mid, left, w));
-            if (w > 0 && w <= pmax) acc = op<DILATE>(acc, __funnelshift_lc(right, mid, w));
-            xr[(int64_t) w * words + idx] = acc;
-        }
-    }
+constexpr int kTileRows = 16;
+
+struct PlaneTile {
+    int nw, ny, radius, pmax, tile_words;  // tile_words: words per tile along x (<= 32)
+    int64_t x_tiles, y_tiles, tiles;
+};
+
+size_t plane_tile_smem(int radius, int tile_words) {
+    const int rows = kTileRows + 2 * radius;
+    return (size_t) rows * (tile_words + 2) * 4 + (size_t) (radius + 1) * rows * tile_words * 4 +
+           (size_t) (radius + 1) * (2 * radius + 1);
 }
 
-// Pass 2.  One thread per word (lanes along x); all disc radii for that word.
+// Pass 1 (x-runs and discs).  Block: 32 lanes along x by 8 warps along y.  Bits at x
+// offset d of word j come from the stream (left, word, right): d < 0 from
+// funnelshift_rc(word, left, -d), d > 0 from funnelshift_lc(right, word, d).
 template <bool DILATE>
-__global__ void morph_discs(const uint32_t *__restrict__ xr, uint32_t *__restrict__ disc, int64_t words, int ny,
-                            int nw, int radius) {
+__global__ void __launch_bounds__(256) morph_plane_discs(const uint32_t *__restrict__ in, uint32_t *__restrict__ disc,
+                                                         int64_t words, PlaneTile t) {
     const uint32_t neutral = DILATE ? 0u : 0xffffffffu;
-    const int64_t plane = (int64_t) ny * nw;
-    for (int64_t idx = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; idx < words;
-         idx += (int64_t) gridDim.x * blockDim.x) {
-        const int y = (int) ((idx % plane) / nw);
-        for (int k = 0; k <= radius; k++) {
-            const int r2 = radius * radius - k * k;
-            const int h = isqrt_small(r2);
-            const int lo = max(-h, -y), hi = min(h, ny - 1 - y);
+    const int r = t.radius, rows = kTileRows + 2 * r, tw = t.tile_words, hw = tw + 2;
+    extern __shared__ uint32_t sh[];
+    uint32_t *in_s = sh;                                   // [rows][tw + 2]
+    uint32_t *xr_s = in_s + rows * hw;                     // [r + 1][rows][tw]
+    uint8_t *wtab = reinterpret_cast<uint8_t *>(xr_s + (r + 1) * rows * tw);  // [r + 1][2r + 1]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < (r + 1) * (2 * r + 1); i += blockDim.x) {
+        const int k = i / (2 * r + 1), py = i % (2 * r + 1) - r;
+        const int n = r * r - k * k - py * py;
+        wtab[i] = (uint8_t) (n < 0 ? 0xff : isqrt_small(n));
+    }
+    const int64_t plane = (int64_t) t.ny * t.nw;
+    for (int64_t tile = blockIdx.x; tile < t.tiles; tile += gridDim.x) {
+        const int64_t xt = tile % t.x_tiles, rest = tile / t.x_tiles;
+        const int64_t yt = rest % t.y_tiles, z = rest / t.y_tiles;
+        const int x0 = (int) xt * tw, y0 = (int) yt * kTileRows;
+        const uint32_t *pl = in + z * plane;
+        __syncthreads();  // the previous tile is done with the shared arrays
+        for (int i = threadIdx.x; i < rows * hw; i += blockDim.x) {
+            const int row = i / hw, c = i % hw;
+            const int y = y0 - r + row, x = x0 - 1 + c;
+            in_s[i] = (y >= 0 && y < t.ny && x >= 0 && x < t.nw) ? __ldg(pl + (int64_t) y * t.nw + x) : neutral;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < rows * tw; i += blockDim.x) {
+            const int row = i / tw, j = i % tw;
+            const int y = y0 - r + row;
+            const bool inside = y >= 0 && y < t.ny && x0 + j < t.nw;
+            const uint32_t left = in_s[row * hw + j], mid = in_s[row * hw + j + 1], right = in_s[row * hw + j + 2];
             uint32_t acc = neutral;
-            for (int py = lo; py <= hi; py++) {
-                const int w = isqrt_small(r2 - py * py);
-                acc = op<DILATE>(acc, __ldg(xr + (int64_t) w * words + idx + (int64_t) py * nw));
+            for (int w = 0; w <= r; w++) {
+                if (inside) {
+                    if (-w <= t.pmax) acc = op<DILATE>(acc, w == 0 ? mid : __funnelshift_rc(mid, left, w));
+                    if (w > 0 && w <= t.pmax) acc = op<DILATE>(acc, __funnelshift_lc(right, mid, w));
+                }
+                xr_s[(w * rows + row) * tw + j] = acc;
             }
-            disc[(int64_t) k * words + idx] = acc;
+        }
+        __syncthreads();
+        if (lane < tw && x0 + lane < t.nw) {
+            for (int ty = warp; ty < kTileRows; ty += blockDim.x >> 5) {
+                const int y = y0 + ty;
+                if (y >= t.ny) break;
+                uint32_t *dst = disc + z * plane + (int64_t) y * t.nw + x0 + lane;
+                const uint32_t *col = xr_s + (ty + r) * tw + lane;  // row y of X_0
+                for (int k = 0; k <= r; k++) {
+                    // rows y +- py of X_w with w = isqrt(r^2 - k^2 - py^2), py = 0 .. isqrt(r^2 - k^2)
+                    const uint8_t *wk = wtab + k * (2 * r + 1) + r;
+                    uint32_t acc = col[wk[0] * rows * tw];
+                    for (int py = 1; py <= r && wk[py] != 0xff; py++) {
+                        const uint32_t *c = col + wk[py] * rows * tw;
+                        acc = op<DILATE>(acc, op<DILATE>(c[py * tw], c[-py * tw]));
+                    }
+                    dst[(int64_t) k * words] = acc;
+                }
+            }
         }
     }
 }
@@ -144,17 +184,33 @@ unsigned grid_for(int64_t n) {
     return (unsigned) std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), (int64_t) sms * 16));
 }
 
-// The three passes from `in` to `out` (both packed, words = nz * ny * nw) with the
-// x offsets clipped at pmax; scratch holds 2 * (radius + 1) * words words.
+// The passes from `in` to `out` (both packed, words = nz * ny * nw) with the x offsets
+// clipped at pmax; scratch holds (radius + 1) * words words.
 template <bool DILATE>
-void morph_passes(const uint32_t *in, uint32_t *out, uint32_t *scratch, int64_t nz, int64_t ny, int64_t nw,
-                  int radius, int pmax, cudaStream_t st) {
+int morph_passes(const uint32_t *in, uint32_t *out, uint32_t *scratch, int64_t nz, int64_t ny, int64_t nw,
+                 int radius, int pmax, cudaStream_t st) {
     const int64_t words = nz * ny * nw;
-    uint32_t *xr = scratch, *disc = scratch + (int64_t) (radius + 1) * words;
-    const unsigned g = grid_for(words);
-    morph_xruns<DILATE><<<g, 256, 0, st>>>(in, xr, words, (int) nw, radius, pmax);
-    morph_discs<DILATE><<<g, 256, 0, st>>>(xr, disc, words, (int) ny, (int) nw, radius);
-    morph_z<DILATE><<<g, 256, 0, st>>>(disc, out, words, (int) nz, ny * nw, radius);
+    PlaneTile t{};
+    t.nw = (int) nw;
+    t.ny = (int) ny;
+    t.radius = radius;
+    t.pmax = pmax;
+    t.tile_words = 32;
+    while (t.tile_words > 8 && plane_tile_smem(radius, t.tile_words) > 200 * 1024) t.tile_words /= 2;
+    t.x_tiles = ceil_div(nw, t.tile_words);
+    t.y_tiles = ceil_div(ny, kTileRows);
+    t.tiles = t.x_tiles * t.y_tiles * nz;
+    const size_t smem = plane_tile_smem(radius, t.tile_words);
+    cudaError_t e = cudaFuncSetAttribute(morph_plane_discs<DILATE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int) smem);
+    if (e != cudaSuccess) return set_cuda_error(e, "morphology set-up");
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned g1 = (unsigned) std::min<int64_t>(t.tiles, (int64_t) sms * 8);
+    morph_plane_discs<DILATE><<<g1, 256, smem, st>>>(in, scratch, words, t);
+    morph_z<DILATE><<<grid_for(words), 256, 0, st>>>(scratch, out, words, (int) nz, ny * nw, radius);
+    return MAXI_OK;
 }
 
 int check_shape(int64_t nz, int64_t ny, int64_t n_inner, int64_t radius) {
@@ -171,16 +227,63 @@ int check_shape(int64_t nz, int64_t ny, int64_t n_inner, int64_t radius) {
     return MAXI_OK;
 }
 
-int alloc_scratch(uint32_t **p, size_t bytes, cudaStream_t st) {
-    if (cudaMallocAsync(reinterpret_cast<void **>(p), bytes, st) != cudaSuccess) {
-        cudaGetLastError();
-        *p = nullptr;
-        return set_error(MAXI_ERR_OUT_OF_MEMORY, "could not allocate %zu bytes of morphology scratch", bytes);
+// Scratch kept between calls, one grow-only buffer per device: the pipeline applies
+// radius-16 spheres over and over, and mapping gigabytes afresh for each call would
+// cost more than the passes.  A call holds its device's buffer until it returns.
+struct Scratch {
+    std::mutex mu;
+    uint32_t *buf = nullptr;
+    size_t bytes = 0;
+};
+std::mutex g_scratch_mu;
+std::map<int, Scratch *> g_scratch;
+
+// Locks and returns the device's scratch, grown to `bytes`.
+int acquire_scratch(size_t bytes, std::unique_lock<std::mutex> &lock, uint32_t **p) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaGetDevice");
+    Scratch *s;
+    {
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        Scratch *&slot = g_scratch[dev];
+        if (!slot) slot = new Scratch();
+        s = slot;
     }
+    lock = std::unique_lock<std::mutex>(s->mu);
+    if (s->bytes < bytes) {
+        if (s->buf) {
+            cudaDeviceSynchronize();  // earlier calls' work on the old buffer
+            cudaFree(s->buf);
+            s->buf = nullptr;
+            s->bytes = 0;
+        }
+        if (cudaMalloc(reinterpret_cast<void **>(&s->buf), bytes) != cudaSuccess) {
+            cudaGetLastError();
+            s->buf = nullptr;
+            return set_error(MAXI_ERR_OUT_OF_MEMORY, "could not allocate %zu bytes of morphology scratch", bytes);
+        }
+        s->bytes = bytes;
+    }
+    *p = s->buf;
     return MAXI_OK;
 }
 
 }  // namespace
+
+void release_morphology_scratch() {
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    for (auto &kv : g_scratch) {
+        std::lock_guard<std::mutex> lk2(kv.second->mu);
+        if (kv.second->buf) {
+            cudaDeviceSynchronize();
+            cudaFree(kv.second->buf);
+            kv.second->buf = nullptr;
+            kv.second->bytes = 0;
+        }
+    }
+}
+
 }  // namespace maxi
 
 using namespace maxi;
@@ -197,13 +300,15 @@ extern "C" int maxi_morphology_sphere_bitpacked(const uint32_t *voxels, uint32_t
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int64_t words = nz * ny * nw;
     uint32_t *scratch = nullptr;
-    if ((rc = alloc_scratch(&scratch, (size_t) 2 * (radius + 1) * words * sizeof(uint32_t), st))) return rc;
+    std::unique_lock<std::mutex> hold;
+    if ((rc = acquire_scratch((size_t) (radius + 1) * words * sizeof(uint32_t), hold, &scratch))) return rc;
     const int r = (int) radius, pmax = 31 - r;
-    if (dilate) morph_passes<true>(voxels, result, scratch, nz, ny, nw, r, pmax, st);
-    else morph_passes<false>(voxels, result, scratch, nz, ny, nw, r, pmax, st);
+    rc = dilate ? morph_passes<true>(voxels, result, scratch, nz, ny, nw, r, pmax, st)
+                : morph_passes<false>(voxels, result, scratch, nz, ny, nw, r, pmax, st);
     cudaError_t e = cudaGetLastError();
-    cudaFreeAsync(scratch, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaError_t e2 = cudaStreamSynchronize(st);  // the scratch is free for the next call
+    if (rc) return rc;
+    if (e == cudaSuccess) e = e2;
     return e == cudaSuccess ? MAXI_OK : set_cuda_error(e, "bit-packed sphere morphology");
 }
 
@@ -217,22 +322,27 @@ extern "C" int maxi_morphology_sphere(const uint8_t *voxels, uint8_t *result, in
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int64_t nw = ceil_div(nx, 32), words = nz * ny * nw;
     uint32_t *scratch = nullptr;
+    std::unique_lock<std::mutex> hold;
     // packed input, packed result, then the pass scratch
-    if ((rc = alloc_scratch(&scratch, (size_t) (2 + 2 * (radius + 1)) * words * sizeof(uint32_t), st))) return rc;
+    if ((rc = acquire_scratch((size_t) (2 + (radius + 1)) * words * sizeof(uint32_t), hold, &scratch))) return rc;
     uint32_t *packed = scratch, *packed_out = scratch + words, *pass = scratch + 2 * words;
     const int r = (int) radius;
     const unsigned g = grid_for(words);
     if (dilate) {
         morph_pack<true><<<g, 256, 0, st>>>(voxels, packed, words, (int) nx, (int) nw);
-        morph_passes<true>(packed, packed_out, pass, nz, ny, nw, r, r, st);
+        rc = morph_passes<true>(packed, packed_out, pass, nz, ny, nw, r, r, st);
     } else {
         morph_pack<false><<<g, 256, 0, st>>>(voxels, packed, words, (int) nx, (int) nw);
-        morph_passes<false>(packed, packed_out, pass, nz, ny, nw, r, r, st);
+        rc = morph_passes<false>(packed, packed_out, pass, nz, ny, nw, r, r, st);
+    }
+    if (rc) {
+        cudaStreamSynchronize(st);
+        return rc;
     }
     const int64_t voxels_n = nz * ny * nx;
     morph_unpack<<<grid_for(voxels_n), 256, 0, st>>>(packed_out, result, voxels_n, (int) nx, (int) nw);
     cudaError_t e = cudaGetLastError();
-    cudaFreeAsync(scratch, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaError_t e2 = cudaStreamSynchronize(st);  // the scratch is free for the next call
+    if (e == cudaSuccess) e = e2;
     return e == cudaSuccess ? MAXI_OK : set_cuda_error(e, "sphere morphology");
 }

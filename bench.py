@@ -28,7 +28,10 @@ Also reported on the same line:
                 (`--downstream-only` runs just these and the morphology);
   morphology    the sphere dilation that prepares masks (radius 16, uint8 and
                 bit-packed) on the workload's mask, beside the reference's CPU
-                module on a bounded sample.
+                module on a bounded sample;
+  implant_masks the implant solid / shell / front / back masks that feed the
+                diffusion, on the workload's mask, beside the reference's CPU
+                geometry module on a bounded sample.
 
 `--impl reference` times only the reference CPU module on the bounded sample.
 """
@@ -492,6 +495,60 @@ def morphology_section(torch, np, mask, stream):
     return res
 
 
+def implant_section(torch, np, mask, stream):
+    """The implant masks that feed the diffusion (compute_front_back_masks,
+    src/processing_steps/0750_bone_region.py:62) on the workload's mask with a seeded
+    frame of reference, against the reference's compiled geometry module on a bounded
+    sample."""
+    import oracle
+    from maxibone_b200.geometry import compute_front_back_masks
+
+    shape = tuple(mask.shape)
+    vox = int(np.prod(shape))
+    m = (mask != 0).to(torch.uint8).contiguous()
+    rng = np.random.default_rng(5)
+    E = np.linalg.qr(rng.normal(size=(3, 3)))[0]
+    UVWp = np.linalg.qr(rng.normal(size=(3, 3)))[0]
+    cm = torch.nonzero(m[:: 8]).to(torch.float64).mean(0).cpu().numpy() * np.array([8, 1, 1])
+    cp = rng.normal(size=3) * 20
+    outs = [torch.empty_like(m) for _ in range(4)]
+    compute_front_back_masks(m, 1.875, E, cm, cp, UVWp, *outs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_t = 3
+    e0.record(stream)
+    for _ in range(n_t):
+        compute_front_back_masks(m, 1.875, E, cm, cp, UVWp, *outs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n_t
+    peak, _ = load_peaks()
+    alg = 7 * vox  # three reads of the 1-byte mask, four 1-byte masks written
+    res = {"workload": f"{shape[0]}x{shape[1]}x{shape[2]} bone-implant mask, seeded frame of reference",
+           "value": vox / (ms / 1e3) / 1e9, "unit": "Gvox/s", "ms": ms, "hbm_gbs": alg / (ms / 1e3) / 1e9,
+           "hbm_frac": alg / (ms / 1e3) / 1e9 / peak, "alg_bytes_per_voxel": 7,
+           "timing": "CUDA events around 3 synchronous calls"}
+    geo = oracle.reference_module("geometry")
+    sample = (64, 512, 512)
+    sm = np.ascontiguousarray(m[: sample[0], : sample[1], : sample[2]].cpu().numpy())
+    want = [np.empty(sm.shape, np.uint8) for _ in range(4)]
+    t0 = time.perf_counter()
+    if geo is not None:
+        geo.compute_front_back_masks(sm, 1.875, E, cm, cp, UVWp, *want)
+    else:
+        want = list(oracle.implant_masks(sm, 1.875, E, cm, cp, UVWp))
+    cpu_s = time.perf_counter() - t0
+    got = [np.empty(sm.shape, np.uint8) for _ in range(4)]
+    compute_front_back_masks(sm, 1.875, E, cm, cp, UVWp, *got)
+    res["cpu_baseline"] = {"value": sm.size / cpu_s / 1e9, "unit": "Gvox/s",
+                           "kind": "reference" if geo is not None else "port",
+                           "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+                           "sample": f"{sample} crop, one compute_front_back_masks call",
+                           "gpu_equals_reference": all(np.array_equal(a, b) for a, b in zip(got, want))}
+    del m, outs
+    return res
+
+
 def batched_plan_on_volume(device, torch, np, mask, kernel, reps, stream):
     """The BF16 batch plan (CUDA graph of persistent tensor-core launches, one per
     pass) over the workload's single volume: the batched form on the 1024^3 mask."""
@@ -657,7 +714,8 @@ def main():
             print(json.dumps({"workload": args.workload, "shape": list(shape), "field": args.field,
                               "fields": {"combine_fields": fields_section(torch, np, out, stream),
                                          **histogram_section(torch, np, mask, out, stream)},
-                              "morphology": morphology_section(torch, np, mask, stream)}), flush=True)
+                              "morphology": morphology_section(torch, np, mask, stream),
+                              "implant_masks": implant_section(torch, np, mask, stream)}), flush=True)
         return
 
     for _ in range(args.warmup):
@@ -807,6 +865,7 @@ def main():
         line["fields"] = {"combine_fields": fields_section(torch, np, out, stream),
                           **histogram_section(torch, np, mask, out, stream)}
         line["morphology"] = morphology_section(torch, np, mask, stream)
+        line["implant_masks"] = implant_section(torch, np, mask, stream)
         line["batched"] = batched_section(device, torch, np, stream)
         line["batched"]["bf16_plan_on_workload_volume"] = bv = batched_plan_on_volume(
             device, torch, np, mask, kernel, reps, stream)

@@ -287,6 +287,20 @@ int maxi_morphology_sphere_bitpacked(const uint32_t *voxels, uint32_t *result, i
                                      int64_t nw, int64_t radius, int dilate, void *stream);
 
 /*
+ * The implant's front / back / shell / solid masks in its frame of reference: the
+ * reference's compute_front_back_masks (src/lib/cpp/cpu_seq/geometry.cc:112-215,
+ * bound by src/pybind/geometry-pybind.cc:283-310), run by
+ * src/processing_steps/0750_bone_region.py:62 to make the implant_solid mask the
+ * diffusion step diffuses.  mask and the four outputs: device uint8[nz][ny][nx];
+ * E, cm, cp, UVWp: HOST float arrays of 9, 3, 3 and 9 values (row-major 3x3).
+ * Identical to the reference (FP32 in its operation order, no fused multiply-add;
+ * the 0.7 * rmax comparisons in FP64).  Axes up to 2^24.  Synchronises the stream.
+ */
+int maxi_implant_masks(const uint8_t *mask, int64_t nz, int64_t ny, int64_t nx, float voxel_size, const float *E,
+                       const float *cm, const float *cp, const float *UVWp, uint8_t *front_mask, uint8_t *back_mask,
+                       uint8_t *implant_shell_mask, uint8_t *solid_implant, void *stream);
+
+/*
  * 2-D histogram of (field value, voxel value) pairs, added into bins: the
  * reference's field_histogram (src/lib/cpp/cpu/histograms.cc:231-305, bound by
  * src/pybind/histograms-pybind.cc:81-107), the consumer of the diffusion field

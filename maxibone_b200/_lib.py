@@ -45,6 +45,7 @@ SIGNATURES = {
     "maxi_mask_cylinder": (_int, [_p, _i64, _i64, _i64, _p]),
     "maxi_morphology_sphere": (_int, [_p, _p, _i64, _i64, _i64, _i64, _int, _p]),
     "maxi_morphology_sphere_bitpacked": (_int, [_p, _p, _i64, _i64, _i64, _i64, _int, _p]),
+    "maxi_implant_masks": (_int, [_p, _i64, _i64, _i64, ctypes.c_float, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "maxi_field_histogram": (_int, [_p, _i64, _i64, _i64, _p, _i64, _i64, _i64, _i64, _i64, _p, _i64, _i64,
                                     ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, _p]),
     "maxi_axis_histograms": (_int, [_p, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _p, _p, _p, _p, _i64, _i64,

@@ -27,13 +27,17 @@ The oracles:
   (src/lib/cpp/cpu_seq/morphology.cc, gpu/morphology.cc) in numpy, pinned to the
   compiled module by tests/golden.
 
+* ``implant_masks``: the front / back / implant-shell / solid-implant masks of the
+  reference's geometry module (src/lib/cpp/cpu_seq/geometry.cc:112-215) in numpy
+  float32, pinned to the compiled module by tests/golden.
+
 * ``field_histogram`` and ``axis_histograms``: the 2-D (field, voxel) and the
   per-axis / radial histograms of the reference's histograms module
   (src/lib/cpp/cpu/histograms.cc:231-305 and :14-80) in numpy, pinned to the
   compiled module by tests/golden.
 
 ``reference_module()`` imports the reference's own ``diffusion`` (and
-``bitpacking``, ``general``, ``histograms``, ``morphology``) pybind modules from ``oracle/_ref`` when they have
+``bitpacking``, ``general``, ``histograms``, ``morphology``, ``geometry``) pybind modules from ``oracle/_ref`` when they have
 been built (``make -C oracle ref``).
 """
 from __future__ import annotations
@@ -325,6 +329,58 @@ def morphology_sphere_bitpacked(words: np.ndarray, radius: int, dilate: bool) ->
     res = morphology_sphere(bits, radius, dilate, px_max=31 - int(radius))
     packed = np.packbits(res.astype(np.uint8), axis=-1).view(">u4").astype(np.uint32)
     return packed.reshape(w.shape)
+
+
+def implant_masks(mask: np.ndarray, voxel_size, E, cm, cp, UVWp, planes=None):
+    """(front, back, implant_shell, solid_implant) uint8 masks of the reference's
+    compute_front_back_masks (src/lib/cpp/cpu_seq/geometry.cc:112-215, bound by
+    src/pybind/geometry-pybind.cc:283-310, called by src/processing_steps/0750_bone_region.py:62),
+    in float32 with the reference's operation order (no fused multiply-add, as its
+    x86-64 build): uvw = (zyx - cm) @ E, w0 = min(0, min of w over the mask),
+    UVW = (uvw - (0, 0, w0)) * voxel_size, (Vp, Wp) from (UVW - cp) @ UVWp,
+    r = sqrt(Vp^2 + Wp^2), rmax = per-plane max of r * mask; the comparisons with
+    0.7 * rmax are in FP64.  `planes`: evaluate only these z planes (the outputs are
+    [len(planes), ny, nx]); w0 still comes from the whole mask."""
+    f32 = np.float32
+    m = np.asarray(mask)
+    E = np.asarray(E, f32).reshape(9)
+    cm = np.asarray(cm, f32).reshape(3)
+    cp = np.asarray(cp, f32).reshape(3)
+    P = np.asarray(UVWp, f32).reshape(9)
+    vs = f32(voxel_size)
+    nz, ny, nx = m.shape
+
+    def comp(zs, ys, xs, k):
+        return (zs * E[k] + ys * E[3 + k]) + xs * E[6 + k]
+
+    w0 = f32(0)
+    nzs = np.nonzero(m)
+    if nzs[0].size:
+        wz = comp(nzs[0].astype(f32) - cm[0], nzs[1].astype(f32) - cm[1], nzs[2].astype(f32) - cm[2], 2)
+        w0 = min(f32(0), f32(wz.min()))
+    ys = (np.arange(ny, dtype=np.int64).astype(f32) - cm[1])[:, None]
+    xs = (np.arange(nx, dtype=np.int64).astype(f32) - cm[2])[None, :]
+    zlist = range(nz) if planes is None else list(planes)
+    outs = [np.empty((len(zlist), ny, nx), np.uint8) for _ in range(4)]
+    for i, z in enumerate(zlist):
+        zs = f32(z) - cm[0]
+        U = (comp(zs, ys, xs, 0) - f32(0)) * vs
+        V = (comp(zs, ys, xs, 1) - f32(0)) * vs
+        W = (comp(zs, ys, xs, 2) - f32(w0)) * vs
+        a, b, c = U - cp[0], V - cp[1], W - cp[2]
+        Vp = (a * P[1] + b * P[4]) + c * P[7]
+        Wp = (a * P[2] + b * P[5]) + c * P[8]
+        r = np.sqrt(Vp * Vp + Wp * Wp).astype(f32)
+        mz = m[z]
+        rmax = max(f32(0), f32((r * mz.astype(f32)).max()))
+        lim = 0.7 * float(rmax)
+        rd = r.astype(np.float64)
+        solid = (mz | ((rd < lim) & (W >= 0)).astype(np.uint8)).astype(np.uint8)
+        outs[0][i] = ((W > 50) & (solid == 0)).astype(np.uint8)
+        outs[1][i] = (W < 0).astype(np.uint8)
+        outs[2][i] = (mz & (rd >= lim).astype(np.uint8)).astype(np.uint8)
+        outs[3][i] = solid
+    return tuple(outs)
 
 
 def reference_module(name: str = "diffusion"):

@@ -14,7 +14,9 @@ fields and the result of the reference's 0975_combine_fields steps on them; the
 histogram cases store a voxel volume, a field and the reference's
 histograms.field_histogram bins, and a voxel block with the reference's
 histograms.axis_histograms x / y / z / radial bins; the morphology case stores a
-uint8 mask and the reference's morphology.dilate_3d_sphere / erode_3d_sphere results.  The tests then check the oracle bit-for-bit against
+uint8 mask and the reference's morphology.dilate_3d_sphere / erode_3d_sphere results;
+the implant case stores an implant mask, its frame of reference and the reference's
+geometry.compute_front_back_masks outputs.  The tests then check the oracle bit-for-bit against
 these files, and the CUDA library against the oracle.
 """
 from __future__ import annotations
@@ -157,6 +159,28 @@ def main():
     np.savez_compressed(os.path.join(HERE, "morphology_u8.npz"), mask=mmask, **results)
     index["morphology_u8"] = {"file": "morphology_u8.npz", "shape": list(mshape),
                               "counts": {k: int(v.sum()) for k, v in results.items()}}
+    geo = oracle.reference_module("geometry")
+    if geo is None:
+        sys.exit("reference geometry module not built: run `make -C oracle ref`")
+    # compute_front_back_masks (src/lib/cpp/cpu_seq/geometry.cc:112-215) on a tilted
+    # cylinder with stray voxels, a rotation E, a second rotation UVWp and an offset cp,
+    # as src/processing_steps/0750_bone_region.py:62 passes them (float64, cast by the binding).
+    ishape = (28, 40, 44)
+    irng = np.random.default_rng(17)
+    zz, yy, xx = np.meshgrid(*(np.arange(n) for n in ishape), indexing="ij")
+    implant = ((((yy - 21.0 - 0.2 * zz) ** 2 + (xx - 20.5) ** 2) < 64.0) & (zz > 2)).astype(np.uint8)
+    implant[irng.random(ishape) > 0.999] = 1
+    E = np.linalg.qr(irng.normal(size=(3, 3)))[0]
+    UVWp = np.linalg.qr(irng.normal(size=(3, 3)))[0]
+    cm = np.array(np.nonzero(implant)).mean(axis=1)
+    cp = irng.normal(size=3) * 4
+    voxel_size = 1.875
+    outs = [np.empty(ishape, np.uint8) for _ in range(4)]
+    geo.compute_front_back_masks(implant, voxel_size, E, cm, cp, UVWp, *outs)
+    np.savez_compressed(os.path.join(HERE, "implant_masks_u8.npz"), mask=implant, E=E, cm=cm, cp=cp, UVWp=UVWp,
+                        voxel_size=np.array(voxel_size), front=outs[0], back=outs[1], shell=outs[2], solid=outs[3])
+    index["implant_masks_u8"] = {"file": "implant_masks_u8.npz", "shape": list(ishape),
+                                 "counts": {k: int(v.sum()) for k, v in zip(("front", "back", "shell", "solid"), outs)}}
     with open(os.path.join(HERE, "index.json"), "w") as f:
         json.dump(index, f, indent=1, sort_keys=True)
 

@@ -196,3 +196,33 @@ def test_oracle_morphology_matches_reference_module(shape, r):
         want = np.zeros(shape, np.uint8)
         fn(m, r, want)
         np.testing.assert_array_equal(oracle.morphology_sphere(m, r, dilate), want)
+
+
+def test_oracle_implant_masks_match_reference_golden():
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "implant_masks_u8.npz"))
+    got = oracle.implant_masks(z["mask"], float(z["voxel_size"]), z["E"], z["cm"], z["cp"], z["UVWp"])
+    for g, name in zip(got, ("front", "back", "shell", "solid")):
+        np.testing.assert_array_equal(g, z[name], err_msg=name)
+
+
+@pytest.mark.parametrize("seed,shape", [(1, (24, 40, 48)), (2, (33, 31, 29)), (3, (16, 64, 64))])
+def test_oracle_implant_masks_match_reference_module(seed, shape):
+    geo = oracle.reference_module("geometry")
+    if geo is None:
+        pytest.skip("reference geometry module not built (make -C oracle ref)")
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    zz, yy, xx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    implant = ((((yy - ny / 2 - 2) ** 2 + (xx - nx / 2 + 1) ** 2) < (min(ny, nx) / 4) ** 2) & (zz > 3)).astype(np.uint8)
+    implant[rng.random(shape) > 0.999] = 1
+    implant[rng.random(shape) > 0.9995] = 3  # a byte other than 1: mask & and | act on its bits
+    E = np.linalg.qr(rng.normal(size=(3, 3)))[0]
+    UVWp = np.linalg.qr(rng.normal(size=(3, 3)))[0]
+    cm = np.array(np.nonzero(implant)).mean(axis=1)
+    cp = rng.normal(size=3) * 5
+    want = [np.empty(shape, np.uint8) for _ in range(4)]
+    geo.compute_front_back_masks(implant, 1.875, E, cm, cp, UVWp, *want)
+    for g, w in zip(oracle.implant_masks(implant, 1.875, E, cm, cp, UVWp), want):
+        np.testing.assert_array_equal(g, w)

@@ -110,22 +110,25 @@ __global__ void __launch_bounds__(256) morph_plane_discs(const uint32_t *__restr
             }
         }
         __syncthreads();
-        if (lane < tw && x0 + lane < t.nw) {
-            for (int ty = warp; ty < kTileRows; ty += blockDim.x >> 5) {
-                const int y = y0 + ty;
-                if (y >= t.ny) break;
-                uint32_t *dst = disc + z * plane + (int64_t) y * t.nw + x0 + lane;
-                const uint32_t *col = xr_s + (ty + r) * tw + lane;  // row y of X_0
-                for (int k = 0; k <= r; k++) {
-                    // rows y +- py of X_w with w = isqrt(r^2 - k^2 - py^2), py = 0 .. isqrt(r^2 - k^2)
-                    const uint8_t *wk = wtab + k * (2 * r + 1) + r;
-                    uint32_t acc = col[wk[0] * rows * tw];
-                    for (int py = 1; py <= r && wk[py] != 0xff; py++) {
-                        const uint32_t *c = col + wk[py] * rows * tw;
-                        acc = op<DILATE>(acc, op<DILATE>(c[py * tw], c[-py * tw]));
-                    }
-                    dst[(int64_t) k * words] = acc;
+        // Each warp writes rows `warp` and `warp + 8` of the tile (8 warps, 16 rows), the
+        // two dependency chains sharing the table lookups.
+        if (lane < tw && x0 + lane < t.nw && y0 + warp < t.ny) {
+            const bool second = y0 + warp + 8 < t.ny;
+            const int stride = rows * tw;
+            const uint32_t *c0 = xr_s + (warp + r) * tw + lane, *c1 = c0 + 8 * tw;  // row y of X_0
+            uint32_t *d0 = disc + z * plane + (int64_t) (y0 + warp) * t.nw + x0 + lane;
+            uint32_t *d1 = d0 + (int64_t) 8 * t.nw;
+            for (int k = 0; k <= r; k++) {
+                // rows y +- py of X_w with w = isqrt(r^2 - k^2 - py^2), py = 0 .. isqrt(r^2 - k^2)
+                const uint8_t *wk = wtab + k * (2 * r + 1) + r;
+                uint32_t a0 = c0[wk[0] * stride], a1 = c1[wk[0] * stride];
+                for (int py = 1; py <= r && wk[py] != 0xff; py++) {
+                    const int o = wk[py] * stride, d = py * tw;
+                    a0 = op<DILATE>(a0, op<DILATE>(c0[o + d], c0[o - d]));
+                    a1 = op<DILATE>(a1, op<DILATE>(c1[o + d], c1[o - d]));
                 }
+                d0[(int64_t) k * words] = a0;
+                if (second) d1[(int64_t) k * words] = a1;
             }
         }
     }
@@ -147,33 +150,57 @@ __global__ void morph_z(const uint32_t *__restrict__ disc, uint32_t *__restrict_
     }
 }
 
-// uint8 rows -> packed words (MSB first), padding bits neutral.  One thread per word.
-template <bool DILATE>
+// uint8 rows -> packed words (MSB first), padding bits neutral.  One thread per word;
+// VEC: rows are whole words (nx % 32 == 0) and 16-byte aligned, two 16-byte loads.
+template <bool DILATE, bool VEC>
 __global__ void morph_pack(const uint8_t *__restrict__ in, uint32_t *__restrict__ packed, int64_t words, int nx,
                            int nw) {
     for (int64_t idx = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; idx < words;
          idx += (int64_t) gridDim.x * blockDim.x) {
-        const int64_t row = idx / nw;
-        const int x0 = (int) (idx - row * nw) * 32;
-        const uint8_t *p = in + row * nx;
         uint32_t w = 0;
-        for (int b = 0; b < 32; b++) {
-            const int x = x0 + b;
-            const uint32_t bit = x < nx ? (DILATE ? (p[x] != 0) : (p[x] & 1)) : (DILATE ? 0u : 1u);
-            w |= bit << (31 - b);
+        if (VEC) {
+            const uint4 *p = reinterpret_cast<const uint4 *>(in + idx * 32);
+            const uint4 q0 = __ldcs(p), q1 = __ldcs(p + 1);
+            const uint32_t u[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+            for (int b = 0; b < 32; b++) {
+                const uint32_t byte = (u[b >> 2] >> (8 * (b & 3))) & 0xffu;
+                w |= (DILATE ? (uint32_t) (byte != 0) : (byte & 1u)) << (31 - b);
+            }
+        } else {
+            const int64_t row = idx / nw;
+            const int x0 = (int) (idx - row * nw) * 32;
+            const uint8_t *p = in + row * nx;
+            for (int b = 0; b < 32; b++) {
+                const int x = x0 + b;
+                const uint32_t bit = x < nx ? (DILATE ? (p[x] != 0) : (p[x] & 1)) : (DILATE ? 0u : 1u);
+                w |= bit << (31 - b);
+            }
         }
         packed[idx] = w;
     }
 }
 
-// Packed words -> uint8 0/1 voxels.  One thread per voxel.
-__global__ void morph_unpack(const uint32_t *__restrict__ packed, uint8_t *__restrict__ out, int64_t voxels, int nx,
+// Packed words -> uint8 0/1 voxels.  One thread per word; VEC as for morph_pack.
+template <bool VEC>
+__global__ void morph_unpack(const uint32_t *__restrict__ packed, uint8_t *__restrict__ out, int64_t words, int nx,
                              int nw) {
-    for (int64_t v = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; v < voxels;
-         v += (int64_t) gridDim.x * blockDim.x) {
-        const int64_t row = v / nx;
-        const int x = (int) (v - row * nx);
-        out[v] = (uint8_t) ((__ldg(packed + row * nw + (x >> 5)) >> (31 - (x & 31))) & 1u);
+    for (int64_t idx = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; idx < words;
+         idx += (int64_t) gridDim.x * blockDim.x) {
+        const uint32_t w = __ldg(packed + idx);
+        if (VEC) {
+            uint32_t u[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int b = 0; b < 32; b++) u[b >> 2] |= ((w >> (31 - b)) & 1u) << (8 * (b & 3));
+            uint4 *p = reinterpret_cast<uint4 *>(out + idx * 32);
+            __stcs(p, make_uint4(u[0], u[1], u[2], u[3]));
+            __stcs(p + 1, make_uint4(u[4], u[5], u[6], u[7]));
+        } else {
+            const int64_t row = idx / nw;
+            const int x0 = (int) (idx - row * nw) * 32;
+            uint8_t *p = out + row * nx;
+            for (int b = 0; b < 32 && x0 + b < nx; b++) p[x0 + b] = (uint8_t) ((w >> (31 - b)) & 1u);
+        }
     }
 }
 
@@ -328,19 +355,22 @@ extern "C" int maxi_morphology_sphere(const uint8_t *voxels, uint8_t *result, in
     uint32_t *packed = scratch, *packed_out = scratch + words, *pass = scratch + 2 * words;
     const int r = (int) radius;
     const unsigned g = grid_for(words);
+    const bool vec = nx % 32 == 0 && ((reinterpret_cast<uintptr_t>(voxels) | reinterpret_cast<uintptr_t>(result)) & 15) == 0;
     if (dilate) {
-        morph_pack<true><<<g, 256, 0, st>>>(voxels, packed, words, (int) nx, (int) nw);
+        if (vec) morph_pack<true, true><<<g, 256, 0, st>>>(voxels, packed, words, (int) nx, (int) nw);
+        else morph_pack<true, false><<<g, 256, 0, st>>>(voxels, packed, words, (int) nx, (int) nw);
         rc = morph_passes<true>(packed, packed_out, pass, nz, ny, nw, r, r, st);
     } else {
-        morph_pack<false><<<g, 256, 0, st>>>(voxels, packed, words, (int) nx, (int) nw);
+        if (vec) morph_pack<false, true><<<g, 256, 0, st>>>(voxels, packed, words, (int) nx, (int) nw);
+        else morph_pack<false, false><<<g, 256, 0, st>>>(voxels, packed, words, (int) nx, (int) nw);
         rc = morph_passes<false>(packed, packed_out, pass, nz, ny, nw, r, r, st);
     }
     if (rc) {
         cudaStreamSynchronize(st);
         return rc;
     }
-    const int64_t voxels_n = nz * ny * nx;
-    morph_unpack<<<grid_for(voxels_n), 256, 0, st>>>(packed_out, result, voxels_n, (int) nx, (int) nw);
+    if (vec) morph_unpack<true><<<g, 256, 0, st>>>(packed_out, result, words, (int) nx, (int) nw);
+    else morph_unpack<false><<<g, 256, 0, st>>>(packed_out, result, words, (int) nx, (int) nw);
     cudaError_t e = cudaGetLastError();
     cudaError_t e2 = cudaStreamSynchronize(st);  // the scratch is free for the next call
     if (e == cudaSuccess) e = e2;

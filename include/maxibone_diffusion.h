@@ -27,7 +27,7 @@ typedef enum maxi_status {
     MAXI_ERR_CUDA = 2,             /* a CUDA runtime call failed */
     MAXI_ERR_OUT_OF_MEMORY = 3,    /* device or pinned host allocation failed */
     MAXI_ERR_IO = 4,               /* file open / read / write failed (on-disk form) */
-    MAXI_ERR_UNSUPPORTED = 5,      /* a valid request this build does not serve */
+    MAXI_ERR_UNSUPPORTED = 5,      /* a valid request this library does not serve */
     MAXI_ERR_NO_DEVICE = 6         /* no CUDA device visible */
 } maxi_status;
 

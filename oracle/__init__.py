@@ -1,7 +1,7 @@
 """Test oracle for the mask-diffusion path (test infrastructure only).
 
 Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` may import this package, and only as the checker or the timed CPU
+``bench.py`` may import this package, and only to check results or as the timed CPU
 baseline.  The product (``maxibone_b200``) never imports it.
 
 The oracles:

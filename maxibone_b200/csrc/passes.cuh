@@ -162,7 +162,7 @@ template <int R> constexpr int contig_smem_bytes() { return kConTR * contig_stri
 // re-illuminated and rounded with error feedback along x in registers (the
 // carry restarts after every mask voxel, which is stored as exactly 1.0).
 template <int R, typename S, int MASK_FMT, bool FINAL, bool EF = false>
-__global__ void __launch_bounds__(kConThreads)
+__global__ void __launch_bounds__(kConThreads, (sizeof(S) == 4 && !FINAL && R <= 32) ? 5 : 1)
 contig_pass(const S *__restrict__ in, S *__restrict__ out, const void *__restrict__ mask,
             uint16_t *__restrict__ out_u16, float *__restrict__ field_out,
             int64_t rows, int64_t nx, int64_t n_x_tiles, const Taps<R> taps) {

@@ -80,6 +80,17 @@ def test_radius_coverage(radius):
     assert_parity(mask, kernel, 2, got_u16, got_field, want_u16, want_field)
 
 
+# z / y axes spanning several 256-output tiles with a partial last tile (520,
+# 530, 1030, 600) and x extents that leave a partial 32-column tile.
+@pytest.mark.parametrize("shape,sigma", [((520, 530, 40), 8.0), ((1030, 8, 24), 3.0), ((6, 600, 36), 1.0)])
+def test_long_axes(shape, sigma):
+    mask = spheres_mask(shape, 120, (3, 12), seed=sum(shape))
+    kernel = gauss_kernel(sigma).astype(np.float32)
+    want_u16, want_field = oracle.diffusion_in_memory(mask, kernel, 2)
+    got_u16, got_field = run_gpu(mask, kernel, 2)
+    assert_parity(mask, kernel, 2, got_u16, got_field, want_u16, want_field)
+
+
 @pytest.mark.parametrize("shape", [(1, 1, 1), (1, 1, 40), (1, 40, 1), (40, 1, 1), (2, 3, 5), (33, 17, 70),
                                    (130, 7, 9), (5, 129, 260), (3, 2, 513)])
 def test_edge_shapes(shape):

@@ -31,6 +31,31 @@ def test_library_exports_every_declared_symbol():
     assert set(names) <= set(_lib.SIGNATURES), "ctypes signatures missing for some declared symbols"
 
 
+def declared_parameter_counts():
+    """{function: number of parameters} from the prototypes in include/*.h."""
+    counts = {}
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        for m in re.finditer(r"\b(maxi_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text):
+            params = m.group(2).strip()
+            counts[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return counts
+
+
+def test_ctypes_signatures_match_the_header_prototypes():
+    counts = declared_parameter_counts()
+    assert len(counts) == len(declared_functions())
+    for name, n in counts.items():
+        restype, argtypes = _lib.SIGNATURES[name]
+        assert len(argtypes) == n, f"{name}: header has {n} parameters, ctypes binding {len(argtypes)}"
+        if name == "maxi_diffusion_workspace_size":
+            assert restype is ctypes.c_int64
+        elif name in ("maxi_last_error", "maxi_version"):
+            assert restype is ctypes.c_char_p
+        else:
+            assert restype is ctypes.c_int, name
+
+
 def test_version_string():
     assert b"sm_100a" in _lib.lib().maxi_version()
 

@@ -1,10 +1,10 @@
 #!/usr/bin/env python
 """Throughput benchmark of the mask-diffusion path on B200.
 
-Workload (default): a 1024^3 uint8 mask shaped like a bone sample with a metal
-implant (solid cylinder of radius 120 voxels along z through the centre plus
-seeded value-noise structures, ~25% foreground), a normalised Gaussian with
-sigma = 8 (radius 32, 65 taps, float32), R = 100 repetitions, FP32 field,
+Headline workload (`value`): a 1024^3 uint8 mask shaped like a bone sample with
+a metal implant (solid cylinder of radius 120 voxels along z through the centre
+plus seeded value-noise structures, ~25% foreground), a normalised Gaussian
+with sigma = 8 (radius 32, 65 taps, float32), R = 100 repetitions, FP32 field,
 uint16 output.  One step = one full diffusion call over the resident mask
 (mask -> field, 100 x (z, y, x, re-illuminate), quantise).
 
@@ -13,25 +13,29 @@ summed over ranks).  Each rank diffuses its own volume (independent units, no
 collective): scaling is weak.
 
 Also reported on the same line:
-  roofline      dominant kernel's algorithmic HBM bytes per launch / its average
-                CUDA-event duration, against the measured HBM copy bandwidth;
-  e2e           the same metric through the reference-facing host call
-                (numpy in / numpy out from pinned memory, host<->device copies and
-                device allocation inside the timed region);
-  precision     BF16 and FP16 field forms: throughput and max/mean abs error of
-                the final field against the FP64 form (and the FP32 form's);
+  roofline      the repetition's algorithmic HBM bytes, V R (2 s_field + s_mask)
+                (9 B per voxel-repetition for the FP32 field with a uint8 mask,
+                4.125 B for a 16-bit field with the bit-packed mask), over the
+                device time, against the measured HBM copy bandwidth; the
+                dominant kernel's own figure beside it;
+  e2e           the same metric through the reference-facing host call, numpy
+                in and out, from pinned and from pageable host buffers;
+  cfg0          the 128^3 sphere mask, sigma 3, R = 10, FP32, beside the
+                reference module on the same input;
+  precision     the 1024^3 mask bit-packed, BF16 and FP16 fields (fused y + x
+                tensor-core kernel, both coefficient forms, and the separate
+                passes), R = 100 and R = 500, max / mean abs error against the
+                FP64 form and the FP32 form; sigma = 32 (257 taps), CUDA-core
+                stencil vs banded-Toeplitz tensor cores;
+  batched       64 uneven volumes, sigma in {2, 4, 8}, R = 50, BF16 plan vs
+                per-volume FP32 launches, error of every volume vs FP64;
+  out_of_core   3456 x 3456 x 4096 (z, y, x) mask streamed from pinned host
+                memory, sigma 8, R = 20, BF16, end to end (PCIe included);
   cpu_baseline  the reference's OpenMP CPU module (oracle/_ref, built from the
                 reference sources) timed on this host on a bounded sample;
-  fields        the downstream steps on the workload's output: the Gaussian + EDT
-                field combination and the reference's field / axis histograms,
-                each beside the reference's own CPU form on a bounded sample
-                (`--downstream-only` runs just these and the morphology);
-  morphology    the sphere dilation that prepares masks (radius 16, uint8 and
-                bit-packed) on the workload's mask, beside the reference's CPU
-                module on a bounded sample;
-  implant_masks the implant solid / shell / front / back masks that feed the
-                diffusion, on the workload's mask, beside the reference's CPU
-                geometry module on a bounded sample.
+  fields, morphology, implant_masks   the steps either side of the path,
+                beside the reference's own CPU modules on bounded samples.
+Each section carries the SM clocks sampled while it ran.
 
 `--impl reference` times only the reference CPU module on the bounded sample.
 """
@@ -59,6 +63,24 @@ WORKLOADS = {
     "spheres128_s3_r10": ((128, 128, 128), 3.0, 10),
 }
 CPU_SAMPLE = ((512, 512, 512), 8.0, 1)  # bounded sample of the workload for the CPU arms
+SECTIONS = ("e2e", "cfg0", "precision", "long", "batched", "out_of_core", "downstream", "cpu")
+
+# DRAM bytes per voxel and repetition measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum over the launches of one repetition, divided by the
+# capture's voxels; captures larger than L2, traffic proportional to voxels):
+# the FP32 CUDA-core passes on a 512^3 capture, the BF16 tensor-core passes on
+# 256 x 1024 x 1024 (z, y and x passes as three kernels; the fused y + x kernel
+# with the z pass).
+NCU_BYTES_PER_VOXEL_REP = {
+    ("f32", "separate"): (8237891584 + 8247201792 + 8356808704) / 2 ** 30,
+    ("bf16", "separate"): (4136156160 + 4180311040 + 4272011263) / 2 ** 30,
+}
+
+
+def alg_bytes_per_voxel_rep(field: str, mask: str) -> float:
+    """Algorithmic HBM bytes per voxel and repetition: the field read and
+    written once, the mask read once (2 s_field + s_mask)."""
+    return 2 * FIELD_BYTES[field] + (1.0 if mask == "u8" else 0.125)
 
 
 def parse_args():
@@ -69,14 +91,16 @@ def parse_args():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload", choices=sorted(WORKLOADS), default="bone1024_s8_r100")
     p.add_argument("--field", choices=["f32", "bf16", "f16"], default="f32")
-    p.add_argument("--quick", action="store_true", help="skip e2e, precision forms and CPU baseline")
-    p.add_argument("--extended", action="store_true",
-                   help="also run the out-of-core workload, R=500 errors and the sigma=32 case")
+    p.add_argument("--quick", action="store_true", help="headline only: skip every section")
+    p.add_argument("--sections", type=str, default=",".join(SECTIONS),
+                   help="comma-separated sections to run after the headline (default: all): " + ",".join(SECTIONS))
     p.add_argument("--downstream-only", action="store_true",
-                   help="run one diffusion of the workload, then only the downstream steps (field combination and "
-                        "histograms) on its output, and print their JSON object")
+                   help="run one diffusion of the workload, then only the downstream steps (field combination, "
+                        "histograms, morphology, implant masks) on its output, and print their JSON object")
     p.add_argument("--shape", type=str, default=None,
                    help="override the workload's volume shape, e.g. 256x1024x1024 (profiling of smaller cases)")
+    p.add_argument("--ooc-shape", type=str, default="3456x3456x4096",
+                   help="out-of-core section's volume, z x y x x")
     return p.parse_args()
 
 
@@ -234,17 +258,22 @@ def batched_section(device, torch, np, stream, reps=50):
     device.tensor_core_status()
     t_bf16 = e0.elapsed_time(e1) / n_t
     peak, _ = load_peaks()
-    gbs = (6 * 2 + 0.125) * vox * reps / (t_bf16 / 1e3) / 1e9  # three passes of a 2-byte field + the 1-bit mask
+    gbs = alg_bytes_per_voxel_rep("bf16", "bitpacked") * vox * reps / (t_bf16 / 1e3) / 1e9
     res["bf16_batch"] = {"value": vox * reps / (t_bf16 / 1e3) / 1e9, "unit": UNIT, "ms": t_bf16,
-                         "hbm_gbs": gbs, "hbm_frac": gbs / peak}
-    # Accuracy of every fourth volume against the FP64 form.
-    errs = []
-    for i in range(0, 64, 4):
+                         "hbm_gbs": gbs, "hbm_frac": gbs / peak,
+                         "hbm_frac_definition": "V R (2 s_field + s_mask) / t / peak, 4.125 B per voxel-repetition"}
+    # Accuracy of every volume against the FP64 form.
+    errs, means = [], []
+    for i in range(64):
         want = torch.empty(specs[i][0], dtype=torch.float64, device="cuda")
         device.diffuse(masks[i], kernels[i], reps, field="f64", field_out=want)
-        errs.append(float((fouts[i].double() - want).abs().max().item()))
-        del want
-    res["bf16_batch"]["max_abs_err_vs_f64_sampled"] = max(errs)
+        d = (fouts[i].double() - want).abs_()
+        errs.append(float(d.max().item()))
+        means.append(float(d.mean().item()))
+        del want, d
+    res["bf16_batch"]["max_abs_err_vs_f64"] = max(errs)
+    res["bf16_batch"]["mean_abs_err_vs_f64"] = sum(means) / len(means)
+    res["bf16_batch"]["volumes_checked"] = len(errs)
     plan.close()
     # Per-volume FP32 launches (the plain form, one call per volume).
     ws = torch.empty(max(device.workspace_bytes(sh, "f32") for sh, _, _ in specs), dtype=torch.uint8, device="cuda")
@@ -568,96 +597,257 @@ def batched_plan_on_volume(device, torch, np, mask, kernel, reps, stream):
     plan.close()
     t = e0.elapsed_time(e1) / n_t
     peak, _ = load_peaks()
-    gbs = (6 * 2 + 0.125) * vox * reps / (t / 1e3) / 1e9
+    gbs = alg_bytes_per_voxel_rep("bf16", "bitpacked") * vox * reps / (t / 1e3) / 1e9
     del out
     return {"value": vox * reps / (t / 1e3) / 1e9, "unit": UNIT, "ms": t, "hbm_gbs": gbs, "hbm_frac": gbs / peak}
 
 
-def out_of_core_section(torch, np, reps=20, shape=(4096, 1728, 2048), slab=1024):
-    """Out-of-core z-slabs streamed from pinned host memory: sigma 8, R = 20, BF16
-    field, slabs of 1024 planes with 640-plane halos (repetition k computes the
-    planes at least 32k from a cut side).  The plane is a quarter of the
-    3456 x 4096 plane of the full-size case so host and device memory stay bounded."""
+def sampled(local_rank, fn):
+    """Runs fn() while nvidia-smi samples the clocks; returns (result, clocks)."""
+    sampler = ClockSampler(local_rank)
+    try:
+        res = fn()
+    finally:
+        clocks = sampler.stop()
+    return res, clocks
+
+
+def out_of_core_section(torch, np, shape, reps=20):
+    """cfg4: a bone-implant mask larger than the device in pinned host memory
+    (3456 x 3456 x 4096, z x y x x, 49 GB), sigma 8, R = 20, BF16 field, through
+    the out-of-core form end to end: one timed call from host mask to host
+    uint16 output, PCIe copies included.  The planner chooses slab depth and
+    plan from the free device memory.  If the host lacks the RAM for the pinned
+    mask and output, the z extent is reduced and the reason recorded."""
+    import ctypes
+
+    import psutil
+
+    from maxibone_b200 import _lib
     from maxibone_b200.diffusion import diffusion_out_of_core
     from maxibone_b200.kernels import gauss_kernel
     from maxibone_b200.synthetic import bone_implant_mask
 
+    nz, ny, nx = shape
+    avail = psutil.virtual_memory().available
+    note = None
+    need = 3 * nz * ny * nx  # uint8 mask + uint16 output
+    if need > 0.7 * avail:
+        nz_fit = max(64, int(0.7 * avail / (3 * ny * nx)) // 64 * 64)
+        note = (f"host RAM {avail / 1e9:.0f} GB available: z reduced from {nz} to {nz_fit} "
+                f"(the pinned mask and output need 3 bytes per voxel)")
+        nz = min(nz, nz_fit)
+    shape = (nz, ny, nx)
+    vox = nz * ny * nx
     kernel = gauss_kernel(8.0).astype(np.float32)
+    t0 = time.perf_counter()
     host_m = torch.empty(shape, dtype=torch.uint8, pin_memory=True)
-    for z0 in range(0, shape[0], 512):  # generate on the GPU in chunks
-        z1 = min(shape[0], z0 + 512)
-        host_m[z0:z1].copy_(bone_implant_mask((z1 - z0, shape[1], shape[2]), seed=z0, implant_radius=60.0,
-                                              device="cuda"))
     host_o = torch.empty(shape, dtype=torch.int16, pin_memory=True)
-    vox = int(np.prod(shape))
-    call = lambda: diffusion_out_of_core(host_m.numpy(), kernel, host_o.numpy().view(np.uint16),
-                                         (slab, shape[1], shape[2]), reps, field="bf16")
+    t_alloc = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    chunk = 128
+    for z0 in range(0, nz, chunk):  # generate on the GPU in chunks of planes
+        z1 = min(nz, z0 + chunk)
+        host_m[z0:z1].copy_(bone_implant_mask((z1 - z0, ny, nx), seed=z0, implant_radius=120.0 * ny / 1024,
+                                              device="cuda"))
     torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t0
+    s_, k_, r_ = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+    _lib.check(_lib.lib().maxi_out_of_core_plan(nz, ny, nx, 0, kernel.shape[0], reps, _lib.FIELD_TYPES["bf16"], 0, 0,
+                                                ctypes.byref(s_), ctypes.byref(k_), ctypes.byref(r_)))
+    m_np, o_np = host_m.numpy(), host_o.numpy().view(np.uint16)
     t0 = time.perf_counter()
-    call()  # warm-up: the first call in a process also pays one-time set-up (kernel loading, first touches)
-    first = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    call()
+    diffusion_out_of_core(m_np, kernel, o_np, (0, ny, nx), reps, field="bf16")
     dt = time.perf_counter() - t0
-    halo = reps * (kernel.shape[0] // 2)
-    res = {"workload": f"{shape[0]}x{shape[1]}x{shape[2]} bone-implant mask in pinned host memory, sigma 8, R={reps}, "
-                       f"BF16 field, slabs of {slab} planes + {halo}-plane halos", "voxels": vox,
-           "value": vox * reps / dt / 1e9, "unit": UNIT, "seconds": dt,
-           "h2d_bytes": None, "d2h_bytes": 2 * vox, "first_call_seconds": first,
-           "timing": "host clock around the second of two identical synchronous out-of-core calls "
-                     "(slab buffers, uploads, compute, downloads)"}
-    n_slabs = -(-shape[0] // slab)
+    S, k = s_.value, k_.value
     r = kernel.shape[0] // 2
-    ext = computed = 0
-    for s in range(n_slabs):
-        e0, e1 = max(0, s * slab - halo), min(shape[0], (s + 1) * slab + halo)
-        ext += e1 - e0
-        computed += sum(e1 - e0 - k * r * ((e0 > 0) + (e1 < shape[0])) for k in range(reps))
-    res["h2d_bytes"] = ext * shape[1] * shape[2]
-    res["redundancy"] = ext / shape[0]
-    res["compute_redundancy"] = computed / (shape[0] * reps)
+    n_slabs = -(-nz // S)
+    halo = min(nz, k * r)
+    computed = 0
+    for sl in range(n_slabs):
+        z0, z1 = sl * S, min(nz, (sl + 1) * S)
+        cuts = (z0 > 0) + (z1 < nz)
+        computed += (z1 - z0) * reps + cuts * r * k * (k + 1) // 2 * (-(-reps // k))
+    zs = np.linspace(0, nz - 1, 8).astype(int)
+    mask_exact = all(bool(np.all(o_np[z][m_np[z] > 0] == 65535)) for z in zs)
+    res = {"workload": f"{nz}x{ny}x{nx} (z x y x x) bone-implant mask in pinned host memory, sigma 8 (65 taps), "
+                       f"R={reps}, BF16 field, uint16 output to pinned host memory", "voxels": vox,
+           "value": vox * reps / dt / 1e9, "unit": UNIT, "seconds": dt,
+           "plan": {"slab_planes": S, "slabs": n_slabs, "reps_per_round": k, "halo_planes": halo,
+                    "resident_bitpacked_mask": bool(r_.value),
+                    "compute_redundancy": computed / (nz * reps)},
+           "h2d_bytes": vox, "d2h_bytes": 2 * vox,
+           "mask_voxels_exact_on_sampled_planes": mask_exact,
+           "timing": "host clock around one synchronous out-of-core call (mask upload, slabs, downloads)",
+           "setup_seconds": {"pinned_allocation": t_alloc, "mask_generation": t_gen}}
+    if note:
+        res["note"] = note
     del host_m, host_o
     return res
 
 
-def long_section(device, torch, np, mask, shape, stream):
-    """R = 500 error growth of the 16-bit forms, and the sigma = 32 (radius 128,
-    257 taps) case: CUDA-core FP32 and BF16 passes against the BF16 / FP16
-    banded-Toeplitz tensor-core passes, each with its error against FP64."""
-    from maxibone_b200.kernels import gauss_kernel
-
-    vox = int(np.prod(shape))
-
-    def timed(kernel, reps, form, fo, **opts):
-        device.diffuse(mask, kernel, 1, field=form, field_out=fo, **opts)  # warm-up
+def form_runs(device, torch, np, mask, kernel, reps, forms, stream, shape=None, n_t=2, packed=False):
+    """Runs each (name, field, opts) form: a timed run (CUDA events, n_t calls,
+    uint16 output only) and one run writing the field for the errors against
+    the FP64 form (and the FP32 form where run).  mask: uint8 tensor, or
+    bit-packed words with `shape`."""
+    peak, _ = load_peaks()
+    vox = int(np.prod(shape if shape is not None else tuple(mask.shape)))
+    shp = shape if shape is not None else tuple(mask.shape)
+    f64 = torch.empty(shp, dtype=torch.float64, device="cuda")
+    device.diffuse(mask, kernel, reps, field="f64", field_out=f64, shape=shape)
+    out = torch.empty(shp, dtype=torch.uint16, device="cuda")
+    res, f32_field = {}, None
+    for name, form, opts in forms:
+        fo = torch.empty(shp, dtype=torch.float32, device="cuda")
+        w = torch.empty(device.workspace_bytes(shp, form), dtype=torch.uint8, device="cuda")
+        device.diffuse(mask, kernel, reps, output=out, field=form, field_out=fo, workspace=w, shape=shape, **opts)
+        path = device.last_path()
         torch.cuda.synchronize()
+        device.profile_enable(True)
+        device.profile_read()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        device.diffuse(mask, kernel, reps, field=form, field_out=fo, **opts)
+        for _ in range(n_t):
+            device.diffuse(mask, kernel, reps, output=out, field=form, workspace=w, shape=shape, **opts)
         e1.record(stream)
         torch.cuda.synchronize()
+        prof = device.profile_read()
+        device.profile_enable(False)
         device.tensor_core_status()
-        return vox * reps / (e0.elapsed_time(e1) / 1e3) / 1e9
-
-    res = {}
-    for sigma, reps, forms in ((8.0, 500, (("bf16", {}), ("f16", {}))),
-                               (32.0, 10, (("f32", {}), ("bf16", {}), ("f16", {}),
-                                           ("bf16", {"tensor_cores": False})))):
-        kernel = gauss_kernel(sigma).astype(np.float32)
-        f64 = torch.empty(shape, dtype=torch.float64, device="cuda")
-        device.diffuse(mask, kernel, reps, field="f64", field_out=f64)
-        for form, opts in forms:
-            fo = torch.empty(shape, dtype=torch.float32, device="cuda")
-            value = timed(kernel, reps, form, fo, **opts)
-            err = (fo.double() - f64).abs_()
-            name = (f"sigma{int(sigma)}_r{reps}_{form}" + ("_cuda_cores" if opts else "")
-                    + ("_tensor_cores" if form != "f32" and not opts else ""))
-            res[name] = {"value": value, "unit": UNIT, "reps": reps, "kernel_size": int(kernel.shape[0]),
-                         "max_abs_err_vs_f64": float(err.max().item()),
-                         "mean_abs_err_vs_f64": float(err.mean().item())}
-            del fo, err
-        del f64
+        t_ms = e0.elapsed_time(e1) / n_t
+        err = (fo.double() - f64).abs_()
+        b_alg = alg_bytes_per_voxel_rep(form, "bitpacked" if packed else "u8")
+        gbs = b_alg * vox * reps / (t_ms / 1e3) / 1e9
+        entry = {"value": vox * reps / (t_ms / 1e3) / 1e9, "unit": UNIT, "field": form, **opts,
+                 "ms_per_call": t_ms, "hbm_gbs": gbs, "hbm_frac": gbs / peak, "alg_bytes_per_voxel_rep": b_alg,
+                 "max_abs_err_vs_f64": float(err.max().item()), "mean_abs_err_vs_f64": float(err.mean().item()),
+                 "mask_voxels_exact": bool((out.view(torch.int16)[mask > 0] == -1).all().item())
+                 if shape is None else None,
+                 "path_bits": path, "per_kind_ms": {k: v[0] / v[1] for k, v in prof.items()},
+                 "launches_per_call": sum(v[1] for v in prof.values()) // n_t}
+        if form == "f32" and not opts:
+            f32_field = fo
+        elif f32_field is not None:
+            entry["max_abs_err_vs_f32"] = float((fo - f32_field).abs_().max().item())
+        res[name] = entry
+        del err, w
+        if fo is not f32_field:
+            del fo
         torch.cuda.empty_cache()
+    del f64, out, f32_field
+    torch.cuda.empty_cache()
+    return res
+
+
+PRECISION_FORMS = [
+    ("f32", "f32", {}),
+    ("bf16", "bf16", {}),
+    ("bf16_single_coefficients", "bf16", {"single_coefficients": True}),
+    ("bf16_separate_passes", "bf16", {"fuse_passes": False}),
+    ("f16", "f16", {}),
+    ("f16_single_coefficients", "f16", {"single_coefficients": True}),
+    ("bf16_nearest", "bf16", {"error_feedback": False}),
+    ("bf16_cuda_cores", "bf16", {"tensor_cores": False}),
+]
+
+
+def precision_section(device, torch, np, mask, kernel, reps, stream):
+    """cfg2 at R = 100: the workload's mask bit-packed (1 bit per voxel), the
+    FP32 field and the 16-bit field forms, each with its error against the FP64
+    form and the FP32 form."""
+    shape = tuple(mask.shape)
+    packed = device.bitpack(mask)
+    res = form_runs(device, torch, np, packed, kernel, reps, PRECISION_FORMS, stream, shape=shape, packed=True)
+    for name in res:  # mask exactness on the uint8 view of the same runs
+        res[name].pop("mask_voxels_exact", None)
+    out = torch.empty(shape, dtype=torch.uint16, device="cuda")
+    for form in ("bf16", "f16"):
+        device.diffuse(packed, kernel, reps, output=out, field=form, shape=shape)
+        res[form]["mask_voxels_exact"] = bool((out.view(torch.int16)[mask > 0] == -1).all().item())
+    del packed, out
+    return res
+
+
+def long_section(device, torch, np, mask, kernel, stream):
+    """cfg2's R = 500 runs (BF16 and FP16, both coefficient forms) and the
+    sigma = 32 (radius 128, 257 taps) case at R = 20: the FP32 CUDA-core
+    stencil and the BF16 CUDA-core passes against the BF16 / FP16 banded-Toeplitz
+    tensor-core passes, each against the FP64 form."""
+    from maxibone_b200.kernels import gauss_kernel
+
+    shape = tuple(mask.shape)
+    packed = device.bitpack(mask)
+    res = {"r500": form_runs(device, torch, np, packed, kernel, 500,
+                             [("bf16", "bf16", {}), ("bf16_single_coefficients", "bf16", {"single_coefficients": True}),
+                              ("f16", "f16", {})], stream, shape=shape, n_t=1, packed=True)}
+    k32 = gauss_kernel(32.0).astype(np.float32)
+    res["sigma32_r20"] = form_runs(device, torch, np, packed, k32, 20,
+                                   [("f32_cuda_cores", "f32", {}), ("bf16_tensor_cores", "bf16", {}),
+                                    ("f16_tensor_cores", "f16", {}),
+                                    ("bf16_cuda_cores", "bf16", {"tensor_cores": False})],
+                                   stream, shape=shape, n_t=1, packed=True)
+    for part in res.values():
+        for entry in part.values():
+            entry.pop("mask_voxels_exact", None)
+    res["sigma32_r20"]["kernel_size"] = int(k32.shape[0])
+    del packed
+    return res
+
+
+def cfg0_section(device, torch, np, stream):
+    """cfg0: the 128^3 union of 40 spheres, sigma 3 (25 taps), R = 10, FP32
+    field: device rate, the reference-facing host call, and the reference
+    module on the same input (full run, median of 3) with the uint16 outputs
+    compared."""
+    import oracle
+    from maxibone_b200.diffusion import diffusion
+    from maxibone_b200.kernels import gauss_kernel
+    from maxibone_b200.synthetic import spheres_mask
+
+    shape, reps = (128, 128, 128), 10
+    mask_np = spheres_mask(shape, 40, (4, 20), seed=0)
+    kernel = gauss_kernel(3.0).astype(np.float32)
+    vox = int(np.prod(shape))
+    m = torch.from_numpy(mask_np).cuda()
+    out = torch.empty(shape, dtype=torch.uint16, device="cuda")
+    ws = torch.empty(device.workspace_bytes(shape, "f32"), dtype=torch.uint8, device="cuda")
+    for _ in range(3):
+        device.diffuse(m, kernel, reps, output=out, workspace=ws)
+    torch.cuda.synchronize()
+    n_t = 20
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(n_t):
+        device.diffuse(m, kernel, reps, output=out, workspace=ws)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_ms = e0.elapsed_time(e1) / n_t
+    host_out = np.empty(shape, np.uint16)
+    diffusion(mask_np, kernel, host_out, reps)
+    tw = time.perf_counter()
+    for _ in range(5):
+        diffusion(mask_np, kernel, host_out, reps)
+    e2e_s = (time.perf_counter() - tw) / 5
+    res = {"workload": "128^3 union of 40 spheres (radii 4-20, seed 0), sigma 3 (25 taps), R=10, FP32 field",
+           "foreground": float(mask_np.mean()), "value": vox * reps / (t_ms / 1e3) / 1e9, "unit": UNIT,
+           "ms_per_call": t_ms,
+           "e2e": {"value": vox * reps / e2e_s / 1e9, "unit": UNIT, "ms_per_call": e2e_s * 1e3,
+                   "timing": "host clock around 5 synchronous drop-in diffusion() calls (numpy in / out)"}}
+    ref = oracle.reference_module("diffusion")
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    if ref is not None:
+        want = np.empty(shape, np.uint16)
+        times = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            ref.diffusion(mask_np, kernel, want, reps)
+            times.append(time.perf_counter() - t0)
+        d = np.abs(host_out.astype(np.int32) - want.astype(np.int32))
+        res["cpu_baseline"] = {"value": vox * reps / statistics.median(times) / 1e9, "unit": UNIT, "cores": cores,
+                               "kind": "reference", "sample": "the whole cfg0 call, median of 3"}
+        res["vs_reference_u16"] = {"max_lsb": int(d.max()), "voxels_differing": int((d > 0).sum())}
+    del m, out, ws
     return res
 
 
@@ -675,7 +865,7 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from maxibone_b200 import device
+    from maxibone_b200 import _lib, device
     from maxibone_b200.diffusion import diffusion
     from maxibone_b200.kernels import gauss_kernel
     from maxibone_b200.synthetic import bone_implant_mask, spheres_mask
@@ -720,6 +910,7 @@ def main():
 
     for _ in range(args.warmup):
         step()
+    path = device.last_path()
     torch.cuda.synchronize()
     barrier()
     device.profile_enable(True)
@@ -736,38 +927,47 @@ def main():
     prof = device.profile_read()
     device.profile_enable(False)
     barrier()
-    ms = max_over_ranks(t0.elapsed_time(t1), world, "cuda")
+    ms_local = t0.elapsed_time(t1)
+    ms = max_over_ranks(ms_local, world, "cuda")
     value = whole_job_rate(world, vox, reps, args.steps, ms / 1e3)
     launches = sum(c for _, c in prof.values())
 
-    # Roofline of the dominant kernel: algorithmic bytes per launch / event duration.
+    # Roofline: the repetition's algorithmic bytes V (2 s_field + s_mask) over its
+    # device time (this GPU's volume and time), against the measured HBM bandwidth.
     peak, peak_kind = load_peaks()
     s = FIELD_BYTES[args.field]
-    alg_bytes = {"z": 2 * s * vox, "y": 2 * s * vox, "x": (2 * s + 1) * vox, "x_final": (s + 1 + 2) * vox,
-                 "yx": (2 * s + 1) * vox, "init": (1 + s) * vox}
+    b_alg = alg_bytes_per_voxel_rep(args.field, "u8")
+    rep_ms = ms_local / (args.steps * reps)
+    achieved = b_alg * vox / (rep_ms / 1e3) / 1e9
+    fused = bool(path & _lib.PATH_FUSED_YX)
+    per_voxel_traffic = NCU_BYTES_PER_VOXEL_REP.get((args.field, "fused" if fused else "separate"))
+    kernel_bytes = {"z": 2 * s, "y": 2 * s, "x": 2 * s + 0.125, "x_final": s + 0.125 + 2, "yx": 2 * s + 0.125,
+                    "init": 0.125 + s}
+    per_kernel = {}
+    for kind, (k_ms, k_n) in prof.items():
+        if kind in kernel_bytes:
+            gbs = kernel_bytes[kind] * vox / (k_ms / k_n / 1e3) / 1e9
+            per_kernel[kind] = {"launches": k_n, "ms_per_launch": k_ms / k_n, "alg_bytes_per_launch":
+                                kernel_bytes[kind] * vox, "gbs": gbs, "frac": gbs / peak}
     dom = max(prof, key=lambda k: prof[k][0])
-    dom_ms = prof[dom][0] / prof[dom][1]
-    achieved = alg_bytes.get(dom, 0) / (dom_ms / 1e3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as f:
-            traffic = json.load(f).get(args.workload, {}).get(args.field, {}).get(dom)
-    # Whole step: three passes read and write the field once each, the x pass reads the 1-bit mask.
-    rep_bytes = (6 * s + 0.125) * vox
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": dom, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "alg_bytes_per_launch": alg_bytes.get(dom), "ms_per_launch": dom_ms,
-                "per_kind_ms": {k: v[0] / v[1] for k, v in prof.items()},
-                "whole_step_gbs": rep_bytes * reps * args.steps / (ms / 1e3) / 1e9,
-                "whole_step_frac": rep_bytes * reps * args.steps / (ms / 1e3) / 1e9 / peak}
+                "traffic": per_voxel_traffic * vox if per_voxel_traffic else None,
+                "unit_of_work": f"one repetition (z, y and x passes with re-illumination) over {nz}x{ny}x{nx}",
+                "alg_bytes_per_voxel_rep": b_alg,
+                "alg_bytes_definition": "2 s_field + s_mask: the field read and written once, the uint8 mask read "
+                                        "once, per voxel and repetition",
+                "ms_per_repetition": rep_ms, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic_definition": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one repetition's "
+                                      "launches, scaled from a capture larger than L2 by voxel count",
+                "dominant_kernel": {"kind": dom, **per_kernel.get(dom, {})}, "per_kernel": per_kernel}
     if args.field == "f32":
-        roofline["fp32_tflops_dominant"] = 2 * (2 * radius + 1) * vox / (dom_ms / 1e3) / 1e12
-        roofline["fp32_tflops_whole_step"] = 2 * 3 * (2 * radius + 1) * vox * reps * args.steps / (ms / 1e3) / 1e12
-        roofline["note"] = ("the direct FP32 stencil at radius 32 is bound by the FP32 pipe (2*65 flop per 8 B "
-                            "of field traffic); fp32_peak_tflops = 148 SMs x 128 FMA/clk x 2 x median SM clock")
-        if clocks:
-            roofline["fp32_peak_tflops"] = 148 * 128 * 2 * clocks["sm_mhz"] * 1e6 / 1e12
+        flop = 2 * 3 * (2 * radius + 1) * vox
+        roofline["fp32_pipe"] = {
+            "achieved_tflops": flop / (rep_ms / 1e3) / 1e12,
+            "peak_tflops_computed": 148 * 128 * 2 * clocks["sm_mhz"] * 1e6 / 1e12 if clocks else None,
+            "peak_source": "computed, not measured: 148 SMs x 128 FP32 lanes x 2 flop x the median SM clock",
+            "note": "the direct FP32 stencil at radius 32 is bound by the FP32 pipe: 2 x 65 flop per 8 B of "
+                    "field traffic per pass"}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -776,119 +976,105 @@ def main():
                    "shape": list(shape), "sigma": sigma, "kernel_size": int(2 * radius + 1),
                    "reps": reps, "field": args.field, "mask": "u8", "foreground": round(fg, 4),
                    "parallelism": f"{world} independent volumes (one per rank)",
-                   "l2": "inputs larger than L2 (field %d MiB per buffer)" % (s * vox >> 20)},
+                   "l2": "inputs larger than L2 (field %d MiB per buffer)" % (s * vox >> 20),
+                   "path_bits": path},
         "gpu_launches": launches, "roofline": roofline, "clocks": clocks,
     }
+    sections = [] if args.quick else [x for x in args.sections.split(",") if x]
 
-    if not args.quick:
-        # End to end through the reference-facing call: numpy in, numpy out, pinned host memory.
+    if "e2e" in sections:
+        # End to end through the reference-facing call: numpy in, numpy out, from
+        # pinned host memory and from pageable host memory (maxibone's callers
+        # pass np.empty arrays).
         host_mask = torch.empty(shape, dtype=torch.uint8, pin_memory=True)
         host_mask.copy_(mask)
         host_out = torch.empty(shape, dtype=torch.int16, pin_memory=True)
         m_np, o_np = host_mask.numpy(), host_out.numpy().view(np.uint16)
         del ws
         torch.cuda.empty_cache()
-        diffusion(m_np, kernel, o_np, reps)  # warm-up
-        e2e_steps = max(1, min(args.steps, 2))
-        barrier()
-        tw = time.perf_counter()
-        for _ in range(e2e_steps):
-            diffusion(m_np, kernel, o_np, reps)
-        e2e_s = max_over_ranks(time.perf_counter() - tw, world, "cuda")
-        line["e2e"] = {"value": whole_job_rate(world, vox, reps, e2e_steps, e2e_s), "unit": UNIT,
-                       "h2d_bytes_per_step": vox, "d2h_bytes_per_step": 2 * vox, "steps": e2e_steps,
-                       "timing": "host clock around the synchronous drop-in diffusion() call (max over ranks)"}
+        e2e = {}
+        for kind, (mi, oi) in (("pinned", (m_np, o_np)),
+                               ("pageable", (np.array(m_np), np.empty(shape, np.uint16)))):
+            diffusion(mi, kernel, oi, reps)  # warm-up
+            n_e2e = max(1, min(args.steps, 2))
+            barrier()
+            tw = time.perf_counter()
+            for _ in range(n_e2e):
+                diffusion(mi, kernel, oi, reps)
+            e2e_s = max_over_ranks(time.perf_counter() - tw, world, "cuda")
+            e2e[kind] = {"value": whole_job_rate(world, vox, reps, n_e2e, e2e_s), "steps": n_e2e,
+                         "ms_per_call": e2e_s / n_e2e * 1e3}
+        line["e2e"] = {"value": e2e["pinned"]["value"], "unit": UNIT, "h2d_bytes_per_step": vox,
+                       "d2h_bytes_per_step": 2 * vox, "steps": e2e["pinned"]["steps"],
+                       "pageable": e2e["pageable"],
+                       "timing": "host clock around the synchronous drop-in diffusion() call (max over ranks); the "
+                                 "call allocates and frees its device buffers, as the reference does"}
         del host_mask, host_out
+        ws = None
+    else:
+        del ws
+        torch.cuda.empty_cache()
 
-        # Precision forms vs the FP64 form.
-        f64 = torch.empty(shape, dtype=torch.float64, device="cuda")
-        device.diffuse(mask, kernel, reps, field="f64", field_out=f64)
-        forms = {}
-        f32_field = None
-        variants = [("f32", "f32", {}), ("bf16", "bf16", {}), ("f16", "f16", {}),
-                    ("bf16_nearest", "bf16", {"error_feedback": False}),
-                    ("bf16_cuda_cores", "bf16", {"tensor_cores": False}),
-                    ("f16_cuda_cores", "f16", {"tensor_cores": False})]
-        for name, form, opts in variants:
-            fo = torch.empty(shape, dtype=torch.float32, device="cuda")
-            w = torch.empty(device.workspace_bytes(shape, form), dtype=torch.uint8, device="cuda")
-            device.diffuse(mask, kernel, reps, output=out, field=form, field_out=fo, workspace=w, **opts)
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            n_t = 2
-            device.profile_enable(True)
-            device.profile_read()
-            e0.record(stream)
-            for _ in range(n_t):
-                device.diffuse(mask, kernel, reps, output=out, field=form, workspace=w, **opts)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            fprof = device.profile_read()
-            device.profile_enable(False)
-            device.tensor_core_status()
-            t_ms = e0.elapsed_time(e1)
-            err = (fo.double() - f64).abs_()
-            fb = FIELD_BYTES[form]
-            f_bytes = {"z": 2 * fb * vox, "y": 2 * fb * vox, "x": (2 * fb + 0.125) * vox}
-            fdom = max(("z", "y", "x"), key=lambda k: fprof.get(k, (0, 1))[0])
-            fms = fprof[fdom][0] / fprof[fdom][1]
-            f_traffic = None
-            if os.path.exists(tpath):
-                with open(tpath) as f:
-                    f_traffic = json.load(f).get(args.workload, {}).get(form, {}).get(fdom)
-            froof = {"bound": "hbm", "kernel": fdom, "achieved": f_bytes[fdom] / (fms / 1e3) / 1e9, "peak": peak,
-                     "unit": "GB/s", "frac": f_bytes[fdom] / (fms / 1e3) / 1e9 / peak, "traffic": f_traffic,
-                     "whole_rep_frac": (6 * fb + 0.125) * vox * reps * n_t / (t_ms / 1e3) / 1e9 / peak}
-            forms[name] = {"value": vox * reps * n_t / (t_ms / 1e3) / 1e9, "unit": UNIT, "field": form, **opts,
-                           "roofline": froof,
-                           "max_abs_err_vs_f64": float(err.max().item()),
-                           "mean_abs_err_vs_f64": float(err.mean().item()),
-                           "mask_voxels_exact": bool((out.view(torch.int16)[mask > 0] == -1).all().item()),
-                           "per_kind_ms": {k: v[0] / v[1] for k, v in fprof.items()}}
-            if name == "f32":
-                f32_field = fo
-            else:
-                forms[name]["_vs_f32"] = float((fo - f32_field).abs_().max().item())
-            del err, fo, w
-            torch.cuda.empty_cache()
-        del f32_field
-        line["precision"] = forms
-        for name in forms:
-            if name != "f32":
-                forms[name]["max_abs_err_vs_f32"] = forms[name].pop("_vs_f32", None)
-        # The BF16 form against the plain FP32 form on this workload.
-        line["bf16_vs_f32"] = {"speedup": forms["bf16"]["value"] / forms["f32"]["value"],
-                               "bf16_whole_rep_hbm_frac": forms["bf16"]["roofline"]["whole_rep_frac"],
-                               "bf16_max_abs_err_vs_f64": forms["bf16"]["max_abs_err_vs_f64"]}
-        del f64
-
-        line["fields"] = {"combine_fields": fields_section(torch, np, out, stream),
-                          **histogram_section(torch, np, mask, out, stream)}
+    if "precision" in sections:
+        res, ck = sampled(local_rank, lambda: precision_section(device, torch, np, mask, kernel, reps, stream))
+        res["clocks"] = ck
+        res["workload"] = (f"{nz}x{ny}x{nx} bone-implant mask bit-packed (1 bit per voxel), sigma {sigma}, R={reps}; "
+                           "hbm_frac = V R (2 s_field + 1/8) / t / peak")
+        line["precision"] = res
+        line["bf16_vs_f32"] = {"speedup": res["bf16"]["value"] / res["f32"]["value"],
+                               "bf16_hbm_frac": res["bf16"]["hbm_frac"],
+                               "bf16_max_abs_err_vs_f64": res["bf16"]["max_abs_err_vs_f64"],
+                               "bf16_single_coefficients_speedup": res["bf16_single_coefficients"]["value"] /
+                               res["f32"]["value"],
+                               "bf16_single_coefficients_hbm_frac": res["bf16_single_coefficients"]["hbm_frac"]}
+    if "long" in sections:
+        res, ck = sampled(local_rank, lambda: long_section(device, torch, np, mask, kernel, stream))
+        res["clocks"] = ck
+        line["long"] = res
+    if "cfg0" in sections:
+        res, ck = sampled(local_rank, lambda: cfg0_section(device, torch, np, stream))
+        res["clocks"] = ck
+        line["cfg0"] = res
+    if "downstream" in sections:
+        out_u16 = torch.empty(shape, dtype=torch.uint16, device="cuda")
+        device.diffuse(mask, kernel, reps, output=out_u16)
+        line["fields"] = {"combine_fields": fields_section(torch, np, out_u16, stream),
+                          **histogram_section(torch, np, mask, out_u16, stream)}
         line["morphology"] = morphology_section(torch, np, mask, stream)
         line["implant_masks"] = implant_section(torch, np, mask, stream)
-        line["batched"] = batched_section(device, torch, np, stream)
-        line["batched"]["bf16_plan_on_workload_volume"] = bv = batched_plan_on_volume(
-            device, torch, np, mask, kernel, reps, stream)
-        bv["speedup_vs_f32"] = bv["value"] / forms["f32"]["value"]
+        del out_u16
+    if "batched" in sections:
+        res, ck = sampled(local_rank, lambda: batched_section(device, torch, np, stream))
+        res["clocks"] = ck
+        line["batched"] = res
+        res["bf16_plan_on_workload_volume"] = bv = batched_plan_on_volume(device, torch, np, mask, kernel, reps,
+                                                                          stream)
+        if "precision" in line:
+            bv["speedup_vs_f32"] = bv["value"] / line["precision"]["f32"]["value"]
+    torch.cuda.empty_cache()
+    if "out_of_core" in sections and world == 1:
+        ooc_shape = tuple(int(v) for v in args.ooc_shape.lower().split("x"))
+        del mask
+        torch.cuda.empty_cache()
+        res, ck = sampled(local_rank, lambda: out_of_core_section(torch, np, ooc_shape))
+        res["clocks"] = ck
+        line["out_of_core"] = res
+        mask = None
 
-        if args.extended:
-            line["out_of_core"] = out_of_core_section(torch, np)
-            line["long"] = long_section(device, torch, np, mask, shape, stream)
-
-        if rank == 0 and world == 1:
-            cshape, csig, creps = CPU_SAMPLE
-            times, kind, cores, cvox, (cmask, ckernel, cref) = cpu_reference_time(cshape, csig, creps, 2)
-            line["cpu_baseline"] = {"value": cvox * creps / min(times) / 1e9, "unit": UNIT, "cores": cores,
-                                    "kind": kind,
-                                    "sample": f"bone-implant mask {cshape[0]}^3, sigma={csig} (65 taps), R={creps}, "
-                                              f"best of 2 calls"}
-            if cref is not None:
-                # The FP32 path against the reference module's own uint16 output on the sample.
-                gout = torch.empty(cshape, dtype=torch.uint16, device="cuda")
-                device.diffuse(torch.from_numpy(cmask).cuda(), ckernel, creps, output=gout, field="f32")
-                d = np.abs(gout.cpu().numpy().astype(np.int32) - cref.astype(np.int32))
-                line["cpu_baseline"]["f32_vs_reference_u16"] = {"max_lsb": int(d.max()),
-                                                                "voxels_differing": int((d > 0).sum())}
+    if "cpu" in sections and rank == 0 and world == 1:
+        cshape, csig, creps = CPU_SAMPLE
+        times, kind, cores, cvox, (cmask, ckernel, cref) = cpu_reference_time(cshape, csig, creps, 2)
+        line["cpu_baseline"] = {"value": cvox * creps / min(times) / 1e9, "unit": UNIT, "cores": cores,
+                                "kind": kind,
+                                "sample": f"bone-implant mask {cshape[0]}^3, sigma={csig} (65 taps), R={creps}, "
+                                          f"best of 2 calls"}
+        if cref is not None:
+            # The FP32 path against the reference module's own uint16 output on the sample.
+            gout = torch.empty(cshape, dtype=torch.uint16, device="cuda")
+            device.diffuse(torch.from_numpy(cmask).cuda(), ckernel, creps, output=gout, field="f32")
+            d = np.abs(gout.cpu().numpy().astype(np.int32) - cref.astype(np.int32))
+            line["cpu_baseline"]["f32_vs_reference_u16"] = {"max_lsb": int(d.max()),
+                                                            "voxels_differing": int((d > 0).sum())}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -62,9 +62,33 @@ typedef enum maxi_mask_format {
                                             error-feedback rounding along x (the default for
                                             radius >= 4, which keeps the stored rounding noise
                                             out of the result) */
+#define MAXI_FLAG_SEPARATE_PASSES 0x20   /* BF16/FP16 tensor cores: run the y and x passes as two
+                                            kernels (two HBM round trips) instead of the fused
+                                            y + x kernel used for radius <= 32 */
+#define MAXI_FLAG_SINGLE_COEFFICIENTS 0x40 /* BF16/FP16 fused y + x kernel: one 16-bit coefficient
+                                            set, rounded so that the kernel's sum and second
+                                            moment are kept, instead of high + low halves (half
+                                            the tensor-core work; adds ~2e-4 to the error) */
 
 const char *maxi_last_error(void);
 const char *maxi_version(void);
+
+/* Kernel families a diffusion call enqueued (bits of maxi_last_path()). */
+#define MAXI_PATH_CUDA_CORES 0x1         /* unrolled CUDA-core passes (any of z, y, x) */
+#define MAXI_PATH_TENSOR_CORES_ZY 0x2    /* tcgen05 z and y passes */
+#define MAXI_PATH_TENSOR_CORES_X 0x4     /* tcgen05 x pass + re-illumination */
+#define MAXI_PATH_FUSED_YX 0x8           /* tcgen05 y and x passes fused in one kernel */
+#define MAXI_PATH_GENERIC 0x10           /* generic passes: FP64, reference rounding, radius > 128 */
+#define MAXI_PATH_FP32_FALLBACK 0x20     /* a 16-bit field was requested on a shape the tensor-core
+                                            passes do not take; the FP32 form ran instead */
+
+/*
+ * MAXI_PATH_* bits of the last maxi_diffusion_device() call made by this
+ * thread (no reference counterpart: the reference has one code path per
+ * build).  Lets callers and tests see which kernels served a request, e.g.
+ * that a BF16 request ran on the tensor cores and not on a fallback.
+ */
+int maxi_last_path(void);
 
 /*
  * Status of the tensor-core passes since the last call: their waits are
@@ -109,12 +133,17 @@ int maxi_diffusion_in_memory(const uint8_t *voxels, int64_t nz, int64_t ny, int6
                              uint16_t *output, int verbose);
 
 /*
- * maxi_diffusion_in_memory() keeps its device buffers between calls (one
- * grow-only allocation per device) so repeated calls do not map gigabytes each
- * time; volumes larger than the device go to the out-of-core form, as the
- * reference's pybind module does (src/pybind/diffusion-pybind.cc:40-45).
- * maxi_release_cached_memory() frees those buffers.
+ * maxi_diffusion_in_memory() allocates its device buffers per call and frees
+ * them before it returns, as the reference does (src/lib/cpp/cpu/diffusion.cc:
+ * 343-345,371-373).  maxi_keep_device_buffers(1) makes it keep them between
+ * calls instead (one grow-only allocation per device), so repeated calls do
+ * not map gigabytes each time; maxi_keep_device_buffers(0) restores the
+ * default and frees them, as does maxi_release_cached_memory() (which also
+ * frees the sphere-morphology scratch).  Volumes larger than the device go to
+ * the out-of-core form, as the reference's pybind module does
+ * (src/pybind/diffusion-pybind.cc:40-45).
  */
+int maxi_keep_device_buffers(int keep);
 int maxi_release_cached_memory(void);
 
 /*
@@ -133,7 +162,9 @@ int64_t maxi_diffusion_workspace_size(int64_t nz, int64_t ny, int64_t nx, int32_
  *              float[N] for F32/BF16/F16 (taken from the FP32 accumulator),
  *              double[N] for F64;
  *   workspace: device memory of at least maxi_diffusion_workspace_size() bytes,
- *              or NULL to let the library allocate (and free) it per call;
+ *              256-byte aligned, or NULL to let the library allocate (and
+ *              free) it per call;  a bit-packed mask must be 4-byte aligned
+ *              (misaligned pointers are rejected with MAXI_ERR_INVALID_ARGUMENT);
  *   flags: MAXI_FLAG_* bits.
  */
 int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,
@@ -152,9 +183,12 @@ int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int
  *   - at most 8,388,608 voxels (2^23) per call, radius <= 128, repititions >= 1;
  *     anything larger is rejected with MAXI_ERR_INVALID_ARGUMENT (radius:
  *     MAXI_ERR_UNSUPPORTED) before GPU work starts;
- *   - the array is reserved on each GPU that uses this call until the process
- *     exits; the first call on a device looks up its address (cudaGetSymbolAddress),
- *     so make that first call before any stream capture;
+ *   - the array stays reserved until the process exits on each GPU where the
+ *     library's device code is loaded: with CUDA's default lazy module loading
+ *     the GPUs that use this call, with CUDA_MODULE_LOADING=EAGER every GPU the
+ *     process creates a context on; the first call on a device looks up its
+ *     address (cudaGetSymbolAddress), so make that first call before any
+ *     stream capture;
  *   - all calls share the array: calls whose GPU work overlaps (different
  *     streams or threads without ordering) race and give wrong results.
  * mask, output (uint16, or NULL) and field_out (float, or NULL) are device
@@ -202,19 +236,38 @@ int maxi_diffusion_batched(const maxi_volume *volumes, int64_t n_volumes, int32_
  * Out-of-core diffusion of a HOST volume that need not fit the device.
  * Replaces NS::diffusion_out_of_core, src/lib/cpp/include/diffusion.hh:74
  * (GPU body src/lib/cpp/gpu/diffusion.cc:947-1129).  The volume is processed as
- * z-slabs of global_z planes, each loaded with repititions x radius halo planes
- * per side so all repetitions run on the device without exchanges; slabs span
- * the full y and x extent (global_y / global_x only have to be positive).
+ * z-slabs of at most global_z planes (thinner when such slabs do not fit the
+ * device) that span the full y and x extent (global_y / global_x only have to
+ * be positive).  Each slab is loaded with repititions x radius halo planes per
+ * side so all repetitions run on the device without exchanges; when such halos
+ * leave no room for useful slabs (large repititions x radius), the repetitions
+ * run in rounds of k with k x radius halos and the field goes through host
+ * memory between rounds (8 bytes per voxel of pinned host memory).  Planes of
+ * a multiple of 32 voxels keep the whole mask bit-packed on the device.
  * FP32 field; results equal maxi_diffusion_in_memory().
  */
 int maxi_diffusion_out_of_core(const uint8_t *voxels, int64_t total_z, int64_t total_y, int64_t total_x,
                                int64_t global_z, int64_t global_y, int64_t global_x, const float *kernel,
                                int64_t kernel_size, int64_t repititions, uint16_t *output, int verbose);
 
-/* The same with the field storage type and MAXI_FLAG_* options. */
+/* The same with the field storage type and MAXI_FLAG_* options; slab_z = 0
+ * lets the library choose the slab depth. */
 int maxi_diffusion_out_of_core_ex(const uint8_t *voxels, int64_t nz, int64_t ny, int64_t nx, int64_t slab_z,
                                   const float *kernel, int64_t kernel_size, int64_t repititions, uint16_t *output,
                                   int32_t field_type, int32_t flags, int verbose);
+
+/*
+ * The out-of-core plan maxi_diffusion_out_of_core_ex() would use (no
+ * reference counterpart: the reference's block size is fixed by the caller).
+ * For `device_bytes` of free device memory (0: the current device's free
+ * memory, or MAXIBONE_OOC_DEVICE_BUDGET bytes when that environment variable
+ * is set and smaller) writes the slab depth, the repetitions per round (equal
+ * to repititions: one round with deep halos, no exchange) and whether the mask
+ * stays bit-packed on the device.  MAXI_ERR_OUT_OF_MEMORY when no slab fits.
+ */
+int maxi_out_of_core_plan(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, int64_t kernel_size,
+                          int64_t repititions, int32_t field_type, int32_t flags, int64_t device_bytes,
+                          int64_t *slab_planes, int64_t *reps_per_round, int32_t *resident_mask);
 
 /*
  * On-disk diffusion: raw uint8 volume file in, raw uint16 file out.  Replaces

@@ -23,6 +23,14 @@ FLAG_NO_TENSOR_CORES = 0x2
 FLAG_NEAREST_ROUNDING = 0x4
 FLAG_MASK_FROM_FIELD = 0x8
 FLAG_AUTOTUNE = 0x10
+FLAG_SEPARATE_PASSES = 0x20
+FLAG_SINGLE_COEFFICIENTS = 0x40
+PATH_CUDA_CORES = 0x1
+PATH_TENSOR_CORES_ZY = 0x2
+PATH_TENSOR_CORES_X = 0x4
+PATH_FUSED_YX = 0x8
+PATH_GENERIC = 0x10
+PATH_FP32_FALLBACK = 0x20
 
 
 class MaxiVolume(ctypes.Structure):
@@ -53,6 +61,8 @@ SIGNATURES = {
     "maxi_diffusion_device_noalloc": (_int, [_p, _i32, _i64, _i64, _i64, _p, _i64, _i64, _p, _p, _p]),
     "maxi_tensor_core_status": (_int, []),
     "maxi_release_cached_memory": (_int, []),
+    "maxi_keep_device_buffers": (_int, [_int]),
+    "maxi_last_path": (_int, []),
     "maxi_batch_plan_create": (_int, [_p, _i64, _i32, _i32, _p, ctypes.POINTER(ctypes.c_void_p)]),
     "maxi_batch_plan_run": (_int, [_p, _p]),
     "maxi_batch_plan_describe": (_int, [_p, ctypes.c_char_p, _i64]),
@@ -62,6 +72,7 @@ SIGNATURES = {
     "maxi_diffusion_out_of_core_ex": (_int, [_p, _i64, _i64, _i64, _i64, _p, _i64, _i64, _p, _i32, _i32, _int]),
     "maxi_diffusion_on_disk": (_int, [ctypes.c_char_p, _p, _i64, ctypes.c_char_p, _i64, _i64, _i64, _i64, _i64,
                                       _i64, _i64, _int]),
+    "maxi_out_of_core_plan": (_int, [_i64, _i64, _i64, _i64, _i64, _i64, _i32, _i32, _i64, _p, _p, _p]),
     "maxi_profile_enable": (_int, [_int]),
     "maxi_profile_read": (_int, [_p, _p, _i32]),
 }

@@ -98,9 +98,13 @@ static cudaError_t enqueue_single(maxi_batch_plan *p, BatchVolume &bv, int32_t e
     cudaError_t e = launch_bitpack_encode(static_cast<const uint8_t *>(bv.v.mask), n, vol_packed(p, bv), false, st);
     if (e != cudaSuccess) return e;
     const Volume vol{bv.v.nz, bv.v.ny, bv.v.nx};
+    // The batched tensor-core launches run the y and x passes as separate
+    // kernels; the per-volume path does the same, so that every volume of a
+    // plan is computed by the same form.
     return dispatch_unrolled<S>(vol, vol_packed(p, bv), MAXI_MASK_BITPACKED, bv.kernel.data(),
                                 (int) (bv.v.kernel_size / 2), bv.v.repititions, vol_buf<S>(p, bv, 0),
-                                vol_buf<S>(p, bv, 1), bv.v.output, bv.v.field_out, p->flags | extra_flags, st);
+                                vol_buf<S>(p, bv, 1), bv.v.output, bv.v.field_out,
+                                p->flags | extra_flags | MAXI_FLAG_SEPARATE_PASSES, st);
 }
 
 // All repetitions of a tensor-core group as batched launches.

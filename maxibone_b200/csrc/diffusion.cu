@@ -11,6 +11,7 @@
 #include <vector>
 #include <map>
 #include <mutex>
+#include <atomic>
 
 #include "common.cuh"
 #include "passes.cuh"
@@ -26,7 +27,7 @@ namespace maxi {
 template <typename S, bool EXACT, int MF>
 static cudaError_t run_generic_fmt(const Volume &v, const void *mask, const float *kernel, int radius,
                                    int64_t reps, S *b0, S *b1, uint16_t *out_u16, void *field_out,
-                                   cudaStream_t st) {
+                                   const RunOpts &o, cudaStream_t st) {
     using Acc = typename FieldIO<S>::Acc;
     auto *taps = new GenericTaps<Acc>();
     for (int i = 0; i < 2 * radius + 1; i++) taps->k[i] = (Acc) kernel[i];
@@ -35,9 +36,19 @@ static cudaError_t run_generic_fmt(const Volume &v, const void *mask, const floa
     const int64_t blocks = ceil_div(n, threads);
     {
         ProfScope ps(MAXI_KERNEL_INIT, st);
-        mask_to_field<S, MF, false><<<std::min<int64_t>(blocks, 148 * 64), threads, 0, st>>>(mask, b0, nullptr, nullptr, n);
+        if (o.init_field)
+            field_from_f32<S><<<std::min<int64_t>(blocks, 148 * 64), threads, 0, st>>>(o.init_field, b0, n);
+        else
+            mask_to_field<S, MF, false><<<std::min<int64_t>(blocks, 148 * 64), threads, 0, st>>>(mask, b0, nullptr, nullptr, n);
     }
     for (int64_t rep = 0; rep < reps; rep++) {
+        if (o.final_wait && rep + 1 == reps) {
+            const cudaError_t e = cudaStreamWaitEvent(st, o.final_wait, 0);
+            if (e != cudaSuccess) {
+                delete taps;
+                return e;
+            }
+        }
         {
             ProfScope ps(MAXI_KERNEL_Z, st);
             generic_pass<S, EXACT, false, MF, false><<<blocks, threads, 0, st>>>(b0, b1, mask, nullptr, nullptr, n, v.nz, v.ny * v.nx, radius, *taps);
@@ -61,10 +72,11 @@ static cudaError_t run_generic_fmt(const Volume &v, const void *mask, const floa
 
 template <typename S, bool EXACT>
 static cudaError_t run_generic(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
-                               int64_t reps, S *b0, S *b1, uint16_t *out_u16, void *field_out, cudaStream_t st) {
+                               int64_t reps, S *b0, S *b1, uint16_t *out_u16, void *field_out, const RunOpts &o,
+                               cudaStream_t st) {
     if (mask_fmt == MAXI_MASK_U8)
-        return run_generic_fmt<S, EXACT, MAXI_MASK_U8>(v, mask, kernel, radius, reps, b0, b1, out_u16, field_out, st);
-    return run_generic_fmt<S, EXACT, MAXI_MASK_BITPACKED>(v, mask, kernel, radius, reps, b0, b1, out_u16, field_out, st);
+        return run_generic_fmt<S, EXACT, MAXI_MASK_U8>(v, mask, kernel, radius, reps, b0, b1, out_u16, field_out, o, st);
+    return run_generic_fmt<S, EXACT, MAXI_MASK_BITPACKED>(v, mask, kernel, radius, reps, b0, b1, out_u16, field_out, o, st);
 }
 
 template <typename S>
@@ -99,15 +111,16 @@ static int64_t workspace_bytes_for(int64_t n, int32_t ft) {
 template <typename S>
 static cudaError_t run_typed(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
                              int64_t reps, uint16_t *out_u16, void *field_out, int32_t flags, char *ws,
-                             cudaStream_t st, int64_t shrink_lo, int64_t shrink_hi) {
+                             cudaStream_t st, const RunOpts &o) {
     if (reps == 0) return zero_reps<S>(v, mask, mask_fmt, out_u16, field_out, st);
     S *b0 = reinterpret_cast<S *>(ws);
     S *b1 = reinterpret_cast<S *>(ws + round_up((int64_t) sizeof(S) * v.n(), 256));
     constexpr bool is_f64 = std::is_same<S, double>::value;
     const bool exact = (flags & MAXI_FLAG_REFERENCE_ROUNDING) != 0;
     if (is_f64 || exact || radius_bucket(radius) < 0) {
-        if (exact) return run_generic<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, st);
-        return run_generic<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, st);
+        note_path(MAXI_PATH_GENERIC);
+        if (exact) return run_generic<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, o, st);
+        return run_generic<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, o, st);
     }
     if constexpr (!is_f64) {
         uint32_t *packed = reinterpret_cast<uint32_t *>(ws + 2 * round_up((int64_t) sizeof(S) * v.n(), 256));
@@ -124,13 +137,15 @@ static cudaError_t run_typed(const Volume &v, const void *mask, int mask_fmt, co
             mask = packed;
         }
         return dispatch_unrolled<S>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16,
-                                    static_cast<float *>(field_out), flags, st, shrink_lo, shrink_hi);
+                                    static_cast<float *>(field_out), flags, st, o);
     }
     return cudaErrorInvalidValue;
 }
 
-// Device buffers of the host entry point, kept between calls (one per device,
-// grow-only) so repeated calls do not map and unmap gigabytes each time.
+// Device buffers of the host entry point (one per device, grow-only): freed
+// before the call returns unless the caller asked to keep them between calls
+// (maxi_keep_device_buffers), so that repeated calls do not map and unmap
+// gigabytes each time.
 struct DeviceCache {
     std::mutex mu;
     void *buf = nullptr;
@@ -139,6 +154,18 @@ struct DeviceCache {
 };
 static std::mutex g_cache_mu;
 static std::map<int, DeviceCache *> g_caches;
+// Whether maxi_diffusion_in_memory() keeps its device buffers after it
+// returns (maxi_keep_device_buffers); off by default, as the reference frees
+// its working buffers before returning (src/lib/cpp/cpu/diffusion.cc:371-373).
+static std::atomic<int> g_keep_buffers{0};
+
+static void cache_drop(DeviceCache *c) {
+    if (!c->buf) return;
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->buf);
+    c->buf = nullptr;
+    c->bytes = 0;
+}
 
 static int device_cache(DeviceCache **out) {
     int dev = 0;
@@ -157,12 +184,7 @@ static int device_cache(DeviceCache **out) {
 
 static int cache_reserve(DeviceCache *c, int64_t bytes) {
     if (c->bytes >= bytes) return MAXI_OK;
-    if (c->buf) {
-        cudaStreamSynchronize(c->stream);
-        cudaFree(c->buf);
-        c->buf = nullptr;
-        c->bytes = 0;
-    }
+    cache_drop(c);
     if (cudaMalloc(&c->buf, bytes) != cudaSuccess) {
         cudaGetLastError();
         c->buf = nullptr;
@@ -176,12 +198,7 @@ static void release_device_caches() {
     std::lock_guard<std::mutex> lk(g_cache_mu);
     for (auto &kv : g_caches) {
         std::lock_guard<std::mutex> lk2(kv.second->mu);
-        if (kv.second->buf) {
-            cudaStreamSynchronize(kv.second->stream);
-            cudaFree(kv.second->buf);
-            kv.second->buf = nullptr;
-            kv.second->bytes = 0;
-        }
+        cache_drop(kv.second);
     }
 }
 
@@ -199,6 +216,8 @@ extern "C" {
 const char *maxi_version(void) { return "maxibone_b200 diffusion 0.1 (sm_100a)"; }
 
 const char *maxi_last_error(void) { return last_error_cstr(); }
+
+int maxi_last_path(void) { return last_path_ref(); }
 
 int maxi_tensor_core_status(void) {
     clear_error();
@@ -219,7 +238,7 @@ int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int
                           uint16_t *output, void *field_out, int32_t field_type, int32_t flags,
                           void *workspace, int64_t workspace_bytes, void *stream) {
     return diffusion_device_shrinking(mask, mask_format, nz, ny, nx, kernel, kernel_size, repititions, output,
-                                      field_out, field_type, flags, workspace, workspace_bytes, stream, 0, 0);
+                                      field_out, field_type, flags, workspace, workspace_bytes, stream, RunOpts{});
 }
 
 }  // extern "C"
@@ -227,8 +246,7 @@ int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int
 int maxi::diffusion_device_shrinking(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,
                                      const float *kernel, int64_t kernel_size, int64_t repititions,
                                      uint16_t *output, void *field_out, int32_t field_type, int32_t flags,
-                                     void *workspace, int64_t workspace_bytes, void *stream, int64_t shrink_lo,
-                                     int64_t shrink_hi) {
+                                     void *workspace, int64_t workspace_bytes, void *stream, const RunOpts &opts) {
     clear_error();
     int rc = validate_common(mask, nz, ny, nx, kernel, kernel_size, repititions);
     if (rc) return rc;
@@ -244,13 +262,33 @@ int maxi::diffusion_device_shrinking(const void *mask, int32_t mask_format, int6
                          "the rebuilt-mask semantics are served for the FP32 field with the fast passes (radius <= 128)");
     if (!output && !field_out)
         return set_error(MAXI_ERR_INVALID_ARGUMENT, "neither output nor field_out given");
+    // The passes read the workspace's field buffers with 16-byte vector and
+    // TMA loads, and a bit-packed mask as 32-bit words: misaligned pointers
+    // would fault on the device, so they are rejected here.
+    if (workspace && (reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "workspace is not 256-byte aligned");
+    if (mask_format == MAXI_MASK_BITPACKED && (reinterpret_cast<uintptr_t>(mask) & 3) != 0)
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "a bit-packed mask must be 4-byte aligned");
     if ((rc = require_device())) return rc;
+    last_path_ref() = 0;
 
     const Volume v{nz, ny, nx};
     const int radius = (int) (kernel_size / 2);
-    const int64_t need = workspace_bytes_for(v.n(), field_type);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     char *ws = static_cast<char *>(workspace);
+    // A 16-bit field on a shape the tensor-core passes do not take (nx not a
+    // multiple of 8, nx < 64) would run the 16-bit CUDA-core passes, which are
+    // slower than the FP32 form as well as less accurate: such a request runs
+    // the FP32 form instead when the workspace allows it (reported by
+    // maxi_last_path()).  MAXI_FLAG_NO_TENSOR_CORES keeps the 16-bit passes.
+    int32_t run_type = field_type;
+    if ((field_type == MAXI_FIELD_BF16 || field_type == MAXI_FIELD_F16) && !(flags & MAXI_FLAG_NO_TENSOR_CORES) &&
+        repititions > 0 && radius_bucket(radius) >= 0 && !tc::tc_supported(radius, nz, ny, nx) &&
+        (!ws || workspace_bytes >= workspace_bytes_for(v.n(), MAXI_FIELD_F32))) {
+        run_type = MAXI_FIELD_F32;
+        note_path(MAXI_PATH_FP32_FALLBACK);
+    }
+    const int64_t need = workspace_bytes_for(v.n(), run_type);
     bool owned = false;
     if (repititions > 0) {
         if (ws && workspace_bytes < need)
@@ -267,14 +305,15 @@ int maxi::diffusion_device_shrinking(const void *mask, int32_t mask_format, int6
     }
     // Plane windows start at multiples of ny*nx voxels: keep them on whole
     // 32-bit words of the bit-packed mask (and 16-byte aligned for TMA).
-    if ((ny * nx) % 32 != 0 || shrink_lo < 0 || shrink_hi < 0) shrink_lo = shrink_hi = 0;
-    const int64_t slo = shrink_lo, shi = shrink_hi;
+    RunOpts o = opts;
+    if ((ny * nx) % 32 != 0 || o.shrink_lo < 0 || o.shrink_hi < 0 || run_type == MAXI_FIELD_F64)
+        o.shrink_lo = o.shrink_hi = 0;
     cudaError_t e;
-    switch (field_type) {
-    case MAXI_FIELD_F32: e = run_typed<float>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st, slo, shi); break;
-    case MAXI_FIELD_BF16: e = run_typed<__nv_bfloat16>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st, slo, shi); break;
-    case MAXI_FIELD_F16: e = run_typed<__half>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st, slo, shi); break;
-    default: e = run_typed<double>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st, 0, 0); break;
+    switch (run_type) {
+    case MAXI_FIELD_F32: e = run_typed<float>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st, o); break;
+    case MAXI_FIELD_BF16: e = run_typed<__nv_bfloat16>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st, o); break;
+    case MAXI_FIELD_F16: e = run_typed<__half>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st, o); break;
+    default: e = run_typed<double>(v, mask, mask_format, kernel, radius, repititions, output, field_out, flags, ws, st, o); break;
     }
     if (owned) cudaFreeAsync(ws, st);
     if (e != cudaSuccess) return set_cuda_error(e, "diffusion launch");
@@ -303,16 +342,12 @@ int maxi_diffusion_in_memory(const uint8_t *voxels, int64_t nz, int64_t ny, int6
     std::lock_guard<std::mutex> lk(cache->mu);
     if ((rc = cache_reserve(cache, total))) {
         // Larger than the device: the reference's pybind module sends such volumes to
-        // its out-of-core form (src/pybind/diffusion-pybind.cc:40-45); do the same.
-        const int64_t plane = ny * nx;
-        size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
-        const int64_t halo = std::min(nz, repititions * (kernel_size / 2));
-        int64_t slab = (int64_t) (free_b / 2) / std::max<int64_t>(1, plane * 15) - 2 * halo;
-        if (slab < 1) slab = 1;
-        if (verbose >= 1) printf("Volume exceeds device memory: out-of-core slabs of %lld planes\n", (long long) slab);
+        // its out-of-core form (src/pybind/diffusion-pybind.cc:40-45); do the same,
+        // with the slab depth (and exchange rounds, for large R x radius) chosen
+        // from the free device memory.
+        if (verbose >= 1) printf("Volume exceeds device memory: out-of-core form\n");
         clear_error();
-        return maxi_diffusion_out_of_core_ex(voxels, nz, ny, nx, slab, kernel, kernel_size, repititions, output,
+        return maxi_diffusion_out_of_core_ex(voxels, nz, ny, nx, 0, kernel, kernel_size, repititions, output,
                                              MAXI_FIELD_F32, 0, verbose);
     }
     char *base = static_cast<char *>(cache->buf);
@@ -323,12 +358,23 @@ int maxi_diffusion_in_memory(const uint8_t *voxels, int64_t nz, int64_t ny, int6
     if (e == cudaSuccess) {
         rc = maxi_diffusion_device(d_mask, MAXI_MASK_U8, nz, ny, nx, kernel, kernel_size, repititions, d_out, nullptr,
                                    MAXI_FIELD_F32, 0, base + ws_off, need, st);
-        if (rc) return rc;
+        if (rc) {
+            if (!g_keep_buffers.load()) cache_drop(cache);
+            return rc;
+        }
         e = cudaMemcpyAsync(output, d_out, 2 * n, cudaMemcpyDeviceToHost, st);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (!g_keep_buffers.load()) cache_drop(cache);
     if (e != cudaSuccess) return set_cuda_error(e, "in-memory diffusion");
     if (verbose >= 1) printf("Diffusion is complete!\n");
+    return MAXI_OK;
+}
+
+int maxi_keep_device_buffers(int keep) {
+    clear_error();
+    g_keep_buffers.store(keep ? 1 : 0);
+    if (!keep) release_device_caches();
     return MAXI_OK;
 }
 

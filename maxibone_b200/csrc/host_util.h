@@ -35,6 +35,14 @@ inline int set_error(int code, const char *fmt, ...) {
     return code;
 }
 
+// Per-thread record of the kernel families (MAXI_PATH_* bits) the last
+// diffusion call of this thread enqueued, for maxi_last_path().
+inline int &last_path_ref() {
+    static thread_local int path = 0;
+    return path;
+}
+inline void note_path(int bits) { last_path_ref() |= bits; }
+
 inline int set_cuda_error(cudaError_t e, const char *what) {
     const int code = (e == cudaErrorMemoryAllocation) ? MAXI_ERR_OUT_OF_MEMORY : MAXI_ERR_CUDA;
     return set_error(code, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));

@@ -13,8 +13,11 @@
 // Limits and rules of use:
 //   * at most kNoAllocMaxVoxels voxels per call (e.g. 256 x 256 x 128); larger
 //     volumes are rejected with MAXI_ERR_INVALID_ARGUMENT before any GPU work;
-//   * the array (2 * kNoAllocMaxVoxels floats = 64 MiB) is reserved on every
-//     GPU that uses this entry point and stays reserved until the process exits;
+//   * the array (2 * kNoAllocMaxVoxels floats = 64 MiB) stays reserved until the
+//     process exits on every GPU where this library's device code is loaded.
+//     With CUDA's default lazy module loading that is the GPUs that use this
+//     entry point; with eager loading (CUDA_MODULE_LOADING=EAGER) it is every
+//     GPU on which the process creates a context while the library is loaded;
 //   * the first call on each device looks up the array's device address with
 //     cudaGetSymbolAddress (which may load this part of the library), so make
 //     that first call before any stream capture starts;
@@ -77,6 +80,8 @@ extern "C" int maxi_diffusion_device_noalloc(const void *mask, int32_t mask_form
     if (mask_format != MAXI_MASK_U8 && mask_format != MAXI_MASK_BITPACKED)
         return set_error(MAXI_ERR_INVALID_ARGUMENT, "unknown mask_format %d", mask_format);
     if (!output && !field_out) return set_error(MAXI_ERR_INVALID_ARGUMENT, "neither output nor field_out given");
+    if (mask_format == MAXI_MASK_BITPACKED && (reinterpret_cast<uintptr_t>(mask) & 3) != 0)
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "a bit-packed mask must be 4-byte aligned");
     const int64_t n = nz * ny * nx;
     if (n > kNoAllocMaxVoxels)
         return set_error(MAXI_ERR_INVALID_ARGUMENT,
@@ -87,6 +92,7 @@ extern "C" int maxi_diffusion_device_noalloc(const void *mask, int32_t mask_form
     if ((rc = require_device())) return rc;
     float *scratch = nullptr;
     if ((rc = noalloc_scratch(&scratch))) return rc;
+    last_path_ref() = 0;
     const Volume v{nz, ny, nx};
     cudaError_t e = dispatch_unrolled<float>(v, mask, mask_format, kernel, (int) (kernel_size / 2), repititions,
                                              scratch, scratch + kNoAllocMaxVoxels, output, field_out, 0,

@@ -380,4 +380,13 @@ __global__ void mask_to_field(const void *__restrict__ mask, S *__restrict__ fie
     }
 }
 
+// FP32 field -> storage type (the start of an out-of-core exchange round, which
+// continues from the field of the previous round; `src` may be mapped host memory).
+template <typename S>
+__global__ void field_from_f32(const float *__restrict__ src, S *__restrict__ field, int64_t n) {
+    using Acc = typename FieldIO<S>::Acc;
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        field[i] = FieldIO<S>::narrow((Acc) src[i]);
+}
+
 }  // namespace maxi

@@ -8,6 +8,10 @@
 #include "host_util.h"
 #include "profiler.h"
 #include "tc_kernels.cuh"
+#include "tc_yx.cuh"
+
+#include <cmath>
+#include <vector>
 
 namespace maxi {
 namespace tc {
@@ -127,6 +131,154 @@ void tc_split_taps(const float *kernel, int radius, bool is_bf16, float scale, u
         }
     }
 }
+
+// Neighbour of a finite 16-bit float (bit pattern b) towards +inf (up) or -inf.
+static uint16_t step16(uint16_t b, bool up) {
+    const bool neg = (b & 0x8000u) != 0;
+    if ((b & 0x7fffu) == 0) return up ? 0x0001u : 0x8001u;  // +-0 -> smallest subnormal of that direction
+    return (uint16_t) ((up != neg) ? b + 1 : b - 1);
+}
+
+void tc_round_taps_matched(const float *kernel, int radius, bool is_bf16, float scale, uint16_t *out) {
+    const int n = 2 * radius + 1;
+    auto from = [&](uint16_t b) { return (double) (is_bf16 ? from_bf16(b) : from_f16(b)); };
+    std::vector<double> k(n), d0(n), d1(n);
+    std::vector<uint16_t> b0(n), b1(n);
+    for (int i = 0; i < n; i++) {
+        const float v = kernel[i] * scale;
+        k[i] = (double) v;
+        b0[i] = is_bf16 ? bits_bf16(v) : bits_f16(v);
+        const double q = from(b0[i]);
+        b1[i] = q == k[i] ? b0[i] : step16(b0[i], q < k[i]);
+        d0[i] = q - k[i];
+        d1[i] = from(b1[i]) - k[i];
+    }
+    // Groups flipped together: the symmetric pairs (r - j, r + j) of a
+    // symmetric kernel keep it symmetric; otherwise every tap alone.
+    bool sym = true;
+    for (int j = 1; j <= radius; j++) sym = sym && kernel[radius - j] == kernel[radius + j];
+    std::vector<std::vector<int>> groups;
+    if (sym) {
+        groups.push_back({radius});
+        for (int j = 1; j <= radius; j++) groups.push_back({radius - j, radius + j});
+    } else {
+        for (int i = 0; i < n; i++) groups.push_back({i});
+    }
+    const int G = (int) groups.size();
+    std::vector<double> g0(G), g2(G);  // change of the sum / second moment when group g flips
+    double s0 = 0.0, s2 = 0.0;         // current errors of the sum and second moment
+    for (int i = 0; i < n; i++) {
+        const double j2 = (double) (i - radius) * (i - radius);
+        s0 += d0[i];
+        s2 += j2 * d0[i];
+    }
+    for (int g = 0; g < G; g++)
+        for (int i : groups[g]) {
+            const double j2 = (double) (i - radius) * (i - radius);
+            g0[g] += d1[i] - d0[i];
+            g2[g] += j2 * (d1[i] - d0[i]);
+        }
+    const double w2 = 1.0 / std::max(1.0, (double) radius * radius);
+    auto cost = [&](double a, double b) { return std::fabs(a) + w2 * std::fabs(b); };
+    std::vector<int> flip(G, 0);
+    // Greedy local search over single and paired group flips; each accepted
+    // move lowers the cost, so it ends.
+    for (int iter = 0; iter < 4 * G; iter++) {
+        double best = cost(s0, s2);
+        int bi = -1, bj = -1;
+        for (int a = 0; a < G; a++) {
+            if (g0[a] == 0.0 && g2[a] == 0.0) continue;
+            const double sa = flip[a] ? -1.0 : 1.0;
+            const double c1 = cost(s0 + sa * g0[a], s2 + sa * g2[a]);
+            if (c1 < best) { best = c1; bi = a; bj = -1; }
+            for (int b = a + 1; b < G; b++) {
+                const double sb = flip[b] ? -1.0 : 1.0;
+                const double c2 = cost(s0 + sa * g0[a] + sb * g0[b], s2 + sa * g2[a] + sb * g2[b]);
+                if (c2 < best) { best = c2; bi = a; bj = b; }
+            }
+        }
+        if (bi < 0) break;
+        for (int g : {bi, bj}) {
+            if (g < 0) continue;
+            const double sg = flip[g] ? -1.0 : 1.0;
+            s0 += sg * g0[g];
+            s2 += sg * g2[g];
+            flip[g] ^= 1;
+        }
+    }
+    for (int g = 0; g < G; g++)
+        for (int i : groups[g]) out[i] = flip[g] ? b1[i] : b0[i];
+}
+
+bool tc_yx_supported(int radius, int64_t nz, int64_t ny, int64_t nx) {
+    return radius <= kTcMaxRadius && tc_supported(radius, nz, ny, nx) &&
+           nz * ceil_div(ny, kTM) * ceil_div(nx, kXTN) < (int64_t(1) << 31);
+}
+
+template <typename S>
+cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool final_pass, uint16_t *out_u16,
+                  float *field_out, int64_t nz, int64_t ny, int64_t nx, const float *kernel, int radius,
+                  bool error_feedback, bool hi_only, cudaStream_t st, const YzRows *out_rows) {
+    if (radius > kTcMaxRadius) return cudaErrorInvalidValue;
+    const bool is_bf16 = std::is_same<S, __nv_bfloat16>::value;
+    if (final_pass) out_rows = nullptr;
+    YxLaunch p{};
+    const int ra = (int) round_up(radius, 8);
+    fill_pass_taps(p.ty, kernel, radius, 0, (int) round_up(kTM + 2 * radius, 16), is_bf16, error_feedback);
+    fill_pass_taps(p.tx, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback);
+    if (hi_only) {
+        const float scale = is_bf16 ? 1.0f : 1024.0f;
+        tc_round_taps_matched(kernel, radius, is_bf16, scale, p.ty.hi);
+        for (int i = 0; i < 2 * radius + 1; i++) {
+            p.tx.hi[i] = p.ty.hi[i];
+            p.ty.lo[i] = p.tx.lo[i] = 0;
+        }
+    }
+    if (p.tx.kp > 3 * 64 || kYxAccX < (uint32_t) (64 * ((p.tx.kp + 63) / 64)) ||
+        kYxToep + 2 * p.ty.kcols > kYxTmemCols)
+        return cudaErrorInvalidValue;
+    p.hi_only = hi_only ? 1 : 0;
+    p.final_pass = final_pass ? 1 : 0;
+    p.mask = mask;
+    p.out = reinterpret_cast<uint16_t *>(out_rows ? out_rows->base : static_cast<void *>(out));
+    p.out_u16 = out_u16;
+    p.field_out = field_out;
+    p.nz = nz;
+    p.ny = ny;
+    p.nx = nx;
+    p.out_nz = out_rows ? out_rows->nz_total : 0;
+    p.out_z0 = out_rows ? out_rows->z0 : 0;
+    p.n_ty = (int) ceil_div(ny, kTM);
+    p.n_tx = (int) ceil_div(nx, kXTN);
+    p.n_tiles = nz * p.n_ty * p.n_tx;
+
+    CUtensorMap map;
+    const cuuint64_t dims[3] = {(cuuint64_t) nx, (cuuint64_t) ny, (cuuint64_t) nz};
+    const cuuint64_t strides[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (nx * ny * 2)};
+    const cuuint32_t box[3] = {64u, (cuuint32_t) p.ty.kp, 1u};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult cr = tc_encode_fn()(&map, is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
+                                 const_cast<S *>(in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    const int smem = yx_smem_bytes(p.ty.kp, p.tx.kpa, hi_only);
+    auto *kern = mask_fmt == MAXI_MASK_U8 ? tc_yx_kernel<S, MAXI_MASK_U8> : tc_yx_kernel<S, MAXI_MASK_BITPACKED>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t grid = std::min<int64_t>(p.n_tiles, sms);
+    kern<<<(unsigned) grid, kYxThreads, smem, st>>>(map, p);
+    return cudaGetLastError();
+}
+
+template cudaError_t tc_yx<__nv_bfloat16>(const __nv_bfloat16 *, __nv_bfloat16 *, const void *, int, bool, uint16_t *,
+                                          float *, int64_t, int64_t, int64_t, const float *, int, bool, bool,
+                                          cudaStream_t, const YzRows *);
+template cudaError_t tc_yx<__half>(const __half *, __half *, const void *, int, bool, uint16_t *, float *, int64_t,
+                                   int64_t, int64_t, const float *, int, bool, bool, cudaStream_t, const YzRows *);
 
 // The x pass in its transposed form (radius above kTcMaxRadius).
 template <typename S>

@@ -44,6 +44,28 @@ cudaError_t tc_contig(const S *in, S *out, const void *mask, int mask_fmt, bool 
                       float *field_out, int64_t nz, int64_t ny, int64_t nx, const float *kernel, int radius,
                       bool error_feedback, cudaStream_t st, const YzRows *out_rows = nullptr);
 
+// True when the fused y + x pass serves the shape (radius <= kTcMaxRadius and
+// the tensor-core passes' shape rules).
+bool tc_yx_supported(int radius, int64_t nz, int64_t ny, int64_t nx);
+
+// The y and x passes and the re-illumination fused in one kernel per z-plane
+// tile: reads the z pass's output `in` ([z][y][x]) and writes the next field
+// to `out` ([z][y][x], or [y][z][x] rows at out_rows), or on the last
+// repetition (final_pass) the uint16 output and/or the FP32 field.  hi_only:
+// one 16-bit coefficient set with the kernel's sum and second moment kept
+// (tc_round_taps_matched) instead of the high and low halves.
+template <typename S>
+cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool final_pass, uint16_t *out_u16,
+                  float *field_out, int64_t nz, int64_t ny, int64_t nx, const float *kernel, int radius,
+                  bool error_feedback, bool hi_only, cudaStream_t st, const YzRows *out_rows = nullptr);
+
+// One 16-bit coefficient per tap of kernel x scale: each tap is one of the two
+// representable values around it, chosen (symmetric pairs together) so that
+// the rounded kernel's sum and second moment are as close as the format allows
+// to the FP32 kernel's.  Plain round-to-nearest changes the sum by ~1e-4, and
+// that gain error compounds over the 3 R passes of a diffusion.
+void tc_round_taps_matched(const float *kernel, int radius, bool is_bf16, float scale, uint16_t *out);
+
 // Reads (and clears) the device error word of the tensor-core kernels:
 // 0 = fine, 1..3 = a bounded wait timed out, -1 = could not be read.
 int tc_read_and_clear_error();

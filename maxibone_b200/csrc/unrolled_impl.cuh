@@ -42,8 +42,9 @@ static cudaError_t set_smem(F *f, int bytes) {
 template <int R, typename S, bool EF>
 static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel,
                                 int radius, int64_t reps, S *buf0, S *buf1, uint16_t *out_u16,
-                                float *field_out, bool use_tc, uint32_t *rebuild_mask, int64_t shrink_lo,
-                                int64_t shrink_hi, cudaStream_t st) {
+                                float *field_out, bool use_tc, bool fuse_yx, bool hi_only, uint32_t *rebuild_mask,
+                                const RunOpts &o, cudaStream_t st) {
+    const int64_t shrink_lo = o.shrink_lo, shrink_hi = o.shrink_hi;
     const Taps<R> taps = make_taps<R>(kernel, radius);
     const int str_smem = strided_smem_bytes<R>();
     const int con_smem = contig_smem_bytes<R>();
@@ -64,7 +65,9 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
         const int threads = 256;
         const int64_t blocks = std::min<int64_t>((n + threads - 1) / threads, 148 * 64);
         ProfScope ps(MAXI_KERNEL_INIT, st);
-        if (mask_fmt == MAXI_MASK_U8)
+        if (o.init_field)
+            field_from_f32<S><<<blocks, threads, 0, st>>>(o.init_field, buf0, n);
+        else if (mask_fmt == MAXI_MASK_U8)
             mask_to_field<S, MAXI_MASK_U8, false><<<blocks, threads, 0, st>>>(mask, buf0, nullptr, nullptr, n);
         else
             mask_to_field<S, MAXI_MASK_BITPACKED, false><<<blocks, threads, 0, st>>>(mask, buf0, nullptr, nullptr, n);
@@ -74,6 +77,13 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
     const bool tc_x = use_tc &&
                       ((reinterpret_cast<uintptr_t>(out_u16) | reinterpret_cast<uintptr_t>(field_out) |
                         (mask_fmt == MAXI_MASK_U8 ? reinterpret_cast<uintptr_t>(mask) : 0)) & 15) == 0;
+    // Fused y + x kernel: z pass buf0 -> buf1, y + x buf1 -> buf0 ([y][z][x] rows
+    // between repetitions), so the buffers do not swap.
+    const bool yx = tc_x && fuse_yx && tc::tc_yx_supported(radius, v.nz, v.ny, v.nx);
+    if (reps > 0)
+        note_path(yx ? (MAXI_PATH_TENSOR_CORES_ZY | MAXI_PATH_FUSED_YX)
+                     : ((use_tc ? MAXI_PATH_TENSOR_CORES_ZY : MAXI_PATH_CUDA_CORES) |
+                        (tc_x ? MAXI_PATH_TENSOR_CORES_X : MAXI_PATH_CUDA_CORES)));
     for (int64_t rep = 0; rep < reps; rep++) {
         // Plane window of this repetition (the whole volume unless shrinking).
         const int64_t lo = std::min(v.nz - 1, shrink_lo * rep);
@@ -88,7 +98,10 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
         const int64_t zI = plane, zA = nzv, zat = ceil_div(zA, kStrTA), zit = ceil_div(zI, kStrTI);
         const int64_t yI = v.nx, yA = v.ny, yO = nzv, yat = ceil_div(yA, kStrTA), yit = ceil_div(yI, kStrTI);
         const int64_t rows = nzv * v.ny, xt = ceil_div(v.nx, kConTX), xrb = ceil_div(rows, kConTR);
-        if (rebuild_mask && rep > 0) {
+        if (o.final_wait && rep + 1 == reps && (e = cudaStreamWaitEvent(st, o.final_wait, 0)) != cudaSuccess) return e;
+        // The rebuilt-mask semantics: before every repetition after the first of
+        // the whole run (a continued run's first repetition is not the first).
+        if (rebuild_mask && (rep > 0 || o.init_field)) {
             ProfScope ps(MAXI_KERNEL_OTHER, st);
             const int64_t blocks = std::min<int64_t>(ceil_div(ceil_div(nzv * plane, 32), 256), 148 * 16);
             mask_from_field<S><<<blocks, 256, 0, st>>>(b0, rebuild_mask + off / 32, nzv * plane);
@@ -107,6 +120,17 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
             }
         }
         if (e != cudaSuccess) return e;
+        const bool last = rep + 1 == reps;
+        if constexpr (sizeof(S) == 2) {
+            if (yx) {
+                ProfScope ps(MAXI_KERNEL_YX, st);
+                const tc::YzRows yz{buf0, v.nz, lo};
+                e = tc::tc_yx<S>(b1, b0, mv, mask_fmt, last, last ? ou : nullptr, last ? fo : nullptr, nzv, v.ny,
+                                 v.nx, kernel, radius, EF, hi_only, st, &yz);
+                if (e != cudaSuccess) return e;
+                continue;
+            }
+        }
         {
             ProfScope ps(MAXI_KERNEL_Y, st);
             if constexpr (sizeof(S) == 2) {
@@ -117,7 +141,6 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
             }
         }
         if (e != cudaSuccess) return e;
-        const bool last = rep + 1 == reps;
         {
             ProfScope ps(last ? MAXI_KERNEL_X_FINAL : MAXI_KERNEL_X, st);
             if (tc_x) {
@@ -151,10 +174,10 @@ cudaError_t launch_init_field(const void *mask, int mask_fmt, S *field, int64_t 
 template <typename S, bool EF>
 static cudaError_t dispatch_radius(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
                                    int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, bool use_tc,
-                                   uint32_t *rebuild, int64_t shrink_lo, int64_t shrink_hi, cudaStream_t st) {
+                                   bool fuse_yx, bool hi_only, uint32_t *rebuild, const RunOpts &o, cudaStream_t st) {
     switch (radius_bucket_impl(radius)) {
 #define MAXI_CASE(RB) \
-    case RB: return run_unrolled<RB, S, EF>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, rebuild, shrink_lo, shrink_hi, st);
+    case RB: return run_unrolled<RB, S, EF>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, fuse_yx, hi_only, rebuild, o, st);
         MAXI_CASE(1) MAXI_CASE(2) MAXI_CASE(3) MAXI_CASE(4) MAXI_CASE(6) MAXI_CASE(8) MAXI_CASE(12)
         MAXI_CASE(16) MAXI_CASE(24) MAXI_CASE(32) MAXI_CASE(48) MAXI_CASE(64) MAXI_CASE(96) MAXI_CASE(128)
 #undef MAXI_CASE
@@ -165,7 +188,7 @@ static cudaError_t dispatch_radius(const Volume &v, const void *mask, int mask_f
 template <typename S>
 cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, const float *kernel, int radius,
                               int64_t reps, S *b0, S *b1, uint16_t *out_u16, float *field_out, int32_t flags,
-                              cudaStream_t st, int64_t shrink_lo, int64_t shrink_hi) {
+                              cudaStream_t st, const RunOpts &o) {
     // Mask rebuilt from the field each repetition: the caller passes a writable
     // bit-packed copy (the workspace's).
     uint32_t *rebuild = (flags & MAXI_FLAG_MASK_FROM_FIELD) && mask_fmt == MAXI_MASK_BITPACKED
@@ -176,10 +199,14 @@ cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, c
         // kernels narrower than radius 4 (sigma < 1) pass too much of it.
         const bool ef = (flags & MAXI_FLAG_NEAREST_ROUNDING) == 0 && radius >= 4;
         const bool use_tc = (flags & MAXI_FLAG_NO_TENSOR_CORES) == 0 && tc::tc_supported(radius, v.nz, v.ny, v.nx);
-        if (ef) return dispatch_radius<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, rebuild, shrink_lo, shrink_hi, st);
-        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, rebuild, shrink_lo, shrink_hi, st);
+        // The rebuilt-mask semantics rewrite the mask between repetitions from the
+        // x pass's output; they keep the separate passes.
+        const bool fuse = (flags & (MAXI_FLAG_SEPARATE_PASSES | MAXI_FLAG_MASK_FROM_FIELD)) == 0;
+        const bool hi_only = (flags & MAXI_FLAG_SINGLE_COEFFICIENTS) != 0;
+        if (ef) return dispatch_radius<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, fuse, hi_only, rebuild, o, st);
+        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, fuse, hi_only, rebuild, o, st);
     } else {
-        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, false, rebuild, shrink_lo, shrink_hi, st);
+        return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, false, false, false, rebuild, o, st);
     }
 }
 

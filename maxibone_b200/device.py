@@ -24,7 +24,7 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
             field: str = "f32", field_out: torch.Tensor | None = None, shape=None,
             reference_rounding: bool = False, workspace: torch.Tensor | None = None,
             stream: torch.cuda.Stream | None = None, tensor_cores: bool = True,
-            error_feedback: bool = True) -> None:
+            error_feedback: bool = True, fuse_passes: bool = True, single_coefficients: bool = False) -> None:
     """Run the diffusion on device buffers.
 
     mask: uint8 [nz, ny, nx] CUDA tensor (set when > 0), or a bit-packed int32/uint32
@@ -36,6 +36,10 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
     workspace: uint8 CUDA tensor of at least workspace_bytes(shape, field), or None.
     tensor_cores: 16-bit fields: z and y passes on tcgen05 tensor cores where supported.
     error_feedback: 16-bit fields: error-feedback rounding along x (else round to nearest).
+    fuse_passes: 16-bit tensor-core fields, radius <= 32: the y and x passes in one
+          kernel per z-plane tile (else two kernels, two HBM round trips).
+    single_coefficients: fused kernel: one 16-bit coefficient set with the kernel's
+          sum and second moment kept, instead of high + low halves.
     """
     if not mask.is_cuda:
         raise ValueError("mask must be a CUDA tensor")
@@ -74,12 +78,22 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
         flags |= _lib.FLAG_NO_TENSOR_CORES
     if not error_feedback:
         flags |= _lib.FLAG_NEAREST_ROUNDING
+    if not fuse_passes:
+        flags |= _lib.FLAG_SEPARATE_PASSES
+    if single_coefficients:
+        flags |= _lib.FLAG_SINGLE_COEFFICIENTS
     with torch.cuda.device(mask.device):
         _lib.check(_lib.lib().maxi_diffusion_device(
             mask.data_ptr(), fmt, nz, ny, nx, k.ctypes.data, k.shape[0], int(repititions),
             output.data_ptr() if output is not None else None,
             field_out.data_ptr() if field_out is not None else None,
             _lib.FIELD_TYPES[field], flags, ws_ptr, ws_bytes, st.cuda_stream))
+
+
+def last_path() -> int:
+    """MAXI_PATH_* bits of the kernels the last diffuse() call on this thread
+    enqueued (e.g. _lib.PATH_TENSOR_CORES_ZY | _lib.PATH_TENSOR_CORES_X)."""
+    return int(_lib.lib().maxi_last_path())
 
 
 def bitpack(mask: torch.Tensor, stream: torch.cuda.Stream | None = None) -> torch.Tensor:

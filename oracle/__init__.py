@@ -56,8 +56,9 @@ _LIB = None
 def build() -> None:
     """Compile the C restatement (and the reference modules where the reference tree exists)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if os.path.isdir(os.environ.get("MAXI_REFERENCE_SRC", "/root/reference/src")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    ref_src = os.environ.get("MAXI_REFERENCE_SRC", "/root/reference/src")
+    if os.path.isdir(ref_src):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_src}"], check=True)
 
 
 def _lib():
@@ -74,6 +75,10 @@ def _lib():
         lib.oracle_diffusion_f64.restype = ctypes.c_int
         lib.oracle_diffusion_on_disk_semantics.argtypes = [p, i64, i64, i64, p, i64, i64, p]
         lib.oracle_diffusion_on_disk_semantics.restype = ctypes.c_int
+        lib.oracle_diffusion_on_disk_field.argtypes = [p, i64, i64, i64, p, i64, i64, p]
+        lib.oracle_diffusion_on_disk_field.restype = ctypes.c_int
+        lib.oracle_f32_to_u8.argtypes = [p, p, i64]
+        lib.oracle_f32_to_u8.restype = None
         lib.oracle_convolve_axis_f32.argtypes = [p, p, p, i64, i64, i64, ctypes.c_int, i64]
         lib.oracle_convolve_axis_f32.restype = None
         lib.oracle_bitpack_encode_u32.argtypes = [p, i64, p]
@@ -124,6 +129,23 @@ def diffusion_on_disk_semantics(mask: np.ndarray, kernel: np.ndarray, repitition
                                                    int(repititions), _ptr(out))
     if rc != 0:
         raise MemoryError("oracle could not allocate its working buffers")
+    return out
+
+
+def diffusion_on_disk_u8(mask: np.ndarray, kernel: np.ndarray, repititions: int) -> np.ndarray:
+    """uint8 output of the reference CPU backend's on-disk variant: the field of
+    the on-disk semantics (mask rebuilt as field == 1.0f each step) converted
+    as (uint8) floor(v * 255.0f) (src/lib/cpp/cpu/diffusion.cc:139-144, 459)."""
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    k = np.ascontiguousarray(kernel, dtype=np.float32)
+    nz, ny, nx = m.shape
+    field = np.empty(m.shape, np.float32)
+    rc = _lib().oracle_diffusion_on_disk_field(_ptr(m), nz, ny, nx, _ptr(k), k.shape[0], int(repititions),
+                                               _ptr(field))
+    if rc != 0:
+        raise MemoryError("oracle could not allocate its working buffers")
+    out = np.empty(m.shape, np.uint8)
+    _lib().oracle_f32_to_u8(_ptr(field), _ptr(out), field.size)
     return out
 
 

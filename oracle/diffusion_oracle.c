@@ -152,9 +152,9 @@ int oracle_diffusion_f64(const uint8_t *voxels, int64_t nz, int64_t ny, int64_t 
  * GPU backend's final uint16 conversion (src/lib/cpp/gpu/diffusion.cc:937).
  * The slab decomposition of the reference is exact for the z-pass of the core
  * layers (radius-layer halos), so the whole-volume form gives the same values. */
-int oracle_diffusion_on_disk_semantics(const uint8_t *voxels, int64_t nz, int64_t ny, int64_t nx,
-                                       const float *kernel, int64_t kernel_size, int64_t repititions,
-                                       uint16_t *output) {
+int oracle_diffusion_on_disk_field(const uint8_t *voxels, int64_t nz, int64_t ny, int64_t nx,
+                                   const float *kernel, int64_t kernel_size, int64_t repititions,
+                                   float *field_out) {
     const int64_t n = nz * ny * nx, radius = kernel_size / 2;
     float *b0 = (float *) malloc((size_t) n * sizeof(float));
     float *b1 = (float *) malloc((size_t) n * sizeof(float));
@@ -170,11 +170,31 @@ int oracle_diffusion_on_disk_semantics(const uint8_t *voxels, int64_t nz, int64_
         }
         oracle_illuminate_f32(mask, b0, n);
     }
-    oracle_f32_to_u16(b0, output, n);
+    memcpy(field_out, b0, (size_t) n * sizeof(float));
     free(b0);
     free(b1);
     free(mask);
     return 0;
+}
+
+int oracle_diffusion_on_disk_semantics(const uint8_t *voxels, int64_t nz, int64_t ny, int64_t nx,
+                                       const float *kernel, int64_t kernel_size, int64_t repititions,
+                                       uint16_t *output) {
+    const int64_t n = nz * ny * nx;
+    float *f = (float *) malloc((size_t) n * sizeof(float));
+    if (!f) return -1;
+    const int rc = oracle_diffusion_on_disk_field(voxels, nz, ny, nx, kernel, kernel_size, repititions, f);
+    if (rc == 0) oracle_f32_to_u16(f, output, n);
+    free(f);
+    return rc;
+}
+
+/* The CPU backend's final conversion of its on-disk variant,
+ * convert_float_to_uint8 (src/lib/cpp/cpu/diffusion.cc:139-144):
+ * (uint8_t) floor(v * 255.0f) in FP32. */
+void oracle_f32_to_u8(const float *field, uint8_t *out, int64_t n) {
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) out[i] = (uint8_t) floorf(field[i] * 255.0f);
 }
 
 /* Bit-packing, uint32 words, most significant bit first.  Restates

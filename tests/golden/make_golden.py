@@ -16,7 +16,9 @@ histograms.field_histogram bins, and a voxel block with the reference's
 histograms.axis_histograms x / y / z / radial bins; the morphology case stores a
 uint8 mask and the reference's morphology.dilate_3d_sphere / erode_3d_sphere results;
 the implant case stores an implant mask, its frame of reference and the reference's
-geometry.compute_front_back_masks outputs.  The tests then check the oracle bit-for-bit against
+geometry.compute_front_back_masks outputs; the on-disk case stores a mask and the
+uint8 file the reference CPU backend's on-disk overload writes for it
+(``--on-disk`` regenerates only that case).  The tests then check the oracle bit-for-bit against
 these files, and the CUDA library against the oracle.
 """
 from __future__ import annotations
@@ -185,5 +187,46 @@ def main():
         json.dump(index, f, indent=1, sort_keys=True)
 
 
+def on_disk_case():
+    """The reference CPU backend's on-disk overload, diffusion(input_file,
+    np_kernel, output_file, total_shape, global_shape, repititions)
+    (src/pybind/diffusion-pybind.cc:67-77, src/lib/cpp/cpu/diffusion.cc:376-468):
+    a raw uint8 mask file in, a raw uint8 file of floor(v * 255) out, computed in
+    z-blocks of global_shape[0] planes with the mask rebuilt as field == 1.0f
+    before every repetition.  The block depth leaves a partial last block.  The
+    reference keeps its float temporaries in /tmp/maxibone (a path fixed in its
+    source); they are removed afterwards."""
+    import shutil
+    import tempfile
+
+    ref = oracle.reference_module("diffusion")
+    if ref is None:
+        sys.exit("reference modules not built: run `make -C oracle ref`")
+    shape, global_z, reps = (40, 24, 32), 12, 4
+    mask = spheres_mask(shape, 10, (2, 7), seed=21)
+    kernel = test_kernel(1.5)
+    temp_existed = os.path.exists("/tmp/maxibone")
+    with tempfile.TemporaryDirectory() as d:
+        fin, fout = os.path.join(d, "mask.uint8"), os.path.join(d, "field.uint8")
+        mask.tofile(fin)
+        ref.diffusion(fin, kernel, fout, shape, (global_z, shape[1], shape[2]), reps, 0)
+        out = np.fromfile(fout, dtype=np.uint8).reshape(shape)
+    if not temp_existed:
+        shutil.rmtree("/tmp/maxibone", ignore_errors=True)
+    np.savez_compressed(os.path.join(HERE, "on_disk_cpu_u8.npz"), mask=mask, kernel=kernel, reps=np.int64(reps),
+                        global_z=np.int64(global_z), output=out)
+    with open(os.path.join(HERE, "index.json")) as f:
+        index = json.load(f)
+    index["on_disk_cpu_u8"] = {"file": "on_disk_cpu_u8.npz", "shape": list(shape), "global_z": global_z,
+                               "reps": reps, "sha256": hashlib.sha256(out.tobytes()).hexdigest()}
+    with open(os.path.join(HERE, "index.json"), "w") as f:
+        json.dump(index, f, indent=1, sort_keys=True)
+    print("on_disk_cpu_u8", index["on_disk_cpu_u8"]["sha256"][:16])
+
+
 if __name__ == "__main__":
-    main()
+    if "--on-disk" in sys.argv:
+        on_disk_case()
+    else:
+        main()
+        on_disk_case()

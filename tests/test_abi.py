@@ -120,3 +120,28 @@ def test_no_device_is_an_error_not_a_fallback():
     k = np.ones(3, np.float32) / 3
     o = np.zeros((4, 4, 4), np.uint16)
     assert _call_in_memory(m, k, o) == 6
+
+
+def test_device_entry_rejects_misaligned_workspace_and_packed_mask():
+    # Both are rejected on the host, before any device work: the passes read the
+    # workspace with 16-byte vector / TMA loads and a bit-packed mask as words.
+    lib = _lib.lib()
+    k = np.ones(3, np.float32) / 3
+    mask, out = ctypes.c_void_p(4096), ctypes.c_void_p(8192)  # never dereferenced
+    ws_bytes = lib.maxi_diffusion_workspace_size(4, 4, 32, 0)
+    for off in (1, 16, 128):
+        rc = lib.maxi_diffusion_device(mask, 0, 4, 4, 32, k.ctypes.data, 3, 1, out, None, 0, 0,
+                                       ctypes.c_void_p(65536 + off), ws_bytes, None)
+        assert rc == 1 and b"256-byte" in lib.maxi_last_error()
+    rc = lib.maxi_diffusion_device(ctypes.c_void_p(4098), 1, 4, 4, 32, k.ctypes.data, 3, 1, out, None, 0, 0,
+                                   None, 0, None)
+    assert rc == 1 and b"4-byte" in lib.maxi_last_error()
+    rc = lib.maxi_diffusion_device_noalloc(ctypes.c_void_p(4098), 1, 4, 4, 32, k.ctypes.data, 3, 1, out, None, None)
+    assert rc == 1 and b"4-byte" in lib.maxi_last_error()
+
+
+def test_keep_device_buffers_and_last_path_need_no_device():
+    lib = _lib.lib()
+    assert lib.maxi_keep_device_buffers(1) == 0
+    assert lib.maxi_keep_device_buffers(0) == 0
+    assert lib.maxi_last_path() >= 0

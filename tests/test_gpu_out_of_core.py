@@ -92,3 +92,77 @@ def test_on_disk_short_file_is_an_io_error(tmp_path):
     np.zeros(100, np.uint8).tofile(fin)
     with pytest.raises(MaxiError, match="IO"):
         diffusion(str(fin), gauss_kernel(1), str(tmp_path / "o"), (10, 10, 10), (5, 10, 10), 1)
+
+
+def _plan(shape, kernel_size, reps, device_bytes, field="f32"):
+    import ctypes
+    from maxibone_b200 import _lib
+    s, k, res = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+    _lib.check(_lib.lib().maxi_out_of_core_plan(*shape, 0, kernel_size, reps, _lib.FIELD_TYPES[field], 0,
+                                                device_bytes, ctypes.byref(s), ctypes.byref(k), ctypes.byref(res)))
+    return s.value, k.value, bool(res.value)
+
+
+@pytest.mark.parametrize("budget", [4_000_000, 2_500_000])
+def test_exchange_rounds_equal_in_memory_fp32(budget, monkeypatch):
+    # A device budget too small for R x radius halos makes the planner run the
+    # repetitions in rounds of k < R, the field going through host memory
+    # between rounds; FP32 results equal the in-memory form bit for bit.
+    shape, reps = (96, 64, 64), 12
+    kernel = gauss_kernel(1.0).astype(np.float32)  # radius 4
+    S, k, _ = _plan(shape, kernel.shape[0], reps, budget)
+    assert k < reps and S < shape[0], (S, k)
+    mask = spheres_mask(shape, 12, (3, 9), seed=budget % 97)
+    want = np.empty(shape, np.uint16)
+    diffusion(mask, kernel, want, reps)
+    monkeypatch.setenv("MAXIBONE_OOC_DEVICE_BUDGET", str(budget))
+    got = np.zeros(shape, np.uint16)
+    diffusion_out_of_core(mask, kernel, got, (0, shape[1], shape[2]), reps)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_exchange_rounds_bf16_within_bounds(monkeypatch):
+    shape, reps = (80, 64, 128), 10
+    kernel = gauss_kernel(1.5).astype(np.float32)  # radius 6
+    mask = spheres_mask(shape, 10, (3, 9), seed=5)
+    S, k, _ = _plan(shape, kernel.shape[0], reps, 4_000_000, field="bf16")
+    assert k < reps
+    want = np.empty(shape, np.uint16)
+    diffusion(mask, kernel, want, reps)  # FP32 in memory
+    monkeypatch.setenv("MAXIBONE_OOC_DEVICE_BUDGET", "4000000")
+    got = np.zeros(shape, np.uint16)
+    diffusion_out_of_core(mask, kernel, got, (0, shape[1], shape[2]), reps, field="bf16")
+    assert np.abs(got.astype(np.int32) - want.astype(np.int32)).max() <= 2e-3 * 65535
+    assert np.all(got[mask > 0] == 65535)
+
+
+def test_planner_auto_slab_pageable_and_pinned_agree():
+    shape = (130, 32, 96)
+    mask = random_mask(shape, 0.05, seed=6)
+    kernel = gauss_kernel(2.0).astype(np.float32)
+    want = np.empty(shape, np.uint16)
+    diffusion(mask, kernel, want, 4)
+    got = np.zeros(shape, np.uint16)
+    diffusion_out_of_core(mask, kernel, got, (0, shape[1], shape[2]), 4)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_on_disk_against_the_reference_cpu_on_disk_file(tmp_path):
+    # The golden holds the uint8 file the reference CPU backend's on-disk overload
+    # wrote (floor(v * 255)); this library's on-disk overload writes the GPU
+    # backend's uint16 (floor(v * 65535)).  Since 65535 = 255 * 257,
+    # floor(u16 / 257) is the same quantity, so the two agree to 1 unit wherever
+    # the FP32 fields agree to summation order.
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "on_disk_cpu_u8.npz"))
+    mask, kernel, reps, gz = z["mask"], z["kernel"], int(z["reps"]), int(z["global_z"])
+    shape = mask.shape
+    fin, fout = tmp_path / "mask.uint8", tmp_path / "field.uint16"
+    mask.tofile(fin)
+    diffusion(str(fin), kernel, str(fout), shape, (gz, shape[1], shape[2]), reps)
+    got = np.fromfile(fout, dtype=np.uint16).reshape(shape)
+    d = np.abs((got // 257).astype(np.int32) - z["output"].astype(np.int32))
+    assert d.max() <= 1
+    assert (d > 0).mean() < 1e-3
+    assert np.all(got[mask > 0] == 65535)

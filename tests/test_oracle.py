@@ -226,3 +226,15 @@ def test_oracle_implant_masks_match_reference_module(seed, shape):
     geo.compute_front_back_masks(implant, 1.875, E, cm, cp, UVWp, *want)
     for g, w in zip(oracle.implant_masks(implant, 1.875, E, cm, cp, UVWp), want):
         np.testing.assert_array_equal(g, w)
+
+
+def test_on_disk_semantics_pinned_to_the_reference_cpu_on_disk_overload():
+    # The reference CPU backend's on-disk overload (z-blocks with radius halos,
+    # mask rebuilt as field == 1.0f every repetition, float temporaries on disk)
+    # writes (uint8) floor(v * 255); the oracle's whole-volume restatement of the
+    # same semantics, converted the same way, must equal that file bit for bit.
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "on_disk_cpu_u8.npz"))
+    got = oracle.diffusion_on_disk_u8(z["mask"], z["kernel"], int(z["reps"]))
+    np.testing.assert_array_equal(got, z["output"])

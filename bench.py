@@ -99,6 +99,8 @@ def parse_args():
                         "histograms, morphology, implant masks) on its output, and print their JSON object")
     p.add_argument("--shape", type=str, default=None,
                    help="override the workload's volume shape, e.g. 256x1024x1024 (profiling of smaller cases)")
+    p.add_argument("--reps", type=int, default=None,
+                   help="override the workload's repetition count (profiling of smaller cases)")
     p.add_argument("--ooc-shape", type=str, default="3456x3456x4096",
                    help="out-of-core section's volume, z x y x x")
     return p.parse_args()
@@ -877,6 +879,8 @@ def main():
     shape, sigma, reps = WORKLOADS[args.workload]
     if args.shape:
         shape = tuple(int(v) for v in args.shape.lower().split("x"))
+    if args.reps is not None:
+        reps = args.reps
     nz, ny, nx = shape
     vox = nz * ny * nx
     kernel = gauss_kernel(sigma).astype(np.float32)
@@ -972,7 +976,8 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": args.field, "data": "synthetic (seeded bone+implant mask, random-init)",
-        "config": {"workload": args.workload + (f" (shape override {args.shape})" if args.shape else ""),
+        "config": {"workload": args.workload + (f" (shape override {args.shape})" if args.shape else "")
+                   + (f" (repetitions override {args.reps})" if args.reps is not None else ""),
                    "shape": list(shape), "sigma": sigma, "kernel_size": int(2 * radius + 1),
                    "reps": reps, "field": args.field, "mask": "u8", "foreground": round(fg, 4),
                    "parallelism": f"{world} independent volumes (one per rank)",

@@ -173,6 +173,32 @@ int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int
                           void *workspace, int64_t workspace_bytes, void *stream);
 
 /*
+ * maxi_diffusion_device() for one z-slab of a volume split over several GPUs
+ * or processed in rounds (no reference counterpart; the reference's blocks
+ * exchange halos through host memory every repetition,
+ * src/lib/cpp/gpu/diffusion.cc:1013-1073).
+ *   init_field: device FP32 field of the slab's nz planes to start from
+ *               (the field after earlier repetitions), or NULL to start from
+ *               the mask as maxi_diffusion_device() does;
+ *   shrink_lo / shrink_hi: repetition k runs only on planes
+ *               [k * shrink_lo, nz - k * shrink_hi) -- the planes that can still
+ *               reach the slab's core when the slab's first / last planes are
+ *               halo planes of a cut, not the volume's edge (pass the radius
+ *               there, else 0); shrinking needs (ny * nx) % 32 == 0 and the
+ *               unrolled passes (else the whole slab is computed, also exact).
+ *               With shrinking, the last repetition writes output / field_out
+ *               only on planes [(R-1) * shrink_lo, nz - (R-1) * shrink_hi).
+ * After R repetitions the planes at least R x radius from every cut side hold
+ * the whole volume's values.  The rebuilt-mask flag (MAXI_FLAG_MASK_FROM_FIELD)
+ * rebuilds the mask from init_field before the first repetition as well.
+ */
+int maxi_diffusion_device_ex(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,
+                             const float *kernel, int64_t kernel_size, int64_t repititions, uint16_t *output,
+                             void *field_out, int32_t field_type, int32_t flags, void *workspace,
+                             int64_t workspace_bytes, void *stream, const float *init_field, int64_t shrink_lo,
+                             int64_t shrink_hi);
+
+/*
  * Allocation-free variant of maxi_diffusion_device() for the FP32 field.  It
  * has no counterpart in the reference.  It serves callers that may not
  * allocate device memory while they run (a host that owns the whole device

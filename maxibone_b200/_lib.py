@@ -47,6 +47,8 @@ SIGNATURES = {
     "maxi_diffusion_in_memory": (_int, [_p, _i64, _i64, _i64, _p, _i64, _i64, _p, _int]),
     "maxi_diffusion_workspace_size": (_i64, [_i64, _i64, _i64, _i32]),
     "maxi_diffusion_device": (_int, [_p, _i32, _i64, _i64, _i64, _p, _i64, _i64, _p, _p, _i32, _i32, _p, _i64, _p]),
+    "maxi_diffusion_device_ex": (_int, [_p, _i32, _i64, _i64, _i64, _p, _i64, _i64, _p, _p, _i32, _i32, _p, _i64,
+                                        _p, _p, _i64, _i64]),
     "maxi_bitpack_encode": (_int, [_p, _i64, _p, _p]),
     "maxi_bitpack_decode": (_int, [_p, _i64, _p, _p]),
     "maxi_combine_fields": (_int, [_p, _p, _i64, _i64, _i64, _p, _p]),

@@ -34,6 +34,11 @@ struct BatchVolume {
     std::vector<float> kernel;
     int64_t ws_offset = 0;
     int group = -1;  // tensor-core group index, or -1 for the per-volume path
+    // Storage type this volume runs in: the plan's, or FP32 for a 16-bit plan's
+    // volume whose shape the tensor-core passes do not take (the FP32 form is
+    // faster and more accurate than the 16-bit CUDA-core passes), as
+    // maxi_diffusion_device() does.
+    int32_t run_type = MAXI_FIELD_F32;
 };
 
 struct TcGroup {
@@ -75,7 +80,7 @@ static S *vol_buf(maxi_batch_plan *p, const BatchVolume &bv, int b) {
 }
 static uint32_t *vol_packed(maxi_batch_plan *p, const BatchVolume &bv) {
     const int64_t n = bv.v.nz * bv.v.ny * bv.v.nx;
-    return reinterpret_cast<uint32_t *>(p->d_ws + bv.ws_offset + 2 * round_up((int64_t) field_size(p->field_type) * n, 256));
+    return reinterpret_cast<uint32_t *>(p->d_ws + bv.ws_offset + 2 * round_up((int64_t) field_size(bv.run_type) * n, 256));
 }
 
 // Enqueues mask packing and the rep-0 field of every member volume.
@@ -142,8 +147,12 @@ static cudaError_t enqueue_all(maxi_batch_plan *p, cudaStream_t st) {
                 if ((e = enqueue_single<S>(p, p->vols[i], MAXI_FLAG_NO_TENSOR_CORES, st)) != cudaSuccess) break;
         if (e != cudaSuccess) return e;
     }
-    for (BatchVolume &bv : p->vols)
-        if (bv.group < 0 && (e = enqueue_single<S>(p, bv, 0, st)) != cudaSuccess) return e;
+    for (BatchVolume &bv : p->vols) {
+        if (bv.group >= 0) continue;
+        e = (sizeof(S) == 2 && bv.run_type == MAXI_FIELD_F32) ? enqueue_single<float>(p, bv, 0, st)
+                                                               : enqueue_single<S>(p, bv, 0, st);
+        if (e != cudaSuccess) return e;
+    }
     return cudaSuccess;
 }
 
@@ -292,9 +301,13 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
                  g.note.empty() ? "" : "; ", g.note.c_str());
         p->description += line;
     }
-    size_t singles = 0;
-    for (const BatchVolume &bv : p->vols) singles += bv.group < 0;
-    snprintf(line, sizeof(line), "%zu volumes on the per-volume path\n", singles);
+    size_t singles = 0, fp32 = 0;
+    for (const BatchVolume &bv : p->vols) {
+        singles += bv.group < 0;
+        fp32 += bv.group < 0 && bv.run_type != p->field_type;
+    }
+    snprintf(line, sizeof(line), "%zu volumes on the per-volume path (%zu in the FP32 form: shapes the tensor-core "
+             "passes do not take)\n", singles, fp32);
     p->description += line;
     return MAXI_OK;
 }
@@ -349,7 +362,12 @@ int maxi_batch_plan_create(const maxi_volume *volumes, int64_t n_volumes, int32_
         bv.kernel.assign(volumes[i].kernel, volumes[i].kernel + volumes[i].kernel_size);
         bv.v.kernel = nullptr;  // the plan keeps its own copy
         bv.ws_offset = total;
-        total += round_up(maxi_diffusion_workspace_size(bv.v.nz, bv.v.ny, bv.v.nx, field_type), 1024);
+        bv.run_type = field_type;
+        const int radius = (int) (bv.v.kernel_size / 2);
+        if (field_type != MAXI_FIELD_F32 && !(flags & MAXI_FLAG_NO_TENSOR_CORES) && radius_bucket(radius) >= 0 &&
+            !tc::tc_supported(radius, bv.v.nz, bv.v.ny, bv.v.nx))
+            bv.run_type = MAXI_FIELD_F32;
+        total += round_up(maxi_diffusion_workspace_size(bv.v.nz, bv.v.ny, bv.v.nx, bv.run_type), 1024);
         p->vols.push_back(bv);
     }
     if (cudaMalloc(&p->d_ws, total) != cudaSuccess) {

@@ -241,6 +241,31 @@ int maxi_diffusion_device(const void *mask, int32_t mask_format, int64_t nz, int
                                       field_out, field_type, flags, workspace, workspace_bytes, stream, RunOpts{});
 }
 
+int maxi_diffusion_device_ex(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,
+                             const float *kernel, int64_t kernel_size, int64_t repititions, uint16_t *output,
+                             void *field_out, int32_t field_type, int32_t flags, void *workspace,
+                             int64_t workspace_bytes, void *stream, const float *init_field, int64_t shrink_lo,
+                             int64_t shrink_hi) {
+    if (shrink_lo < 0 || shrink_hi < 0) {
+        clear_error();
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "negative window shrink");
+    }
+    if (init_field && (reinterpret_cast<uintptr_t>(init_field) & 3) != 0) {
+        clear_error();
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "init_field is not 4-byte aligned");
+    }
+    if (init_field && repititions == 0) {
+        clear_error();
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "a run continued from a field needs at least one repetition");
+    }
+    RunOpts o;
+    o.shrink_lo = shrink_lo;
+    o.shrink_hi = shrink_hi;
+    o.init_field = init_field;
+    return diffusion_device_shrinking(mask, mask_format, nz, ny, nx, kernel, kernel_size, repititions, output,
+                                      field_out, field_type, flags, workspace, workspace_bytes, stream, o);
+}
+
 }  // extern "C"
 
 int maxi::diffusion_device_shrinking(const void *mask, int32_t mask_format, int64_t nz, int64_t ny, int64_t nx,

@@ -71,21 +71,42 @@ struct SlabPlan {
 
 static int64_t field_size(int32_t ft) { return ft == MAXI_FIELD_F32 ? 4 : ft == MAXI_FIELD_F64 ? 8 : 2; }
 
-// Planes of a slab's output window: the last repetition's plane window, S +
-// 2 radius planes when the repetition loop shrinks its window towards the core
-// (else the whole extended slab of E planes).
-static int64_t window_planes(int64_t S, int64_t E, int64_t radius, bool shrinks) {
-    return shrinks ? std::min(E, S + 2 * radius) : E;
+// Largest output window over the slabs of a round of kr repetitions: the
+// planes its last repetition computes, which the output buffers must hold.
+// With shrinking windows that is the core and `radius` planes on each cut
+// side, and down to the volume's edge where the halo reaches it; without
+// shrinking, the whole extended slab.
+static int64_t max_window(int64_t nz, int64_t S, int64_t radius, int64_t kr, bool shrinks) {
+    const int64_t H = std::min(nz, kr * radius), n_slabs = ceil_div(nz, S);
+    int64_t w = 0;
+    for (int64_t s = 0; s < n_slabs; s++) {
+        const int64_t z0 = s * S, z1 = std::min(nz, z0 + S);
+        const int64_t e0 = std::max<int64_t>(0, z0 - H), e1 = std::min(nz, z1 + H);
+        if (!shrinks) {
+            w = std::max(w, e1 - e0);
+            continue;
+        }
+        const int64_t ez = e1 - e0, j = std::max<int64_t>(0, kr - 1);
+        const int64_t lo = std::min(ez - 1, (e0 > 0 ? radius : 0) * j);
+        const int64_t hi = std::max(lo + 1, ez - (e1 < nz ? radius : 0) * j);
+        w = std::max(w, hi - lo);
+    }
+    return w;
 }
 
 // Device bytes of one slab context: the workspace of an extended slab of E
 // planes, its uint8 mask when the mask is not resident, and the output window
-// (uint16; plus the FP32 field in exchange rounds).
-static int64_t slab_bytes(int64_t S, int64_t E, int64_t plane, int64_t radius, int32_t ft, bool resident,
-                          bool exchange, bool shrinks) {
+// of `win` planes (uint16; plus the FP32 field in exchange rounds).
+static int64_t slab_bytes(int64_t E, int64_t win, int64_t plane, int32_t ft, bool resident, bool exchange) {
     const int64_t ws = maxi_diffusion_workspace_size(E, plane, 1, ft);
-    const int64_t win = window_planes(S, E, radius, shrinks) * plane * (2 + (exchange ? 4 : 0));
-    return ws + (resident ? 0 : E * plane) + win + 4096;
+    return ws + (resident ? 0 : E * plane) + win * plane * (2 + (exchange ? 4 : 0)) + 4096;
+}
+
+// The window buffers of a plan: the largest window of its full rounds (k
+// repetitions) and of its last round (the remainder).
+static int64_t plan_window(int64_t nz, int64_t S, int64_t radius, int64_t reps, int64_t k, bool shrinks) {
+    const int64_t last = reps > 0 ? reps - (ceil_div(reps, k) - 1) * k : 0;
+    return std::max(max_window(nz, S, radius, k, shrinks), max_window(nz, S, radius, std::max<int64_t>(1, last), shrinks));
 }
 
 // Chooses the plan.  budget: device bytes available for the slab context.
@@ -100,13 +121,19 @@ static SlabPlan plan_slabs(int64_t nz, int64_t plane, int64_t radius, int64_t re
         const int64_t H = std::min(nz, k * radius);
         // Largest S with slab_bytes(S, min(nz, S + 2H)) <= budget (bisection; the
         // bytes grow with S).
+        auto bytes_for = [&](int64_t S) {
+            const int64_t n_slabs = ceil_div(nz, S), Sb = ceil_div(nz, n_slabs);  // balanced, as run
+            return slab_bytes(std::min(nz, Sb + 2 * H), plan_window(nz, Sb, radius, reps, k, shrinks), plane, ft,
+                              resident, exchange);
+        };
         int64_t lo = 0, hi = std::min(nz, max_slab);
         while (lo < hi) {
             const int64_t mid = (lo + hi + 1) / 2;
-            if (slab_bytes(mid, std::min(nz, mid + 2 * H), plane, radius, ft, resident, exchange, shrinks) <= budget)
-                lo = mid;
+            if (bytes_for(mid) <= budget) lo = mid;
             else hi = mid - 1;
         }
+        // the balanced depth's bytes are not strictly monotonic: step down until it fits
+        while (lo >= 1 && bytes_for(lo) > budget) lo--;
         if (lo >= 1) {
             const int64_t n_slabs = ceil_div(nz, lo), S = ceil_div(nz, n_slabs);  // balanced slabs
             const int64_t rounds = ceil_div(reps, k);
@@ -197,8 +224,8 @@ static int run_slabs(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, const f
                          "a %lld-plane halo on each side needs %lld bytes); the volume's planes are too large for "
                          "this device",
                          (long long) ny, (long long) nx, (long long) device_budget(free_b), (long long) radius,
-                         (long long) slab_bytes(1, std::min(nz, 1 + 2 * radius), plane, radius, field_type, resident,
-                                                true, shrinks));
+                         (long long) slab_bytes(std::min(nz, 1 + 2 * radius), std::min(nz, 1 + 2 * radius), plane,
+                                                field_type, resident, true));
     const int64_t S = pl.S, k = std::min(pl.k, std::max<int64_t>(1, repititions)), E = pl.E;
     const bool exchange = k < repititions;
     const int64_t n_slabs = ceil_div(nz, S), rounds = repititions == 0 ? 1 : ceil_div(repititions, k);
@@ -242,7 +269,7 @@ static int run_slabs(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, const f
         }
     } b;
     const int64_t ws_bytes = maxi_diffusion_workspace_size(E, ny, nx, field_type);
-    const int64_t win = window_planes(S, E, radius, shrinks);
+    const int64_t win = plan_window(nz, S, radius, repititions, k, shrinks);
     auto oom = [&](const char *what) {
         cudaGetLastError();
         return set_error(MAXI_ERR_OUT_OF_MEMORY, "could not allocate %s for slabs of %lld planes (%lld with halos)",

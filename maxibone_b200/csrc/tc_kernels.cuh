@@ -512,8 +512,9 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                     float va[32];
                     __syncwarp();
                     tmem_ld32(tbase + (c0 + cc) * 32, va);
-                    uint16_t q[32];
-                    narrow32<S>(va, tp.inv_scale, tp.error_feedback, q);
+                    uint32_t qd[16], q[16];  // q[i]: voxels 2i, 2i + 1
+                    narrow32_pairs<S, false>(va, tp.inv_scale, tp.error_feedback, 0u, 0xffffffffu, qd);
+                    pairs_to_adjacent(qd, q);
                     const int64_t xb = (int64_t) c.x0 + (c0 + cc) * 32;
                     if (AXIS_Z) {
                         // z pass: lanes' rows lie on different planes (2 MB apart at 1024^2);
@@ -521,7 +522,8 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                         __syncwarp();
 #pragma unroll
                         for (int i = 0; i < 4; i++)
-                            *reinterpret_cast<uint4 *>(stg + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) = pack8(q + 8 * i);
+                            *reinterpret_cast<uint4 *>(stg + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) =
+                                make_uint4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
                         __syncwarp();
                         const int sub = lane & 3, rsub = lane >> 2;
 #pragma unroll
@@ -541,7 +543,8 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                         uint8_t *sb = stg + sbuf * 2048;
 #pragma unroll
                         for (int i = 0; i < 4; i++)
-                            *reinterpret_cast<uint4 *>(sb + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) = pack8(q + 8 * i);
+                            *reinterpret_cast<uint4 *>(sb + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) =
+                                make_uint4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
                         fence_proxy_async_smem();
                         __syncwarp();
                         // Every chunk commits exactly one bulk group (an empty one when the
@@ -691,13 +694,15 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
                 // 16-bit field: narrow with error feedback, stage the warp's 32 x 32
                 // chunk and write 8 rows (8 x 64 bytes) per instruction -- in [y][z][x]
                 // order the warp's rows lie 2 MB apart at 1024^3.
-                uint16_t q[32];
-                narrow32_masked<S>(h, mw, tp.inv_scale, tp.error_feedback, q);
+                uint32_t qd[16], q[16];  // q[i]: voxels 2i, 2i + 1
+                narrow32_pairs<S, true>(h, tp.inv_scale, tp.error_feedback, mw, 0xffffffffu, qd);
+                pairs_to_adjacent(qd, q);
                 const int64_t oi = row < t.rows ? contig_out_index(t, row, xb) : -1;
                 __syncwarp();
 #pragma unroll
                 for (int i = 0; i < 4; i++)
-                    *reinterpret_cast<uint4 *>(stg + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) = pack8(q + 8 * i);
+                    *reinterpret_cast<uint4 *>(stg + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) =
+                        make_uint4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
                 __syncwarp();
                 const int sub = lane & 3, rsub = lane >> 2;
 #pragma unroll

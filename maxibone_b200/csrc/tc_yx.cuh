@@ -12,10 +12,11 @@
 //      the plane are zero-filled: the zero boundary).  Y accumulates in FP32 in
 //      tensor memory, one lane per y-output.
 //   2. Conversion warps read Y back lane by lane (tcgen05.ld), narrow it to the
-//      16-bit storage type with error-feedback rounding along x, zero the
-//      columns outside the volume (the x pass's zero boundary), and write it
-//      back packed two per column (tcgen05.st) over the first KX/2 columns of
-//      the accumulator: the K-major layout of an A operand in tensor memory.
+//      16-bit storage type with error-feedback rounding along x (two chains per
+//      32 columns, two voxels per instruction), zero the columns outside the
+//      volume (the x pass's zero boundary), and write it back packed two per
+//      column (tcgen05.st) over the first KX/2 columns of the accumulator: the
+//      K-major layout of an A operand in tensor memory.
 //   3. x MMAs: D[o, x] = sum_j Y'[o, j] Tt[j, x] with the x Toeplitz Tt in
 //      shared memory as the B operand (K-major), into a second accumulator.
 //   4. Epilogue warps: re-illumination from the bit-packed mask, then either
@@ -34,10 +35,13 @@
 // Tensor memory (512 columns): [0, 192) y accumulator, then Y' packed over its
 // first KX/2 columns; [192, 320) x accumulator; [320, 512) the y Toeplitz
 // halves (96 columns each at radius 32).  Warp roles: 0 TMA producer, 1 MMA
-// issuer, 2-5 conversion (one per TMEM lane quadrant), 6-13 epilogue (two per
-// quadrant, 64 x-outputs each).  Every wait is bounded; on a timeout the
-// kernel records a code in g_tc_error, lets the copies and MMAs it started
-// finish (bounded) and winds down.
+// issuer, 2-9 conversion (two per TMEM lane quadrant, 32 columns of each
+// 64-column chunk each), 10-17 epilogue (two per quadrant, 64 x-outputs each).
+// The pipeline runs at chunk granularity: the y MMAs commit chunk by chunk,
+// the conversion of a chunk starts while the next chunks multiply, and the x
+// MMAs of a chunk start as soon as it is converted.  Every wait is bounded; on
+// a timeout the kernel records a code in g_tc_error, lets the copies and MMAs
+// it started finish (bounded) and winds down.
 #pragma once
 
 #include "tc_kernels.cuh"
@@ -46,9 +50,10 @@ namespace maxi {
 namespace tc {
 
 constexpr int kYxStages = 4;                                     // F chunk ring (64 x-columns x KP rows each)
-constexpr int kYxConvWarps = 4;                                  // one per TMEM lane quadrant
+constexpr int kYxConvWarps = 8;                                  // two per TMEM lane quadrant
 constexpr int kYxEpiWarps = 8;                                   // two per lane quadrant
-constexpr int kYxThreads = 64 + 32 * (kYxConvWarps + kYxEpiWarps);  // 448
+constexpr int kYxThreads = 64 + 32 * (kYxConvWarps + kYxEpiWarps);  // 576
+constexpr int kYxMaxChunks = 3;                                  // 64-column chunks of the x window (radius <= 32)
 constexpr uint32_t kYxAccY = 0;                                  // y accumulator, up to 192 columns
 constexpr uint32_t kYxAccX = 192;                                // x accumulator, 128 columns
 constexpr uint32_t kYxToep = 320;                                // y Toeplitz halves
@@ -74,34 +79,23 @@ struct YxLaunch {
     int64_t n_tiles;
 };
 
-// 32 consecutive 16-bit values of the intermediate field, packed two per
-// 32-bit word (even x in the low half): error-feedback rounding along x in
-// two interleaved 16-voxel chains, and exact zeros at x outside [0, nx) --
-// the zero boundary the x convolution sees.
-template <typename S>
-__device__ __forceinline__ void narrow32_packed(const float (&a)[32], float scale, bool ef, int64_t xs, int64_t nx,
-                                                uint32_t (&w)[16]) {
-    float c[2] = {0.0f, 0.0f};
-    uint16_t q[32];
-#pragma unroll
-    for (int j = 0; j < 16; j++) {
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const int i = k * 16 + j;
-            const float v = ef ? fmaf(a[i], scale, c[k]) : a[i] * scale;
-            float dummy = 0.0f;
-            uint16_t b = Narrow16<S>::bits(v, dummy, false);
-            if (ef) c[k] = v - Narrow16<S>::widen(b);
-            const int64_t x = xs + i;
-            if (x < 0 || x >= nx) {
-                b = 0;
-                c[k] = 0.0f;
-            }
-            q[i] = b;
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < 16; i++) w[i] = (uint32_t) q[2 * i] | ((uint32_t) q[2 * i + 1] << 16);
+// Bits [lo, hi) of a 32-bit word (the voxels of a 32-voxel run inside [0, nx)).
+__device__ __forceinline__ uint32_t live_bits(int64_t xs, int64_t nx) {
+    if (xs >= 0 && xs + 32 <= nx) return 0xffffffffu;
+    const int64_t lo = xs < 0 ? -xs : 0, hi = nx - xs < 32 ? nx - xs : 32;
+    if (hi <= lo) return 0u;
+    const uint32_t upto = hi >= 32 ? 0xffffffffu : ((1u << hi) - 1u);
+    return upto & ~((1u << lo) - 1u);
+}
+
+// Named barrier of the two conversion warps of one TMEM lane quadrant that
+// also ANDs `v` over both: the pair leaves a wait that timed out together.
+__device__ __forceinline__ bool pair_barrier_and(int quad, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %2, 0;\n bar.red.and.pred q, %1, 64, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r) : "r"(1 + quad), "r"((uint32_t) v) : "memory");
+    return r != 0;
 }
 
 template <typename S, int FMT>
@@ -118,9 +112,10 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
     const int nch = (tx.kp + 63) / 64;                          // chunks per tile (<= 3)
     uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kYxStages * chunk_bytes);
     uint64_t *full = bars, *empty = bars + kYxStages;
-    uint64_t *yfull = bars + 2 * kYxStages, *ypacked = yfull + 1, *xfull = yfull + 2, *xempty = yfull + 3,
-             *drain = yfull + 4;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(yfull + 5);
+    uint64_t *ychunk = bars + 2 * kYxStages;                    // [kYxMaxChunks]: y chunk accumulated
+    uint64_t *ypacked = ychunk + kYxMaxChunks;                  // [kYxMaxChunks]: chunk converted to Y'
+    uint64_t *xfull = ypacked + kYxMaxChunks, *xempty = xfull + 1, *drain = xfull + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(xfull + 3);
     uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 1024;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t total = p.n_tiles;
@@ -136,8 +131,7 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
     }
     if (threadIdx.x == 0) {
         for (int s = 0; s < kYxStages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-        mbar_init(yfull, 1);
-        mbar_init(ypacked, kYxConvWarps);
+        for (int c = 0; c < kYxMaxChunks; c++) { mbar_init(&ychunk[c], 1); mbar_init(&ypacked[c], kYxConvWarps); }
         mbar_init(xfull, 1);
         mbar_init(xempty, kYxEpiWarps);
         mbar_init(drain, 1);
@@ -216,22 +210,24 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
         for (int64_t k = cl - kYxStages; k < cl; k++)
             if (k >= 0) mbar_wait(&full[k % kYxStages], (uint32_t) ((k / kYxStages) & 1), 1);
     } else if (warp == 1 && lane == 0) {
-        // MMA issuer.
+        // MMA issuer.  Per tile: the y MMAs chunk by chunk (each chunk committed
+        // on its own barrier, so its conversion starts while the next chunks
+        // multiply), then the x MMAs chunk by chunk as each chunk of Y' lands.
+        // The y MMAs of a tile overwrite the previous tile's Y', which the x MMAs
+        // issued before them have read (tcgen05.mma of one thread run in issue order).
         const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
         const uint32_t idesc_y = idesc_f16(fmt, 0 /*A K-major*/, 1 /*B MN-major*/, kTM, 64);
         const uint32_t idesc_x = idesc_f16(fmt, 0 /*A K-major*/, 0 /*B K-major*/, kTM, kXTN);
         const uint32_t r0 = smem_u32(ring), t0 = smem_u32(tt);
         const uint32_t a_hi = tmem + kYxToep, a_lo = a_hi + ty.kcols;
+        const int ksx = tx.kp / 16;
         int64_t cl = 0, tl = 0;
         bool ok = true;
         for (int64_t g = blockIdx.x; ok && g < total; g += gridDim.x, tl++) {
-            // y MMAs, one 64-column chunk at a time.  They overwrite Y' of the
-            // previous tile, which the x MMAs issued before them have read
-            // (tcgen05.mma of one thread execute in issue order).
+            const uint32_t ph = (uint32_t) (tl & 1);
             for (int c = 0; c < nch; c++, cl++) {
                 const int s = (int) (cl % kYxStages);
-                const uint32_t ph = (uint32_t) ((cl / kYxStages) & 1);
-                if (!mbar_wait(&full[s], ph, 1)) { ok = false; break; }
+                if (!mbar_wait(&full[s], (uint32_t) ((cl / kYxStages) & 1), 1)) { ok = false; break; }
                 tc_fence_after();
                 const uint64_t bd = smem_desc_sw128(r0 + s * chunk_bytes, chunk_bytes, 1024);
                 const uint32_t d = tmem + kYxAccY + 64 * c;
@@ -240,53 +236,61 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
                     if (!p.hi_only) umma_f16_ts(d, a_lo + ks * 8, bd + (uint64_t) (ks * 128), idesc_y, 1u);
                 }
                 umma_commit(&empty[s]);
+                umma_commit(&ychunk[c]);
             }
             if (!ok) break;
-            umma_commit(yfull);
-            // x MMAs once Y' is in place and the epilogue has drained the x accumulator.
-            if (!mbar_wait(ypacked, (uint32_t) (tl & 1), 3) || !mbar_wait(xempty, (uint32_t) ((tl & 1) ^ 1), 3)) {
-                ok = false;
-                break;
-            }
-            tc_fence_after();
+            if (!mbar_wait(xempty, ph ^ 1, 3)) break;  // the epilogue has drained the x accumulator
             const uint32_t dx = tmem + kYxAccX;
-            for (int ks = 0; ks < tx.kp / 16; ks++) {
-                const uint32_t kin = (ks & 3) * 32;
-                const uint32_t bhi = t0 + (ks >> 2) * (tt_rows * 128) + kin;
-                umma_f16_ts(dx, tmem + kYxAccY + ks * 8, smem_desc_sw128(bhi, 16, 1024), idesc_x, ks > 0 ? 1u : 0u);
-                if (!p.hi_only)
-                    umma_f16_ts(dx, tmem + kYxAccY + ks * 8, smem_desc_sw128(bhi + kXTN * 128, 16, 1024), idesc_x, 1u);
+            for (int c = 0; c < nch && ok; c++) {
+                if (!mbar_wait(&ypacked[c], ph, 3)) { ok = false; break; }
+                tc_fence_after();
+                for (int ks = 4 * c; ks < 4 * c + 4 && ks < ksx; ks++) {
+                    const uint32_t kin = (ks & 3) * 32;
+                    const uint32_t bhi = t0 + (ks >> 2) * (tt_rows * 128) + kin;
+                    umma_f16_ts(dx, tmem + kYxAccY + ks * 8, smem_desc_sw128(bhi, 16, 1024), idesc_x, ks > 0 ? 1u : 0u);
+                    if (!p.hi_only)
+                        umma_f16_ts(dx, tmem + kYxAccY + ks * 8, smem_desc_sw128(bhi + kXTN * 128, 16, 1024), idesc_x, 1u);
+                }
             }
+            if (!ok) break;
             umma_commit(xfull);
         }
         // Every MMA this thread issued has completed before the CTA winds down.
         umma_commit(drain);
         mbar_wait(drain, 0, 2);
     } else if (warp >= 2 && warp < 2 + kYxConvWarps) {
-        // Conversion: y accumulator (FP32) -> Y' (16-bit, packed) in place.
-        // Chunk cc's packed words overwrite FP32 columns of chunk cc / 2, which
-        // this thread has already read: one warp per quadrant, in order.
-        const int quad = warp & 3;
+        // Conversion: y accumulator (FP32) -> Y' (16-bit, packed) in place, one
+        // 64-column chunk at a time; the two warps of a quadrant take 32 columns
+        // each.  Chunk c's packed words land on FP32 columns of chunk c / 2: both
+        // warps have read those (the pair barrier orders the reads of chunk c
+        // before either warp's writes of chunk c).
+        const int quad = warp & 3, half = (warp - 2) >> 2;
         const uint32_t lb = tmem + ((uint32_t) (quad * 32) << 16);
-        const int ncc = (tx.kp + 31) / 32;
         int64_t tl = 0;
-        for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
+        bool ok = true;
+        for (int64_t g = blockIdx.x; ok && g < total; g += gridDim.x, tl++) {
             int z, y0, x0;
             decode(g, z, y0, x0);
-            if (!mbar_wait(yfull, (uint32_t) (tl & 1), 2)) break;
-            tc_fence_after();
-            for (int cc = 0; cc < ncc; cc++) {
+            for (int c = 0; c < nch; c++) {
+                // warp-uniform, then pair-uniform outcome of the wait: both warps
+                // of the pair reach the barrier either way and leave together
+                ok = __all_sync(0xffffffffu, mbar_wait(&ychunk[c], (uint32_t) (tl & 1), 2));
+                tc_fence_after();
                 float v[32];
                 __syncwarp();
-                tmem_ld32(lb + kYxAccY + 32 * cc, v);
-                uint32_t w[16];
-                narrow32_packed<S>(v, ty.inv_scale, ty.error_feedback, (int64_t) x0 - tx.ra + 32 * cc, p.nx, w);
-                tmem_st16(lb + kYxAccY + 16 * cc, w);
+                if (ok) tmem_ld32(lb + kYxAccY + 64 * c + 32 * half, v);
+                ok = pair_barrier_and(quad, ok);
+                if (!ok) break;
+                const int64_t xs = (int64_t) x0 - tx.ra + 64 * c + 32 * half;
+                uint32_t d[16], w[16];
+                narrow32_pairs<S, true>(v, ty.inv_scale, ty.error_feedback, 0u, live_bits(xs, p.nx), d);
+                pairs_to_adjacent(d, w);
+                tmem_st16(lb + kYxAccY + 32 * c + 16 * half, w);
+                tmem_st_wait();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&ypacked[c]);
             }
-            tmem_st_wait();
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(ypacked);
         }
     } else if (warp >= 2 + kYxConvWarps) {
         // Epilogue: x accumulator -> re-illumination -> next field / final outputs.
@@ -309,7 +313,7 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
                 if (live_row && xb < p.nx)
                     mw[k] = load_mask_words<FMT>(p.mask, row * p.nx + xb, p.nx - xb < 32 ? (int) (p.nx - xb) : 32, n_vox);
             }
-            if (!mbar_wait(xfull, (uint32_t) (tl & 1), 2)) break;
+            if (!__all_sync(0xffffffffu, mbar_wait(xfull, (uint32_t) (tl & 1), 2))) break;
             tc_fence_after();
 #pragma unroll
             for (int k = 0; k < 2; k++) {
@@ -321,15 +325,17 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
                 if (p.final_pass) {
                     contig_final32(h, m, live_row ? row : rows, rows, p.nx, xb, tx.inv_scale, p.out_u16, p.field_out);
                 } else if (xb < p.nx) {  // warp-uniform
-                    uint16_t q[32];
-                    narrow32_masked<S>(h, m, tx.inv_scale, tx.error_feedback, q);
+                    uint32_t d[16], q[16];
+                    narrow32_pairs<S, true>(h, tx.inv_scale, tx.error_feedback, m, 0xffffffffu, d);
+                    pairs_to_adjacent(d, q);
                     const int64_t oi = !live_row ? -1
                                        : p.out_nz == 0 ? row * p.nx + xb
                                                         : ((y * p.out_nz + p.out_z0 + z) * p.nx) + xb;
                     __syncwarp();
 #pragma unroll
                     for (int i = 0; i < 4; i++)
-                        *reinterpret_cast<uint4 *>(stg + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) = pack8(q + 8 * i);
+                        *reinterpret_cast<uint4 *>(stg + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) =
+                            make_uint4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
                     __syncwarp();
                     const int sub = lane & 3, rsub = lane >> 2;
 #pragma unroll

@@ -77,6 +77,8 @@ def _lib():
         lib.oracle_diffusion_on_disk_semantics.restype = ctypes.c_int
         lib.oracle_diffusion_on_disk_field.argtypes = [p, i64, i64, i64, p, i64, i64, p]
         lib.oracle_diffusion_on_disk_field.restype = ctypes.c_int
+        lib.oracle_diffusion_from_field.argtypes = [p, p, i64, i64, i64, p, i64, i64, p]
+        lib.oracle_diffusion_from_field.restype = ctypes.c_int
         lib.oracle_f32_to_u8.argtypes = [p, p, i64]
         lib.oracle_f32_to_u8.restype = None
         lib.oracle_convolve_axis_f32.argtypes = [p, p, p, i64, i64, i64, ctypes.c_int, i64]
@@ -146,6 +148,22 @@ def diffusion_on_disk_u8(mask: np.ndarray, kernel: np.ndarray, repititions: int)
         raise MemoryError("oracle could not allocate its working buffers")
     out = np.empty(m.shape, np.uint8)
     _lib().oracle_f32_to_u8(_ptr(field), _ptr(out), field.size)
+    return out
+
+
+def diffusion_from_field(field: np.ndarray, mask: np.ndarray, kernel: np.ndarray, repititions: int) -> np.ndarray:
+    """FP32 field after `repititions` more repetitions from `field` (zero
+    boundary at the array's edges): the reference's steps without the initial
+    mask -> field conversion (src/lib/cpp/cpu/diffusion.cc:314-320,354-358)."""
+    f = np.ascontiguousarray(field, dtype=np.float32)
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    k = np.ascontiguousarray(kernel, dtype=np.float32)
+    out = np.empty_like(f)
+    nz, ny, nx = f.shape
+    rc = _lib().oracle_diffusion_from_field(_ptr(f), _ptr(m), nz, ny, nx, _ptr(k), k.shape[0], int(repititions),
+                                            _ptr(out))
+    if rc != 0:
+        raise MemoryError("oracle could not allocate its working buffers")
     return out
 
 

@@ -189,6 +189,32 @@ int oracle_diffusion_on_disk_semantics(const uint8_t *voxels, int64_t nz, int64_
     return rc;
 }
 
+/* Repetitions continued from a given FP32 field (the field after earlier
+ * repetitions) on a sub-volume whose first / last planes may be halo planes:
+ * the same steps as oracle_diffusion_in_memory (conv z, y, x with a zero
+ * boundary at the sub-volume's edges, illuminate) without the initial
+ * mask -> field conversion.  Planes at least reps x radius from a cut edge
+ * hold the whole volume's values afterwards. */
+int oracle_diffusion_from_field(const float *field_in, const uint8_t *voxels, int64_t nz, int64_t ny, int64_t nx,
+                                const float *kernel, int64_t kernel_size, int64_t repititions, float *field_out) {
+    const int64_t n = nz * ny * nx, radius = kernel_size / 2;
+    float *b0 = (float *) malloc((size_t) n * sizeof(float));
+    float *b1 = (float *) malloc((size_t) n * sizeof(float));
+    if (!b0 || !b1) { free(b0); free(b1); return -1; }
+    memcpy(b0, field_in, (size_t) n * sizeof(float));
+    for (int64_t rep = 0; rep < repititions; rep++) {
+        for (int dim = 0; dim < 3; dim++) {
+            oracle_convolve_axis_f32(b0, kernel, b1, nz, ny, nx, dim, radius);
+            float *t = b0; b0 = b1; b1 = t;
+        }
+        oracle_illuminate_f32(voxels, b0, n);
+    }
+    memcpy(field_out, b0, (size_t) n * sizeof(float));
+    free(b0);
+    free(b1);
+    return 0;
+}
+
 /* The CPU backend's final conversion of its on-disk variant,
  * convert_float_to_uint8 (src/lib/cpp/cpu/diffusion.cc:139-144):
  * (uint8_t) floor(v * 255.0f) in FP32. */

@@ -67,9 +67,11 @@ def test_fused_radius_range(radius):
     kernel = gauss_kernel(radius / 4.0).astype(np.float32)
     assert kernel.shape[0] == 2 * radius + 1
     _, want = run(mask, kernel, 3, "f64")
+    # below radius 4 the 16-bit stores round to nearest (no error feedback)
+    bound = VS_F64 if radius >= 4 else {"bf16": 8e-3, "f16": 1e-3}
     for field in ("bf16", "f16"):
         u16, got = run(mask, kernel, 3, field)
-        assert np.abs(got.astype(np.float64) - want).max() <= VS_F64[field], field
+        assert np.abs(got.astype(np.float64) - want).max() <= bound[field], field
         assert np.all(u16[mask > 0] == 65535)
 
 

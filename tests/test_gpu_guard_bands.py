@@ -73,7 +73,7 @@ DIFFUSION_CASES = [
     ("f64", (20, 30, 40), 2.0, "u8", 2, True),          # FP64 form
     ("bf16", (30, 70, 100), 2.0, "u8", 3, False),       # 16-bit CUDA-core passes, error feedback
     ("bf16", (40, 136, 264), 8.0, "u8", 3, True),       # tensor-core z pass + fused y/x kernel, partial tiles
-    ("f16", (21, 130, 200), 3.0, "bitpacked", 3, True), # fused y/x kernel, bit-packed mask, ragged tiles
+    ("f16", (24, 130, 200), 3.0, "bitpacked", 3, True), # fused y/x kernel, bit-packed mask, ragged tiles
     ("f16", (24, 160, 200), 10.0, "u8", 2, True),       # tensor-core wide-radius passes (r = 40)
 ]
 

@@ -169,7 +169,10 @@ def test_fp64_form_matches_cpu_fp64_oracle():
     assert np.abs(got - want).max() < 1e-12
 
 
-TC_PATH = _lib.PATH_TENSOR_CORES_ZY | _lib.PATH_TENSOR_CORES_X
+def tensor_cores_ran(path: int) -> bool:
+    """z and y passes on the tensor cores and the x pass too, alone or fused
+    with the y pass."""
+    return bool(path & _lib.PATH_TENSOR_CORES_ZY) and bool(path & (_lib.PATH_TENSOR_CORES_X | _lib.PATH_FUSED_YX))
 
 
 @pytest.mark.parametrize("field", ["bf16", "f16"])
@@ -181,9 +184,10 @@ def test_low_precision_fields_vs_fp64(field, shape, tc):
     got_u16, got = run_gpu(mask, kernel, 20, field=field, tensor_cores=tc)
     path = device.last_path()
     if tc:
-        assert path & TC_PATH == TC_PATH, hex(path)
+        assert tensor_cores_ran(path), hex(path)
     else:
-        assert path & _lib.PATH_CUDA_CORES and not path & (TC_PATH | _lib.PATH_FP32_FALLBACK), hex(path)
+        assert path & _lib.PATH_CUDA_CORES and not tensor_cores_ran(path) and not path & _lib.PATH_FP32_FALLBACK, \
+            hex(path)
     err = np.abs(got.astype(np.float64) - want)
     assert err.max() <= LOWP_TOL[field], err.max()
     assert np.all(got_u16[mask > 0] == 65535)
@@ -200,7 +204,7 @@ def test_low_precision_contract_case(field):
     kernel = gauss_kernel(8.0).astype(np.float32)
     _, want = run_gpu(mask, kernel, 100, field="f64")
     got_u16, got = run_gpu(mask, kernel, 100, field=field)
-    assert device.last_path() & TC_PATH == TC_PATH
+    assert tensor_cores_ran(device.last_path())
     device.tensor_core_status()
     err = np.abs(got.astype(np.float64) - want)
     assert err.max() <= LOWP_TOL[field], err.max()

@@ -24,14 +24,14 @@ VS_F64_NEAREST = {"bf16": 8e-3, "f16": 1e-3}
 # Max abs difference between the tensor-core and CUDA-core forms (same storage
 # type, each within its bound of FP64).
 TC_VS_CC = {"bf16": 4e-3, "f16": 1e-3}
-TC_PATH = _lib.PATH_TENSOR_CORES_ZY | _lib.PATH_TENSOR_CORES_X
+TC_X = _lib.PATH_TENSOR_CORES_X | _lib.PATH_FUSED_YX  # the x pass alone or fused with the y pass
 
 
 def run(mask, kernel, reps, field, tensor_cores=True, error_feedback=True):
     """Runs one diffusion; with 16-bit fields asserts which passes ran (the
-    tensor-core z, y and x passes, or only CUDA-core passes), so that a silent
-    fallback cannot make a tensor-core vs CUDA-core comparison compare a path
-    with itself."""
+    tensor-core z and y passes and a tensor-core x pass, alone or fused with
+    the y pass; or only CUDA-core passes), so that a silent fallback cannot make
+    a tensor-core vs CUDA-core comparison compare a path with itself."""
     m = torch.from_numpy(np.ascontiguousarray(mask, np.uint8)).cuda()
     fo = torch.empty(mask.shape, dtype=torch.float64 if field == "f64" else torch.float32, device="cuda")
     out = torch.empty(mask.shape, dtype=torch.uint16, device="cuda")
@@ -40,9 +40,9 @@ def run(mask, kernel, reps, field, tensor_cores=True, error_feedback=True):
     path = device.last_path()
     if field in ("bf16", "f16"):
         if tensor_cores:
-            assert path & TC_PATH == TC_PATH and not path & _lib.PATH_CUDA_CORES, hex(path)
+            assert path & _lib.PATH_TENSOR_CORES_ZY and path & TC_X and not path & _lib.PATH_CUDA_CORES, hex(path)
         else:
-            assert path & _lib.PATH_CUDA_CORES and not path & TC_PATH, hex(path)
+            assert path & _lib.PATH_CUDA_CORES and not path & (_lib.PATH_TENSOR_CORES_ZY | TC_X), hex(path)
     torch.cuda.synchronize()
     device.tensor_core_status()
     return out.cpu().numpy(), fo.cpu().numpy()
@@ -59,6 +59,7 @@ def test_tensor_core_matches_cuda_core_and_fp64(field, shape, sigma, ef):
     _, want = run(mask, kernel, reps, "f64")
     tc_u16, tc = run(mask, kernel, reps, field, True, ef)
     _, cc = run(mask, kernel, reps, field, False, ef)
+    ef = ef and kernel.shape[0] // 2 >= 4  # narrower kernels always round to nearest
     assert np.abs(tc - cc).max() <= (TC_VS_CC if ef else VS_F64_NEAREST)[field]
     assert np.abs(tc.astype(np.float64) - want).max() <= (VS_F64 if ef else VS_F64_NEAREST)[field]
     assert np.all(tc_u16[mask > 0] == 65535)
@@ -73,8 +74,11 @@ def test_tensor_core_radius_range(radius):
     for field in ("f16", "bf16"):
         _, got = run(mask, kernel, 4, field, True, True)
         _, cc = run(mask, kernel, 4, field, False, True)
-        assert np.abs(got - cc).max() <= TC_VS_CC[field]
-        assert np.abs(got.astype(np.float64) - want).max() <= VS_F64[field]
+        # below radius 4 the stores round to nearest (error feedback needs the
+        # next x pass to remove its noise, which a kernel that narrow does not)
+        bound = VS_F64 if radius >= 4 else VS_F64_NEAREST
+        assert np.abs(got - cc).max() <= (TC_VS_CC if radius >= 4 else VS_F64_NEAREST)[field]
+        assert np.abs(got.astype(np.float64) - want).max() <= bound[field]
 
 
 # Radii above 32: z / y passes with the Toeplitz halves in tensor memory (64-column

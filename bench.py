@@ -22,9 +22,9 @@ Also reported on the same line:
                 in and out, from pinned and from pageable host buffers;
   cfg0          the 128^3 sphere mask, sigma 3, R = 10, FP32, beside the
                 reference module on the same input;
-  precision     the 1024^3 mask bit-packed, BF16 and FP16 fields (fused y + x
-                tensor-core kernel, both coefficient forms, and the separate
-                passes), R = 100 and R = 500, max / mean abs error against the
+  precision     the 1024^3 mask bit-packed, BF16 and FP16 fields (z pass and the
+                fused y + x tensor-core kernel; the separate passes; the split
+                coefficient halves), R = 100 and R = 500, max / mean abs error against the
                 FP64 form and the FP32 form; sigma = 32 (257 taps), CUDA-core
                 stencil vs banded-Toeplitz tensor cores;
   batched       64 uneven volumes, sigma in {2, 4, 8}, R = 50, BF16 plan vs
@@ -745,10 +745,10 @@ def form_runs(device, torch, np, mask, kernel, reps, forms, stream, shape=None, 
 PRECISION_FORMS = [
     ("f32", "f32", {}),
     ("bf16", "bf16", {}),
-    ("bf16_single_coefficients", "bf16", {"single_coefficients": True}),
+    ("bf16_split_coefficients", "bf16", {"split_coefficients": True}),
     ("bf16_separate_passes", "bf16", {"fuse_passes": False}),
     ("f16", "f16", {}),
-    ("f16_single_coefficients", "f16", {"single_coefficients": True}),
+    ("f16_split_coefficients", "f16", {"split_coefficients": True}),
     ("bf16_nearest", "bf16", {"error_feedback": False}),
     ("bf16_cuda_cores", "bf16", {"tensor_cores": False}),
 ]
@@ -781,7 +781,7 @@ def long_section(device, torch, np, mask, kernel, stream):
     shape = tuple(mask.shape)
     packed = device.bitpack(mask)
     res = {"r500": form_runs(device, torch, np, packed, kernel, 500,
-                             [("bf16", "bf16", {}), ("bf16_single_coefficients", "bf16", {"single_coefficients": True}),
+                             [("bf16", "bf16", {}), ("bf16_split_coefficients", "bf16", {"split_coefficients": True}),
                               ("f16", "f16", {})], stream, shape=shape, n_t=1, packed=True)}
     k32 = gauss_kernel(32.0).astype(np.float32)
     res["sigma32_r20"] = form_runs(device, torch, np, packed, k32, 20,
@@ -890,12 +890,29 @@ def main():
     else:
         mask = bone_implant_mask(shape, seed=0, device="cuda")
     fg = float(mask.float().mean().item())
-    out = torch.empty(shape, dtype=torch.uint16, device="cuda")
-    ws = torch.empty(device.workspace_bytes(shape, args.field), dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
+    split = None
+    if world > 1:
+        # One volume split into z-slabs over the ranks (strong scaling): every rank
+        # holds its slab with the halos of its rounds and exchanges halo planes with
+        # its neighbours between rounds (NCCL P2P over NVLink).
+        from maxibone_b200.zsplit import diffuse_split, library_step, split_plan
+        split = split_plan(nz, world, radius, reps)
+        e0, e1 = split.extended(rank)
+        z0, z1 = split.bounds[rank]
+        mask = mask[e0:e1].contiguous()
+        out = torch.empty((z1 - z0, ny, nx), dtype=torch.uint16, device="cuda")
+        ws = None
+        slab_step = library_step(args.field)
 
-    def step(field=args.field, output=out, workspace=ws, field_out=None):
-        device.diffuse(mask, kernel, reps, output=output, field=field, workspace=workspace, field_out=field_out)
+        def step(field=args.field, output=out, workspace=None, field_out=None):
+            diffuse_split(mask, kernel, split, rank, world, slab_step, output=output)
+    else:
+        out = torch.empty(shape, dtype=torch.uint16, device="cuda")
+        ws = torch.empty(device.workspace_bytes(shape, args.field), dtype=torch.uint8, device="cuda")
+
+        def step(field=args.field, output=out, workspace=ws, field_out=None):
+            device.diffuse(mask, kernel, reps, output=output, field=field, workspace=workspace, field_out=field_out)
 
     def barrier():
         if world > 1:
@@ -933,7 +950,9 @@ def main():
     barrier()
     ms_local = t0.elapsed_time(t1)
     ms = max_over_ranks(ms_local, world, "cuda")
-    value = whole_job_rate(world, vox, reps, args.steps, ms / 1e3)
+    # split: the ranks share one volume (its voxels counted once); otherwise each
+    # rank diffuses its own volume
+    value = whole_job_rate(1 if split else world, vox, reps, args.steps, ms / 1e3)
     launches = sum(c for _, c in prof.values())
 
     # Roofline: the repetition's algorithmic bytes V (2 s_field + s_mask) over its
@@ -942,7 +961,8 @@ def main():
     s = FIELD_BYTES[args.field]
     b_alg = alg_bytes_per_voxel_rep(args.field, "u8")
     rep_ms = ms_local / (args.steps * reps)
-    achieved = b_alg * vox / (rep_ms / 1e3) / 1e9
+    vox_local = int(mask.numel()) if split else vox  # this GPU's voxels (a split rank's slab with halos)
+    achieved = b_alg * vox_local / (rep_ms / 1e3) / 1e9
     fused = bool(path & _lib.PATH_FUSED_YX)
     per_voxel_traffic = NCU_BYTES_PER_VOXEL_REP.get((args.field, "fused" if fused else "separate"))
     kernel_bytes = {"z": 2 * s, "y": 2 * s, "x": 2 * s + 0.125, "x_final": s + 0.125 + 2, "yx": 2 * s + 0.125,
@@ -974,18 +994,47 @@ def main():
                     "field traffic per pass"}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong" if split else "weak",
         "vs_baseline": None, "dtype": args.field, "data": "synthetic (seeded bone+implant mask, random-init)",
         "config": {"workload": args.workload + (f" (shape override {args.shape})" if args.shape else "")
                    + (f" (repetitions override {args.reps})" if args.reps is not None else ""),
                    "shape": list(shape), "sigma": sigma, "kernel_size": int(2 * radius + 1),
                    "reps": reps, "field": args.field, "mask": "u8", "foreground": round(fg, 4),
-                   "parallelism": f"{world} independent volumes (one per rank)",
+                   "parallelism": (f"one volume split into {world} z-slabs (one per rank), halo planes exchanged "
+                                   f"every {split.k} repetitions by NCCL P2P" if split else
+                                   f"{world} independent volumes (one per rank)"),
                    "l2": "inputs larger than L2 (field %d MiB per buffer)" % (s * vox >> 20),
                    "path_bits": path},
         "gpu_launches": launches, "roofline": roofline, "clocks": clocks,
     }
-    sections = [] if args.quick else [x for x in args.sections.split(",") if x]
+    # the sections describe one GPU's forms: a split run reports the headline only
+    sections = [] if (args.quick or split) else [x for x in args.sections.split(",") if x]
+    if split and not args.quick:
+        # End to end at N GPUs: each rank uploads its mask slab from pinned host
+        # memory, runs the split, and downloads its core planes of the output.
+        host_mask = torch.empty(tuple(mask.shape), dtype=torch.uint8, pin_memory=True)
+        host_mask.copy_(mask)
+        host_out = torch.empty(tuple(out.shape), dtype=torch.int16, pin_memory=True)
+
+        def e2e_call():
+            mask.copy_(host_mask, non_blocking=True)
+            step()
+            host_out.view(torch.uint16).copy_(out, non_blocking=True)
+            torch.cuda.synchronize()
+
+        e2e_call()
+        barrier()
+        tw = time.perf_counter()
+        n_e2e = max(1, min(args.steps, 2))
+        for _ in range(n_e2e):
+            e2e_call()
+        e2e_s = max_over_ranks(time.perf_counter() - tw, world, "cuda")
+        line["e2e"] = {"value": whole_job_rate(1, vox, reps, n_e2e, e2e_s), "unit": UNIT,
+                       "h2d_bytes_per_step": int(mask.numel()), "d2h_bytes_per_step": 2 * int(out.numel()),
+                       "steps": n_e2e, "timing": "host clock around upload, split run and download (max over ranks); "
+                                                 "bytes per rank"}
+        del host_mask, host_out
 
     if "e2e" in sections:
         # End to end through the reference-facing call: numpy in, numpy out, from
@@ -1017,7 +1066,7 @@ def main():
         del host_mask, host_out
         ws = None
     else:
-        del ws
+        ws = None
         torch.cuda.empty_cache()
 
     if "precision" in sections:
@@ -1029,9 +1078,10 @@ def main():
         line["bf16_vs_f32"] = {"speedup": res["bf16"]["value"] / res["f32"]["value"],
                                "bf16_hbm_frac": res["bf16"]["hbm_frac"],
                                "bf16_max_abs_err_vs_f64": res["bf16"]["max_abs_err_vs_f64"],
-                               "bf16_single_coefficients_speedup": res["bf16_single_coefficients"]["value"] /
+                               "bf16_split_coefficients_speedup": res["bf16_split_coefficients"]["value"] /
                                res["f32"]["value"],
-                               "bf16_single_coefficients_hbm_frac": res["bf16_single_coefficients"]["hbm_frac"]}
+                               "bf16_split_coefficients_max_abs_err_vs_f64":
+                                   res["bf16_split_coefficients"]["max_abs_err_vs_f64"]}
     if "long" in sections:
         res, ck = sampled(local_rank, lambda: long_section(device, torch, np, mask, kernel, stream))
         res["clocks"] = ck

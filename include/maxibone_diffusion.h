@@ -65,10 +65,11 @@ typedef enum maxi_mask_format {
 #define MAXI_FLAG_SEPARATE_PASSES 0x20   /* BF16/FP16 tensor cores: run the y and x passes as two
                                             kernels (two HBM round trips) instead of the fused
                                             y + x kernel used for radius <= 32 */
-#define MAXI_FLAG_SINGLE_COEFFICIENTS 0x40 /* BF16/FP16 fused y + x kernel: one 16-bit coefficient
-                                            set, rounded so that the kernel's sum and second
-                                            moment are kept, instead of high + low halves (half
-                                            the tensor-core work; adds ~2e-4 to the error) */
+#define MAXI_FLAG_SPLIT_COEFFICIENTS 0x40 /* BF16/FP16 tensor cores: Toeplitz coefficients as high +
+                                            low 16-bit halves (two MMAs per K step) instead of the
+                                            default single set whose taps are rounded so that the
+                                            kernel's sum and second moment are kept; implies
+                                            separate y and x passes */
 
 const char *maxi_last_error(void);
 const char *maxi_version(void);

@@ -123,14 +123,15 @@ static cudaError_t enqueue_group_tc(maxi_batch_plan *p, TcGroup &g, cudaStream_t
     if (e != cudaSuccess) return e;
     const bool bf16 = std::is_same<S, __nv_bfloat16>::value;
     const bool ef = (p->flags & MAXI_FLAG_NEAREST_ROUNDING) == 0 && g.geo.radius >= 4;
+    const bool hi_only = (p->flags & MAXI_FLAG_SPLIT_COEFFICIENTS) == 0;
     const int n = (int) g.members.size();
     int in = 0;
     for (int64_t rep = 0; rep < g.reps; rep++) {
         const bool last = rep + 1 == g.reps;
         // The x pass hands the next repetition its field in [y][z][x] row order.
-        if ((e = tc::tc_batch_pass(g.d_vols, g.d_prefix, g.totals[0], n, 0, in, false, g.kernel.data(), g.geo, bf16, ef, rep > 0, st)) != cudaSuccess ||
-            (e = tc::tc_batch_pass(g.d_vols, g.d_prefix + (n + 1), g.totals[1], n, 1, in ^ 1, false, g.kernel.data(), g.geo, bf16, ef, false, st)) != cudaSuccess ||
-            (e = tc::tc_batch_pass(g.d_vols, g.d_prefix + 2 * (n + 1), g.totals[2], n, 2, in, last, g.kernel.data(), g.geo, bf16, ef, true, st)) != cudaSuccess)
+        if ((e = tc::tc_batch_pass(g.d_vols, g.d_prefix, g.totals[0], n, 0, in, false, g.kernel.data(), g.geo, bf16, ef, rep > 0, st, hi_only)) != cudaSuccess ||
+            (e = tc::tc_batch_pass(g.d_vols, g.d_prefix + (n + 1), g.totals[1], n, 1, in ^ 1, false, g.kernel.data(), g.geo, bf16, ef, false, st, hi_only)) != cudaSuccess ||
+            (e = tc::tc_batch_pass(g.d_vols, g.d_prefix + 2 * (n + 1), g.totals[2], n, 2, in, last, g.kernel.data(), g.geo, bf16, ef, true, st, hi_only)) != cudaSuccess)
             return e;
         in ^= 1;
     }

@@ -80,7 +80,7 @@ int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_ma
 
 cudaError_t tc_batch_pass(const TcVol *d_vols, const int64_t *d_prefix, int64_t total, int n_vol, int pass, int in_buf,
                           bool final_pass, const float *kernel, const TcGeometry &g, bool is_bf16, bool error_feedback,
-                          bool rows_yz, cudaStream_t st) {
+                          bool rows_yz, cudaStream_t st, bool hi_only) {
     if (total == 0) return cudaSuccess;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -90,7 +90,7 @@ cudaError_t tc_batch_pass(const TcVol *d_vols, const int64_t *d_prefix, int64_t 
     cudaError_t e;
     if (pass == 2) {
         ContigLaunch<ManyVolumesContig> p{};
-        fill_pass_taps(p.taps, kernel, g.radius, g.ra, g.kp_contig, is_bf16, error_feedback);
+        fill_pass_taps(p.taps, kernel, g.radius, g.ra, g.kp_contig, is_bf16, error_feedback, hi_only);
         p.final_pass = final_pass ? 1 : 0;
         p.sched.vols = d_vols;
         p.sched.prefix = d_prefix;
@@ -105,7 +105,7 @@ cudaError_t tc_batch_pass(const TcVol *d_vols, const int64_t *d_prefix, int64_t 
     } else {
         const bool axis_z = pass == 0;
         StridedLaunch<ManyVolumesStrided> p{};
-        fill_pass_taps(p.taps, kernel, g.radius, 0, g.kp_strided, is_bf16, error_feedback);
+        fill_pass_taps(p.taps, kernel, g.radius, 0, g.kp_strided, is_bf16, error_feedback, hi_only);
         p.sched.vols = d_vols;
         p.sched.prefix = d_prefix;
         p.sched.n_vol = n_vol;

@@ -45,10 +45,12 @@ int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_ma
 // One pass (0 z, 1 y, 2 x) over all volumes of a device table; d_prefix holds
 // n_vol + 1 prefix sums of the volumes' columns (z: cols_z, y: cols_y) or x tiles.
 // rows_yz: the z pass reads its input as [y][z][x] rows, the x pass (not
-// final) writes its output in that order.
+// final) writes its output in that order.  hi_only: one matched 16-bit
+// coefficient set (the default of the single-volume passes) instead of the
+// high and low halves.
 cudaError_t tc_batch_pass(const TcVol *d_vols, const int64_t *d_prefix, int64_t total, int n_vol, int pass, int in_buf,
                           bool final_pass, const float *kernel, const TcGeometry &g, bool is_bf16, bool error_feedback,
-                          bool rows_yz, cudaStream_t st);
+                          bool rows_yz, cudaStream_t st, bool hi_only);
 
 int tc_batch_read_and_clear_error();
 

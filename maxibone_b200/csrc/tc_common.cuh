@@ -325,6 +325,54 @@ __device__ __forceinline__ void narrow32_pairs(const float (&a)[32], float scale
     }
 }
 
+// 32 voxels in four error-feedback chains of 8 (x = 8k + j, k = 0..3): chains
+// 0 / 1 and 2 / 3 advance together as two packed pairs, so each step has two
+// independent dependency chains and a run takes 8 steps instead of 16.  Used
+// for the intermediate field of the fused y + x kernel, which the x MMAs
+// consume at once (its rounding noise, high-pass within 8 voxels, is removed
+// by the x convolution that follows).  d[j] holds voxels j (low) and 8 + j
+// (high); d[8 + j] holds 16 + j and 24 + j.
+template <typename S, bool MASKED>
+__device__ __forceinline__ void narrow32_quads(const float (&a)[32], float scale, bool ef, uint32_t force1,
+                                               uint32_t live, uint32_t (&d)[16]) {
+    float2 c0 = make_float2(0.0f, 0.0f), c1 = make_float2(0.0f, 0.0f);
+    const float2 s2 = make_float2(scale, scale), m1 = make_float2(-1.0f, -1.0f);
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        float2 w0 = make_float2(a[j], a[8 + j]), w1 = make_float2(a[16 + j], a[24 + j]);
+        w0 = ef ? __ffma2_rn(w0, s2, c0) : __fmul2_rn(w0, s2);
+        w1 = ef ? __ffma2_rn(w1, s2, c1) : __fmul2_rn(w1, s2);
+        if (MASKED) {
+            if (!((live >> j) & 1u)) w0.x = 0.0f;
+            if (!((live >> (8 + j)) & 1u)) w0.y = 0.0f;
+            if (!((live >> (16 + j)) & 1u)) w1.x = 0.0f;
+            if (!((live >> (24 + j)) & 1u)) w1.y = 0.0f;
+            if ((force1 >> j) & 1u) w0.x = 1.0f;
+            if ((force1 >> (8 + j)) & 1u) w0.y = 1.0f;
+            if ((force1 >> (16 + j)) & 1u) w1.x = 1.0f;
+            if ((force1 >> (24 + j)) & 1u) w1.y = 1.0f;
+        }
+        const uint32_t q0 = Pair16<S>::cvt(w0.x, w0.y), q1 = Pair16<S>::cvt(w1.x, w1.y);
+        if (ef) {
+            c0 = __ffma2_rn(Pair16<S>::widen(q0), m1, w0);
+            c1 = __ffma2_rn(Pair16<S>::widen(q1), m1, w1);
+        }
+        d[j] = q0;
+        d[8 + j] = q1;
+    }
+}
+
+// narrow32_quads' words -> pairs of neighbours: o[i] = voxels (2i, 2i + 1).
+__device__ __forceinline__ void quads_to_adjacent(const uint32_t (&d)[16], uint32_t (&o)[16]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        o[i] = __byte_perm(d[2 * i], d[2 * i + 1], 0x5410);           // voxels 2i, 2i + 1 (chain 0)
+        o[4 + i] = __byte_perm(d[2 * i], d[2 * i + 1], 0x7632);       // 8 + 2i, 9 + 2i (chain 1)
+        o[8 + i] = __byte_perm(d[8 + 2 * i], d[9 + 2 * i], 0x5410);   // 16 + 2i, 17 + 2i (chain 2)
+        o[12 + i] = __byte_perm(d[8 + 2 * i], d[9 + 2 * i], 0x7632);  // 24 + 2i, 25 + 2i (chain 3)
+    }
+}
+
 // Pairs (j, 16 + j) -> pairs of neighbours: o[i] = voxels (2i, 2i + 1), i < 16.
 __device__ __forceinline__ void pairs_to_adjacent(const uint32_t (&d)[16], uint32_t (&o)[16]) {
 #pragma unroll

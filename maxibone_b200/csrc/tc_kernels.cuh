@@ -25,7 +25,11 @@
 // so the effective kernel keeps ~16 significant bits and its sum stays 1 to
 // ~1e-6: with single-rounded 16-bit coefficients the kernel's gain error
 // compounds over 3 x R passes.  FP16 coefficients are scaled by 2^10 to stay in
-// the normal range; the epilogue undoes the scale exactly.
+// the normal range; the epilogue undoes the scale exactly.  With hi_only the
+// passes use one 16-bit set instead, each tap rounded up or down so that the
+// set keeps the kernel's sum and second moment (tc_round_taps_matched): one MMA
+// per K step.  Consecutive MMAs into one accumulator are latency-bound (about
+// 130 cycles each on B200 for N <= 192), so this halves the passes' tensor time.
 //
 // Row order of the 16-bit field between repetitions.  The z pass is the only
 // pass whose tile rows lie on different planes: read from the [z][y][x] volume
@@ -52,9 +56,12 @@
 // z / y passes, 16 in the x pass) drain TMEM (tcgen05.ld), narrow to the
 // storage type and store.  With error feedback on,
 // the rounding error of each stored value is carried to its x-neighbour
-// (32-voxel chains along x): the stored field's rounding noise becomes
-// high-pass along x and the next x pass removes it.  Every wait is bounded:
-// on a timeout the kernel records a code in g_tc_error and winds down.
+// (chains of 16 voxels along x, two of them advancing together): the stored
+// field's rounding noise becomes high-pass along x and the next x pass
+// removes it.  Every wait is bounded:
+// on a timeout the kernel records a code in g_tc_error and winds down, the
+// producer first letting the copies it started land and the MMA issuer its
+// MMAs complete (both bounded), so no asynchronous write outlives the CTA.
 #pragma once
 
 #include <cudaTypedefs.h>
@@ -120,6 +127,7 @@ struct PassTaps {
     int radius, ra, kp, kpa;  // radius, x-pass left pad, K (multiple of 16), K rounded to 64
     int kcols, nbox, box_rows;
     int error_feedback;
+    int hi_only;  // one coefficient set (hi, rounded to keep the kernel's sum and second moment), no lo MMAs
     float inv_scale;
     uint16_t hi[2 * kTcMaxRadiusWide + 1];
     uint16_t lo[2 * kTcMaxRadiusWide + 1];
@@ -368,7 +376,8 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
     const int stage_bytes = CHUNKS * tp.kp * 128;
     uint64_t *bars = reinterpret_cast<uint64_t *>(ring + STAGES * stage_bytes);
     uint64_t *full = bars, *empty = bars + STAGES, *tfull = bars + 2 * STAGES, *tempty = bars + 2 * STAGES + 2;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 4);
+    uint64_t *drain = bars + 2 * STAGES + 4;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 5);
     uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 1024;  // 1024-byte aligned
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t total = p.sched.total();
@@ -376,6 +385,7 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], kEpiWarps); }
+        mbar_init(drain, 1);
         fence_barrier_init();
         if (Sched::kParamMaps) prefetch_tmap(&tmap);
     }
@@ -458,6 +468,10 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
             }
             cur = nxt;
         }
+        // The copies this thread started land before the CTA can exit (the last
+        // use of each ring stage; bounded, so an aborted run still ends).
+        for (int64_t k = tl - STAGES; k < tl; k++)
+            if (k >= 0) mbar_wait(&full[k % STAGES], (uint32_t) ((k / STAGES) & 1), 1);
     } else if (warp == 1 && lane == 0) {
         // MMA issuer.
         const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
@@ -482,12 +496,15 @@ tc_strided_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constan
                 const uint32_t a_hi = tmem + 2 * TN, a_lo = a_hi + tp.kcols;
                 for (int ks = 0; ks < tp.kp / 16; ks++) {
                     umma_f16_ts(dt, a_hi + ks * 8, bd + (uint64_t) (ks * 128), idesc, ks > 0 ? 1u : 0u);
-                    umma_f16_ts(dt, a_lo + ks * 8, bd + (uint64_t) (ks * 128), idesc, 1u);
+                    if (!tp.hi_only) umma_f16_ts(dt, a_lo + ks * 8, bd + (uint64_t) (ks * 128), idesc, 1u);
                 }
                 umma_commit(&empty[s]);
                 umma_commit(&tfull[d]);
             }
         }
+        // Every MMA this thread issued completes before the CTA winds down.
+        umma_commit(drain);
+        mbar_wait(drain, 0, 2);
     } else if (warp >= 2) {
         // Epilogue: TMEM -> registers -> storage type -> global.
         const int quad = warp & 3;           // TMEM lane quadrant this warp may access
@@ -587,7 +604,8 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
     const int stage_bytes = nkb * kTM * 128;
     uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kXStages * stage_bytes);
     uint64_t *full = bars, *empty = bars + kXStages, *tfull = bars + 2 * kXStages, *tempty = bars + 2 * kXStages + 2;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kXStages + 4);
+    uint64_t *drain = bars + 2 * kXStages + 4;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kXStages + 5);
     uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 1024;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t total = p.sched.total();
@@ -603,6 +621,7 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
     if (threadIdx.x == 0) {
         for (int s = 0; s < kXStages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], kXEpiWarps); }
+        mbar_init(drain, 1);
         fence_barrier_init();
         if (Sched::kParamMaps) prefetch_tmap(&tmap);
     }
@@ -634,6 +653,8 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
             for (int kb = 0; kb < nkb; kb++)
                 tma_load_3d(ring + s * stage_bytes + kb * kTM * 128, t.in, t.x0 - tp.ra + 64 * kb, (int) t.r0, 0, &full[s]);
         }
+        for (int64_t k = tl - kXStages; k < tl; k++)  // the started copies land before exit (bounded)
+            if (k >= 0) mbar_wait(&full[k % kXStages], (uint32_t) ((k / kXStages) & 1), 1);
     } else if (warp == 1 && lane == 0) {
         const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
         const uint32_t idesc = idesc_f16(fmt, 0 /*A K-major*/, 0 /*B K-major*/, kTM, kXTN);
@@ -652,11 +673,14 @@ tc_contig_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant
                 const uint64_t ad = smem_desc_sw128(a0 + s * stage_bytes + (ks >> 2) * (kTM * 128) + kin, 16, 1024);
                 const uint32_t bhi = b0 + (ks >> 2) * (2 * kXTN * 128) + kin;  // rows 0..127: Tt_hi
                 umma_f16(dt, ad, smem_desc_sw128(bhi, 16, 1024), idesc, ks > 0 ? 1u : 0u);
-                umma_f16(dt, ad, smem_desc_sw128(bhi + kXTN * 128, 16, 1024), idesc, 1u);  // rows 128..255: Tt_lo
+                if (!tp.hi_only)
+                    umma_f16(dt, ad, smem_desc_sw128(bhi + kXTN * 128, 16, 1024), idesc, 1u);  // rows 128..255: Tt_lo
             }
             umma_commit(&empty[s]);
             umma_commit(&tfull[d]);
         }
+        umma_commit(drain);  // the issued MMAs complete before the CTA winds down (bounded)
+        mbar_wait(drain, 0, 2);
     } else if (warp >= 2) {
         const int quad = warp & 3;         // TMEM lane quadrant this warp may access
         const int part = (warp - 2) >> 2;  // which 32 of the 128 columns it drains
@@ -801,7 +825,8 @@ tc_contig_t_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_consta
     const int stage_bytes = nkb * kXtRows * 128;
     uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kXtStages * stage_bytes);
     uint64_t *full = bars, *empty = bars + kXtStages, *tfull = bars + 2 * kXtStages, *tempty = bars + 2 * kXtStages + 2;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kXtStages + 4);
+    uint64_t *drain = bars + 2 * kXtStages + 4;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * kXtStages + 5);
     uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 1024;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t total = p.sched.total();
@@ -810,6 +835,7 @@ tc_contig_t_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_consta
     if (threadIdx.x == 0) {
         for (int s = 0; s < kXtStages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         for (int d = 0; d < 2; d++) { mbar_init(&tfull[d], 1); mbar_init(&tempty[d], kXtEpiWarps); }
+        mbar_init(drain, 1);
         fence_barrier_init();
         prefetch_tmap(&tmap);
     }
@@ -866,6 +892,8 @@ tc_contig_t_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_consta
                 tma_load_3d(ring + s * stage_bytes + kb * kXtRows * 128, t.in, t.x0 - tp.ra + 64 * kb, (int) t.r0, 0,
                             &full[s]);
         }
+        for (int64_t k = tl - kXtStages; k < tl; k++)  // the started copies land before exit (bounded)
+            if (k >= 0) mbar_wait(&full[k % kXtStages], (uint32_t) ((k / kXtStages) & 1), 1);
     } else if (warp == 1 && lane == 0) {
         const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
         const uint32_t idesc = idesc_f16(fmt, 0 /*A K-major*/, 0 /*B K-major*/, kTM, kXtRows);
@@ -885,11 +913,13 @@ tc_contig_t_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_consta
                 const uint64_t bd = smem_desc_sw128(b0 + s * stage_bytes + (ks >> 2) * (kXtRows * 128) + (ks & 3) * 32, 16,
                                                     1024);
                 umma_f16_ts(dt, a_hi + ks * 8, bd, idesc, ks > 0 ? 1u : 0u);
-                umma_f16_ts(dt, a_lo + ks * 8, bd, idesc, 1u);
+                if (!tp.hi_only) umma_f16_ts(dt, a_lo + ks * 8, bd, idesc, 1u);
             }
             umma_commit(&empty[s]);
             umma_commit(&tfull[d]);
         }
+        umma_commit(drain);  // the issued MMAs complete before the CTA winds down (bounded)
+        mbar_wait(drain, 0, 2);
     } else if (warp >= 2) {
         const int quad = warp & 3;             // TMEM lane quadrant: x outputs quad * 32 + lane
         const int half = (warp - 2) >> 2;      // rows half * 32 .. + 32 of the tile
@@ -961,7 +991,7 @@ tc_contig_t_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_consta
 
 // Fills the taps of one pass: hi/lo halves of kernel x scale (1 for BF16, 2^10 for FP16).
 inline void fill_pass_taps(PassTaps &t, const float *kernel, int radius, int ra, int kp, bool is_bf16,
-                           bool error_feedback) {
+                           bool error_feedback, bool hi_only = false) {
     t.radius = radius;
     t.ra = ra;
     t.kp = kp;
@@ -972,7 +1002,13 @@ inline void fill_pass_taps(PassTaps &t, const float *kernel, int radius, int ra,
     t.error_feedback = error_feedback ? 1 : 0;
     const float scale = is_bf16 ? 1.0f : 1024.0f;
     t.inv_scale = 1.0f / scale;
-    tc_split_taps(kernel, radius, is_bf16, scale, t.hi, t.lo);
+    t.hi_only = hi_only ? 1 : 0;
+    if (hi_only) {
+        tc_round_taps_matched(kernel, radius, is_bf16, scale, t.hi);
+        for (int i = 0; i < 2 * radius + 1; i++) t.lo[i] = 0;
+    } else {
+        tc_split_taps(kernel, radius, is_bf16, scale, t.hi, t.lo);
+    }
 }
 
 }  // namespace tc

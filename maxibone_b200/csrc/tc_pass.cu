@@ -55,12 +55,12 @@ bool tc_supported(int radius, int64_t nz, int64_t ny, int64_t nx) {
 
 template <typename S>
 cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, bool axis_z, const float *kernel,
-                       int radius, bool error_feedback, cudaStream_t st, const YzRows *in_rows) {
+                       int radius, bool error_feedback, cudaStream_t st, const YzRows *in_rows, bool hi_only) {
     if (!axis_z) in_rows = nullptr;
     const bool is_bf16 = std::is_same<S, __nv_bfloat16>::value;
     const int tn = strided_tn(radius), stages = kStridedStages;
     StridedLaunch<OneVolumeStrided> p{};
-    fill_pass_taps(p.taps, kernel, radius, 0, (int) round_up(kTM + 2 * radius, 16), is_bf16, error_feedback);
+    fill_pass_taps(p.taps, kernel, radius, 0, (int) round_up(kTM + 2 * radius, 16), is_bf16, error_feedback, hi_only);
     OneVolumeStrided &sc = p.sched;
     sc.out = out;
     sc.nx = nx;
@@ -115,9 +115,9 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
 }
 
 template cudaError_t tc_strided<__nv_bfloat16>(const __nv_bfloat16 *, __nv_bfloat16 *, int64_t, int64_t, int64_t,
-                                               bool, const float *, int, bool, cudaStream_t, const YzRows *);
+                                               bool, const float *, int, bool, cudaStream_t, const YzRows *, bool);
 template cudaError_t tc_strided<__half>(const __half *, __half *, int64_t, int64_t, int64_t, bool, const float *, int,
-                                        bool, cudaStream_t, const YzRows *);
+                                        bool, cudaStream_t, const YzRows *, bool);
 
 void tc_split_taps(const float *kernel, int radius, bool is_bf16, float scale, uint16_t *hi, uint16_t *lo) {
     for (int i = 0; i < 2 * radius + 1; i++) {
@@ -224,20 +224,12 @@ cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool fina
     if (final_pass) out_rows = nullptr;
     YxLaunch p{};
     const int ra = (int) round_up(radius, 8);
-    fill_pass_taps(p.ty, kernel, radius, 0, (int) round_up(kTM + 2 * radius, 16), is_bf16, error_feedback);
-    fill_pass_taps(p.tx, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback);
-    if (hi_only) {
-        const float scale = is_bf16 ? 1.0f : 1024.0f;
-        tc_round_taps_matched(kernel, radius, is_bf16, scale, p.ty.hi);
-        for (int i = 0; i < 2 * radius + 1; i++) {
-            p.tx.hi[i] = p.ty.hi[i];
-            p.ty.lo[i] = p.tx.lo[i] = 0;
-        }
-    }
-    if (p.tx.kp > 3 * 64 || kYxAccX < (uint32_t) (64 * ((p.tx.kp + 63) / 64)) ||
-        kYxToep + 2 * p.ty.kcols > kYxTmemCols)
+    if (!hi_only) return cudaErrorInvalidValue;  // the fused kernel holds one coefficient set
+    fill_pass_taps(p.ty, kernel, radius, 0, (int) round_up(kTM + 2 * radius, 16), is_bf16, error_feedback, true);
+    fill_pass_taps(p.tx, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback, true);
+    if (p.tx.kp > kYxMaxChunks * 64 || kYxYp < (uint32_t) (64 * ((p.tx.kp + 63) / 64)) ||
+        kYxYp + p.tx.kp / 2 > kYxAccX || kYxToep + p.ty.kcols > kYxTmemCols)
         return cudaErrorInvalidValue;
-    p.hi_only = hi_only ? 1 : 0;
     p.final_pass = final_pass ? 1 : 0;
     p.mask = mask;
     p.out = reinterpret_cast<uint16_t *>(out_rows ? out_rows->base : static_cast<void *>(out));
@@ -262,13 +254,16 @@ cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool fina
                                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
-    const int smem = yx_smem_bytes(p.ty.kp, p.tx.kpa, hi_only);
+    int dev = 0, sms = 148, smem_max = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    p.stages = yx_stages(p.ty.kp, p.tx.kpa, smem_max);
+    const int smem = yx_smem_bytes(p.ty.kp, p.tx.kpa, p.stages);
+    if (smem > smem_max || p.stages < (p.tx.kp + 63) / 64) return cudaErrorInvalidValue;
     auto *kern = mask_fmt == MAXI_MASK_U8 ? tc_yx_kernel<S, MAXI_MASK_U8> : tc_yx_kernel<S, MAXI_MASK_BITPACKED>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int64_t grid = std::min<int64_t>(p.n_tiles, sms);
     kern<<<(unsigned) grid, kYxThreads, smem, st>>>(map, p);
     return cudaGetLastError();
@@ -285,11 +280,12 @@ template <typename S>
 static cudaError_t tc_contig_t(const S *in, S *out, const void *mask, int mask_fmt, bool final_pass,
                                uint16_t *out_u16, float *field_out, int64_t nz, int64_t ny, int64_t nx,
                                const float *kernel, int radius, bool error_feedback, cudaStream_t st,
-                               const YzRows *out_rows) {
+                               const YzRows *out_rows, bool hi_only) {
     const bool is_bf16 = std::is_same<S, __nv_bfloat16>::value;
     ContigLaunch<OneVolumeContigT> p{};
     const int ra = (int) round_up(radius, 8);
-    fill_pass_taps(p.taps, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback);
+    fill_pass_taps(p.taps, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback,
+                   hi_only);
     if (kXtRows * 2 + 2 * p.taps.kcols > (int) kTmemColsStrided) return cudaErrorInvalidValue;
     p.final_pass = final_pass ? 1 : 0;
     OneVolumeContigT &sc = p.sched;
@@ -330,15 +326,16 @@ static cudaError_t tc_contig_t(const S *in, S *out, const void *mask, int mask_f
 template <typename S>
 cudaError_t tc_contig(const S *in, S *out, const void *mask, int mask_fmt, bool final_pass, uint16_t *out_u16,
                       float *field_out, int64_t nz, int64_t ny, int64_t nx, const float *kernel, int radius,
-                      bool error_feedback, cudaStream_t st, const YzRows *out_rows) {
+                      bool error_feedback, cudaStream_t st, const YzRows *out_rows, bool hi_only) {
     const bool is_bf16 = std::is_same<S, __nv_bfloat16>::value;
     if (final_pass) out_rows = nullptr;
     if (radius > kTcMaxRadius)
         return tc_contig_t<S>(in, out, mask, mask_fmt, final_pass, out_u16, field_out, nz, ny, nx, kernel, radius,
-                              error_feedback, st, out_rows);
+                              error_feedback, st, out_rows, hi_only);
     ContigLaunch<OneVolumeContig> p{};
     const int ra = (int) round_up(radius, 8);
-    fill_pass_taps(p.taps, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback);
+    fill_pass_taps(p.taps, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback,
+                   hi_only);
     p.final_pass = final_pass ? 1 : 0;
     OneVolumeContig &sc = p.sched;
     sc.out = out_rows ? out_rows->base : out;
@@ -378,10 +375,10 @@ cudaError_t tc_contig(const S *in, S *out, const void *mask, int mask_fmt, bool 
 
 template cudaError_t tc_contig<__nv_bfloat16>(const __nv_bfloat16 *, __nv_bfloat16 *, const void *, int, bool,
                                               uint16_t *, float *, int64_t, int64_t, int64_t, const float *, int,
-                                              bool, cudaStream_t, const YzRows *);
+                                              bool, cudaStream_t, const YzRows *, bool);
 template cudaError_t tc_contig<__half>(const __half *, __half *, const void *, int, bool, uint16_t *, float *,
                                        int64_t, int64_t, int64_t, const float *, int, bool, cudaStream_t,
-                                       const YzRows *);
+                                       const YzRows *, bool);
 
 int tc_read_and_clear_error() {
     int v = 0;

@@ -33,7 +33,8 @@ struct YzRows {
 // gives it in [y][z][x] row order.
 template <typename S>
 cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, bool axis_z, const float *kernel,
-                       int radius, bool error_feedback, cudaStream_t st, const YzRows *in_rows = nullptr);
+                       int radius, bool error_feedback, cudaStream_t st, const YzRows *in_rows = nullptr,
+                       bool hi_only = false);
 
 // The x pass fused with re-illumination; on the last repetition (final_pass)
 // it writes the uint16 output and/or the FP32 field (either may be NULL)
@@ -42,7 +43,7 @@ cudaError_t tc_strided(const S *in, S *out, int64_t nz, int64_t ny, int64_t nx, 
 template <typename S>
 cudaError_t tc_contig(const S *in, S *out, const void *mask, int mask_fmt, bool final_pass, uint16_t *out_u16,
                       float *field_out, int64_t nz, int64_t ny, int64_t nx, const float *kernel, int radius,
-                      bool error_feedback, cudaStream_t st, const YzRows *out_rows = nullptr);
+                      bool error_feedback, cudaStream_t st, const YzRows *out_rows = nullptr, bool hi_only = false);
 
 // True when the fused y + x pass serves the shape (radius <= kTcMaxRadius and
 // the tensor-core passes' shape rules).
@@ -51,9 +52,9 @@ bool tc_yx_supported(int radius, int64_t nz, int64_t ny, int64_t nx);
 // The y and x passes and the re-illumination fused in one kernel per z-plane
 // tile: reads the z pass's output `in` ([z][y][x]) and writes the next field
 // to `out` ([z][y][x], or [y][z][x] rows at out_rows), or on the last
-// repetition (final_pass) the uint16 output and/or the FP32 field.  hi_only:
-// one 16-bit coefficient set with the kernel's sum and second moment kept
-// (tc_round_taps_matched) instead of the high and low halves.
+// repetition (final_pass) the uint16 output and/or the FP32 field.  The fused
+// kernel uses one 16-bit coefficient set with the kernel's sum and second
+// moment kept (tc_round_taps_matched); hi_only must be true.
 template <typename S>
 cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool final_pass, uint16_t *out_u16,
                   float *field_out, int64_t nz, int64_t ny, int64_t nx, const float *kernel, int radius,

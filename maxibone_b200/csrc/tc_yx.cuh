@@ -10,38 +10,38 @@
 //      memory) is the A operand, F arrives by TMA in chunks of 64 x-columns x
 //      KP = 128 + 2R rows (MN-major, 128-byte swizzle; rows and columns outside
 //      the plane are zero-filled: the zero boundary).  Y accumulates in FP32 in
-//      tensor memory, one lane per y-output.
+//      tensor memory, one lane per y-output, one accumulator per chunk.
 //   2. Conversion warps read Y back lane by lane (tcgen05.ld), narrow it to the
-//      16-bit storage type with error-feedback rounding along x (two chains per
-//      32 columns, two voxels per instruction), zero the columns outside the
-//      volume (the x pass's zero boundary), and write it back packed two per
-//      column (tcgen05.st) over the first KX/2 columns of the accumulator: the
-//      K-major layout of an A operand in tensor memory.
+//      16-bit storage type with error-feedback rounding along x (four chains of
+//      8 per 32 columns, two voxels per instruction), zero the columns outside
+//      the volume (the x pass's zero boundary), and write it packed two per
+//      column (tcgen05.st) into its own tensor-memory region: the K-major
+//      layout of an A operand in tensor memory.
 //   3. x MMAs: D[o, x] = sum_j Y'[o, j] Tt[j, x] with the x Toeplitz Tt in
-//      shared memory as the B operand (K-major), into a second accumulator.
+//      shared memory as the B operand (K-major), into the x accumulator.
 //   4. Epilogue warps: re-illumination from the bit-packed mask, then either
 //      the next field (error-feedback rounding, [y][z][x] or [z][y][x] rows) or,
 //      on the last repetition, the uint16 output and the FP32 field.
 //
 // The field between the y and the x convolution is rounded to the storage
-// type exactly as the separate passes store it, so the arithmetic is that of
-// the y pass followed by the x pass; only the HBM round trip of the
-// intermediate field is gone (4 + 1/8 instead of 8 + 1/8 bytes per voxel for
-// the two passes).  Coefficients are the high and low 16-bit halves of the
-// kernel (two MMAs per K step) or, with hi_only, one 16-bit set whose
-// rounding directions keep the kernel's sum and second moment (one MMA per
-// K step: half the tensor-core work).
+// type as the separate passes store it, so the arithmetic is that of the y
+// pass followed by the x pass; only the HBM round trip of the intermediate
+// field is gone (4 + 1/8 instead of 8 + 1/8 bytes per voxel for the two
+// passes).  Coefficients: one 16-bit set rounded to keep the kernel's sum and
+// second moment (tc_round_taps_matched).
 //
-// Tensor memory (512 columns): [0, 192) y accumulator, then Y' packed over its
-// first KX/2 columns; [192, 320) x accumulator; [320, 512) the y Toeplitz
-// halves (96 columns each at radius 32).  Warp roles: 0 TMA producer, 1 MMA
-// issuer, 2-9 conversion (two per TMEM lane quadrant, 32 columns of each
-// 64-column chunk each), 10-17 epilogue (two per quadrant, 64 x-outputs each).
-// The pipeline runs at chunk granularity: the y MMAs commit chunk by chunk,
-// the conversion of a chunk starts while the next chunks multiply, and the x
-// MMAs of a chunk start as soon as it is converted.  Every wait is bounded; on
-// a timeout the kernel records a code in g_tc_error, lets the copies and MMAs
-// it started finish (bounded) and winds down.
+// Tensor-core schedule.  Consecutive MMAs into one accumulator are bound by the
+// MMA latency (about 130 cycles on B200 for N <= 192), so the MMA issuer keeps
+// several accumulation chains in flight: the three 64-column y chunks of tile t
+// (three accumulators) and the x MMAs of tile t - 1 (a fourth), one K step of
+// each in turn.  That needs Y' of tile t - 1 to stay in place while tile t's y
+// accumulates, hence its own region.  Tensor memory (512 columns): [0, 192) y
+// accumulator, [192, 288) Y' packed, [288, 416) x accumulator, [416, 512) the
+// y Toeplitz.  Warp roles: 0 TMA producer, 1 MMA issuer, 2-9 conversion (two
+// per TMEM lane quadrant, 96 columns each), 10-17 epilogue (two per quadrant,
+// 64 x-outputs each).  Every wait is bounded; on a timeout the kernel records a
+// code in g_tc_error, lets the copies and MMAs it started finish (bounded) and
+// winds down.
 #pragma once
 
 #include "tc_kernels.cuh"
@@ -49,27 +49,37 @@
 namespace maxi {
 namespace tc {
 
-constexpr int kYxStages = 4;                                     // F chunk ring (64 x-columns x KP rows each)
+constexpr int kYxMaxStages = 8;                                  // F chunk ring (64 x-columns x KP rows each)
 constexpr int kYxConvWarps = 8;                                  // two per TMEM lane quadrant
 constexpr int kYxEpiWarps = 8;                                   // two per lane quadrant
 constexpr int kYxThreads = 64 + 32 * (kYxConvWarps + kYxEpiWarps);  // 576
 constexpr int kYxMaxChunks = 3;                                  // 64-column chunks of the x window (radius <= 32)
-constexpr uint32_t kYxAccY = 0;                                  // y accumulator, up to 192 columns
-constexpr uint32_t kYxAccX = 192;                                // x accumulator, 128 columns
-constexpr uint32_t kYxToep = 320;                                // y Toeplitz halves
+constexpr uint32_t kYxAccY = 0;                                  // y accumulators, up to 3 x 64 columns
+constexpr uint32_t kYxYp = 192;                                  // Y' packed, up to 96 columns
+constexpr uint32_t kYxAccX = 288;                                // x accumulator, 128 columns
+constexpr uint32_t kYxToep = 416;                                // y Toeplitz, up to 96 columns
 constexpr uint32_t kYxTmemCols = 512;
 
-// Shared memory: x Toeplitz (kpa K x 128 or 256 rows), the F chunk ring, the
-// barriers and the epilogue's store staging.
-__host__ __device__ constexpr int yx_smem_bytes(int kp_y, int kpa_x, bool hi_only) {
-    return 1024 + kpa_x * (hi_only ? 1 : 2) * kXTN * 2 + kYxStages * kp_y * 128 + 1024 + kYxEpiWarps * kXStageWarpBytes;
+// Shared memory: x Toeplitz (kpa K x 128 rows), the F chunk ring of `stages`
+// chunks, the barriers and the epilogue's store staging.
+__host__ __device__ constexpr int yx_smem_bytes(int kp_y, int kpa_x, int stages) {
+    return 1024 + kpa_x * kXTN * 2 + stages * kp_y * 128 + 1024 + kYxEpiWarps * kXStageWarpBytes;
+}
+
+// The deepest F ring (at most kYxMaxStages chunks) that fits `smem_max` bytes.
+// A tile's y MMAs need its chunks together, so the ring holds two tiles'
+// chunks where it can: the loads of the next tile run while this one multiplies.
+__host__ __device__ constexpr int yx_stages(int kp_y, int kpa_x, int smem_max) {
+    int st = kYxMaxStages;
+    while (st > 3 && yx_smem_bytes(kp_y, kpa_x, st) > smem_max) st--;
+    return st;
 }
 
 struct YxLaunch {
     PassTaps ty;  // y convolution: kp = 128 + 2R rounded to 16, kcols
     PassTaps tx;  // x convolution: ra, kp = 128 + RA + R rounded to 16, kpa
-    int hi_only;
     int final_pass;
+    int stages;         // F ring depth (chunks), at least the chunks of one tile
     const void *mask;
     uint16_t *out;      // next field (not final): [z][y][x], or [y][z][x] rows when out_nz > 0
     uint16_t *out_u16;  // final
@@ -88,16 +98,6 @@ __device__ __forceinline__ uint32_t live_bits(int64_t xs, int64_t nx) {
     return upto & ~((1u << lo) - 1u);
 }
 
-// Named barrier of the two conversion warps of one TMEM lane quadrant that
-// also ANDs `v` over both: the pair leaves a wait that timed out together.
-__device__ __forceinline__ bool pair_barrier_and(int quad, bool v) {
-    uint32_t r;
-    asm volatile(
-        "{\n .reg .pred p, q;\n setp.ne.u32 p, %2, 0;\n bar.red.and.pred q, %1, 64, p;\n selp.u32 %0, 1, 0, q;\n}\n"
-        : "=r"(r) : "r"(1 + quad), "r"((uint32_t) v) : "memory");
-    return r != 0;
-}
-
 template <typename S, int FMT>
 __global__ void __launch_bounds__(kYxThreads, 1)
 tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ YxLaunch p) {
@@ -105,33 +105,40 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     uint8_t *smem = smem_raw + (((raw + 1023) & ~1023u) - raw);
-    const int tt_rows = p.hi_only ? kXTN : 2 * kXTN;          // x Toeplitz rows: hi (and lo)
-    uint8_t *tt = smem;
-    uint8_t *ring = tt + tx.kpa * tt_rows * 2;                 // a multiple of 16 KB: 1024-aligned
+    uint8_t *tt = smem;                                         // x Toeplitz, K-major, 128 rows
+    uint8_t *ring = tt + tx.kpa * kXTN * 2;                     // a multiple of 16 KB: 1024-aligned
     const int chunk_bytes = ty.kp * 128;                        // 64 x-columns x KP rows of 16-bit
     const int nch = (tx.kp + 63) / 64;                          // chunks per tile (<= 3)
-    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kYxStages * chunk_bytes);
-    uint64_t *full = bars, *empty = bars + kYxStages;
-    uint64_t *ychunk = bars + 2 * kYxStages;                    // [kYxMaxChunks]: y chunk accumulated
-    uint64_t *ypacked = ychunk + kYxMaxChunks;                  // [kYxMaxChunks]: chunk converted to Y'
-    uint64_t *xfull = ypacked + kYxMaxChunks, *xempty = xfull + 1, *drain = xfull + 2;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(xfull + 3);
+    const int ncc = (tx.kp + 31) / 32;                          // 32-column runs of Y' (<= 6)
+    const int stages = p.stages;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + stages * chunk_bytes);
+    uint64_t *full = bars, *empty = bars + kYxMaxStages;
+    uint64_t *yfull = bars + 2 * kYxMaxStages;  // y accumulators complete (MMA commit)
+    uint64_t *yfree = yfull + 1;                // y accumulators read (conversion warps)
+    uint64_t *ypacked = yfull + 2;              // Y' written (conversion warps)
+    uint64_t *ypfree = yfull + 3;               // Y' read by the x MMAs (MMA commit)
+    uint64_t *xfull = yfull + 4;                // x accumulator complete (MMA commit)
+    uint64_t *xempty = yfull + 5;               // x accumulator drained (epilogue warps)
+    uint64_t *drain = yfull + 6;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(yfull + 7);
     uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 1024;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t total = p.n_tiles;
     const uint32_t n_tx = (uint32_t) p.n_tx, n_ty = (uint32_t) p.n_ty;
 
-    for (int e = threadIdx.x; e < tt_rows * tx.kpa; e += kYxThreads) {
+    for (int e = threadIdx.x; e < kXTN * tx.kpa; e += kYxThreads) {
         const int n = e / tx.kpa, j = e - n * tx.kpa;
-        const int o = n & (kXTN - 1);
-        const int t = j - o - tx.ra + tx.radius;  // tap index 0..2R
+        const int t = j - n - tx.ra + tx.radius;  // tap index 0..2R
         uint16_t v = 0;
-        if (t >= 0 && t <= 2 * tx.radius && j < tx.kp) v = n < kXTN ? tx.hi[t] : tx.lo[t];
-        *reinterpret_cast<uint16_t *>(tt + sw128_kmajor_offset(n, j, tt_rows)) = v;
+        if (t >= 0 && t <= 2 * tx.radius && j < tx.kp) v = tx.hi[t];
+        *reinterpret_cast<uint16_t *>(tt + sw128_kmajor_offset(n, j, kXTN)) = v;
     }
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kYxStages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-        for (int c = 0; c < kYxMaxChunks; c++) { mbar_init(&ychunk[c], 1); mbar_init(&ypacked[c], kYxConvWarps); }
+        for (int s = 0; s < stages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        mbar_init(yfull, 1);
+        mbar_init(yfree, kYxConvWarps);
+        mbar_init(ypacked, kYxConvWarps);
+        mbar_init(ypfree, 1);
         mbar_init(xfull, 1);
         mbar_init(xempty, kYxEpiWarps);
         mbar_init(drain, 1);
@@ -148,36 +155,32 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    if (warp >= 2 && warp < 10) {
-        // y Toeplitz halves into tensor memory (zero outside the band): the two
-        // warps of a lane quadrant write Ty_hi and Ty_lo of its 32 rows.
-        const int quad = warp & 3, lo_half = (warp - 2) >> 2;
-        if (!(lo_half && p.hi_only)) {
-            const int o = quad * 32 + lane;
-            const uint16_t *taps = lo_half ? ty.lo : ty.hi;
-            for (int ch = 0; ch < ty.kcols / 32; ch++) {
-                uint32_t r[32];
+    if (warp >= 2 && warp < 6) {
+        // y Toeplitz into tensor memory (zero outside the band): one warp per quadrant.
+        const int quad = warp & 3;
+        const int o = quad * 32 + lane;
+        for (int ch = 0; ch < ty.kcols / 32; ch++) {
+            uint32_t r[32];
 #pragma unroll
-                for (int j = 0; j < 32; j++) {
-                    uint32_t v = 0;
+            for (int j = 0; j < 32; j++) {
+                uint32_t v = 0;
 #pragma unroll
-                    for (int e = 0; e < 2; e++) {
-                        const int k = 2 * (ch * 32 + j) + e, t = k - o;
-                        if (t >= 0 && t <= 2 * ty.radius && k < ty.kp) v |= (uint32_t) taps[t] << (16 * e);
-                    }
-                    r[j] = v;
+                for (int e = 0; e < 2; e++) {
+                    const int k = 2 * (ch * 32 + j) + e, t = k - o;
+                    if (t >= 0 && t <= 2 * ty.radius && k < ty.kp) v |= (uint32_t) ty.hi[t] << (16 * e);
                 }
-                tmem_st32(tmem + ((uint32_t) (quad * 32) << 16) + kYxToep + (lo_half ? ty.kcols : 0) + ch * 32, r);
+                r[j] = v;
             }
-            tmem_st_wait();
+            tmem_st32(tmem + ((uint32_t) (quad * 32) << 16) + kYxToep + ch * 32, r);
         }
+        tmem_st_wait();
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
 
-    // Tile g: plane z, y-tile ty_, x-tile tx_ (x fastest, so the CTAs in flight
-    // work on neighbouring tiles of one or two planes and share their halos in L2).
+    // Tile g: plane z, y-tile, x-tile (x fastest, so the CTAs in flight work on
+    // neighbouring tiles of one or two planes and share their halos in L2).
     auto decode = [&](int64_t g, int &z, int &y0, int &x0) {
         const uint32_t gg = (uint32_t) g, rest = gg / n_tx, t_y = rest % n_ty;
         x0 = (int) (gg - rest * n_tx) * kXTN;
@@ -198,8 +201,8 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
             }
             decode(g, z, y0, x0);
             for (int c = 0; c < nch; c++, cl++) {
-                const int s = (int) (cl % kYxStages);
-                const uint32_t ph = (uint32_t) ((cl / kYxStages) & 1);
+                const int s = (int) (cl % stages);
+                const uint32_t ph = (uint32_t) ((cl / stages) & 1);
                 if (!mbar_wait(&empty[s], ph ^ 1, 1)) { ok = false; break; }
                 mbar_arrive_expect_tx(&full[s], chunk_bytes);
                 tma_load_3d(ring + s * chunk_bytes, &tmap, x0 - tx.ra + 64 * c, y0 - ty.radius, z, &full[s]);
@@ -207,90 +210,109 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
         }
         // Let every copy this thread started land before the CTA can exit: the
         // last use of each ring stage (bounded, so an aborted run still ends).
-        for (int64_t k = cl - kYxStages; k < cl; k++)
-            if (k >= 0) mbar_wait(&full[k % kYxStages], (uint32_t) ((k / kYxStages) & 1), 1);
+        for (int64_t k = cl - stages; k < cl; k++)
+            if (k >= 0) mbar_wait(&full[k % stages], (uint32_t) ((k / stages) & 1), 1);
     } else if (warp == 1 && lane == 0) {
-        // MMA issuer.  Per tile: the y MMAs chunk by chunk (each chunk committed
-        // on its own barrier, so its conversion starts while the next chunks
-        // multiply), then the x MMAs chunk by chunk as each chunk of Y' lands.
-        // The y MMAs of a tile overwrite the previous tile's Y', which the x MMAs
-        // issued before them have read (tcgen05.mma of one thread run in issue order).
+        // MMA issuer.  Step tl issues the y MMAs of tile tl (one chain per chunk)
+        // and the x MMAs of tile tl - 1, one K step of every chain in turn.
         const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
         const uint32_t idesc_y = idesc_f16(fmt, 0 /*A K-major*/, 1 /*B MN-major*/, kTM, 64);
         const uint32_t idesc_x = idesc_f16(fmt, 0 /*A K-major*/, 0 /*B K-major*/, kTM, kXTN);
         const uint32_t r0 = smem_u32(ring), t0 = smem_u32(tt);
-        const uint32_t a_hi = tmem + kYxToep, a_lo = a_hi + ty.kcols;
-        const int ksx = tx.kp / 16;
-        int64_t cl = 0, tl = 0;
+        const int ksy = ty.kp / 16, ksx = tx.kp / 16, ks_max = ksy > ksx ? ksy : ksx;
+        int64_t cl = 0;
         bool ok = true;
-        for (int64_t g = blockIdx.x; ok && g < total; g += gridDim.x, tl++) {
-            const uint32_t ph = (uint32_t) (tl & 1);
-            for (int c = 0; c < nch; c++, cl++) {
-                const int s = (int) (cl % kYxStages);
-                if (!mbar_wait(&full[s], (uint32_t) ((cl / kYxStages) & 1), 1)) { ok = false; break; }
-                tc_fence_after();
-                const uint64_t bd = smem_desc_sw128(r0 + s * chunk_bytes, chunk_bytes, 1024);
-                const uint32_t d = tmem + kYxAccY + 64 * c;
-                for (int ks = 0; ks < ty.kp / 16; ks++) {
-                    umma_f16_ts(d, a_hi + ks * 8, bd + (uint64_t) (ks * 128), idesc_y, ks > 0 ? 1u : 0u);
-                    if (!p.hi_only) umma_f16_ts(d, a_lo + ks * 8, bd + (uint64_t) (ks * 128), idesc_y, 1u);
+        for (int64_t tl = 0;; tl++) {
+            const int64_t g = blockIdx.x + tl * (int64_t) gridDim.x;
+            const bool has_y = g < total, has_x = tl > 0 && g - gridDim.x < total;
+            if (!has_y && !has_x) break;
+            int s[kYxMaxChunks] = {0, 0, 0};
+            if (has_y) {
+                for (int c = 0; c < nch && ok; c++) {
+                    s[c] = (int) ((cl + c) % stages);
+                    ok = mbar_wait(&full[s[c]], (uint32_t) (((cl + c) / stages) & 1), 1);
                 }
-                umma_commit(&empty[s]);
-                umma_commit(&ychunk[c]);
+                // the conversion warps have read the previous tile's y accumulators
+                if (ok && tl > 0) ok = mbar_wait(yfree, (uint32_t) ((tl - 1) & 1), 3);
+            }
+            if (ok && has_x) {
+                // Y' of tile tl - 1 is in place and the epilogue has drained the x accumulator
+                ok = mbar_wait(ypacked, (uint32_t) ((tl - 1) & 1), 3) &&
+                     mbar_wait(xempty, (uint32_t) (((tl - 1) & 1) ^ 1), 3);
             }
             if (!ok) break;
-            if (!mbar_wait(xempty, ph ^ 1, 3)) break;  // the epilogue has drained the x accumulator
-            const uint32_t dx = tmem + kYxAccX;
-            for (int c = 0; c < nch && ok; c++) {
-                if (!mbar_wait(&ypacked[c], ph, 3)) { ok = false; break; }
-                tc_fence_after();
-                for (int ks = 4 * c; ks < 4 * c + 4 && ks < ksx; ks++) {
-                    const uint32_t kin = (ks & 3) * 32;
-                    const uint32_t bhi = t0 + (ks >> 2) * (tt_rows * 128) + kin;
-                    umma_f16_ts(dx, tmem + kYxAccY + ks * 8, smem_desc_sw128(bhi, 16, 1024), idesc_x, ks > 0 ? 1u : 0u);
-                    if (!p.hi_only)
-                        umma_f16_ts(dx, tmem + kYxAccY + ks * 8, smem_desc_sw128(bhi + kXTN * 128, 16, 1024), idesc_x, 1u);
+            tc_fence_after();
+            for (int ks = 0; ks < ks_max; ks++) {
+                if (has_y && ks < ksy) {
+                    for (int c = 0; c < nch; c++) {
+                        const uint64_t bd = smem_desc_sw128(r0 + s[c] * chunk_bytes, chunk_bytes, 1024);
+                        umma_f16_ts(tmem + kYxAccY + 64 * c, tmem + kYxToep + ks * 8, bd + (uint64_t) (ks * 128),
+                                    idesc_y, ks > 0 ? 1u : 0u);
+                    }
+                }
+                if (has_x && ks < ksx) {
+                    const uint32_t bhi = t0 + (ks >> 2) * (kXTN * 128) + (ks & 3) * 32;
+                    umma_f16_ts(tmem + kYxAccX, tmem + kYxYp + ks * 8, smem_desc_sw128(bhi, 16, 1024), idesc_x,
+                                ks > 0 ? 1u : 0u);
                 }
             }
-            if (!ok) break;
-            umma_commit(xfull);
+            if (has_y) {
+                for (int c = 0; c < nch; c++) umma_commit(&empty[s[c]]);
+                umma_commit(yfull);
+                cl += nch;
+            }
+            if (has_x) {
+                umma_commit(xfull);
+                umma_commit(ypfree);
+            }
         }
         // Every MMA this thread issued has completed before the CTA winds down.
         umma_commit(drain);
         mbar_wait(drain, 0, 2);
     } else if (warp >= 2 && warp < 2 + kYxConvWarps) {
-        // Conversion: y accumulator (FP32) -> Y' (16-bit, packed) in place, one
-        // 64-column chunk at a time; the two warps of a quadrant take 32 columns
-        // each.  Chunk c's packed words land on FP32 columns of chunk c / 2: both
-        // warps have read those (the pair barrier orders the reads of chunk c
-        // before either warp's writes of chunk c).
+        // Conversion: y accumulators (FP32) -> Y' (16-bit, packed).  The two warps
+        // of a quadrant take the 32-column runs [3 half, 3 half + 3) of the window.
         const int quad = warp & 3, half = (warp - 2) >> 2;
         const uint32_t lb = tmem + ((uint32_t) (quad * 32) << 16);
+        const int c_lo = 3 * half, c_hi = ncc < c_lo + 3 ? ncc : c_lo + 3;
         int64_t tl = 0;
         bool ok = true;
         for (int64_t g = blockIdx.x; ok && g < total; g += gridDim.x, tl++) {
             int z, y0, x0;
             decode(g, z, y0, x0);
-            for (int c = 0; c < nch; c++) {
-                // warp-uniform, then pair-uniform outcome of the wait: both warps
-                // of the pair reach the barrier either way and leave together
-                ok = __all_sync(0xffffffffu, mbar_wait(&ychunk[c], (uint32_t) (tl & 1), 2));
-                tc_fence_after();
+            ok = __all_sync(0xffffffffu, mbar_wait(yfull, (uint32_t) (tl & 1), 2));
+            if (!ok) break;
+            tc_fence_after();
+            for (int cc = c_lo; cc < c_hi || (cc == c_lo && c_lo >= c_hi); cc++) {
+                const bool live = cc < c_hi;  // a half with no runs still signals
                 float v[32];
                 __syncwarp();
-                if (ok) tmem_ld32(lb + kYxAccY + 64 * c + 32 * half, v);
-                ok = pair_barrier_and(quad, ok);
-                if (!ok) break;
-                const int64_t xs = (int64_t) x0 - tx.ra + 64 * c + 32 * half;
-                uint32_t d[16], w[16];
-                narrow32_pairs<S, true>(v, ty.inv_scale, ty.error_feedback, 0u, live_bits(xs, p.nx), d);
-                pairs_to_adjacent(d, w);
-                tmem_st16(lb + kYxAccY + 32 * c + 16 * half, w);
-                tmem_st_wait();
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&ypacked[c]);
+                if (live) tmem_ld32(lb + kYxAccY + 32 * cc, v);
+                if (cc + 1 >= c_hi) {
+                    // every read of this warp is done: the y accumulators may be reused
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(yfree);
+                }
+                if (cc == c_lo && tl > 0) {
+                    // the x MMAs of the previous tile have read Y'
+                    ok = __all_sync(0xffffffffu, mbar_wait(ypfree, (uint32_t) ((tl - 1) & 1), 2));
+                    if (!ok) break;
+                    tc_fence_after();
+                }
+                if (live) {
+                    const int64_t xs = (int64_t) x0 - tx.ra + 32 * cc;
+                    uint32_t d[16], w[16];
+                    narrow32_quads<S, true>(v, ty.inv_scale, ty.error_feedback, 0u, live_bits(xs, p.nx), d);
+                    quads_to_adjacent(d, w);
+                    tmem_st16(lb + kYxYp + 16 * cc, w);
+                }
             }
+            if (!ok) break;
+            tmem_st_wait();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(ypacked);
         }
     } else if (warp >= 2 + kYxConvWarps) {
         // Epilogue: x accumulator -> re-illumination -> next field / final outputs.

@@ -79,7 +79,7 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
                         (mask_fmt == MAXI_MASK_U8 ? reinterpret_cast<uintptr_t>(mask) : 0)) & 15) == 0;
     // Fused y + x kernel: z pass buf0 -> buf1, y + x buf1 -> buf0 ([y][z][x] rows
     // between repetitions), so the buffers do not swap.
-    const bool yx = tc_x && fuse_yx && tc::tc_yx_supported(radius, v.nz, v.ny, v.nx);
+    const bool yx = tc_x && fuse_yx && hi_only && tc::tc_yx_supported(radius, v.nz, v.ny, v.nx);
     if (reps > 0)
         note_path(yx ? (MAXI_PATH_TENSOR_CORES_ZY | MAXI_PATH_FUSED_YX)
                      : ((use_tc ? MAXI_PATH_TENSOR_CORES_ZY : MAXI_PATH_CUDA_CORES) |
@@ -113,7 +113,7 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
                 // [y][z][x] row order (over all v.nz planes), which the z pass reads faster.
                 const tc::YzRows yz{buf0, v.nz, lo};
                 if (use_tc) e = tc::tc_strided<S>(b0, b1, nzv, v.ny, v.nx, true, kernel, radius, EF, st,
-                                                  tc_x && rep > 0 ? &yz : nullptr);
+                                                  tc_x && rep > 0 ? &yz : nullptr, hi_only);
                 else zy<<<zat * zit, kStrThreads, str_smem, st>>>(b0, b1, zA, zI, zat, zit, taps);
             } else {
                 zy<<<zat * zit, kStrThreads, str_smem, st>>>(b0, b1, zA, zI, zat, zit, taps);
@@ -134,7 +134,7 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
         {
             ProfScope ps(MAXI_KERNEL_Y, st);
             if constexpr (sizeof(S) == 2) {
-                if (use_tc) e = tc::tc_strided<S>(b1, b0, nzv, v.ny, v.nx, false, kernel, radius, EF, st);
+                if (use_tc) e = tc::tc_strided<S>(b1, b0, nzv, v.ny, v.nx, false, kernel, radius, EF, st, nullptr, hi_only);
                 else zy<<<yat * yit * yO, kStrThreads, str_smem, st>>>(b1, b0, yA, yI, yat, yit, taps);
             } else {
                 zy<<<yat * yit * yO, kStrThreads, str_smem, st>>>(b1, b0, yA, yI, yat, yit, taps);
@@ -147,7 +147,7 @@ static cudaError_t run_unrolled(const Volume &v, const void *mask, int mask_fmt,
                 if constexpr (sizeof(S) == 2) {
                     const tc::YzRows yz{buf1, v.nz, lo};
                     e = tc::tc_contig<S>(b0, b1, mv, mask_fmt, last, last ? ou : nullptr, last ? fo : nullptr, nzv,
-                                         v.ny, v.nx, kernel, radius, EF, st, &yz);
+                                         v.ny, v.nx, kernel, radius, EF, st, &yz, hi_only);
                 }
             } else if (!last) {
                 xpass<<<xt * xrb, kConThreads, con_smem, st>>>(b0, b1, mv, nullptr, nullptr, rows, v.nx, xt, taps);
@@ -202,7 +202,7 @@ cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, c
         // The rebuilt-mask semantics rewrite the mask between repetitions from the
         // x pass's output; they keep the separate passes.
         const bool fuse = (flags & (MAXI_FLAG_SEPARATE_PASSES | MAXI_FLAG_MASK_FROM_FIELD)) == 0;
-        const bool hi_only = (flags & MAXI_FLAG_SINGLE_COEFFICIENTS) != 0;
+        const bool hi_only = (flags & MAXI_FLAG_SPLIT_COEFFICIENTS) == 0;
         if (ef) return dispatch_radius<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, fuse, hi_only, rebuild, o, st);
         return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, fuse, hi_only, rebuild, o, st);
     } else {

@@ -24,7 +24,7 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
             field: str = "f32", field_out: torch.Tensor | None = None, shape=None,
             reference_rounding: bool = False, workspace: torch.Tensor | None = None,
             stream: torch.cuda.Stream | None = None, tensor_cores: bool = True,
-            error_feedback: bool = True, fuse_passes: bool = True, single_coefficients: bool = False) -> None:
+            error_feedback: bool = True, fuse_passes: bool = True, split_coefficients: bool = False) -> None:
     """Run the diffusion on device buffers.
 
     mask: uint8 [nz, ny, nx] CUDA tensor (set when > 0), or a bit-packed int32/uint32
@@ -38,8 +38,9 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
     error_feedback: 16-bit fields: error-feedback rounding along x (else round to nearest).
     fuse_passes: 16-bit tensor-core fields, radius <= 32: the y and x passes in one
           kernel per z-plane tile (else two kernels, two HBM round trips).
-    single_coefficients: fused kernel: one 16-bit coefficient set with the kernel's
-          sum and second moment kept, instead of high + low halves.
+    split_coefficients: 16-bit tensor-core passes: high + low 16-bit coefficient halves
+          (two MMAs per K step, separate y and x passes) instead of one set whose
+          taps keep the kernel's sum and second moment.
     """
     if not mask.is_cuda:
         raise ValueError("mask must be a CUDA tensor")
@@ -80,8 +81,8 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
         flags |= _lib.FLAG_NEAREST_ROUNDING
     if not fuse_passes:
         flags |= _lib.FLAG_SEPARATE_PASSES
-    if single_coefficients:
-        flags |= _lib.FLAG_SINGLE_COEFFICIENTS
+    if split_coefficients:
+        flags |= _lib.FLAG_SPLIT_COEFFICIENTS
     with torch.cuda.device(mask.device):
         _lib.check(_lib.lib().maxi_diffusion_device(
             mask.data_ptr(), fmt, nz, ny, nx, k.ctypes.data, k.shape[0], int(repititions),

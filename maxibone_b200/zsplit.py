@@ -226,3 +226,19 @@ def diffuse_slabs_in_process(mask: torch.Tensor, kernel, plan: SplitPlan, step, 
     for rank, s in enumerate(slabs):
         z0, z1 = plan.bounds[rank]
         s.results(output[z0:z1] if output is not None else None, field_out[z0:z1] if field_out is not None else None)
+
+
+def assign_volumes(shapes, radii, reps, world: int) -> list:
+    """Independent volumes of a batch spread over `world` ranks (no collective:
+    each rank runs a batch plan of its own volumes).  Greedy longest-first
+    packing by estimated work: voxels x repetitions x the tensor-core passes' K
+    per output, (128 + 2r) / 128, so heavy volumes are placed first, each on the
+    least loaded rank.  Returns one list of volume indices per rank."""
+    cost = [float(np.prod(s)) * max(1, int(n)) * (1.0 + 2.0 * r / 128.0) for s, r, n in zip(shapes, radii, reps)]
+    loads = [0.0] * world
+    out = [[] for _ in range(world)]
+    for i in sorted(range(len(cost)), key=lambda i: (-cost[i], i)):
+        k = min(range(world), key=lambda w: (loads[w], w))
+        out[k].append(i)
+        loads[k] += cost[i]
+    return [sorted(v) for v in out]

@@ -7,6 +7,8 @@ agree with the separate y and x passes (both round the intermediate field to
 the same type, with error-feedback chains that start at different x), keep
 mask voxels exact, and be deterministic.  Every run asserts that the fused
 kernel is what ran (MAXI_PATH_FUSED_YX), so a fallback cannot pass unnoticed.
+The fused kernel uses the single coefficient set (the default); the split
+high + low halves run the separate passes.
 """
 import numpy as np
 import pytest
@@ -22,7 +24,7 @@ FUSED_VS_SEPARATE = {"bf16": 4e-3, "f16": 1e-3}
 FUSED = _lib.PATH_TENSOR_CORES_ZY | _lib.PATH_FUSED_YX
 
 
-def run(mask, kernel, reps, field, fused=True, single=False, output=True, field_out=True, bitpacked=False):
+def run(mask, kernel, reps, field, fused=True, split=False, output=True, field_out=True, bitpacked=False):
     m = torch.from_numpy(np.ascontiguousarray(mask, np.uint8)).cuda()
     shape = tuple(mask.shape)
     fo = torch.empty(shape, dtype=torch.float64 if field == "f64" else torch.float32, device="cuda") \
@@ -31,10 +33,10 @@ def run(mask, kernel, reps, field, fused=True, single=False, output=True, field_
     if bitpacked:
         m = device.bitpack(m)
     device.diffuse(m, kernel, reps, output=out, field=field, field_out=fo, fuse_passes=fused,
-                   single_coefficients=single, shape=shape)
+                   split_coefficients=split, shape=shape)
     path = device.last_path()
     if field in ("bf16", "f16"):
-        if fused:
+        if fused and not split:
             assert path & FUSED == FUSED and not path & _lib.PATH_TENSOR_CORES_X, hex(path)
         else:
             assert not path & _lib.PATH_FUSED_YX, hex(path)
@@ -76,16 +78,19 @@ def test_fused_radius_range(radius):
 
 
 @pytest.mark.parametrize("field", ["bf16", "f16"])
-def test_fused_single_coefficients_within_bounds(field):
-    # One 16-bit coefficient set (sum and second moment kept) instead of high +
-    # low halves: half the tensor-core work, error still within the bound.
+def test_single_and_split_coefficients_within_bounds(field):
+    # The default single 16-bit coefficient set (sum and second moment kept,
+    # fused y + x kernel) and the split high + low halves (separate passes)
+    # both stay within the bound of the FP64 form, and close to each other.
     from maxibone_b200.synthetic import bone_implant_mask
     mask = bone_implant_mask((128, 128, 256), seed=4, implant_radius=20.0).numpy()
     kernel = gauss_kernel(8.0).astype(np.float32)
     _, want = run(mask, kernel, 40, "f64")
-    u16, got = run(mask, kernel, 40, field, single=True)
+    u16, got = run(mask, kernel, 40, field)
+    u16s, split = run(mask, kernel, 40, field, split=True)
     assert np.abs(got.astype(np.float64) - want).max() <= VS_F64[field]
-    assert np.all(u16[mask > 0] == 65535)
+    assert np.abs(split.astype(np.float64) - want).max() <= VS_F64[field]
+    assert np.all(u16[mask > 0] == 65535) and np.all(u16s[mask > 0] == 65535)
 
 
 @pytest.mark.parametrize("field", ["bf16", "f16"])

@@ -121,3 +121,18 @@ def test_split_rounds_in_one_process_equal_single_volume(world, reps, k):
     want_u16, want = oracle.diffusion_in_memory(mask, kernel, reps)
     np.testing.assert_array_equal(field.numpy(), want)
     np.testing.assert_array_equal(out.view(torch.int16).numpy().view(np.uint16), want_u16)
+
+
+def test_assign_volumes_balances_the_batch():
+    from maxibone_b200.synthetic import batch_shapes
+    from maxibone_b200.zsplit import assign_volumes
+    specs = batch_shapes(64, seed=0)
+    shapes = [s for s, _, _ in specs]
+    radii = [int(round(4 * sig)) for _, sig, _ in specs]
+    for world in (1, 2, 4, 8):
+        parts = assign_volumes(shapes, radii, [50] * 64, world)
+        assert sorted(i for p in parts for i in p) == list(range(64))
+        work = [sum(np.prod(shapes[i]) * (1 + 2 * radii[i] / 128) for i in p) for p in parts]
+        # greedy longest-first: within the largest single volume of the mean
+        biggest = max(np.prod(s) * (1 + 2 * r / 128) for s, r in zip(shapes, radii))
+        assert max(work) - min(work) <= biggest

@@ -22,11 +22,11 @@ Also reported on the same line:
                 in and out, from pinned and from pageable host buffers;
   cfg0          the 128^3 sphere mask, sigma 3, R = 10, FP32, beside the
                 reference module on the same input;
-  precision     the 1024^3 mask bit-packed, BF16 and FP16 fields (z pass and the
-                fused y + x tensor-core kernel; the separate passes; the split
-                coefficient halves), R = 100 and R = 500, max / mean abs error against the
-                FP64 form and the FP32 form; sigma = 32 (257 taps), CUDA-core
-                stencil vs banded-Toeplitz tensor cores;
+  precision     the 1024^3 mask bit-packed, BF16 and FP16 fields (the z, y and x
+                tensor-core passes; the fused y + x kernel; the split coefficient
+                halves; CUDA cores), R = 100 and R = 500, max / mean abs error
+                against the FP64 form and the FP32 form; sigma = 32 (257 taps),
+                CUDA-core stencil vs banded-Toeplitz tensor cores;
   batched       64 uneven volumes, sigma in {2, 4, 8}, R = 50, BF16 plan vs
                 per-volume FP32 launches, error of every volume vs FP64;
   out_of_core   3456 x 3456 x 4096 (z, y, x) mask streamed from pinned host
@@ -99,11 +99,22 @@ def parse_args():
                         "histograms, morphology, implant masks) on its output, and print their JSON object")
     p.add_argument("--shape", type=str, default=None,
                    help="override the workload's volume shape, e.g. 256x1024x1024 (profiling of smaller cases)")
+    p.add_argument("--fuse-passes", action="store_true",
+                   help="16-bit fields: the headline step runs the fused y + x tensor-core kernel")
     p.add_argument("--reps", type=int, default=None,
                    help="override the workload's repetition count (profiling of smaller cases)")
     p.add_argument("--ooc-shape", type=str, default="3456x3456x4096",
                    help="out-of-core section's volume, z x y x x")
     return p.parse_args()
+
+
+_T0 = time.perf_counter()
+
+
+def progress(msg: str) -> None:
+    """One progress line on stderr (the JSON line alone goes to stdout)."""
+    sys.stderr.write(f"[bench {time.perf_counter() - _T0:7.1f} s] {msg}\n")
+    sys.stderr.flush()
 
 
 def load_peaks():
@@ -614,6 +625,26 @@ def sampled(local_rank, fn):
     return res, clocks
 
 
+class PinnedArray:
+    """A numpy array page-locked with cudaHostRegister: exactly its own size
+    (torch's pinned allocator rounds every allocation up to a power of two,
+    which turns 43 + 87 GB into 64 + 128 GB)."""
+
+    def __init__(self, torch, np, shape, dtype):
+        self.torch = torch
+        self.a = np.empty(shape, dtype)
+        self.ptr = self.a.ctypes.data
+        rc = int(torch.cuda.cudart().cudaHostRegister(self.ptr, self.a.nbytes, 0))
+        if rc != 0:
+            raise MemoryError(f"cudaHostRegister of {self.a.nbytes} bytes failed ({rc})")
+
+    def close(self):
+        if self.ptr:
+            self.torch.cuda.cudart().cudaHostUnregister(self.ptr)
+            self.ptr = 0
+            self.a = None
+
+
 def out_of_core_section(torch, np, shape, reps=20):
     """cfg4: a bone-implant mask larger than the device in pinned host memory
     (3456 x 3456 x 4096, z x y x x, 49 GB), sigma 8, R = 20, BF16 field, through
@@ -634,8 +665,8 @@ def out_of_core_section(torch, np, shape, reps=20):
     avail = psutil.virtual_memory().available
     note = None
     need = 3 * nz * ny * nx  # uint8 mask + uint16 output
-    if need > 0.7 * avail:
-        nz_fit = max(64, int(0.7 * avail / (3 * ny * nx)) // 64 * 64)
+    if need > 0.75 * avail:
+        nz_fit = max(64, int(0.75 * avail / (3 * ny * nx)) // 64 * 64)
         note = (f"host RAM {avail / 1e9:.0f} GB available: z reduced from {nz} to {nz_fit} "
                 f"(the pinned mask and output need 3 bytes per voxel)")
         nz = min(nz, nz_fit)
@@ -643,8 +674,9 @@ def out_of_core_section(torch, np, shape, reps=20):
     vox = nz * ny * nx
     kernel = gauss_kernel(8.0).astype(np.float32)
     t0 = time.perf_counter()
-    host_m = torch.empty(shape, dtype=torch.uint8, pin_memory=True)
-    host_o = torch.empty(shape, dtype=torch.int16, pin_memory=True)
+    pin_m = PinnedArray(torch, np, shape, np.uint8)
+    pin_o = PinnedArray(torch, np, shape, np.uint16)
+    host_m = torch.from_numpy(pin_m.a)
     t_alloc = time.perf_counter() - t0
     t0 = time.perf_counter()
     chunk = 128
@@ -657,7 +689,7 @@ def out_of_core_section(torch, np, shape, reps=20):
     s_, k_, r_ = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
     _lib.check(_lib.lib().maxi_out_of_core_plan(nz, ny, nx, 0, kernel.shape[0], reps, _lib.FIELD_TYPES["bf16"], 0, 0,
                                                 ctypes.byref(s_), ctypes.byref(k_), ctypes.byref(r_)))
-    m_np, o_np = host_m.numpy(), host_o.numpy().view(np.uint16)
+    m_np, o_np = pin_m.a, pin_o.a
     t0 = time.perf_counter()
     diffusion_out_of_core(m_np, kernel, o_np, (0, ny, nx), reps, field="bf16")
     dt = time.perf_counter() - t0
@@ -684,7 +716,9 @@ def out_of_core_section(torch, np, shape, reps=20):
            "setup_seconds": {"pinned_allocation": t_alloc, "mask_generation": t_gen}}
     if note:
         res["note"] = note
-    del host_m, host_o
+    del host_m, m_np, o_np
+    pin_m.close()
+    pin_o.close()
     return res
 
 
@@ -746,7 +780,7 @@ PRECISION_FORMS = [
     ("f32", "f32", {}),
     ("bf16", "bf16", {}),
     ("bf16_split_coefficients", "bf16", {"split_coefficients": True}),
-    ("bf16_separate_passes", "bf16", {"fuse_passes": False}),
+    ("bf16_fused_yx", "bf16", {"fuse_passes": True}),
     ("f16", "f16", {}),
     ("f16_split_coefficients", "f16", {"split_coefficients": True}),
     ("bf16_nearest", "bf16", {"error_feedback": False}),
@@ -912,7 +946,8 @@ def main():
         ws = torch.empty(device.workspace_bytes(shape, args.field), dtype=torch.uint8, device="cuda")
 
         def step(field=args.field, output=out, workspace=ws, field_out=None):
-            device.diffuse(mask, kernel, reps, output=output, field=field, workspace=workspace, field_out=field_out)
+            device.diffuse(mask, kernel, reps, output=output, field=field, workspace=workspace, field_out=field_out,
+                           fuse_passes=args.fuse_passes)
 
     def barrier():
         if world > 1:
@@ -1000,7 +1035,8 @@ def main():
         "config": {"workload": args.workload + (f" (shape override {args.shape})" if args.shape else "")
                    + (f" (repetitions override {args.reps})" if args.reps is not None else ""),
                    "shape": list(shape), "sigma": sigma, "kernel_size": int(2 * radius + 1),
-                   "reps": reps, "field": args.field, "mask": "u8", "foreground": round(fg, 4),
+                   "reps": reps, "field": args.field, "fuse_passes": bool(args.fuse_passes), "mask": "u8",
+                   "foreground": round(fg, 4),
                    "parallelism": (f"one volume split into {world} z-slabs (one per rank), halo planes exchanged "
                                    f"every {split.k} repetitions by NCCL P2P" if split else
                                    f"{world} independent volumes (one per rank)"),
@@ -1037,6 +1073,7 @@ def main():
         del host_mask, host_out
 
     if "e2e" in sections:
+        progress("section e2e")
         # End to end through the reference-facing call: numpy in, numpy out, from
         # pinned host memory and from pageable host memory (maxibone's callers
         # pass np.empty arrays).
@@ -1070,6 +1107,7 @@ def main():
         torch.cuda.empty_cache()
 
     if "precision" in sections:
+        progress("section precision")
         res, ck = sampled(local_rank, lambda: precision_section(device, torch, np, mask, kernel, reps, stream))
         res["clocks"] = ck
         res["workload"] = (f"{nz}x{ny}x{nx} bone-implant mask bit-packed (1 bit per voxel), sigma {sigma}, R={reps}; "
@@ -1083,14 +1121,17 @@ def main():
                                "bf16_split_coefficients_max_abs_err_vs_f64":
                                    res["bf16_split_coefficients"]["max_abs_err_vs_f64"]}
     if "long" in sections:
+        progress("section long")
         res, ck = sampled(local_rank, lambda: long_section(device, torch, np, mask, kernel, stream))
         res["clocks"] = ck
         line["long"] = res
     if "cfg0" in sections:
+        progress("section cfg0")
         res, ck = sampled(local_rank, lambda: cfg0_section(device, torch, np, stream))
         res["clocks"] = ck
         line["cfg0"] = res
     if "downstream" in sections:
+        progress("section downstream")
         out_u16 = torch.empty(shape, dtype=torch.uint16, device="cuda")
         device.diffuse(mask, kernel, reps, output=out_u16)
         line["fields"] = {"combine_fields": fields_section(torch, np, out_u16, stream),
@@ -1099,6 +1140,7 @@ def main():
         line["implant_masks"] = implant_section(torch, np, mask, stream)
         del out_u16
     if "batched" in sections:
+        progress("section batched")
         res, ck = sampled(local_rank, lambda: batched_section(device, torch, np, stream))
         res["clocks"] = ck
         line["batched"] = res
@@ -1108,6 +1150,7 @@ def main():
             bv["speedup_vs_f32"] = bv["value"] / line["precision"]["f32"]["value"]
     torch.cuda.empty_cache()
     if "out_of_core" in sections and world == 1:
+        progress("section out_of_core")
         ooc_shape = tuple(int(v) for v in args.ooc_shape.lower().split("x"))
         del mask
         torch.cuda.empty_cache()
@@ -1117,6 +1160,7 @@ def main():
         mask = None
 
     if "cpu" in sections and rank == 0 and world == 1:
+        progress("section cpu")
         cshape, csig, creps = CPU_SAMPLE
         times, kind, cores, cvox, (cmask, ckernel, cref) = cpu_reference_time(cshape, csig, creps, 2)
         line["cpu_baseline"] = {"value": cvox * creps / min(times) / 1e9, "unit": UNIT, "cores": cores,

@@ -56,19 +56,24 @@ typedef enum maxi_mask_format {
 #define MAXI_FLAG_MASK_FROM_FIELD 0x8    /* FP32 only: before every repetition after the first,
                                             the mask is rebuilt as `field == 1.0f` -- the
                                             semantics of the reference's on-disk variant */
-#define MAXI_FLAG_AUTOTUNE 0x10          /* batch plans: time tensor-core vs CUDA-core passes per
-                                            group and keep the faster (cached per process) */
+#define MAXI_FLAG_AUTOTUNE 0x10          /* batch plans: time each tensor-core group's forms
+                                            (one batched launch per pass, per-volume tensor-core
+                                            launches, per-volume CUDA-core passes) and keep the
+                                            fastest (cached per process and in a JSON file) */
 #define MAXI_FLAG_NEAREST_ROUNDING 0x4   /* BF16/FP16: plain round-to-nearest stores instead of
                                             error-feedback rounding along x (the default for
                                             radius >= 4, which keeps the stored rounding noise
                                             out of the result) */
-#define MAXI_FLAG_SEPARATE_PASSES 0x20   /* BF16/FP16 tensor cores: run the y and x passes as two
-                                            kernels (two HBM round trips) instead of the fused
-                                            y + x kernel used for radius <= 32 */
+#define MAXI_FLAG_SEPARATE_PASSES 0x20   /* BF16/FP16 tensor cores: the y and x passes as two
+                                            kernels (two HBM round trips; the default); overrides
+                                            MAXI_FLAG_FUSE_YX */
+#define MAXI_FLAG_FUSE_YX 0x80           /* BF16/FP16 tensor cores, radius <= 32: the y and x
+                                            passes in one kernel per z-plane tile (the field
+                                            between them stays on the SM) */
 #define MAXI_FLAG_SPLIT_COEFFICIENTS 0x40 /* BF16/FP16 tensor cores: Toeplitz coefficients as high +
                                             low 16-bit halves (two MMAs per K step) instead of the
                                             default single set whose taps are rounded so that the
-                                            kernel's sum and second moment are kept; implies
+                                            kernel's sum and second moment are kept; runs the
                                             separate y and x passes */
 
 const char *maxi_last_error(void);
@@ -246,7 +251,12 @@ typedef struct maxi_batch_plan maxi_batch_plan; /* opaque */
 
 /* Allocates the workspace of all volumes, groups them, optionally autotunes
  * (MAXI_FLAG_AUTOTUNE, timing on `stream`) and captures the repetition loop
- * into a CUDA graph.  Field types F32, BF16, F16. */
+ * into a CUDA graph.  Field types F32, BF16, F16.
+ * Tuning choices are keyed by GPU name and SM count, field type, radius and the
+ * group's volume shapes, and persisted in the JSON file named by the
+ * environment variable MAXIBONE_TUNE_CACHE (an empty value: no file), else
+ * $XDG_CACHE_HOME/maxibone_b200/batch_tune.json or
+ * ~/.cache/maxibone_b200/batch_tune.json. */
 int maxi_batch_plan_create(const maxi_volume *volumes, int64_t n_volumes, int32_t field_type, int32_t flags,
                            void *stream, maxi_batch_plan **plan);
 /* Launches the plan's graph on `stream` (asynchronous; may be replayed). */
@@ -255,6 +265,9 @@ int maxi_batch_plan_run(maxi_batch_plan *plan, void *stream);
 int maxi_batch_plan_describe(const maxi_batch_plan *plan, char *buffer, int64_t buffer_bytes);
 /* Waits for the device and frees the plan. */
 int maxi_batch_plan_destroy(maxi_batch_plan *plan);
+/* Drops the process's tuning choices: the next autotuned plan reads the cache
+ * file again (and times what it does not hold). */
+int maxi_batch_tune_forget(void);
 /* create + run + synchronise + destroy. */
 int maxi_diffusion_batched(const maxi_volume *volumes, int64_t n_volumes, int32_t field_type, int32_t flags,
                            void *stream);
@@ -269,7 +282,9 @@ int maxi_diffusion_batched(const maxi_volume *volumes, int64_t n_volumes, int32_
  * side so all repetitions run on the device without exchanges; when such halos
  * leave no room for useful slabs (large repititions x radius), the repetitions
  * run in rounds of k with k x radius halos and the field goes through host
- * memory between rounds (8 bytes per voxel of pinned host memory).  Planes of
+ * memory between rounds (8 bytes per voxel of pinned host memory; only when
+ * that fits half of the host's available memory, MemAvailable, or
+ * MAXIBONE_OOC_HOST_BUDGET bytes when that environment variable is set).  Planes of
  * a multiple of 32 voxels keep the whole mask bit-packed on the device.
  * FP32 field; results equal maxi_diffusion_in_memory().
  */
@@ -290,7 +305,9 @@ int maxi_diffusion_out_of_core_ex(const uint8_t *voxels, int64_t nz, int64_t ny,
  * memory, or MAXIBONE_OOC_DEVICE_BUDGET bytes when that environment variable
  * is set and smaller) writes the slab depth, the repetitions per round (equal
  * to repititions: one round with deep halos, no exchange) and whether the mask
- * stays bit-packed on the device.  MAXI_ERR_OUT_OF_MEMORY when no slab fits.
+ * stays bit-packed on the device.  Exchange rounds are only planned when their
+ * 8 bytes per voxel fit the host memory that may be pinned (see
+ * maxi_diffusion_out_of_core).  MAXI_ERR_OUT_OF_MEMORY when no slab fits.
  */
 int maxi_out_of_core_plan(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, int64_t kernel_size,
                           int64_t repititions, int32_t field_type, int32_t flags, int64_t device_bytes,

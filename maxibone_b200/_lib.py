@@ -24,6 +24,7 @@ FLAG_NEAREST_ROUNDING = 0x4
 FLAG_MASK_FROM_FIELD = 0x8
 FLAG_AUTOTUNE = 0x10
 FLAG_SEPARATE_PASSES = 0x20
+FLAG_FUSE_YX = 0x80
 FLAG_SPLIT_COEFFICIENTS = 0x40
 PATH_CUDA_CORES = 0x1
 PATH_TENSOR_CORES_ZY = 0x2
@@ -69,6 +70,7 @@ SIGNATURES = {
     "maxi_batch_plan_run": (_int, [_p, _p]),
     "maxi_batch_plan_describe": (_int, [_p, ctypes.c_char_p, _i64]),
     "maxi_batch_plan_destroy": (_int, [_p]),
+    "maxi_batch_tune_forget": (_int, []),
     "maxi_diffusion_batched": (_int, [_p, _i64, _i32, _i32, _p]),
     "maxi_diffusion_out_of_core": (_int, [_p, _i64, _i64, _i64, _i64, _i64, _i64, _p, _i64, _i64, _p, _int]),
     "maxi_diffusion_out_of_core_ex": (_int, [_p, _i64, _i64, _i64, _i64, _p, _i64, _i64, _p, _i32, _i32, _int]),

@@ -10,11 +10,22 @@
 // 64-volume, 50-repetition batch is a single graph launch.
 //
 // Autotuning (MAXI_FLAG_AUTOTUNE): for each tensor-core group the plan times
-// three repetitions of the group's batched tensor-core passes against the
-// per-volume CUDA-core passes and keeps the faster; decisions are cached per
-// process, keyed by the group's kernel length, field type and volume shapes,
-// and reported by maxi_batch_plan_describe().
+// three repetitions of each form the group can run in -- one batched
+// tensor-core launch per pass over all its volumes, the single-volume
+// tensor-core launches volume by volume, and the per-volume CUDA-core passes
+// -- and keeps the fastest.  Choices are keyed by the GPU (name and SM count),
+// field type, radius and the group's volume shapes, kept for the process and
+// persisted in a JSON file (MAXIBONE_TUNE_CACHE, else
+// $XDG_CACHE_HOME/maxibone_b200/batch_tune.json or
+// ~/.cache/maxibone_b200/batch_tune.json; MAXIBONE_TUNE_CACHE set to an empty
+// string keeps them in the process only), so a later process plans without
+// timing.  maxi_batch_plan_describe() reports each group's form and timings.
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -41,6 +52,11 @@ struct BatchVolume {
     int32_t run_type = MAXI_FIELD_F32;
 };
 
+// How a tensor-core group runs: one launch per pass over all its volumes, the
+// single-volume tensor-core launches per volume, or per-volume CUDA-core passes.
+enum GroupForm { kFormBatched = 0, kFormPerVolumeTc = 1, kFormCudaCores = 2, kForms = 3 };
+static const char *const kFormNames[kForms] = {"batched", "per_volume_tc", "cuda_cores"};
+
 struct TcGroup {
     std::vector<int> members;
     std::vector<float> kernel;
@@ -49,12 +65,81 @@ struct TcGroup {
     tc::TcVol *d_vols = nullptr;
     int64_t *d_prefix = nullptr;  // [3][n + 1]: z columns, y columns, x tiles
     int64_t totals[3] = {0, 0, 0};
-    bool use_tc = true;
+    int form = kFormBatched;
     std::string note;
 };
 
+// A tuning decision and the timings it came from (ms for 3 repetitions; < 0: not timed).
+struct TuneEntry {
+    int form = kFormBatched;
+    float ms[kForms] = {-1.0f, -1.0f, -1.0f};
+};
+
 static std::mutex g_tune_mu;
-static std::map<std::string, bool> g_tune_cache;  // group signature -> tensor cores faster
+static std::map<std::string, TuneEntry> g_tune_cache;  // group key -> decision
+static bool g_tune_loaded = false;
+
+// Path of the persistent tuning cache ("" when persistence is off).
+static std::string tune_cache_path() {
+    if (const char *env = getenv("MAXIBONE_TUNE_CACHE")) return env;
+    const char *xdg = getenv("XDG_CACHE_HOME");
+    if (xdg && *xdg) return std::string(xdg) + "/maxibone_b200/batch_tune.json";
+    const char *home = getenv("HOME");
+    if (home && *home) return std::string(home) + "/.cache/maxibone_b200/batch_tune.json";
+    return "";
+}
+
+// Reads the cache file into g_tune_cache (entries already in the process win).
+// One entry per line: "key": {"form": "name", "batched_ms": t, ...}.
+static void tune_load_locked() {
+    g_tune_loaded = true;
+    const std::string path = tune_cache_path();
+    if (path.empty()) return;
+    FILE *f = fopen(path.c_str(), "r");
+    if (!f) return;
+    char line[4096];
+    while (fgets(line, sizeof line, f)) {
+        const char *k0 = strchr(line, '"');
+        const char *k1 = k0 ? strchr(k0 + 1, '"') : nullptr;
+        const char *fm = k1 ? strstr(k1, "\"form\": \"") : nullptr;
+        if (!fm) continue;
+        const std::string key(k0 + 1, k1);
+        fm += strlen("\"form\": \"");
+        TuneEntry e;
+        e.form = -1;
+        for (int i = 0; i < kForms; i++) {
+            const size_t n = strlen(kFormNames[i]);
+            if (strncmp(fm, kFormNames[i], n) == 0 && fm[n] == '"') e.form = i;
+            const std::string tag = std::string("\"") + kFormNames[i] + "_ms\": ";
+            if (const char *t = strstr(fm, tag.c_str())) e.ms[i] = strtof(t + tag.size(), nullptr);
+        }
+        if (e.form >= 0 && !g_tune_cache.count(key)) g_tune_cache[key] = e;
+    }
+    fclose(f);
+}
+
+// Writes g_tune_cache to the cache file (a temporary file renamed over it);
+// failures leave the process cache as it is.
+static void tune_save_locked() {
+    const std::string path = tune_cache_path();
+    if (path.empty()) return;
+    for (size_t i = 1; i < path.size(); i++)  // mkdir -p of the directory
+        if (path[i] == '/') mkdir(path.substr(0, i).c_str(), 0755);
+    const std::string tmp = path + ".tmp" + std::to_string((long long) getpid());
+    FILE *f = fopen(tmp.c_str(), "w");
+    if (!f) return;
+    fprintf(f, "{\n\"format\": \"maxibone_b200 batch tuning cache 1\",\n\"entries\": {\n");
+    size_t i = 0;
+    for (const auto &kv : g_tune_cache) {
+        fprintf(f, "\"%s\": {\"form\": \"%s\"", kv.first.c_str(), kFormNames[kv.second.form]);
+        for (int j = 0; j < kForms; j++)
+            if (kv.second.ms[j] >= 0.0f) fprintf(f, ", \"%s_ms\": %.4f", kFormNames[j], kv.second.ms[j]);
+        fprintf(f, "}%s\n", ++i < g_tune_cache.size() ? "," : "");
+    }
+    fprintf(f, "}\n}\n");
+    const bool ok = fclose(f) == 0;
+    if (!ok || rename(tmp.c_str(), path.c_str()) != 0) remove(tmp.c_str());
+}
 
 }  // namespace maxi
 
@@ -138,16 +223,22 @@ static cudaError_t enqueue_group_tc(maxi_batch_plan *p, TcGroup &g, cudaStream_t
     return cudaSuccess;
 }
 
+// All repetitions of a group in the given form.
+template <typename S>
+static cudaError_t enqueue_group(maxi_batch_plan *p, TcGroup &g, int form, cudaStream_t st) {
+    if (form == kFormBatched) return enqueue_group_tc<S>(p, g, st);
+    cudaError_t e = cudaSuccess;
+    const int32_t extra = form == kFormCudaCores ? MAXI_FLAG_NO_TENSOR_CORES : 0;
+    for (int i : g.members)
+        if ((e = enqueue_single<S>(p, p->vols[i], extra, st)) != cudaSuccess) break;
+    return e;
+}
+
 template <typename S>
 static cudaError_t enqueue_all(maxi_batch_plan *p, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
-    for (TcGroup &g : p->groups) {
-        if (g.use_tc) e = enqueue_group_tc<S>(p, g, st);
-        else
-            for (int i : g.members)
-                if ((e = enqueue_single<S>(p, p->vols[i], MAXI_FLAG_NO_TENSOR_CORES, st)) != cudaSuccess) break;
-        if (e != cudaSuccess) return e;
-    }
+    for (TcGroup &g : p->groups)
+        if ((e = enqueue_group<S>(p, g, g.form, st)) != cudaSuccess) return e;
     for (BatchVolume &bv : p->vols) {
         if (bv.group >= 0) continue;
         e = (sizeof(S) == 2 && bv.run_type == MAXI_FIELD_F32) ? enqueue_single<float>(p, bv, 0, st)
@@ -158,7 +249,7 @@ static cudaError_t enqueue_all(maxi_batch_plan *p, cudaStream_t st) {
 }
 
 template <typename S>
-static cudaError_t time_group(maxi_batch_plan *p, TcGroup &g, bool use_tc, cudaStream_t st, float *ms) {
+static cudaError_t time_group(maxi_batch_plan *p, TcGroup &g, int form, cudaStream_t st, float *ms) {
     // Three repetitions so the one-off mask packing and field set-up of both
     // candidates do not dominate the comparison.
     const int64_t saved = g.reps;
@@ -174,10 +265,7 @@ static cudaError_t time_group(maxi_batch_plan *p, TcGroup &g, bool use_tc, cudaS
     cudaError_t e = cudaSuccess;
     for (int it = 0; it < 2 && e == cudaSuccess; it++) {  // first run warms up
         cudaEventRecord(a, st);
-        if (use_tc) e = enqueue_group_tc<S>(p, g, st);
-        else
-            for (int i : g.members)
-                if ((e = enqueue_single<S>(p, p->vols[i], MAXI_FLAG_NO_TENSOR_CORES, st)) != cudaSuccess) break;
+        e = enqueue_group<S>(p, g, form, st);
         cudaEventRecord(b, st);
     }
     if (e == cudaSuccess) e = cudaEventSynchronize(b);
@@ -189,12 +277,27 @@ static cudaError_t time_group(maxi_batch_plan *p, TcGroup &g, bool use_tc, cudaS
     return e;
 }
 
-static std::string group_signature(const maxi_batch_plan *p, const TcGroup &g) {
-    std::string s = "f" + std::to_string(p->field_type) + ":k" + std::to_string(g.kernel.size()) + ":";
+// Tuning key of a group: GPU name and SM count, field type, radius and the
+// sorted volume shapes (z x y x x).
+static std::string group_key(const maxi_batch_plan *p, const TcGroup &g) {
+    cudaDeviceProp prop;
+    std::string gpu = "unknown";
+    if (cudaGetDeviceProperties(&prop, p->device) == cudaSuccess)
+        gpu = std::string(prop.name) + " sm" + std::to_string(prop.multiProcessorCount);
+    else
+        cudaGetLastError();
+    for (char &c : gpu)
+        if (c == '"' || c == '\\' || c == '|') c = '_';
+    static const char *const types[] = {"f32", "bf16", "f16", "f64"};
+    const int ft = p->field_type;
+    std::string s = gpu + "|" + (ft >= 0 && ft < 4 ? types[ft] : "?") + "|r" + std::to_string(g.kernel.size() / 2) + "|";
+    std::vector<std::string> shapes;
     for (int i : g.members) {
         const maxi_volume &v = p->vols[i].v;
-        s += std::to_string(v.nz) + "x" + std::to_string(v.ny) + "x" + std::to_string(v.nx) + ",";
+        shapes.push_back(std::to_string(v.nz) + "x" + std::to_string(v.ny) + "x" + std::to_string(v.nx));
     }
+    std::sort(shapes.begin(), shapes.end());
+    for (size_t i = 0; i < shapes.size(); i++) s += (i ? "," : "") + shapes[i];
     return s;
 }
 
@@ -248,31 +351,42 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
             cudaMemcpy(g.d_prefix, prefix.data(), sizeof(int64_t) * prefix.size(), cudaMemcpyHostToDevice) != cudaSuccess)
             return set_cuda_error(cudaGetLastError(), "batch table upload");
     }
-    // Autotune: tensor-core batch vs per-volume CUDA-core passes, per group.
+    // Autotune: the fastest form of each group (from the cache when known).
     if (p->flags & MAXI_FLAG_AUTOTUNE) {
         for (TcGroup &g : p->groups) {
-            const std::string sig = group_signature(p, g);
-            bool known = false, tc_wins = true;
+            const std::string key = group_key(p, g);
+            bool known = false;
+            TuneEntry te;
             {
                 std::lock_guard<std::mutex> lk(g_tune_mu);
-                auto it = g_tune_cache.find(sig);
-                if (it != g_tune_cache.end()) known = true, tc_wins = it->second;
+                if (!g_tune_loaded) tune_load_locked();
+                auto it = g_tune_cache.find(key);
+                if (it != g_tune_cache.end()) known = true, te = it->second;
             }
-            float t_tc = 0, t_cc = 0;
             if (!known) {
-                cudaError_t e = time_group<S>(p, g, true, user_st, &t_tc);
-                if (e == cudaSuccess) e = time_group<S>(p, g, false, user_st, &t_cc);
-                if (e != cudaSuccess) return set_cuda_error(e, "batch autotuning");
-                tc_wins = t_tc <= t_cc;
+                // A single volume's batched launch is its per-volume launch.
+                for (int f = 0; f < kForms; f++) {
+                    if (f == kFormPerVolumeTc && g.members.size() == 1) continue;
+                    cudaError_t e = time_group<S>(p, g, f, user_st, &te.ms[f]);
+                    if (e != cudaSuccess) return set_cuda_error(e, "batch autotuning");
+                    if (te.ms[f] < te.ms[te.form]) te.form = f;
+                }
                 std::lock_guard<std::mutex> lk(g_tune_mu);
-                g_tune_cache[sig] = tc_wins;
+                g_tune_cache[key] = te;
+                tune_save_locked();
             }
-            g.use_tc = tc_wins;
-            char buf[160];
-            if (known) snprintf(buf, sizeof(buf), "cached choice: %s", tc_wins ? "tensor cores" : "CUDA cores");
-            else snprintf(buf, sizeof(buf), "tuned: tensor cores %.3f ms vs CUDA cores %.3f ms for 3 repetitions -> %s",
-                          t_tc, t_cc, tc_wins ? "tensor cores" : "CUDA cores");
-            g.note = buf;
+            g.form = te.form;
+            std::string note = known ? "cached choice" : "tuned";
+            char buf[96];
+            bool first = true;
+            for (int f = 0; f < kForms; f++)
+                if (te.ms[f] >= 0.0f) {
+                    snprintf(buf, sizeof(buf), "%s %s %.3f ms", first ? ":" : ",", kFormNames[f], te.ms[f]);
+                    note += buf;
+                    first = false;
+                }
+            note += std::string(" (3 repetitions) -> ") + kFormNames[te.form];
+            g.note = note;
         }
     }
     // Capture the whole repetition loop.
@@ -289,7 +403,7 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
     cudaStreamDestroy(cap);
     if (e != cudaSuccess) return set_cuda_error(e, "batch graph capture");
     // Description.
-    char line[256];
+    char line[512];
     snprintf(line, sizeof(line), "%zu volumes, field type %d, %zu tensor-core groups\n", p->vols.size(),
              p->field_type, p->groups.size());
     p->description = line;
@@ -297,8 +411,9 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
         const TcGroup &g = p->groups[k];
         snprintf(line, sizeof(line), "group %zu: %zu volumes, kernel length %zu, %lld repetitions, %s%s%s\n", k,
                  g.members.size(), g.kernel.size(), (long long) g.reps,
-                 !g.use_tc ? "per-volume CUDA-core passes"
-                 : g.members.size() == 1 ? "single-volume tensor-core launches" : "one tensor-core launch per pass",
+                 g.form == kFormCudaCores ? "per-volume CUDA-core passes"
+                 : g.form == kFormPerVolumeTc || g.members.size() == 1 ? "single-volume tensor-core launches"
+                                                                        : "one tensor-core launch per pass",
                  g.note.empty() ? "" : "; ", g.note.c_str());
         p->description += line;
     }
@@ -401,6 +516,14 @@ int maxi_batch_plan_describe(const maxi_batch_plan *plan, char *buffer, int64_t 
     clear_error();
     if (!plan || !buffer || buffer_bytes <= 0) return set_error(MAXI_ERR_INVALID_ARGUMENT, "NULL argument");
     snprintf(buffer, (size_t) buffer_bytes, "%s", plan->description.c_str());
+    return MAXI_OK;
+}
+
+int maxi_batch_tune_forget(void) {
+    clear_error();
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache.clear();
+    g_tune_loaded = false;
     return MAXI_OK;
 }
 

@@ -19,6 +19,8 @@
 //     planes; between rounds the slabs' FP32 fields go to a host copy of the
 //     field (double-buffered, 8 bytes per voxel of pinned host memory) and the
 //     next round starts from it.  FP32 results equal the in-memory form's.
+//     Only where those 8 bytes per voxel fit half of the host's available
+//     memory (MemAvailable; MAXIBONE_OOC_HOST_BUDGET overrides).
 //
 // A planner picks the slab depth (at most the caller's) and the plan from the
 // free device memory and a cost estimate (voxel-repetitions computed, bytes
@@ -28,6 +30,8 @@
 // second stream while the next slab's repetitions run (only its last
 // repetition waits for that copy).  Pageable host buffers are staged through
 // pinned memory by the host thread.
+#include <unistd.h>
+
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -67,6 +71,7 @@ struct SlabPlan {
     bool resident = false, shrinks = false;
     int64_t chunk_planes = 0;  // planes per upload chunk of a resident mask
     double cost = 0.0;         // estimated seconds
+    bool host_limited = false;  // exchange rounds ruled out by the host memory they would pin
 };
 
 static int64_t field_size(int32_t ft) { return ft == MAXI_FIELD_F32 ? 4 : ft == MAXI_FIELD_F64 ? 8 : 2; }
@@ -172,10 +177,34 @@ static int64_t device_budget(size_t free_b) {
     return (int64_t) free_b;
 }
 
-// The whole plan for `free_b` device bytes: resident mask or not, whether the
-// loop shrinks its window, then slab depth and repetitions per round.
+// Host bytes the exchange rounds may pin: half of the available memory
+// (MemAvailable in /proc/meminfo), or the environment variable
+// MAXIBONE_OOC_HOST_BUDGET (bytes) when it is set.
+static int64_t host_budget() {
+    const char *env = getenv("MAXIBONE_OOC_HOST_BUDGET");
+    if (env && *env) {
+        const long long v = atoll(env);
+        if (v >= 0) return v;
+    }
+    long long kb = -1;
+    if (FILE *f = fopen("/proc/meminfo", "r")) {
+        char line[256];
+        while (fgets(line, sizeof line, f))
+            if (sscanf(line, "MemAvailable: %lld kB", &kb) == 1) break;
+        fclose(f);
+    }
+    if (kb < 0) {
+        const long pages = sysconf(_SC_AVPHYS_PAGES), page = sysconf(_SC_PAGESIZE);
+        if (pages > 0 && page > 0) kb = (long long) pages * (page / 1024);
+    }
+    return kb > 0 ? (int64_t) kb * 1024 / 2 : 0;
+}
+
+// The whole plan for `free_b` device bytes and `host_b` pinnable host bytes:
+// resident mask or not, whether the loop shrinks its window, then slab depth
+// and repetitions per round.
 static SlabPlan full_plan(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, int64_t kernel_size, int64_t repititions,
-                          int32_t field_type, int32_t flags, int64_t free_b) {
+                          int32_t field_type, int32_t flags, int64_t free_b, int64_t host_b) {
     const int64_t plane = ny * nx, n = nz * plane;
     const int64_t radius = kernel_size / 2, R = std::max<int64_t>(1, repititions);
     const bool rebuild = (flags & MAXI_FLAG_MASK_FROM_FIELD) != 0;
@@ -187,8 +216,10 @@ static SlabPlan full_plan(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, in
     const bool resident = !rebuild && plane % 32 == 0 && repititions > 0 &&
                           packed_bytes + 2 * chunk_planes * plane < budget / 4;
     if (resident) budget -= packed_bytes + 2 * chunk_planes * plane;
-    // Exchange rounds keep FP32 fields on the host: not for the FP64 form.
-    const bool allow_exchange = field_type != MAXI_FIELD_F64 && repititions > 1;
+    // Exchange rounds keep two FP32 fields on the host: not for the FP64 form,
+    // and only where the host can pin them.
+    const bool exchange_form = field_type != MAXI_FIELD_F64 && repititions > 1;
+    const bool allow_exchange = exchange_form && 8 * n <= host_b;
     // The repetition loop shrinks its plane window towards the slab's core on
     // the unrolled passes (not the generic ones: FP64, reference rounding,
     // radius > 128) when planes are whole mask words.
@@ -199,6 +230,7 @@ static SlabPlan full_plan(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, in
     pl.resident = resident;
     pl.shrinks = shrinks;
     pl.chunk_planes = chunk_planes;
+    pl.host_limited = exchange_form && !allow_exchange;
     return pl;
 }
 
@@ -215,9 +247,18 @@ static int run_slabs(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, const f
 
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    const SlabPlan pl = full_plan(nz, ny, nx, slab_z, kernel_size, repititions, field_type, flags, device_budget(free_b));
+    const SlabPlan pl = full_plan(nz, ny, nx, slab_z, kernel_size, repititions, field_type, flags, device_budget(free_b),
+                                  host_budget());
     const bool resident = pl.resident, shrinks = pl.shrinks;
     const int64_t packed_bytes = round_up(ceil_div(n, 32) * 4, 256), chunk_planes = pl.chunk_planes;
+    if (pl.S < 1 && pl.host_limited)
+        return set_error(MAXI_ERR_OUT_OF_MEMORY,
+                         "%lld repetitions x radius %lld need halos of %lld planes per slab side, which leave no "
+                         "slab that fits the %lld free bytes of the device, and rounds that exchange the field "
+                         "through host memory need %lld bytes of pinned host memory (8 per voxel) where %lld may "
+                         "be pinned (half of MemAvailable, or MAXIBONE_OOC_HOST_BUDGET)",
+                         (long long) repititions, (long long) radius, (long long) std::min(nz, repititions * radius),
+                         (long long) device_budget(free_b), (long long) (8 * n), (long long) host_budget());
     if (pl.S < 1)
         return set_error(MAXI_ERR_OUT_OF_MEMORY,
                          "no slab of whole %lld x %lld planes fits the %lld free bytes of the device (one plane with "
@@ -521,10 +562,17 @@ extern "C" int maxi_out_of_core_plan(int64_t nz, int64_t ny, int64_t nx, int64_t
         if (e != cudaSuccess) return set_cuda_error(e, "cudaMemGetInfo");
         device_bytes = device_budget(free_b);
     }
-    const SlabPlan pl = full_plan(nz, ny, nx, slab_z, kernel_size, repititions, field_type, flags, device_bytes);
+    const SlabPlan pl = full_plan(nz, ny, nx, slab_z, kernel_size, repititions, field_type, flags, device_bytes,
+                                  host_budget());
     *slab_planes = pl.S;
     *reps_per_round = std::min(pl.k, std::max<int64_t>(1, repititions));
     *resident_mask = pl.resident ? 1 : 0;
+    if (pl.S < 1 && pl.host_limited)
+        return set_error(MAXI_ERR_OUT_OF_MEMORY,
+                         "no slab with %lld-plane halos fits %lld device bytes, and exchange rounds need %lld bytes "
+                         "of pinned host memory where %lld may be pinned",
+                         (long long) std::min(nz, std::max<int64_t>(1, repititions) * (kernel_size / 2)),
+                         (long long) device_bytes, (long long) (8 * nz * ny * nx), (long long) host_budget());
     if (pl.S < 1) return set_error(MAXI_ERR_OUT_OF_MEMORY, "no slab fits %lld device bytes", (long long) device_bytes);
     return MAXI_OK;
 }

@@ -225,11 +225,8 @@ cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool fina
     YxLaunch p{};
     const int ra = (int) round_up(radius, 8);
     if (!hi_only) return cudaErrorInvalidValue;  // the fused kernel holds one coefficient set
-    fill_pass_taps(p.ty, kernel, radius, 0, (int) round_up(kTM + 2 * radius, 16), is_bf16, error_feedback, true);
-    fill_pass_taps(p.tx, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback, true);
-    if (p.tx.kp > kYxMaxChunks * 64 || kYxYp < (uint32_t) (64 * ((p.tx.kp + 63) / 64)) ||
-        kYxYp + p.tx.kp / 2 > kYxAccX || kYxToep + p.ty.kcols > kYxTmemCols)
-        return cudaErrorInvalidValue;
+    fill_pass_taps(p.t, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback, true);
+    if (p.t.kp > kYxMaxCols || (uint32_t) p.t.kp / 2 > kYxYpCols) return cudaErrorInvalidValue;
     p.final_pass = final_pass ? 1 : 0;
     p.mask = mask;
     p.out = reinterpret_cast<uint16_t *>(out_rows ? out_rows->base : static_cast<void *>(out));
@@ -247,7 +244,7 @@ cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool fina
     CUtensorMap map;
     const cuuint64_t dims[3] = {(cuuint64_t) nx, (cuuint64_t) ny, (cuuint64_t) nz};
     const cuuint64_t strides[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (nx * ny * 2)};
-    const cuuint32_t box[3] = {64u, (cuuint32_t) p.ty.kp, 1u};
+    const cuuint32_t box[3] = {64u, (cuuint32_t) p.t.kp, 1u};
     const cuuint32_t estr[3] = {1, 1, 1};
     CUresult cr = tc_encode_fn()(&map, is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
                                  const_cast<S *>(in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -258,9 +255,9 @@ cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool fina
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    p.stages = yx_stages(p.ty.kp, p.tx.kpa, smem_max);
-    const int smem = yx_smem_bytes(p.ty.kp, p.tx.kpa, p.stages);
-    if (smem > smem_max || p.stages < (p.tx.kp + 63) / 64) return cudaErrorInvalidValue;
+    p.stages = yx_stages(p.t.kp, p.t.kpa, smem_max);
+    const int smem = yx_smem_bytes(p.t.kp, p.t.kpa, p.stages);
+    if (smem > smem_max) return cudaErrorInvalidValue;
     auto *kern = mask_fmt == MAXI_MASK_U8 ? tc_yx_kernel<S, MAXI_MASK_U8> : tc_yx_kernel<S, MAXI_MASK_BITPACKED>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;

@@ -4,20 +4,22 @@
 // kernel does both convolutions of one z-plane tile of 128 y-outputs x 128
 // x-outputs without the intermediate field ever leaving the SM:
 //
-//   1. y MMAs: Y[o, j] = sum_k Ty[o, k] F[y0 - R + k, x0 - RA + j] for the 128
-//      outputs o along y and KX = 128 + RA + R (rounded to 16) x-columns j --
-//      the x pass's input window, halo included.  Ty (Toeplitz, in tensor
-//      memory) is the A operand, F arrives by TMA in chunks of 64 x-columns x
-//      KP = 128 + 2R rows (MN-major, 128-byte swizzle; rows and columns outside
-//      the plane are zero-filled: the zero boundary).  Y accumulates in FP32 in
-//      tensor memory, one lane per y-output, one accumulator per chunk.
-//   2. Conversion warps read Y back lane by lane (tcgen05.ld), narrow it to the
-//      16-bit storage type with error-feedback rounding along x (four chains of
-//      8 per 32 columns, two voxels per instruction), zero the columns outside
-//      the volume (the x pass's zero boundary), and write it packed two per
-//      column (tcgen05.st) into its own tensor-memory region: the K-major
-//      layout of an A operand in tensor memory.
-//   3. x MMAs: D[o, x] = sum_j Y'[o, j] Tt[j, x] with the x Toeplitz Tt in
+//   1. y MMA: Y[o, j] = sum_k T[o, k] F[y0 - RA + k, x0 - RA + j] for the 128
+//      outputs o along y and the KP = 128 + RA + R (rounded to 16) x-columns j
+//      of the x pass's input window, halo included (RA = R rounded up to 8, the
+//      16-byte alignment of the window's first x).  T[o, k] = tap[k - o - RA + R]
+//      (zero outside the band) is the A operand in shared memory; F arrives by
+//      TMA as KP rows x KP columns (64-column boxes, MN-major, 128-byte swizzle;
+//      rows and columns outside the plane are zero-filled: the zero boundary).
+//      One accumulation chain of N = KP columns, FP32, in tensor memory.
+//   2. Conversion warps read Y back (tcgen05.ld), narrow it to the 16-bit
+//      storage type with error-feedback rounding along x (chains of 8 voxels,
+//      two voxels per instruction) and write it packed two per column
+//      (tcgen05.st) into one of two Y' buffers: the K-major layout of an A
+//      operand in tensor memory.  Columns outside the volume hold exact zeros
+//      (their F columns are zero and nx is a multiple of 8, so every chain lies
+//      wholly inside or wholly outside): the x pass's zero boundary.
+//   3. x MMA: D[o, x] = sum_j Y'[o, j] T[x, j], the same Toeplitz matrix in
 //      shared memory as the B operand (K-major), into the x accumulator.
 //   4. Epilogue warps: re-illumination from the bit-packed mask, then either
 //      the next field (error-feedback rounding, [y][z][x] or [z][y][x] rows) or,
@@ -30,18 +32,16 @@
 // passes).  Coefficients: one 16-bit set rounded to keep the kernel's sum and
 // second moment (tc_round_taps_matched).
 //
-// Tensor-core schedule.  Consecutive MMAs into one accumulator are bound by the
-// MMA latency (about 130 cycles on B200 for N <= 192), so the MMA issuer keeps
-// several accumulation chains in flight: the three 64-column y chunks of tile t
-// (three accumulators) and the x MMAs of tile t - 1 (a fourth), one K step of
-// each in turn.  That needs Y' of tile t - 1 to stay in place while tile t's y
-// accumulates, hence its own region.  Tensor memory (512 columns): [0, 192) y
-// accumulator, [192, 288) Y' packed, [288, 416) x accumulator, [416, 512) the
-// y Toeplitz.  Warp roles: 0 TMA producer, 1 MMA issuer, 2-9 conversion (two
-// per TMEM lane quadrant, 96 columns each), 10-17 epilogue (two per quadrant,
-// 64 x-outputs each).  Every wait is bounded; on a timeout the kernel records a
-// code in g_tc_error, lets the copies and MMAs it started finish (bounded) and
-// winds down.
+// Tensor-core schedule.  A tcgen05.mma of M = 128 costs the issuing thread
+// about 130 cycles on B200 whatever its N (up to 192), so every product is one
+// chain of the widest N: 2 KP / 16 MMAs per tile.  Step t issues y(t), then
+// x(t - 1): the conversion of tile t runs while the tensor cores do x(t - 1),
+// and writes the other Y' buffer.  Tensor memory (512 columns): [0, 192) y
+// accumulator, [192, 384) the two Y' buffers, [384, 512) x accumulator.  Warp
+// roles: 0 TMA producer, 1 MMA issuer, 2-9 conversion (two per TMEM lane
+// quadrant), 10-17 epilogue (two per quadrant, 64 x-outputs each).  Every wait
+// is bounded; on a timeout the kernel records a code in g_tc_error, lets the
+// copies and MMAs it started finish (bounded) and winds down.
 #pragma once
 
 #include "tc_kernels.cuh"
@@ -49,37 +49,37 @@
 namespace maxi {
 namespace tc {
 
-constexpr int kYxMaxStages = 8;                                  // F chunk ring (64 x-columns x KP rows each)
+constexpr int kYxMaxStages = 4;                                  // F tile ring
 constexpr int kYxConvWarps = 8;                                  // two per TMEM lane quadrant
 constexpr int kYxEpiWarps = 8;                                   // two per lane quadrant
 constexpr int kYxThreads = 64 + 32 * (kYxConvWarps + kYxEpiWarps);  // 576
-constexpr int kYxMaxChunks = 3;                                  // 64-column chunks of the x window (radius <= 32)
-constexpr uint32_t kYxAccY = 0;                                  // y accumulators, up to 3 x 64 columns
-constexpr uint32_t kYxYp = 192;                                  // Y' packed, up to 96 columns
-constexpr uint32_t kYxAccX = 288;                                // x accumulator, 128 columns
-constexpr uint32_t kYxToep = 416;                                // y Toeplitz, up to 96 columns
+constexpr int kYxMaxCols = 192;                                  // KP for radius <= 32
+constexpr uint32_t kYxAccY = 0;                                  // y accumulator, KP columns
+constexpr uint32_t kYxYp = 192;                                  // two Y' buffers of KP / 2 columns
+constexpr uint32_t kYxYpCols = 96;
+constexpr uint32_t kYxAccX = 384;                                // x accumulator, 128 columns
 constexpr uint32_t kYxTmemCols = 512;
 
-// Shared memory: x Toeplitz (kpa K x 128 rows), the F chunk ring of `stages`
-// chunks, the barriers and the epilogue's store staging.
-__host__ __device__ constexpr int yx_smem_bytes(int kp_y, int kpa_x, int stages) {
-    return 1024 + kpa_x * kXTN * 2 + stages * kp_y * 128 + 1024 + kYxEpiWarps * kXStageWarpBytes;
+// One F tile: ceil(KP / 64) boxes of 64 x-columns x KP rows.
+__host__ __device__ constexpr int yx_tile_bytes(int kp) { return ((kp + 63) / 64) * kp * 128; }
+
+// Shared memory: the Toeplitz matrix (kpa K x 128 rows), the F tile ring of
+// `stages` tiles, the barriers and the epilogue's store staging.
+__host__ __device__ constexpr int yx_smem_bytes(int kp, int kpa, int stages) {
+    return 1024 + kpa * kXTN * 2 + stages * yx_tile_bytes(kp) + 1024 + kYxEpiWarps * kXStageWarpBytes;
 }
 
-// The deepest F ring (at most kYxMaxStages chunks) that fits `smem_max` bytes.
-// A tile's y MMAs need its chunks together, so the ring holds two tiles'
-// chunks where it can: the loads of the next tile run while this one multiplies.
-__host__ __device__ constexpr int yx_stages(int kp_y, int kpa_x, int smem_max) {
+// The deepest F ring (2 .. kYxMaxStages tiles) that fits `smem_max` bytes.
+__host__ __device__ constexpr int yx_stages(int kp, int kpa, int smem_max) {
     int st = kYxMaxStages;
-    while (st > 3 && yx_smem_bytes(kp_y, kpa_x, st) > smem_max) st--;
+    while (st > 2 && yx_smem_bytes(kp, kpa, st) > smem_max) st--;
     return st;
 }
 
 struct YxLaunch {
-    PassTaps ty;  // y convolution: kp = 128 + 2R rounded to 16, kcols
-    PassTaps tx;  // x convolution: ra, kp = 128 + RA + R rounded to 16, kpa
+    PassTaps t;  // ra = RA, kp = KP = 128 + RA + R rounded to 16, one coefficient set
     int final_pass;
-    int stages;         // F ring depth (chunks), at least the chunks of one tile
+    int stages;         // F ring depth (tiles)
     const void *mask;
     uint16_t *out;      // next field (not final): [z][y][x], or [y][z][x] rows when out_nz > 0
     uint16_t *out_u16;  // final
@@ -89,36 +89,28 @@ struct YxLaunch {
     int64_t n_tiles;
 };
 
-// Bits [lo, hi) of a 32-bit word (the voxels of a 32-voxel run inside [0, nx)).
-__device__ __forceinline__ uint32_t live_bits(int64_t xs, int64_t nx) {
-    if (xs >= 0 && xs + 32 <= nx) return 0xffffffffu;
-    const int64_t lo = xs < 0 ? -xs : 0, hi = nx - xs < 32 ? nx - xs : 32;
-    if (hi <= lo) return 0u;
-    const uint32_t upto = hi >= 32 ? 0xffffffffu : ((1u << hi) - 1u);
-    return upto & ~((1u << lo) - 1u);
-}
-
 template <typename S, int FMT>
 __global__ void __launch_bounds__(kYxThreads, 1)
 tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ YxLaunch p) {
-    const PassTaps &ty = p.ty, &tx = p.tx;
+    const PassTaps &tp = p.t;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     uint8_t *smem = smem_raw + (((raw + 1023) & ~1023u) - raw);
-    uint8_t *tt = smem;                                         // x Toeplitz, K-major, 128 rows
-    uint8_t *ring = tt + tx.kpa * kXTN * 2;                     // a multiple of 16 KB: 1024-aligned
-    const int chunk_bytes = ty.kp * 128;                        // 64 x-columns x KP rows of 16-bit
-    const int nch = (tx.kp + 63) / 64;                          // chunks per tile (<= 3)
-    const int ncc = (tx.kp + 31) / 32;                          // 32-column runs of Y' (<= 6)
+    uint8_t *tt = smem;                                         // Toeplitz, K-major, 128 rows
+    uint8_t *ring = tt + tp.kpa * kXTN * 2;                     // a multiple of 16 KB: 1024-aligned
+    const int kp = tp.kp;
+    const int chunk_bytes = kp * 128;                           // 64 x-columns x KP rows of 16-bit
+    const int nch = (kp + 63) / 64;                             // boxes per tile (<= 3)
+    const int tile_bytes = nch * chunk_bytes;
+    const int ncc = (kp + 31) / 32;                             // 32-column runs of Y (5 or 6)
     const int stages = p.stages;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + stages * chunk_bytes);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + stages * tile_bytes);
     uint64_t *full = bars, *empty = bars + kYxMaxStages;
-    uint64_t *yfull = bars + 2 * kYxMaxStages;  // y accumulators complete (MMA commit)
-    uint64_t *yfree = yfull + 1;                // y accumulators read (conversion warps)
-    uint64_t *ypacked = yfull + 2;              // Y' written (conversion warps)
-    uint64_t *ypfree = yfull + 3;               // Y' read by the x MMAs (MMA commit)
+    uint64_t *yfull = bars + 2 * kYxMaxStages;  // y accumulator complete (MMA commit)
+    uint64_t *yfree = yfull + 1;                // y accumulator read (conversion warps)
+    uint64_t *ypacked = yfull + 2;              // [2] Y' buffer written (conversion warps)
     uint64_t *xfull = yfull + 4;                // x accumulator complete (MMA commit)
-    uint64_t *xempty = yfull + 5;               // x accumulator drained (epilogue warps)
+    uint64_t *xempty = yfull + 5;               // x accumulator read (epilogue warps)
     uint64_t *drain = yfull + 6;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(yfull + 7);
     uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 1024;
@@ -126,19 +118,21 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
     const int64_t total = p.n_tiles;
     const uint32_t n_tx = (uint32_t) p.n_tx, n_ty = (uint32_t) p.n_ty;
 
-    for (int e = threadIdx.x; e < kXTN * tx.kpa; e += kYxThreads) {
-        const int n = e / tx.kpa, j = e - n * tx.kpa;
-        const int t = j - n - tx.ra + tx.radius;  // tap index 0..2R
+    // T[n, j] = tap[j - n - RA + R]: the y pass's A (row n = output o, K = j)
+    // and the x pass's B (row n = x-output, K = j) alike.
+    for (int e = threadIdx.x; e < kXTN * tp.kpa; e += kYxThreads) {
+        const int n = e / tp.kpa, j = e - n * tp.kpa;
+        const int t = j - n - tp.ra + tp.radius;  // tap index 0..2R
         uint16_t v = 0;
-        if (t >= 0 && t <= 2 * tx.radius && j < tx.kp) v = tx.hi[t];
+        if (t >= 0 && t <= 2 * tp.radius && j < kp) v = tp.hi[t];
         *reinterpret_cast<uint16_t *>(tt + sw128_kmajor_offset(n, j, kXTN)) = v;
     }
     if (threadIdx.x == 0) {
         for (int s = 0; s < stages; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         mbar_init(yfull, 1);
         mbar_init(yfree, kYxConvWarps);
-        mbar_init(ypacked, kYxConvWarps);
-        mbar_init(ypfree, 1);
+        mbar_init(&ypacked[0], kYxConvWarps);
+        mbar_init(&ypacked[1], kYxConvWarps);
         mbar_init(xfull, 1);
         mbar_init(xempty, kYxEpiWarps);
         mbar_init(drain, 1);
@@ -155,29 +149,6 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    if (warp >= 2 && warp < 6) {
-        // y Toeplitz into tensor memory (zero outside the band): one warp per quadrant.
-        const int quad = warp & 3;
-        const int o = quad * 32 + lane;
-        for (int ch = 0; ch < ty.kcols / 32; ch++) {
-            uint32_t r[32];
-#pragma unroll
-            for (int j = 0; j < 32; j++) {
-                uint32_t v = 0;
-#pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    const int k = 2 * (ch * 32 + j) + e, t = k - o;
-                    if (t >= 0 && t <= 2 * ty.radius && k < ty.kp) v |= (uint32_t) ty.hi[t] << (16 * e);
-                }
-                r[j] = v;
-            }
-            tmem_st32(tmem + ((uint32_t) (quad * 32) << 16) + kYxToep + ch * 32, r);
-        }
-        tmem_st_wait();
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
 
     // Tile g: plane z, y-tile, x-tile (x fastest, so the CTAs in flight work on
     // neighbouring tiles of one or two planes and share their halos in L2).
@@ -189,130 +160,108 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
     };
 
     if (warp == 0 && lane == 0) {
-        // TMA producer: nch chunks per tile into the ring; L2 prefetch ahead.
-        int64_t cl = 0;
-        bool ok = true;
-        for (int64_t g = blockIdx.x; ok && g < total; g += gridDim.x) {
+        // TMA producer: one F tile (nch boxes) per ring stage; L2 prefetch ahead.
+        int64_t tl = 0;
+        for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
             int z, y0, x0;
             const int64_t gp = g + kPrefetch * (int64_t) gridDim.x;
             if (gp < total) {
                 decode(gp, z, y0, x0);
-                for (int c = 0; c < nch; c++) tma_prefetch_3d(&tmap, x0 - tx.ra + 64 * c, y0 - ty.radius, z);
+                for (int c = 0; c < nch; c++) tma_prefetch_3d(&tmap, x0 - tp.ra + 64 * c, y0 - tp.ra, z);
             }
             decode(g, z, y0, x0);
-            for (int c = 0; c < nch; c++, cl++) {
-                const int s = (int) (cl % stages);
-                const uint32_t ph = (uint32_t) ((cl / stages) & 1);
-                if (!mbar_wait(&empty[s], ph ^ 1, 1)) { ok = false; break; }
-                mbar_arrive_expect_tx(&full[s], chunk_bytes);
-                tma_load_3d(ring + s * chunk_bytes, &tmap, x0 - tx.ra + 64 * c, y0 - ty.radius, z, &full[s]);
-            }
+            const int s = (int) (tl % stages);
+            if (!mbar_wait(&empty[s], (uint32_t) (((tl / stages) & 1) ^ 1), 1)) break;
+            mbar_arrive_expect_tx(&full[s], tile_bytes);
+            for (int c = 0; c < nch; c++)
+                tma_load_3d(ring + s * tile_bytes + c * chunk_bytes, &tmap, x0 - tp.ra + 64 * c, y0 - tp.ra, z,
+                            &full[s]);
         }
         // Let every copy this thread started land before the CTA can exit: the
         // last use of each ring stage (bounded, so an aborted run still ends).
-        for (int64_t k = cl - stages; k < cl; k++)
+        for (int64_t k = tl - stages; k < tl; k++)
             if (k >= 0) mbar_wait(&full[k % stages], (uint32_t) ((k / stages) & 1), 1);
     } else if (warp == 1 && lane == 0) {
-        // MMA issuer.  Step tl issues the y MMAs of tile tl (one chain per chunk)
-        // and the x MMAs of tile tl - 1, one K step of every chain in turn.
+        // MMA issuer.  Step tl issues y(tl), then x(tl - 1).
         const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
-        const uint32_t idesc_y = idesc_f16(fmt, 0 /*A K-major*/, 1 /*B MN-major*/, kTM, 64);
+        const uint32_t idesc_y = idesc_f16(fmt, 0 /*A K-major*/, 1 /*B MN-major*/, kTM, (uint32_t) kp);
         const uint32_t idesc_x = idesc_f16(fmt, 0 /*A K-major*/, 0 /*B K-major*/, kTM, kXTN);
-        const uint32_t r0 = smem_u32(ring), t0 = smem_u32(tt);
-        const int ksy = ty.kp / 16, ksx = tx.kp / 16, ks_max = ksy > ksx ? ksy : ksx;
-        int64_t cl = 0;
+        // T: K step ks at 64-element block ks / 4 (16 KB each), 32 bytes per 16 K inside it.
+        const uint64_t t_desc = smem_desc_sw128(smem_u32(tt), 16, 1024);
+        const uint32_t r0 = smem_u32(ring);
+        const int ks_n = kp / 16;
         bool ok = true;
         for (int64_t tl = 0;; tl++) {
             const int64_t g = blockIdx.x + tl * (int64_t) gridDim.x;
             const bool has_y = g < total, has_x = tl > 0 && g - gridDim.x < total;
             if (!has_y && !has_x) break;
-            int s[kYxMaxChunks] = {0, 0, 0};
             if (has_y) {
-                for (int c = 0; c < nch && ok; c++) {
-                    s[c] = (int) ((cl + c) % stages);
-                    ok = mbar_wait(&full[s[c]], (uint32_t) (((cl + c) / stages) & 1), 1);
-                }
-                // the conversion warps have read the previous tile's y accumulators
+                const int s = (int) (tl % stages);
+                ok = mbar_wait(&full[s], (uint32_t) ((tl / stages) & 1), 1);
+                // the conversion warps have read the previous tile's y accumulator
                 if (ok && tl > 0) ok = mbar_wait(yfree, (uint32_t) ((tl - 1) & 1), 3);
-            }
-            if (ok && has_x) {
-                // Y' of tile tl - 1 is in place and the epilogue has drained the x accumulator
-                ok = mbar_wait(ypacked, (uint32_t) ((tl - 1) & 1), 3) &&
-                     mbar_wait(xempty, (uint32_t) (((tl - 1) & 1) ^ 1), 3);
-            }
-            if (!ok) break;
-            tc_fence_after();
-            for (int ks = 0; ks < ks_max; ks++) {
-                if (has_y && ks < ksy) {
-                    for (int c = 0; c < nch; c++) {
-                        const uint64_t bd = smem_desc_sw128(r0 + s[c] * chunk_bytes, chunk_bytes, 1024);
-                        umma_f16_ts(tmem + kYxAccY + 64 * c, tmem + kYxToep + ks * 8, bd + (uint64_t) (ks * 128),
-                                    idesc_y, ks > 0 ? 1u : 0u);
-                    }
-                }
-                if (has_x && ks < ksx) {
-                    const uint32_t bhi = t0 + (ks >> 2) * (kXTN * 128) + (ks & 3) * 32;
-                    umma_f16_ts(tmem + kYxAccX, tmem + kYxYp + ks * 8, smem_desc_sw128(bhi, 16, 1024), idesc_x,
-                                ks > 0 ? 1u : 0u);
-                }
-            }
-            if (has_y) {
-                for (int c = 0; c < nch; c++) umma_commit(&empty[s[c]]);
+                if (!ok) break;
+                tc_fence_after();
+                // F: MN-major, 64-column atoms chunk_bytes apart (LBO), 8-row groups 1 KB apart (SBO).
+                const uint64_t f_desc = smem_desc_sw128(r0 + s * tile_bytes, chunk_bytes, 1024);
+                for (int ks = 0; ks < ks_n; ks++)
+                    umma_f16(tmem + kYxAccY, t_desc + (uint64_t) ((ks >> 2) * 1024 + (ks & 3) * 2),
+                             f_desc + (uint64_t) (ks * 128), idesc_y, ks > 0 ? 1u : 0u);
+                umma_commit(&empty[s]);
                 umma_commit(yfull);
-                cl += nch;
             }
             if (has_x) {
+                // Y' of tile tl - 1 is in place (one barrier per buffer: the
+                // conversion warps cannot complete a second phase of it before
+                // this wait, since that needs y(tl + 1)) and the epilogue has
+                // read the x accumulator
+                ok = mbar_wait(&ypacked[(tl - 1) & 1], (uint32_t) (((tl - 1) >> 1) & 1), 3) &&
+                     mbar_wait(xempty, (uint32_t) (((tl - 1) & 1) ^ 1), 3);
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t yp = tmem + kYxYp + (uint32_t) ((tl - 1) & 1) * kYxYpCols;
+                for (int ks = 0; ks < ks_n; ks++)
+                    umma_f16_ts(tmem + kYxAccX, yp + ks * 8, t_desc + (uint64_t) ((ks >> 2) * 1024 + (ks & 3) * 2),
+                                idesc_x, ks > 0 ? 1u : 0u);
                 umma_commit(xfull);
-                umma_commit(ypfree);
             }
         }
         // Every MMA this thread issued has completed before the CTA winds down.
         umma_commit(drain);
         mbar_wait(drain, 0, 2);
     } else if (warp >= 2 && warp < 2 + kYxConvWarps) {
-        // Conversion: y accumulators (FP32) -> Y' (16-bit, packed).  The two warps
-        // of a quadrant take the 32-column runs [3 half, 3 half + 3) of the window.
+        // Conversion: y accumulator (FP32) -> Y' (16-bit, packed).  The two warps
+        // of a quadrant take the 32-column runs [3 half, 3 half + 3) of the
+        // window (two or three of them), one at a time; the y accumulator is
+        // free once the last run is read.  Y' of tile tl goes to buffer tl & 1,
+        // which x(tl - 2) read: that MMA was issued before y(tl), so it
+        // completed before yfull of tile tl.
         const int quad = warp & 3, half = (warp - 2) >> 2;
         const uint32_t lb = tmem + ((uint32_t) (quad * 32) << 16);
-        const int c_lo = 3 * half, c_hi = ncc < c_lo + 3 ? ncc : c_lo + 3;
+        const int c0 = 3 * half, c1 = ncc < c0 + 3 ? ncc : c0 + 3;  // 2 or 3 runs
         int64_t tl = 0;
-        bool ok = true;
-        for (int64_t g = blockIdx.x; ok && g < total; g += gridDim.x, tl++) {
-            int z, y0, x0;
-            decode(g, z, y0, x0);
-            ok = __all_sync(0xffffffffu, mbar_wait(yfull, (uint32_t) (tl & 1), 2));
-            if (!ok) break;
+        for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
+            if (!__all_sync(0xffffffffu, mbar_wait(yfull, (uint32_t) (tl & 1), 2))) break;
             tc_fence_after();
-            for (int cc = c_lo; cc < c_hi || (cc == c_lo && c_lo >= c_hi); cc++) {
-                const bool live = cc < c_hi;  // a half with no runs still signals
+            const uint32_t yp = lb + kYxYp + (uint32_t) (tl & 1) * kYxYpCols;
+            for (int cc = c0; cc < c1; cc++) {
                 float v[32];
                 __syncwarp();
-                if (live) tmem_ld32(lb + kYxAccY + 32 * cc, v);
-                if (cc + 1 >= c_hi) {
-                    // every read of this warp is done: the y accumulators may be reused
+                tmem_ld32(lb + kYxAccY + 32 * cc, v);
+                if (cc + 1 == c1) {
                     tc_fence_before();
                     __syncwarp();
                     if (lane == 0) mbar_arrive(yfree);
                 }
-                if (cc == c_lo && tl > 0) {
-                    // the x MMAs of the previous tile have read Y'
-                    ok = __all_sync(0xffffffffu, mbar_wait(ypfree, (uint32_t) ((tl - 1) & 1), 2));
-                    if (!ok) break;
-                    tc_fence_after();
-                }
-                if (live) {
-                    const int64_t xs = (int64_t) x0 - tx.ra + 32 * cc;
-                    uint32_t d[16], w[16];
-                    narrow32_quads<S, true>(v, ty.inv_scale, ty.error_feedback, 0u, live_bits(xs, p.nx), d);
-                    quads_to_adjacent(d, w);
-                    tmem_st16(lb + kYxYp + 16 * cc, w);
-                }
+                uint32_t d[16], w[16];
+                narrow32_quads<S, false>(v, tp.inv_scale, tp.error_feedback, 0u, 0xffffffffu, d);
+                quads_to_adjacent(d, w);
+                tmem_st16(yp + 16 * cc, w);
             }
-            if (!ok) break;
             tmem_st_wait();
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(ypacked);
+            if (lane == 0) mbar_arrive(&ypacked[tl & 1]);
         }
     } else if (warp >= 2 + kYxConvWarps) {
         // Epilogue: x accumulator -> re-illumination -> next field / final outputs.
@@ -340,15 +289,21 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
 #pragma unroll
             for (int k = 0; k < 2; k++) {
                 const int64_t xb = x0 + part * 64 + 32 * k;
-                float h[32];
+                float hk[32];
                 __syncwarp();
-                tmem_ld32(lb + kYxAccX + part * 64 + 32 * k, h);
+                tmem_ld32(lb + kYxAccX + part * 64 + 32 * k, hk);
+                if (k == 1) {
+                    // every read of this warp is done: the x accumulator may be reused
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(xempty);
+                }
                 const uint32_t m = mask_flags<FMT>(mw[k], p.mask);
                 if (p.final_pass) {
-                    contig_final32(h, m, live_row ? row : rows, rows, p.nx, xb, tx.inv_scale, p.out_u16, p.field_out);
+                    contig_final32(hk, m, live_row ? row : rows, rows, p.nx, xb, tp.inv_scale, p.out_u16, p.field_out);
                 } else if (xb < p.nx) {  // warp-uniform
                     uint32_t d[16], q[16];
-                    narrow32_pairs<S, true>(h, tx.inv_scale, tx.error_feedback, m, 0xffffffffu, d);
+                    narrow32_pairs<S, true>(hk, tp.inv_scale, tp.error_feedback, m, 0xffffffffu, d);
                     pairs_to_adjacent(d, q);
                     const int64_t oi = !live_row ? -1
                                        : p.out_nz == 0 ? row * p.nx + xb
@@ -369,9 +324,6 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
                     }
                 }
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(xempty);
         }
     }
     __syncthreads();

@@ -24,7 +24,7 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
             field: str = "f32", field_out: torch.Tensor | None = None, shape=None,
             reference_rounding: bool = False, workspace: torch.Tensor | None = None,
             stream: torch.cuda.Stream | None = None, tensor_cores: bool = True,
-            error_feedback: bool = True, fuse_passes: bool = True, split_coefficients: bool = False) -> None:
+            error_feedback: bool = True, fuse_passes: bool = False, split_coefficients: bool = False) -> None:
     """Run the diffusion on device buffers.
 
     mask: uint8 [nz, ny, nx] CUDA tensor (set when > 0), or a bit-packed int32/uint32
@@ -37,7 +37,7 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
     tensor_cores: 16-bit fields: z and y passes on tcgen05 tensor cores where supported.
     error_feedback: 16-bit fields: error-feedback rounding along x (else round to nearest).
     fuse_passes: 16-bit tensor-core fields, radius <= 32: the y and x passes in one
-          kernel per z-plane tile (else two kernels, two HBM round trips).
+          kernel per z-plane tile (default: two kernels, two HBM round trips).
     split_coefficients: 16-bit tensor-core passes: high + low 16-bit coefficient halves
           (two MMAs per K step, separate y and x passes) instead of one set whose
           taps keep the kernel's sum and second moment.
@@ -79,8 +79,8 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
         flags |= _lib.FLAG_NO_TENSOR_CORES
     if not error_feedback:
         flags |= _lib.FLAG_NEAREST_ROUNDING
-    if not fuse_passes:
-        flags |= _lib.FLAG_SEPARATE_PASSES
+    if fuse_passes:
+        flags |= _lib.FLAG_FUSE_YX
     if split_coefficients:
         flags |= _lib.FLAG_SPLIT_COEFFICIENTS
     with torch.cuda.device(mask.device):
@@ -151,7 +151,7 @@ class BatchPlan:
     (or one for all); reps: an int or one per volume."""
 
     def __init__(self, masks, kernels, reps, outputs=None, field="bf16", field_outs=None, autotune=False,
-                 tensor_cores=True, error_feedback=True, stream=None):
+                 tensor_cores=True, error_feedback=True, stream=None, split_coefficients=False):
         import ctypes
         n = len(masks)
         if not isinstance(kernels, (list, tuple)):
@@ -176,7 +176,8 @@ class BatchPlan:
                                      f.data_ptr() if f is not None else None, nz, ny, nx, k.ctypes.data, k.shape[0],
                                      int(reps[i]))
         flags = (_lib.FLAG_AUTOTUNE if autotune else 0) | (0 if tensor_cores else _lib.FLAG_NO_TENSOR_CORES) | \
-            (0 if error_feedback else _lib.FLAG_NEAREST_ROUNDING)
+            (0 if error_feedback else _lib.FLAG_NEAREST_ROUNDING) | \
+            (_lib.FLAG_SPLIT_COEFFICIENTS if split_coefficients else 0)
         st = stream if stream is not None else torch.cuda.current_stream()
         self._plan = ctypes.c_void_p()
         _lib.check(_lib.lib().maxi_batch_plan_create(ctypes.addressof(arr), n, _lib.FIELD_TYPES[field], flags,

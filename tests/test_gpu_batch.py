@@ -132,6 +132,48 @@ def test_batch_autotune_reports_and_stays_accurate():
     plan.close()
 
 
+def test_batch_autotune_persists_choices(tmp_path, monkeypatch):
+    # Shapes and a radius no other test tunes, so the process has no choice for them yet.
+    from maxibone_b200 import _lib
+    cache = tmp_path / "tune.json"
+    monkeypatch.setenv("MAXIBONE_TUNE_CACHE", str(cache))
+    shapes, sigma, reps = [(72, 80, 128), (48, 64, 192), (40, 96, 64)], 2.5, 2
+    kernel = gauss_kernel(sigma).astype(np.float32)  # radius 10
+    masks = [torch.from_numpy(spheres_mask(sh, 6, (3, 8), seed=7 + i)).cuda() for i, sh in enumerate(shapes)]
+
+    def plan_and_check():
+        outs = [torch.empty(sh, dtype=torch.uint16, device="cuda") for sh in shapes]
+        fouts = [torch.empty(sh, dtype=torch.float32, device="cuda") for sh in shapes]
+        plan = device.BatchPlan(masks, [kernel] * 3, reps, outputs=outs, field="bf16", field_outs=fouts, autotune=True)
+        text = plan.describe()
+        plan.run()
+        torch.cuda.synchronize()
+        for m, sh, f in zip(masks, shapes, fouts):
+            want = torch.empty(sh, dtype=torch.float64, device="cuda")
+            device.diffuse(m, kernel, reps, field="f64", field_out=want)
+            assert (f.double() - want).abs().max().item() <= 2e-3
+        plan.close()
+        return text
+
+    _lib.check(_lib.lib().maxi_batch_tune_forget())
+    first = plan_and_check()
+    assert "tuned: batched" in first and "per_volume_tc" in first and "cuda_cores" in first, first
+    text = cache.read_text()
+    gpu = torch.cuda.get_device_name()
+    key = f"{gpu} sm{torch.cuda.get_device_properties(0).multi_processor_count}|bf16|r10|"
+    lines = [ln for ln in text.splitlines() if key in ln]
+    assert len(lines) == 1 and '"form": ' in lines[0] and "40x96x64,48x64x192,72x80x128" in lines[0], text
+    assert "cached choice" in plan_and_check()
+    # A choice read from the file (here forced to the CUDA-core passes) is used
+    # without timing, after the process forgets its own.
+    forced = lines[0].split('"form": ')[0] + '"form": "cuda_cores"}'
+    cache.write_text('{\n"entries": {\n' + forced + "\n}\n}\n")
+    _lib.check(_lib.lib().maxi_batch_tune_forget())
+    text = plan_and_check()
+    assert "cached choice" in text and "-> cuda_cores" in text and "per-volume CUDA-core passes" in text, text
+    _lib.check(_lib.lib().maxi_batch_tune_forget())
+
+
 def test_batch_rejects_bad_volumes():
     m = torch.zeros((4, 4, 4), dtype=torch.uint8, device="cuda")
     with pytest.raises(ValueError):

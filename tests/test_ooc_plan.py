@@ -26,11 +26,28 @@ def test_full_size_out_of_core_volume_fits_deep_halos():
     assert 512 <= S <= 3456
 
 
-def test_large_r_times_radius_switches_to_exchange_rounds():
+def test_large_r_times_radius_switches_to_exchange_rounds(monkeypatch):
     # R x radius = 6400 planes exceeds the volume: deep halos would make every
-    # slab the whole volume, which does not fit; rounds of k < R do.
+    # slab the whole volume, which does not fit; rounds of k < R do, on a host
+    # that can pin the two FP32 copies of the field (8 bytes per voxel).
+    monkeypatch.setenv("MAXIBONE_OOC_HOST_BUDGET", str(400 * GB))
     rc, S, k, res = plan((3456, 3456, 4096), 65, 200, field="f32")
     assert rc == 0 and 1 <= k < 200 and S >= 1
+
+
+def test_exchange_rounds_need_the_host_memory(monkeypatch):
+    # Without room for the host copies of the field the planner keeps deep
+    # halos (when those fit) or reports the host limit instead of planning
+    # rounds whose pinned allocations would fail.
+    monkeypatch.setenv("MAXIBONE_OOC_HOST_BUDGET", str(100 * GB))
+    rc, S, k, res = plan((3456, 3456, 4096), 65, 20)
+    assert rc == 0 and k == 20
+    rc, S, k, res = plan((3456, 3456, 4096), 65, 200, field="f32")
+    assert rc == 3
+    assert b"pinned host memory" in _lib.lib().maxi_last_error()
+    monkeypatch.setenv("MAXIBONE_OOC_HOST_BUDGET", str(8 * 96 * 64 * 64))
+    rc, S, k, _ = plan((96, 64, 64), 9, 12, field="f32", device_bytes=4 * 10 ** 6)
+    assert rc == 0 and k < 12
 
 
 def test_caller_slab_depth_is_an_upper_bound():

@@ -74,6 +74,7 @@ SECTIONS = ("e2e", "cfg0", "precision", "long", "batched", "out_of_core", "downs
 NCU_BYTES_PER_VOXEL_REP = {
     ("f32", "separate"): (8237891584 + 8247201792 + 8356808704) / 2 ** 30,
     ("bf16", "separate"): (4136156160 + 4180311040 + 4272011263) / 2 ** 30,
+    ("bf16", "fused"): (541974528 + 495319552 + 573645824 + 494644992) / 2 ** 28,
 }
 
 
@@ -99,8 +100,9 @@ def parse_args():
                         "histograms, morphology, implant masks) on its output, and print their JSON object")
     p.add_argument("--shape", type=str, default=None,
                    help="override the workload's volume shape, e.g. 256x1024x1024 (profiling of smaller cases)")
-    p.add_argument("--fuse-passes", action="store_true",
-                   help="16-bit fields: the headline step runs the fused y + x tensor-core kernel")
+    p.add_argument("--separate-passes", action="store_true",
+                   help="16-bit fields: the headline step runs the y and x passes as two kernels instead of the "
+                        "fused y + x tensor-core kernel")
     p.add_argument("--reps", type=int, default=None,
                    help="override the workload's repetition count (profiling of smaller cases)")
     p.add_argument("--ooc-shape", type=str, default="3456x3456x4096",
@@ -780,7 +782,7 @@ PRECISION_FORMS = [
     ("f32", "f32", {}),
     ("bf16", "bf16", {}),
     ("bf16_split_coefficients", "bf16", {"split_coefficients": True}),
-    ("bf16_fused_yx", "bf16", {"fuse_passes": True}),
+    ("bf16_separate_passes", "bf16", {"fuse_passes": False}),
     ("f16", "f16", {}),
     ("f16_split_coefficients", "f16", {"split_coefficients": True}),
     ("bf16_nearest", "bf16", {"error_feedback": False}),
@@ -947,7 +949,7 @@ def main():
 
         def step(field=args.field, output=out, workspace=ws, field_out=None):
             device.diffuse(mask, kernel, reps, output=output, field=field, workspace=workspace, field_out=field_out,
-                           fuse_passes=args.fuse_passes)
+                           fuse_passes=not args.separate_passes)
 
     def barrier():
         if world > 1:
@@ -1035,7 +1037,7 @@ def main():
         "config": {"workload": args.workload + (f" (shape override {args.shape})" if args.shape else "")
                    + (f" (repetitions override {args.reps})" if args.reps is not None else ""),
                    "shape": list(shape), "sigma": sigma, "kernel_size": int(2 * radius + 1),
-                   "reps": reps, "field": args.field, "fuse_passes": bool(args.fuse_passes), "mask": "u8",
+                   "reps": reps, "field": args.field, "separate_passes": bool(args.separate_passes), "mask": "u8",
                    "foreground": round(fg, 4),
                    "parallelism": (f"one volume split into {world} z-slabs (one per rank), halo planes exchanged "
                                    f"every {split.k} repetitions by NCCL P2P" if split else

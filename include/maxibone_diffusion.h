@@ -65,16 +65,15 @@ typedef enum maxi_mask_format {
                                             radius >= 4, which keeps the stored rounding noise
                                             out of the result) */
 #define MAXI_FLAG_SEPARATE_PASSES 0x20   /* BF16/FP16 tensor cores: the y and x passes as two
-                                            kernels (two HBM round trips; the default); overrides
-                                            MAXI_FLAG_FUSE_YX */
-#define MAXI_FLAG_FUSE_YX 0x80           /* BF16/FP16 tensor cores, radius <= 32: the y and x
-                                            passes in one kernel per z-plane tile (the field
-                                            between them stays on the SM) */
+                                            kernels (two HBM round trips) instead of the fused
+                                            y + x kernel, which is the default where it applies
+                                            (radius 12 to 32: the single coefficient set) */
 #define MAXI_FLAG_SPLIT_COEFFICIENTS 0x40 /* BF16/FP16 tensor cores: Toeplitz coefficients as high +
                                             low 16-bit halves (two MMAs per K step) instead of the
-                                            default single set whose taps are rounded so that the
-                                            kernel's sum and second moment are kept; runs the
-                                            separate y and x passes */
+                                            single set whose taps are rounded so that the
+                                            kernel's sum and second moment are kept (the default
+                                            from radius 12; smaller radii always use the halves);
+                                            runs the separate y and x passes */
 
 const char *maxi_last_error(void);
 const char *maxi_version(void);

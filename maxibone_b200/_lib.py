@@ -24,7 +24,6 @@ FLAG_NEAREST_ROUNDING = 0x4
 FLAG_MASK_FROM_FIELD = 0x8
 FLAG_AUTOTUNE = 0x10
 FLAG_SEPARATE_PASSES = 0x20
-FLAG_FUSE_YX = 0x80
 FLAG_SPLIT_COEFFICIENTS = 0x40
 PATH_CUDA_CORES = 0x1
 PATH_TENSOR_CORES_ZY = 0x2

@@ -208,7 +208,7 @@ static cudaError_t enqueue_group_tc(maxi_batch_plan *p, TcGroup &g, cudaStream_t
     if (e != cudaSuccess) return e;
     const bool bf16 = std::is_same<S, __nv_bfloat16>::value;
     const bool ef = (p->flags & MAXI_FLAG_NEAREST_ROUNDING) == 0 && g.geo.radius >= 4;
-    const bool hi_only = (p->flags & MAXI_FLAG_SPLIT_COEFFICIENTS) == 0;
+    const bool hi_only = tc::tc_single_set(g.geo.radius, (p->flags & MAXI_FLAG_SPLIT_COEFFICIENTS) != 0);
     const int n = (int) g.members.size();
     int in = 0;
     for (int64_t rep = 0; rep < g.reps; rep++) {

@@ -50,11 +50,23 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
+// As mbar_try_wait, letting the hardware suspend the thread until the phase
+// completes or `suspend_ns` nanoseconds pass, instead of returning at once: a
+// waiting warp then takes no issue slots from the warps doing the work.
+__device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t *bar, uint32_t parity, uint32_t suspend_ns) {
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity), "r"(suspend_ns) : "memory");
+    return ok != 0;
+}
+
+constexpr uint32_t kWaitSuspendNs = 1000000;  // per try: 1 ms, far inside the bounded wait's ~1 s
+
 // Bounded wait for the phase with the given parity to complete.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int err_code) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity)) {
+    while (!mbar_try_wait_suspend(bar, parity, kWaitSuspendNs)) {
         if (clock64() - t0 > kWaitBudgetCycles) {
             atomicCAS(&g_tc_error, 0, err_code);
             return false;
@@ -347,6 +359,33 @@ __device__ __forceinline__ void narrow32_pairs(const float (&a)[32], float scale
     }
 }
 
+// Two 32-voxel runs narrowed together, each exactly as narrow32_pairs<S, true>
+// with live = all and its own force1 (f0: a[0..31] -> d0, f1: a[32..63] -> d1):
+// the runs' chains are independent, so every step issues both.
+template <typename S>
+__device__ __forceinline__ void narrow64_pairs_forced(const float (&a)[64], float scale, bool ef, uint32_t f0,
+                                                      uint32_t f1, uint32_t (&d0)[16], uint32_t (&d1)[16]) {
+    float2 c0 = make_float2(0.0f, 0.0f), c1 = make_float2(0.0f, 0.0f);
+    const float2 s2 = make_float2(scale, scale), m1 = make_float2(-1.0f, -1.0f);
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        const float2 v0 = make_float2(a[j], a[16 + j]), v1 = make_float2(a[32 + j], a[48 + j]);
+        float2 w0 = ef ? __ffma2_rn(v0, s2, c0) : __fmul2_rn(v0, s2);
+        float2 w1 = ef ? __ffma2_rn(v1, s2, c1) : __fmul2_rn(v1, s2);
+        if ((f0 >> j) & 1u) w0.x = 1.0f;
+        if ((f0 >> (16 + j)) & 1u) w0.y = 1.0f;
+        if ((f1 >> j) & 1u) w1.x = 1.0f;
+        if ((f1 >> (16 + j)) & 1u) w1.y = 1.0f;
+        const uint32_t q0 = Pair16<S>::cvt(w0.x, w0.y), q1 = Pair16<S>::cvt(w1.x, w1.y);
+        if (ef) {
+            c0 = __ffma2_rn(Pair16<S>::widen(q0), m1, w0);
+            c1 = __ffma2_rn(Pair16<S>::widen(q1), m1, w1);
+        }
+        d0[j] = q0;
+        d1[j] = q1;
+    }
+}
+
 // 32 voxels in four error-feedback chains of 8 (x = 8k + j, k = 0..3): chains
 // 0 / 1 and 2 / 3 advance together as two packed pairs, so each step has two
 // independent dependency chains and a run takes 8 steps instead of 16.  Used
@@ -381,6 +420,27 @@ __device__ __forceinline__ void narrow32_quads(const float (&a)[32], float scale
         }
         d[j] = q0;
         d[8 + j] = q1;
+    }
+}
+
+// Two 32-voxel runs as narrow32_quads<S, false> each (a[0..31] -> d0,
+// a[32..63] -> d1), their chains interleaved: four independent chains per step.
+template <typename S>
+__device__ __forceinline__ void narrow64_quads(const float (&a)[64], float scale, bool ef, uint32_t (&d0)[16],
+                                               uint32_t (&d1)[16]) {
+    float2 c[4] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+    const float2 s2 = make_float2(scale, scale), m1 = make_float2(-1.0f, -1.0f);
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+#pragma unroll
+        for (int h = 0; h < 4; h++) {  // h: run h / 2, chains pair h % 2
+            const int b = 32 * (h >> 1) + 16 * (h & 1);
+            float2 w = make_float2(a[b + j], a[b + 8 + j]);
+            w = ef ? __ffma2_rn(w, s2, c[h]) : __fmul2_rn(w, s2);
+            const uint32_t q = Pair16<S>::cvt(w.x, w.y);
+            if (ef) c[h] = __ffma2_rn(Pair16<S>::widen(q), m1, w);
+            ((h >> 1) ? d1 : d0)[8 * (h & 1) + j] = q;
+        }
     }
 }
 

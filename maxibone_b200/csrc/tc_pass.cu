@@ -229,7 +229,6 @@ cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool fina
     if (p.t.kp > kYxMaxCols || (uint32_t) p.t.kp / 2 > kYxYpCols) return cudaErrorInvalidValue;
     p.final_pass = final_pass ? 1 : 0;
     p.mask = mask;
-    p.out = reinterpret_cast<uint16_t *>(out_rows ? out_rows->base : static_cast<void *>(out));
     p.out_u16 = out_u16;
     p.field_out = field_out;
     p.nz = nz;
@@ -251,6 +250,21 @@ cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool fina
                                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    // Store map of the next field (not final): 32 x-voxels x 32 rows per store,
+    // 64-byte swizzle; [y][z][x] rows as (x, z, y) from the window's first plane.
+    CUtensorMap omap = map;
+    if (!final_pass) {
+        const cuuint32_t zbox[3] = {32u, 32u, 1u}, rbox[3] = {32u, 1u, 32u};
+        const cuuint64_t rdims[3] = {(cuuint64_t) nx, (cuuint64_t) nz, (cuuint64_t) ny};
+        const cuuint64_t rstrides[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (out_rows ? out_rows->nz_total * nx * 2 : 0)};
+        void *obase = out_rows ? static_cast<void *>(static_cast<S *>(out_rows->base) + out_rows->z0 * nx)
+                               : static_cast<void *>(out);
+        cr = tc_encode_fn()(&omap, is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3,
+                            obase, out_rows ? rdims : dims, out_rows ? rstrides : strides, out_rows ? rbox : zbox,
+                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    }
     int dev = 0, sms = 148, smem_max = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -258,11 +272,13 @@ cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool fina
     p.stages = yx_stages(p.t.kp, p.t.kpa, smem_max);
     const int smem = yx_smem_bytes(p.t.kp, p.t.kpa, p.stages);
     if (smem > smem_max) return cudaErrorInvalidValue;
-    auto *kern = mask_fmt == MAXI_MASK_U8 ? tc_yx_kernel<S, MAXI_MASK_U8> : tc_yx_kernel<S, MAXI_MASK_BITPACKED>;
+    auto *kern = mask_fmt == MAXI_MASK_U8 ? (final_pass ? tc_yx_kernel<S, MAXI_MASK_U8, true> : tc_yx_kernel<S, MAXI_MASK_U8, false>)
+                                          : (final_pass ? tc_yx_kernel<S, MAXI_MASK_BITPACKED, true>
+                                                        : tc_yx_kernel<S, MAXI_MASK_BITPACKED, false>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     const int64_t grid = std::min<int64_t>(p.n_tiles, sms);
-    kern<<<(unsigned) grid, kYxThreads, smem, st>>>(map, p);
+    kern<<<(unsigned) grid, kYxThreads, smem, st>>>(map, omap, p);
     return cudaGetLastError();
 }
 

@@ -17,6 +17,17 @@ constexpr int kTcMaxRadius = 32;
 // boxes; the x pass above radius 32 runs in its transposed form.
 constexpr int kTcMaxRadiusWide = 128;
 
+// Smallest radius served by one 16-bit coefficient set (tc_round_taps_matched);
+// below it the taps are large enough that their 16-bit rounding steps compound
+// past the error bound (BF16, sigma 2, R = 50: 2.4e-3 with one set, 1.4e-3 with
+// high + low halves), and the passes use the halves.
+constexpr int kTcSingleSetMinRadius = 12;
+
+// Whether a pass of this radius uses the single coefficient set.
+inline bool tc_single_set(int radius, bool split_requested) {
+    return !split_requested && radius >= kTcSingleSetMinRadius;
+}
+
 // True when the device is sm_100 and the shape fits the TMA constraints
 // (single-volume passes, radius <= kTcMaxRadiusWide).
 bool tc_supported(int radius, int64_t nz, int64_t ny, int64_t nx);

@@ -64,9 +64,10 @@ constexpr uint32_t kYxTmemCols = 512;
 __host__ __device__ constexpr int yx_tile_bytes(int kp) { return ((kp + 63) / 64) * kp * 128; }
 
 // Shared memory: the Toeplitz matrix (kpa K x 128 rows), the F tile ring of
-// `stages` tiles, the barriers and the epilogue's store staging.
+// `stages` tiles, the barriers and the epilogue's store staging (two 32 x 32
+// chunks per warp, the sources of its TMA stores).
 __host__ __device__ constexpr int yx_smem_bytes(int kp, int kpa, int stages) {
-    return 1024 + kpa * kXTN * 2 + stages * yx_tile_bytes(kp) + 1024 + kYxEpiWarps * kXStageWarpBytes;
+    return 1024 + kpa * kXTN * 2 + stages * yx_tile_bytes(kp) + 1024 + kYxEpiWarps * 2 * kXStageWarpBytes;
 }
 
 // The deepest F ring (2 .. kYxMaxStages tiles) that fits `smem_max` bytes.
@@ -78,10 +79,11 @@ __host__ __device__ constexpr int yx_stages(int kp, int kpa, int smem_max) {
 
 struct YxLaunch {
     PassTaps t;  // ra = RA, kp = KP = 128 + RA + R rounded to 16, one coefficient set
-    int final_pass;
+    int final_pass;     // selects the FINAL instantiation
     int stages;         // F ring depth (tiles)
     const void *mask;
-    uint16_t *out;      // next field (not final): [z][y][x], or [y][z][x] rows when out_nz > 0
+    // next field (not final), written through the store map: [z][y][x] rows
+    // (map dims x, y, z), or [y][z][x] rows when out_nz > 0 (map dims x, z, y)
     uint16_t *out_u16;  // final
     float *field_out;   // final, optional
     int64_t nz, ny, nx, out_nz, out_z0;
@@ -89,9 +91,13 @@ struct YxLaunch {
     int64_t n_tiles;
 };
 
-template <typename S, int FMT>
+// FINAL: the last repetition (uint16 output and FP32 field instead of the next
+// 16-bit field); a template parameter so that each form holds only its own
+// epilogue's registers.
+template <typename S, int FMT, bool FINAL>
 __global__ void __launch_bounds__(kYxThreads, 1)
-tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ YxLaunch p) {
+tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap omap,
+             const __grid_constant__ YxLaunch p) {
     const PassTaps &tp = p.t;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
@@ -138,6 +144,7 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
         mbar_init(drain, 1);
         fence_barrier_init();
         prefetch_tmap(&tmap);
+        if (!FINAL) prefetch_tmap(&omap);
     }
     __syncwarp();
     if (warp == 0) {
@@ -232,8 +239,8 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
     } else if (warp >= 2 && warp < 2 + kYxConvWarps) {
         // Conversion: y accumulator (FP32) -> Y' (16-bit, packed).  The two warps
         // of a quadrant take the 32-column runs [3 half, 3 half + 3) of the
-        // window (two or three of them), one at a time; the y accumulator is
-        // free once the last run is read.  Y' of tile tl goes to buffer tl & 1,
+        // window (two or three of them): the first two together, then the
+        // third; the y accumulator is free once the last run is read.  Y' of tile tl goes to buffer tl & 1,
         // which x(tl - 2) read: that MMA was issued before y(tl), so it
         // completed before yfull of tile tl.
         const int quad = warp & 3, half = (warp - 2) >> 2;
@@ -244,19 +251,34 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
             if (!__all_sync(0xffffffffu, mbar_wait(yfull, (uint32_t) (tl & 1), 2))) break;
             tc_fence_after();
             const uint32_t yp = lb + kYxYp + (uint32_t) (tl & 1) * kYxYpCols;
-            for (int cc = c0; cc < c1; cc++) {
-                float v[32];
+            {
+                // the first two runs together (four independent chains per step)
+                float v[64];
                 __syncwarp();
-                tmem_ld32(lb + kYxAccY + 32 * cc, v);
-                if (cc + 1 == c1) {
+                tmem_ld64(lb + kYxAccY + 32 * c0, v);
+                if (c1 == c0 + 2) {
                     tc_fence_before();
                     __syncwarp();
                     if (lane == 0) mbar_arrive(yfree);
                 }
+                uint32_t d0[16], d1[16], w[16];
+                narrow64_quads<S>(v, tp.inv_scale, tp.error_feedback, d0, d1);
+                quads_to_adjacent(d0, w);
+                tmem_st16(yp + 16 * c0, w);
+                quads_to_adjacent(d1, w);
+                tmem_st16(yp + 16 * (c0 + 1), w);
+            }
+            if (c1 == c0 + 3) {
+                float v[32];
+                __syncwarp();
+                tmem_ld32(lb + kYxAccY + 32 * (c0 + 2), v);
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(yfree);
                 uint32_t d[16], w[16];
                 narrow32_quads<S, false>(v, tp.inv_scale, tp.error_feedback, 0u, 0xffffffffu, d);
                 quads_to_adjacent(d, w);
-                tmem_st16(yp + 16 * cc, w);
+                tmem_st16(yp + 16 * (c0 + 2), w);
             }
             tmem_st_wait();
             tc_fence_before();
@@ -268,7 +290,8 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
         const int ew = warp - 2 - kYxConvWarps;
         const int quad = warp & 3, part = ew >> 2;  // part: x-outputs part * 64 .. + 64 of the tile
         const uint32_t lb = tmem + ((uint32_t) (quad * 32) << 16);
-        uint8_t *stg = stage_out + ew * kXStageWarpBytes;
+        uint8_t *stg = stage_out + ew * 2 * kXStageWarpBytes;
+        int sbuf = 0;
         const int64_t n_vox = p.nz * p.ny * p.nx, rows = p.nz * p.ny;
         int64_t tl = 0;
         for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
@@ -277,7 +300,7 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
             const int64_t y = y0 + quad * 32 + lane;
             const bool live_row = y < p.ny;
             const int64_t row = (int64_t) z * p.ny + y;
-            MaskWords mw[2];
+            MaskWords mw[2] = {};
 #pragma unroll
             for (int k = 0; k < 2; k++) {
                 const int64_t xb = x0 + part * 64 + 32 * k;
@@ -286,45 +309,53 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ Y
             }
             if (!__all_sync(0xffffffffu, mbar_wait(xfull, (uint32_t) (tl & 1), 2))) break;
             tc_fence_after();
+            // Both runs read at once, so the x accumulator is free for x(tl + 1)
+            // before this warp's rounding and stores.
+            float h[64];
+            tmem_ld64(lb + kYxAccX + part * 64, h);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(xempty);
+            const uint32_t m0 = mask_flags<FMT>(mw[0], p.mask), m1 = mask_flags<FMT>(mw[1], p.mask);
+            // Non-final: both runs rounded together (two independent chains per step).
+            uint32_t dd[2][16];
+            if (!FINAL) narrow64_pairs_forced<S>(h, tp.inv_scale, tp.error_feedback, m0, m1, dd[0], dd[1]);
 #pragma unroll
             for (int k = 0; k < 2; k++) {
                 const int64_t xb = x0 + part * 64 + 32 * k;
-                float hk[32];
-                __syncwarp();
-                tmem_ld32(lb + kYxAccX + part * 64 + 32 * k, hk);
-                if (k == 1) {
-                    // every read of this warp is done: the x accumulator may be reused
-                    tc_fence_before();
+                if (FINAL) {
+                    const float(&hk)[32] = *reinterpret_cast<const float(*)[32]>(h + 32 * k);
+                    contig_final32(hk, k ? m1 : m0, live_row ? row : rows, rows, p.nx, xb, tp.inv_scale, p.out_u16,
+                                   p.field_out);
+                } else {
+                    // TMA store of the warp's 32 rows x 32 voxels (64-byte swizzle of the
+                    // store map, which clips rows and columns outside the volume).  Every
+                    // run commits one bulk group (an empty one outside the volume), so the
+                    // wait below always covers the store that last read the buffer.
+                    uint32_t q[16];
+                    pairs_to_adjacent(dd[k], q);
+                    if (lane == 0) bulk_wait_read<1>();
                     __syncwarp();
-                    if (lane == 0) mbar_arrive(xempty);
-                }
-                const uint32_t m = mask_flags<FMT>(mw[k], p.mask);
-                if (p.final_pass) {
-                    contig_final32(hk, m, live_row ? row : rows, rows, p.nx, xb, tp.inv_scale, p.out_u16, p.field_out);
-                } else if (xb < p.nx) {  // warp-uniform
-                    uint32_t d[16], q[16];
-                    narrow32_pairs<S, true>(hk, tp.inv_scale, tp.error_feedback, m, 0xffffffffu, d);
-                    pairs_to_adjacent(d, q);
-                    const int64_t oi = !live_row ? -1
-                                       : p.out_nz == 0 ? row * p.nx + xb
-                                                        : ((y * p.out_nz + p.out_z0 + z) * p.nx) + xb;
-                    __syncwarp();
+                    uint8_t *sb = stg + sbuf * kXStageWarpBytes;
 #pragma unroll
                     for (int i = 0; i < 4; i++)
-                        *reinterpret_cast<uint4 *>(stg + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) =
+                        *reinterpret_cast<uint4 *>(sb + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) =
                             make_uint4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
+                    fence_proxy_async_smem();
                     __syncwarp();
-                    const int sub = lane & 3, rsub = lane >> 2;
-#pragma unroll
-                    for (int r4 = 0; r4 < 4; r4++) {
-                        const int rr = r4 * 8 + rsub;
-                        const int64_t o = __shfl_sync(0xffffffffu, oi, rr);
-                        const uint4 wv = *reinterpret_cast<const uint4 *>(stg + rr * 64 + ((sub ^ ((rr >> 1) & 3)) << 4));
-                        if (o >= 0 && xb + sub * 8 < p.nx) *reinterpret_cast<uint4 *>(p.out + o + sub * 8) = wv;
+                    if (lane == 0) {
+                        const int yq = y0 + quad * 32;
+                        if (xb < p.nx && yq < p.ny) {
+                            if (p.out_nz > 0) tma_store_3d(&omap, sb, (int) xb, z, yq);
+                            else tma_store_3d(&omap, sb, (int) xb, yq, z);
+                        }
+                        bulk_commit();
                     }
+                    sbuf ^= 1;
                 }
             }
         }
+        if (!FINAL && lane == 0) bulk_wait_all();
     }
     __syncthreads();
     if (warp == 0) {

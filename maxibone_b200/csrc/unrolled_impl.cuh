@@ -201,9 +201,8 @@ cudaError_t dispatch_unrolled(const Volume &v, const void *mask, int mask_fmt, c
         const bool use_tc = (flags & MAXI_FLAG_NO_TENSOR_CORES) == 0 && tc::tc_supported(radius, v.nz, v.ny, v.nx);
         // The rebuilt-mask semantics rewrite the mask between repetitions from the
         // x pass's output; they keep the separate passes.
-        const bool fuse = (flags & MAXI_FLAG_FUSE_YX) != 0 &&
-                          (flags & (MAXI_FLAG_SEPARATE_PASSES | MAXI_FLAG_MASK_FROM_FIELD)) == 0;
-        const bool hi_only = (flags & MAXI_FLAG_SPLIT_COEFFICIENTS) == 0;
+        const bool fuse = (flags & (MAXI_FLAG_SEPARATE_PASSES | MAXI_FLAG_MASK_FROM_FIELD)) == 0;
+        const bool hi_only = tc::tc_single_set(radius, (flags & MAXI_FLAG_SPLIT_COEFFICIENTS) != 0);
         if (ef) return dispatch_radius<S, true>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, fuse, hi_only, rebuild, o, st);
         return dispatch_radius<S, false>(v, mask, mask_fmt, kernel, radius, reps, b0, b1, out_u16, field_out, use_tc, fuse, hi_only, rebuild, o, st);
     } else {

@@ -24,7 +24,7 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
             field: str = "f32", field_out: torch.Tensor | None = None, shape=None,
             reference_rounding: bool = False, workspace: torch.Tensor | None = None,
             stream: torch.cuda.Stream | None = None, tensor_cores: bool = True,
-            error_feedback: bool = True, fuse_passes: bool = False, split_coefficients: bool = False) -> None:
+            error_feedback: bool = True, fuse_passes: bool = True, split_coefficients: bool = False) -> None:
     """Run the diffusion on device buffers.
 
     mask: uint8 [nz, ny, nx] CUDA tensor (set when > 0), or a bit-packed int32/uint32
@@ -36,11 +36,12 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
     workspace: uint8 CUDA tensor of at least workspace_bytes(shape, field), or None.
     tensor_cores: 16-bit fields: z and y passes on tcgen05 tensor cores where supported.
     error_feedback: 16-bit fields: error-feedback rounding along x (else round to nearest).
-    fuse_passes: 16-bit tensor-core fields, radius <= 32: the y and x passes in one
-          kernel per z-plane tile (default: two kernels, two HBM round trips).
+    fuse_passes: 16-bit tensor-core fields, radius 12 to 32: the y and x passes in one
+          kernel per z-plane tile (else two kernels, two HBM round trips).
     split_coefficients: 16-bit tensor-core passes: high + low 16-bit coefficient halves
           (two MMAs per K step, separate y and x passes) instead of one set whose
-          taps keep the kernel's sum and second moment.
+          taps keep the kernel's sum and second moment (the default from radius 12;
+          smaller radii always use the halves).
     """
     if not mask.is_cuda:
         raise ValueError("mask must be a CUDA tensor")
@@ -79,8 +80,8 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
         flags |= _lib.FLAG_NO_TENSOR_CORES
     if not error_feedback:
         flags |= _lib.FLAG_NEAREST_ROUNDING
-    if fuse_passes:
-        flags |= _lib.FLAG_FUSE_YX
+    if not fuse_passes:
+        flags |= _lib.FLAG_SEPARATE_PASSES
     if split_coefficients:
         flags |= _lib.FLAG_SPLIT_COEFFICIENTS
     with torch.cuda.device(mask.device):

@@ -53,9 +53,11 @@ struct BatchVolume {
 };
 
 // How a tensor-core group runs: one launch per pass over all its volumes, the
-// single-volume tensor-core launches per volume, or per-volume CUDA-core passes.
-enum GroupForm { kFormBatched = 0, kFormPerVolumeTc = 1, kFormCudaCores = 2, kForms = 3 };
-static const char *const kFormNames[kForms] = {"batched", "per_volume_tc", "cuda_cores"};
+// single-volume tensor-core launches per volume (separate y and x passes, or
+// the fused y + x kernel where the radius allows it), or per-volume CUDA-core
+// passes.
+enum GroupForm { kFormBatched = 0, kFormPerVolumeTc = 1, kFormPerVolumeFused = 2, kFormCudaCores = 3, kForms = 4 };
+static const char *const kFormNames[kForms] = {"batched", "per_volume_tc", "per_volume_fused", "cuda_cores"};
 
 struct TcGroup {
     std::vector<int> members;
@@ -72,7 +74,7 @@ struct TcGroup {
 // A tuning decision and the timings it came from (ms for 3 repetitions; < 0: not timed).
 struct TuneEntry {
     int form = kFormBatched;
-    float ms[kForms] = {-1.0f, -1.0f, -1.0f};
+    float ms[kForms] = {-1.0f, -1.0f, -1.0f, -1.0f};
 };
 
 static std::mutex g_tune_mu;
@@ -181,20 +183,23 @@ static cudaError_t enqueue_init(maxi_batch_plan *p, const std::vector<int> &idx,
     return cudaSuccess;
 }
 
-// The per-volume path of one volume (all repetitions).
+// The per-volume path of one volume (all repetitions).  fused: the y and x
+// passes as the fused kernel where it applies (else two kernels, the form of
+// the batched launches).
 template <typename S>
-static cudaError_t enqueue_single(maxi_batch_plan *p, BatchVolume &bv, int32_t extra_flags, cudaStream_t st) {
+static cudaError_t enqueue_single(maxi_batch_plan *p, BatchVolume &bv, int32_t extra_flags, cudaStream_t st,
+                                  bool fused = false) {
     const int64_t n = bv.v.nz * bv.v.ny * bv.v.nx;
     cudaError_t e = launch_bitpack_encode(static_cast<const uint8_t *>(bv.v.mask), n, vol_packed(p, bv), false, st);
     if (e != cudaSuccess) return e;
     const Volume vol{bv.v.nz, bv.v.ny, bv.v.nx};
     // The batched tensor-core launches run the y and x passes as separate
-    // kernels; the per-volume path does the same, so that every volume of a
-    // plan is computed by the same form.
+    // kernels; the per-volume path does the same unless asked for the fused
+    // kernel (a group's chosen form applies to all its volumes).
     return dispatch_unrolled<S>(vol, vol_packed(p, bv), MAXI_MASK_BITPACKED, bv.kernel.data(),
                                 (int) (bv.v.kernel_size / 2), bv.v.repititions, vol_buf<S>(p, bv, 0),
                                 vol_buf<S>(p, bv, 1), bv.v.output, bv.v.field_out,
-                                p->flags | extra_flags | MAXI_FLAG_SEPARATE_PASSES, st);
+                                p->flags | extra_flags | (fused ? 0 : MAXI_FLAG_SEPARATE_PASSES), st);
 }
 
 // All repetitions of a tensor-core group as batched launches.
@@ -203,7 +208,7 @@ static cudaError_t enqueue_group_tc(maxi_batch_plan *p, TcGroup &g, cudaStream_t
     // A group of one volume runs the single-volume tensor-core launches (tensor
     // maps as kernel parameters instead of a device table); the arithmetic per
     // tile is the same.
-    if (g.members.size() == 1) return enqueue_single<S>(p, p->vols[g.members[0]], 0, st);
+    if (g.members.size() == 1) return enqueue_single<S>(p, p->vols[g.members[0]], 0, st, false);
     cudaError_t e = enqueue_init<S>(p, g.members, st);
     if (e != cudaSuccess) return e;
     const bool bf16 = std::is_same<S, __nv_bfloat16>::value;
@@ -230,7 +235,7 @@ static cudaError_t enqueue_group(maxi_batch_plan *p, TcGroup &g, int form, cudaS
     cudaError_t e = cudaSuccess;
     const int32_t extra = form == kFormCudaCores ? MAXI_FLAG_NO_TENSOR_CORES : 0;
     for (int i : g.members)
-        if ((e = enqueue_single<S>(p, p->vols[i], extra, st)) != cudaSuccess) break;
+        if ((e = enqueue_single<S>(p, p->vols[i], extra, st, form == kFormPerVolumeFused)) != cudaSuccess) break;
     return e;
 }
 
@@ -326,6 +331,10 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
         p->groups[gi].members.push_back((int) i);
         bv.group = gi;
     }
+    // Default form: one batched launch per pass; a group of one volume runs the
+    // single-volume launches with the fused y + x kernel, as a single-volume
+    // call does.
+    for (TcGroup &g : p->groups) g.form = g.members.size() == 1 ? kFormPerVolumeFused : kFormBatched;
     // Device tables of each group.
     for (TcGroup &g : p->groups) {
         const int n = (int) g.members.size();
@@ -365,11 +374,12 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
             }
             if (!known) {
                 // A single volume's batched launch is its per-volume launch.
+                te.form = -1;
                 for (int f = 0; f < kForms; f++) {
-                    if (f == kFormPerVolumeTc && g.members.size() == 1) continue;
+                    if (f == kFormBatched && g.members.size() == 1) continue;
                     cudaError_t e = time_group<S>(p, g, f, user_st, &te.ms[f]);
                     if (e != cudaSuccess) return set_cuda_error(e, "batch autotuning");
-                    if (te.ms[f] < te.ms[te.form]) te.form = f;
+                    if (te.form < 0 || te.ms[f] < te.ms[te.form]) te.form = f;
                 }
                 std::lock_guard<std::mutex> lk(g_tune_mu);
                 g_tune_cache[key] = te;
@@ -411,7 +421,8 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
         const TcGroup &g = p->groups[k];
         snprintf(line, sizeof(line), "group %zu: %zu volumes, kernel length %zu, %lld repetitions, %s%s%s\n", k,
                  g.members.size(), g.kernel.size(), (long long) g.reps,
-                 g.form == kFormCudaCores ? "per-volume CUDA-core passes"
+                 g.form == kFormCudaCores       ? "per-volume CUDA-core passes"
+                 : g.form == kFormPerVolumeFused ? "single-volume tensor-core launches, fused y + x where it applies"
                  : g.form == kFormPerVolumeTc || g.members.size() == 1 ? "single-volume tensor-core launches"
                                                                         : "one tensor-core launch per pass",
                  g.note.empty() ? "" : "; ", g.note.c_str());

@@ -28,13 +28,23 @@ def make_batch(field):
     return masks, outs, fouts, kernels
 
 
-def single(mask, kernel, reps, field):
+def single(mask, kernel, reps, field, fused=False):
     out = torch.empty(mask.shape, dtype=torch.uint16, device="cuda")
     fo = torch.empty(mask.shape, dtype=torch.float32, device="cuda")
-    # The batch runs the y and x passes as separate kernels: compare with the
-    # same form of the single-volume call.
-    device.diffuse(mask, kernel, reps, output=out, field=field, field_out=fo, fuse_passes=False)
+    # The batched launches run the y and x passes as separate kernels: compare
+    # with the same form of the single-volume call (a tensor-core group of one
+    # volume runs the single-volume launches with the fused y + x kernel).
+    device.diffuse(mask, kernel, reps, output=out, field=field, field_out=fo, fuse_passes=fused)
     return out, fo
+
+
+def alone_in_group(i, shapes, sigmas, reps):
+    """Whether volume i is the only tensor-core-eligible volume of its
+    (kernel, repetitions) group (x extent a multiple of 8 and >= 64, radius <= 32)."""
+    def eligible(j):
+        return shapes[j][2] % 8 == 0 and shapes[j][2] >= 64 and round(4 * sigmas[j]) <= 32
+    return eligible(i) and sum(1 for j in range(len(shapes))
+                               if eligible(j) and sigmas[j] == sigmas[i] and reps[j] == reps[i]) == 1
 
 
 @pytest.mark.parametrize("field", ["bf16", "f16", "f32"])
@@ -46,7 +56,7 @@ def test_batch_equals_single_volume_runs(field):
     torch.cuda.synchronize()
     device.tensor_core_status()
     for i in range(len(SHAPES)):
-        o, f = single(masks[i], kernels[i], REPS[i], field)
+        o, f = single(masks[i], kernels[i], REPS[i], field, fused=alone_in_group(i, SHAPES, SIGMAS, REPS))
         torch.cuda.synchronize()
         assert torch.equal(outs[i], o), (i, text)
         assert torch.equal(fouts[i], f), (i, text)

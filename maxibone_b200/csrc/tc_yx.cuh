@@ -32,16 +32,18 @@
 // passes).  Coefficients: one 16-bit set rounded to keep the kernel's sum and
 // second moment (tc_round_taps_matched).
 //
-// Tensor-core schedule.  A tcgen05.mma of M = 128 costs the issuing thread
-// about 130 cycles on B200 whatever its N (up to 192), so every product is one
-// chain of the widest N: 2 KP / 16 MMAs per tile.  Step t issues y(t), then
-// x(t - 1): the conversion of tile t runs while the tensor cores do x(t - 1),
-// and writes the other Y' buffer.  Tensor memory (512 columns): [0, 192) y
-// accumulator, [192, 384) the two Y' buffers, [384, 512) x accumulator.  Warp
-// roles: 0 TMA producer, 1 MMA issuer, 2-9 conversion (two per TMEM lane
-// quadrant), 10-17 epilogue (two per quadrant, 64 x-outputs each).  Every wait
-// is bounded; on a timeout the kernel records a code in g_tc_error, lets the
-// copies and MMAs it started finish (bounded) and winds down.
+// Tensor-core schedule.  A thread issues a tcgen05.mma of M = 128 about every
+// 100 cycles on B200 whatever its N (up to 192), while two issuing threads
+// reach the tensor cores' peak at N = 128: so every product is one chain of
+// the widest N (KP / 16 MMAs each for y and x per tile), and the y and the x
+// MMAs have an issuing thread each.  The conversion of tile t runs while the
+// tensor cores do x(t - 1) and writes the other Y' buffer.  Tensor memory (512
+// columns): [0, 192) y accumulator, [192, 384) the two Y' buffers, [384, 512) x
+// accumulator.  Warp roles: 0 TMA producer, 1 y MMA issuer, 2-9 conversion (two
+// per TMEM lane quadrant), 10-17 epilogue (two per quadrant, 64 x-outputs
+// each), 18 x MMA issuer.  Every wait is bounded; on a timeout the kernel
+// records a code in g_tc_error, lets the copies and MMAs it started finish
+// (bounded) and winds down.
 #pragma once
 
 #include "tc_kernels.cuh"
@@ -52,7 +54,8 @@ namespace tc {
 constexpr int kYxMaxStages = 4;                                  // F tile ring
 constexpr int kYxConvWarps = 8;                                  // two per TMEM lane quadrant
 constexpr int kYxEpiWarps = 8;                                   // two per lane quadrant
-constexpr int kYxThreads = 64 + 32 * (kYxConvWarps + kYxEpiWarps);  // 576
+constexpr int kYxXWarp = 2 + kYxConvWarps + kYxEpiWarps;       // x MMA issuer (warp 18)
+constexpr int kYxThreads = 32 * (kYxXWarp + 1);                  // 608
 constexpr int kYxMaxCols = 192;                                  // KP for radius <= 32
 constexpr uint32_t kYxAccY = 0;                                  // y accumulator, KP columns
 constexpr uint32_t kYxYp = 192;                                  // two Y' buffers of KP / 2 columns
@@ -115,10 +118,11 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
     uint64_t *yfull = bars + 2 * kYxMaxStages;  // y accumulator complete (MMA commit)
     uint64_t *yfree = yfull + 1;                // y accumulator read (conversion warps)
     uint64_t *ypacked = yfull + 2;              // [2] Y' buffer written (conversion warps)
-    uint64_t *xfull = yfull + 4;                // x accumulator complete (MMA commit)
+    uint64_t *xfull = yfull + 4;                // x accumulator complete (x MMA commit)
     uint64_t *xempty = yfull + 5;               // x accumulator read (epilogue warps)
-    uint64_t *drain = yfull + 6;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(yfull + 7);
+    uint64_t *ypfree = yfull + 6;               // [2] Y' buffer read by the x MMAs (x MMA commit)
+    uint64_t *drain = yfull + 8;                // [2] every MMA of the y / x issuer complete
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(yfull + 10);
     uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 1024;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t total = p.n_tiles;
@@ -141,7 +145,10 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
         mbar_init(&ypacked[1], kYxConvWarps);
         mbar_init(xfull, 1);
         mbar_init(xempty, kYxEpiWarps);
-        mbar_init(drain, 1);
+        mbar_init(&ypfree[0], 1);
+        mbar_init(&ypfree[1], 1);
+        mbar_init(&drain[0], 1);
+        mbar_init(&drain[1], 1);
         fence_barrier_init();
         prefetch_tmap(&tmap);
         if (!FINAL) prefetch_tmap(&omap);
@@ -168,7 +175,11 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
 
     if (warp == 0 && lane == 0) {
         // TMA producer: one F tile (nch boxes) per ring stage; L2 prefetch ahead.
+        // The stage and its phase advance incrementally (the ring depth is a
+        // run-time value: no 64-bit division per tile).
         int64_t tl = 0;
+        int s = 0;
+        uint32_t ph = 0;
         for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
             int z, y0, x0;
             const int64_t gp = g + kPrefetch * (int64_t) gridDim.x;
@@ -177,19 +188,22 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
                 for (int c = 0; c < nch; c++) tma_prefetch_3d(&tmap, x0 - tp.ra + 64 * c, y0 - tp.ra, z);
             }
             decode(g, z, y0, x0);
-            const int s = (int) (tl % stages);
-            if (!mbar_wait(&empty[s], (uint32_t) (((tl / stages) & 1) ^ 1), 1)) break;
+            if (!mbar_wait(&empty[s], ph ^ 1, 1)) break;
             mbar_arrive_expect_tx(&full[s], tile_bytes);
             for (int c = 0; c < nch; c++)
                 tma_load_3d(ring + s * tile_bytes + c * chunk_bytes, &tmap, x0 - tp.ra + 64 * c, y0 - tp.ra, z,
                             &full[s]);
+            if (++s == stages) s = 0, ph ^= 1;
         }
         // Let every copy this thread started land before the CTA can exit: the
         // last use of each ring stage (bounded, so an aborted run still ends).
         for (int64_t k = tl - stages; k < tl; k++)
             if (k >= 0) mbar_wait(&full[k % stages], (uint32_t) ((k / stages) & 1), 1);
-    } else if (warp == 1 && lane == 0) {
-        // MMA issuer.  Step tl issues y(tl), then x(tl - 1).
+    } else if ((warp == 1 || warp == kYxXWarp) && lane == 0) {
+        // MMA issuers.  A thread issues a tcgen05.mma about every 100 cycles
+        // whatever its N, so the y MMAs (warp 1) and the x MMAs (warp 18) have
+        // an issuing thread each; their ordering is through the barriers.
+        const bool is_y = warp == 1;
         const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
         const uint32_t idesc_y = idesc_f16(fmt, 0 /*A K-major*/, 1 /*B MN-major*/, kTM, (uint32_t) kp);
         const uint32_t idesc_x = idesc_f16(fmt, 0 /*A K-major*/, 0 /*B K-major*/, kTM, kXTN);
@@ -197,15 +211,12 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
         const uint64_t t_desc = smem_desc_sw128(smem_u32(tt), 16, 1024);
         const uint32_t r0 = smem_u32(ring);
         const int ks_n = kp / 16;
-        bool ok = true;
-        for (int64_t tl = 0;; tl++) {
-            const int64_t g = blockIdx.x + tl * (int64_t) gridDim.x;
-            const bool has_y = g < total, has_x = tl > 0 && g - gridDim.x < total;
-            if (!has_y && !has_x) break;
-            if (has_y) {
-                const int s = (int) (tl % stages);
-                ok = mbar_wait(&full[s], (uint32_t) ((tl / stages) & 1), 1);
-                // the conversion warps have read the previous tile's y accumulator
+        int s = 0;  // ring stage of tile tl and its phase, advanced incrementally
+        uint32_t ph = 0;
+        for (int64_t tl = 0; blockIdx.x + tl * (int64_t) gridDim.x < total; tl++) {
+            if (is_y) {
+                // y(tl): its F tile has landed and the conversion warps have read y(tl - 1)
+                bool ok = mbar_wait(&full[s], ph, 1);
                 if (ok && tl > 0) ok = mbar_wait(yfree, (uint32_t) ((tl - 1) & 1), 3);
                 if (!ok) break;
                 tc_fence_after();
@@ -216,33 +227,34 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
                              f_desc + (uint64_t) (ks * 128), idesc_y, ks > 0 ? 1u : 0u);
                 umma_commit(&empty[s]);
                 umma_commit(yfull);
-            }
-            if (has_x) {
-                // Y' of tile tl - 1 is in place (one barrier per buffer: the
-                // conversion warps cannot complete a second phase of it before
-                // this wait, since that needs y(tl + 1)) and the epilogue has
-                // read the x accumulator
-                ok = mbar_wait(&ypacked[(tl - 1) & 1], (uint32_t) (((tl - 1) >> 1) & 1), 3) &&
-                     mbar_wait(xempty, (uint32_t) (((tl - 1) & 1) ^ 1), 3);
-                if (!ok) break;
+                if (++s == stages) s = 0, ph ^= 1;
+            } else {
+                // x(tl): Y' of tile tl is in place (one barrier per buffer: the
+                // conversion warps cannot complete a second phase of it before this
+                // wait, since that needs x(tl) itself) and the epilogue has read
+                // x(tl - 1)
+                const int b = (int) (tl & 1);
+                if (!(mbar_wait(&ypacked[b], (uint32_t) ((tl >> 1) & 1), 3) &&
+                      mbar_wait(xempty, (uint32_t) ((tl & 1) ^ 1), 3)))
+                    break;
                 tc_fence_after();
-                const uint32_t yp = tmem + kYxYp + (uint32_t) ((tl - 1) & 1) * kYxYpCols;
+                const uint32_t yp = tmem + kYxYp + (uint32_t) b * kYxYpCols;
                 for (int ks = 0; ks < ks_n; ks++)
                     umma_f16_ts(tmem + kYxAccX, yp + ks * 8, t_desc + (uint64_t) ((ks >> 2) * 1024 + (ks & 3) * 2),
                                 idesc_x, ks > 0 ? 1u : 0u);
                 umma_commit(xfull);
+                umma_commit(&ypfree[b]);
             }
         }
         // Every MMA this thread issued has completed before the CTA winds down.
-        umma_commit(drain);
-        mbar_wait(drain, 0, 2);
+        umma_commit(&drain[is_y ? 0 : 1]);
+        mbar_wait(&drain[is_y ? 0 : 1], 0, 2);
     } else if (warp >= 2 && warp < 2 + kYxConvWarps) {
         // Conversion: y accumulator (FP32) -> Y' (16-bit, packed).  The two warps
         // of a quadrant take the 32-column runs [3 half, 3 half + 3) of the
-        // window (two or three of them): the first two together, then the
-        // third; the y accumulator is free once the last run is read.  Y' of tile tl goes to buffer tl & 1,
-        // which x(tl - 2) read: that MMA was issued before y(tl), so it
-        // completed before yfull of tile tl.
+        // window (two or three of them): a third run first, then two together,
+        // whose reads free the y accumulator for y(tl + 1).  Y' of tile tl goes
+        // to buffer tl & 1, once x(tl - 2) has read it.
         const int quad = warp & 3, half = (warp - 2) >> 2;
         const uint32_t lb = tmem + ((uint32_t) (quad * 32) << 16);
         const int c0 = 3 * half, c1 = ncc < c0 + 3 ? ncc : c0 + 3;  // 2 or 3 runs
@@ -251,41 +263,50 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
             if (!__all_sync(0xffffffffu, mbar_wait(yfull, (uint32_t) (tl & 1), 2))) break;
             tc_fence_after();
             const uint32_t yp = lb + kYxYp + (uint32_t) (tl & 1) * kYxYpCols;
+            // Before the first write to the Y' buffer: x(tl - 2), its last reader, has completed.
+            bool yp_free = tl < 2, ok = true;
+            auto wait_yp = [&]() {
+                if (yp_free) return;
+                ok = __all_sync(0xffffffffu, mbar_wait(&ypfree[tl & 1], (uint32_t) (((tl >> 1) - 1) & 1), 2));
+                tc_fence_after();
+                yp_free = true;
+            };
+            if (c1 == c0 + 3) {
+                // a third run first, so that the last two reads come together
+                float v[32];
+                __syncwarp();
+                tmem_ld32(lb + kYxAccY + 32 * (c0 + 2), v);
+                uint32_t d[16], w[16];
+                narrow32_quads<S, false>(v, tp.inv_scale, tp.error_feedback, 0u, 0xffffffffu, d);
+                wait_yp();
+                if (!ok) break;
+                quads_to_adjacent(d, w);
+                tmem_st16(yp + 16 * (c0 + 2), w);
+            }
             {
-                // the first two runs together (four independent chains per step)
+                // two runs together (four independent chains per step); the y
+                // accumulator is free once they are read
                 float v[64];
                 __syncwarp();
                 tmem_ld64(lb + kYxAccY + 32 * c0, v);
-                if (c1 == c0 + 2) {
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(yfree);
-                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(yfree);
                 uint32_t d0[16], d1[16], w[16];
                 narrow64_quads<S>(v, tp.inv_scale, tp.error_feedback, d0, d1);
+                wait_yp();
+                if (!ok) break;
                 quads_to_adjacent(d0, w);
                 tmem_st16(yp + 16 * c0, w);
                 quads_to_adjacent(d1, w);
                 tmem_st16(yp + 16 * (c0 + 1), w);
-            }
-            if (c1 == c0 + 3) {
-                float v[32];
-                __syncwarp();
-                tmem_ld32(lb + kYxAccY + 32 * (c0 + 2), v);
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(yfree);
-                uint32_t d[16], w[16];
-                narrow32_quads<S, false>(v, tp.inv_scale, tp.error_feedback, 0u, 0xffffffffu, d);
-                quads_to_adjacent(d, w);
-                tmem_st16(yp + 16 * (c0 + 2), w);
             }
             tmem_st_wait();
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&ypacked[tl & 1]);
         }
-    } else if (warp >= 2 + kYxConvWarps) {
+    } else if (warp >= 2 + kYxConvWarps && warp < kYxXWarp) {
         // Epilogue: x accumulator -> re-illumination -> next field / final outputs.
         const int ew = warp - 2 - kYxConvWarps;
         const int quad = warp & 3, part = ew >> 2;  // part: x-outputs part * 64 .. + 64 of the tile

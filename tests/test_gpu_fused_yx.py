@@ -128,3 +128,20 @@ def test_fused_one_repetition_and_empty_full_masks():
     _, want = run(mask, kernel, 1, "f64")
     _, got = run(mask, kernel, 1, "bf16")
     assert np.abs(got.astype(np.float64) - want).max() <= VS_F64["bf16"]
+
+
+@pytest.mark.parametrize("field", ["bf16", "f16"])
+@pytest.mark.parametrize("shape,sigma", [((1, 1, 64), 3.0), ((3, 33, 64), 8.0), ((2, 257, 1000), 4.0),
+                                         ((4, 129, 136), 5.0)])
+def test_fused_thin_and_ragged_shapes(field, shape, sigma):
+    # One plane, one row, the narrowest x extent the tensor-core passes take,
+    # and extents one past a tile: windows and stores clipped on every side.
+    mask = spheres_mask(shape, 4, (1, 4), seed=sum(shape)) if min(shape) > 2 else \
+        random_mask(shape, 0.1, seed=sum(shape))
+    kernel = gauss_kernel(sigma).astype(np.float32)
+    _, want = run(mask, kernel, 3, "f64")
+    u16, got = run(mask, kernel, 3, field)
+    _, sep = run(mask, kernel, 3, field, fused=False)
+    assert np.abs(got.astype(np.float64) - want).max() <= VS_F64[field]
+    assert np.abs(got - sep).max() <= FUSED_VS_SEPARATE[field]
+    assert np.all(u16[mask > 0] == 65535)

@@ -65,8 +65,8 @@ struct TcGroup {
     int64_t reps = 0;
     tc::TcGeometry geo{};
     tc::TcVol *d_vols = nullptr;
-    int64_t *d_prefix = nullptr;  // [3][n + 1]: z columns, y columns, x tiles
-    int64_t totals[3] = {0, 0, 0};
+    int64_t *d_prefix = nullptr;  // [4][n + 1]: z columns, y columns, x tiles, fused y + x tiles
+    int64_t totals[4] = {0, 0, 0, 0};
     int form = kFormBatched;
     std::string note;
 };
@@ -215,9 +215,19 @@ static cudaError_t enqueue_group_tc(maxi_batch_plan *p, TcGroup &g, cudaStream_t
     const bool ef = (p->flags & MAXI_FLAG_NEAREST_ROUNDING) == 0 && g.geo.radius >= 4;
     const bool hi_only = tc::tc_single_set(g.geo.radius, (p->flags & MAXI_FLAG_SPLIT_COEFFICIENTS) != 0);
     const int n = (int) g.members.size();
+    // The y and x passes as the fused kernel where it applies (one coefficient
+    // set, radius <= 32), as the single-volume call runs them.
+    const bool fused = hi_only && (p->flags & MAXI_FLAG_SEPARATE_PASSES) == 0 && g.geo.radius <= tc::kTcMaxRadius;
     int in = 0;
     for (int64_t rep = 0; rep < g.reps; rep++) {
         const bool last = rep + 1 == g.reps;
+        if (fused) {
+            // z: buffer in -> in ^ 1 ([z][y][x]); fused y + x: in ^ 1 -> in ([y][z][x] rows).
+            if ((e = tc::tc_batch_pass(g.d_vols, g.d_prefix, g.totals[0], n, 0, in, false, g.kernel.data(), g.geo, bf16, ef, rep > 0, st, hi_only)) != cudaSuccess ||
+                (e = tc::tc_batch_pass(g.d_vols, g.d_prefix + 3 * (n + 1), g.totals[3], n, 3, in ^ 1, last, g.kernel.data(), g.geo, bf16, ef, true, st, hi_only)) != cudaSuccess)
+                return e;
+            continue;
+        }
         // The x pass hands the next repetition its field in [y][z][x] row order.
         if ((e = tc::tc_batch_pass(g.d_vols, g.d_prefix, g.totals[0], n, 0, in, false, g.kernel.data(), g.geo, bf16, ef, rep > 0, st, hi_only)) != cudaSuccess ||
             (e = tc::tc_batch_pass(g.d_vols, g.d_prefix + (n + 1), g.totals[1], n, 1, in ^ 1, false, g.kernel.data(), g.geo, bf16, ef, false, st, hi_only)) != cudaSuccess ||
@@ -339,7 +349,7 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
     for (TcGroup &g : p->groups) {
         const int n = (int) g.members.size();
         std::vector<tc::TcVol> vols(n);
-        std::vector<int64_t> prefix(3 * (n + 1), 0);
+        std::vector<int64_t> prefix(4 * (n + 1), 0);
         for (int k = 0; k < n; k++) {
             BatchVolume &bv = p->vols[g.members[k]];
             if (tc::tc_fill_volume(vols[k], vol_buf<S>(p, bv, 0), vol_buf<S>(p, bv, 1), vol_packed(p, bv), bv.v.output,
@@ -349,8 +359,9 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
             prefix[k + 1] = prefix[k] + vols[k].cols_z;
             prefix[(n + 1) + k + 1] = prefix[(n + 1) + k] + vols[k].cols_y;
             prefix[2 * (n + 1) + k + 1] = prefix[2 * (n + 1) + k] + vols[k].tiles_x;
+            prefix[3 * (n + 1) + k + 1] = prefix[3 * (n + 1) + k] + vols[k].tiles_yx;
         }
-        for (int q = 0; q < 3; q++) g.totals[q] = prefix[q * (n + 1) + n];
+        for (int q = 0; q < 4; q++) g.totals[q] = prefix[q * (n + 1) + n];
         if (cudaMalloc(&g.d_vols, sizeof(tc::TcVol) * n) != cudaSuccess ||
             cudaMalloc(&g.d_prefix, sizeof(int64_t) * prefix.size()) != cudaSuccess) {
             cudaGetLastError();
@@ -424,7 +435,10 @@ static int build_plan(maxi_batch_plan *p, cudaStream_t user_st) {
                  g.form == kFormCudaCores       ? "per-volume CUDA-core passes"
                  : g.form == kFormPerVolumeFused ? "single-volume tensor-core launches, fused y + x where it applies"
                  : g.form == kFormPerVolumeTc || g.members.size() == 1 ? "single-volume tensor-core launches"
-                                                                        : "one tensor-core launch per pass",
+                 : tc::tc_single_set(g.geo.radius, (p->flags & MAXI_FLAG_SPLIT_COEFFICIENTS) != 0) &&
+                           !(p->flags & MAXI_FLAG_SEPARATE_PASSES) && g.geo.radius <= tc::kTcMaxRadius
+                     ? "one tensor-core launch per pass (z, fused y + x)"
+                     : "one tensor-core launch per pass (z, y, x)",
                  g.note.empty() ? "" : "; ", g.note.c_str());
         p->description += line;
     }

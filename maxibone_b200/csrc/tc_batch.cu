@@ -13,6 +13,7 @@
 
 #include "host_util.h"
 #include "tc_kernels.cuh"
+#include "tc_yx.cuh"
 
 namespace maxi {
 namespace tc {
@@ -46,6 +47,7 @@ int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_ma
     vol.cols_z = (int64_t) vol.n_xc_z * ny;
     vol.cols_y = (int64_t) vol.n_xc_y * nz;
     vol.tiles_x = (int64_t) vol.n_xt * ceil_div(nz * ny, kTM);
+    vol.tiles_yx = (int64_t) vol.n_xt * vol.n_at_y * nz;
     auto enc = tc_encode_fn();
     if (!enc) return -1;
     const CUtensorMapDataType dt = is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
@@ -63,6 +65,7 @@ int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_ma
         const cuuint64_t dr[3] = {(cuuint64_t) nx, (cuuint64_t) nz, (cuuint64_t) ny};
         const cuuint64_t sr[2] = {(cuuint64_t) (nx * 2), (cuuint64_t) (nz * nx * 2)};
         const cuuint32_t boxr[3] = {64u, (cuuint32_t) g.kp_strided, 1u};
+        const cuuint32_t boxyx[3] = {32u, 1u, 32u};
         if (enc(&vol.map[0][b], dt, 3, base, d3, s3, boxz, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
             enc(&vol.map[1][b], dt, 3, base, d3, s3, boxy, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -72,7 +75,9 @@ int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_ma
             enc(&vol.ystore[b], dt, 3, base, d3, s3, boxs, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                 CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
             enc(&vol.zrows[b], dt, 3, base, dr, sr, boxr, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
+            enc(&vol.yxrows[b], dt, 3, base, dr, sr, boxyx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return -1;
     }
     return 0;
@@ -88,7 +93,27 @@ cudaError_t tc_batch_pass(const TcVol *d_vols, const int64_t *d_prefix, int64_t 
     const unsigned grid = (unsigned) std::min<int64_t>(total, sms);
     CUtensorMap unused{};  // the batch kernels read their maps from the volume table
     cudaError_t e;
-    if (pass == 2) {
+    if (pass == 3) {
+        if (!hi_only || g.radius > kTcMaxRadius || g.kp_contig != g.kp_strided) return cudaErrorInvalidValue;
+        YxLaunch<ManyVolumesYx> p{};
+        fill_pass_taps(p.t, kernel, g.radius, g.ra, g.kp_contig, is_bf16, error_feedback, true);
+        p.final_pass = final_pass ? 1 : 0;
+        int smem_max = 0;
+        cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        p.stages = yx_stages(p.t.kp, p.t.kpa, smem_max);
+        p.sched.vols = d_vols;
+        p.sched.prefix = d_prefix;
+        p.sched.n_vol = n_vol;
+        p.sched.in_buf = in_buf;
+        const int smem = yx_smem_bytes(p.t.kp, p.t.kpa, p.stages);
+        if (smem > smem_max) return cudaErrorInvalidValue;
+        auto *k = is_bf16 ? (final_pass ? tc_yx_kernel<__nv_bfloat16, MAXI_MASK_BITPACKED, true, ManyVolumesYx>
+                                        : tc_yx_kernel<__nv_bfloat16, MAXI_MASK_BITPACKED, false, ManyVolumesYx>)
+                          : (final_pass ? tc_yx_kernel<__half, MAXI_MASK_BITPACKED, true, ManyVolumesYx>
+                                        : tc_yx_kernel<__half, MAXI_MASK_BITPACKED, false, ManyVolumesYx>);
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+        k<<<grid, kYxThreads, smem, st>>>(unused, unused, p);
+    } else if (pass == 2) {
         ContigLaunch<ManyVolumesContig> p{};
         fill_pass_taps(p.taps, kernel, g.radius, g.ra, g.kp_contig, is_bf16, error_feedback, hi_only);
         p.final_pass = final_pass ? 1 : 0;

@@ -12,21 +12,22 @@ namespace maxi {
 namespace tc {
 
 // Device-table entry of one volume: tensor maps of the pass inputs
-// ([pass z/y/x][buffer]), of the y pass's stores and of the z pass's input in
-// [y][z][x] row order ([buffer]), the two
-// ping-pong field buffers, the bit-packed mask, the final outputs and the tile
-// counts.
+// ([pass z/y/x][buffer]), of the y pass's stores, of the z pass's input in
+// [y][z][x] row order and of the fused y + x kernel's stores in that order
+// ([buffer]), the two ping-pong field buffers, the bit-packed mask, the final
+// outputs and the tile counts.
 struct alignas(64) TcVol {
     CUtensorMap map[3][2];
     CUtensorMap ystore[2];
-    CUtensorMap zrows[2];  // z-pass input read as [y][z][x] rows ([buffer])
+    CUtensorMap zrows[2];   // z-pass input read as [y][z][x] rows ([buffer])
+    CUtensorMap yxrows[2];  // fused y + x stores to [y][z][x] rows ([buffer]), box 32 x 1 x 32
     void *buf[2];
     const uint32_t *mask;
     uint16_t *out_u16;
     float *field_out;
     int64_t nz, ny, nx;
     int n_at_z, n_at_y, n_xc_z, n_xc_y, n_xt;
-    int64_t cols_z, cols_y, tiles_x;
+    int64_t cols_z, cols_y, tiles_x, tiles_yx;
 };
 
 // K extents of the strided (z/y) and contiguous (x) tensor-core passes.
@@ -42,8 +43,10 @@ void tc_split_taps(const float *kernel, int radius, bool is_bf16, float scale, u
 int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_mask, uint16_t *out_u16,
                    float *field_out, int64_t nz, int64_t ny, int64_t nx, bool is_bf16, const TcGeometry &g);
 
-// One pass (0 z, 1 y, 2 x) over all volumes of a device table; d_prefix holds
-// n_vol + 1 prefix sums of the volumes' columns (z: cols_z, y: cols_y) or x tiles.
+// One pass (0 z, 1 y, 2 x, 3 fused y + x) over all volumes of a device table;
+// d_prefix holds n_vol + 1 prefix sums of the volumes' columns (z: cols_z, y:
+// cols_y) or tiles (x: tiles_x, fused: tiles_yx).  The fused pass needs the
+// single coefficient set (hi_only) and radius <= kTcMaxRadius.
 // rows_yz: the z pass reads its input as [y][z][x] rows, the x pass (not
 // final) writes its output in that order.  hi_only: one matched 16-bit
 // coefficient set (the default of the single-volume passes) instead of the

@@ -222,23 +222,23 @@ cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool fina
     if (radius > kTcMaxRadius) return cudaErrorInvalidValue;
     const bool is_bf16 = std::is_same<S, __nv_bfloat16>::value;
     if (final_pass) out_rows = nullptr;
-    YxLaunch p{};
+    YxLaunch<OneVolumeYx> p{};
     const int ra = (int) round_up(radius, 8);
     if (!hi_only) return cudaErrorInvalidValue;  // the fused kernel holds one coefficient set
     fill_pass_taps(p.t, kernel, radius, ra, (int) round_up(kXTN + ra + radius, 16), is_bf16, error_feedback, true);
     if (p.t.kp > kYxMaxCols || (uint32_t) p.t.kp / 2 > kYxYpCols) return cudaErrorInvalidValue;
     p.final_pass = final_pass ? 1 : 0;
-    p.mask = mask;
-    p.out_u16 = out_u16;
-    p.field_out = field_out;
-    p.nz = nz;
-    p.ny = ny;
-    p.nx = nx;
-    p.out_nz = out_rows ? out_rows->nz_total : 0;
-    p.out_z0 = out_rows ? out_rows->z0 : 0;
-    p.n_ty = (int) ceil_div(ny, kTM);
-    p.n_tx = (int) ceil_div(nx, kXTN);
-    p.n_tiles = nz * p.n_ty * p.n_tx;
+    OneVolumeYx &sc = p.sched;
+    sc.mask = mask;
+    sc.out_u16 = out_u16;
+    sc.field_out = field_out;
+    sc.nz = nz;
+    sc.ny = ny;
+    sc.nx = nx;
+    sc.rows_yzx = out_rows ? 1 : 0;
+    sc.n_ty = (int) ceil_div(ny, kTM);
+    sc.n_tx = (int) ceil_div(nx, kXTN);
+    sc.n_tiles = nz * sc.n_ty * sc.n_tx;
 
     CUtensorMap map;
     const cuuint64_t dims[3] = {(cuuint64_t) nx, (cuuint64_t) ny, (cuuint64_t) nz};
@@ -272,12 +272,14 @@ cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool fina
     p.stages = yx_stages(p.t.kp, p.t.kpa, smem_max);
     const int smem = yx_smem_bytes(p.t.kp, p.t.kpa, p.stages);
     if (smem > smem_max) return cudaErrorInvalidValue;
-    auto *kern = mask_fmt == MAXI_MASK_U8 ? (final_pass ? tc_yx_kernel<S, MAXI_MASK_U8, true> : tc_yx_kernel<S, MAXI_MASK_U8, false>)
-                                          : (final_pass ? tc_yx_kernel<S, MAXI_MASK_BITPACKED, true>
-                                                        : tc_yx_kernel<S, MAXI_MASK_BITPACKED, false>);
+    auto *kern = mask_fmt == MAXI_MASK_U8
+                     ? (final_pass ? tc_yx_kernel<S, MAXI_MASK_U8, true, OneVolumeYx>
+                                   : tc_yx_kernel<S, MAXI_MASK_U8, false, OneVolumeYx>)
+                     : (final_pass ? tc_yx_kernel<S, MAXI_MASK_BITPACKED, true, OneVolumeYx>
+                                   : tc_yx_kernel<S, MAXI_MASK_BITPACKED, false, OneVolumeYx>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    const int64_t grid = std::min<int64_t>(p.n_tiles, sms);
+    const int64_t grid = std::min<int64_t>(sc.n_tiles, sms);
     kern<<<(unsigned) grid, kYxThreads, smem, st>>>(map, omap, p);
     return cudaGetLastError();
 }

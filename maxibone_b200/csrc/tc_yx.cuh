@@ -80,27 +80,105 @@ __host__ __device__ constexpr int yx_stages(int kp, int kpa, int smem_max) {
     return st;
 }
 
+// One tile of the fused kernel: where its volume's field, mask and outputs
+// are, and which plane, y-tile and x-tile it is.
+struct YxTile {
+    const CUtensorMap *in;   // input field (x, y, z), box 64 x KP x 1
+    const CUtensorMap *out;  // next field's store map, box 32 x 32: (x, y, z), or (x, z, y) when rows_yzx
+    const void *mask;
+    uint16_t *out_u16;       // final
+    float *field_out;        // final, optional
+    int64_t ny, nx, rows, n_vox;
+    int z, y0, x0, rows_yzx;
+};
+
+// Tile g: plane z, y-tile, x-tile (x fastest, so the CTAs in flight work on
+// neighbouring tiles of one or two planes and share their halos in L2).
+__device__ __forceinline__ void yx_decode(uint32_t g, uint32_t n_tx, uint32_t n_ty, YxTile &t) {
+    const uint32_t rest = g / n_tx, t_y = rest % n_ty;
+    t.x0 = (int) (g - rest * n_tx) * kXTN;
+    t.y0 = (int) t_y * kTM;
+    t.z = (int) (rest / n_ty);
+}
+
+// One volume: maps are kernel parameters.  The next field goes to [z][y][x]
+// rows, or to [y][z][x] rows (rows_yzx; the store map covers the plane window).
+struct OneVolumeYx {
+    struct Cursor {};
+    const void *mask;
+    uint16_t *out_u16;
+    float *field_out;
+    int64_t nz, ny, nx;
+    int n_ty, n_tx, rows_yzx;
+    int64_t n_tiles;
+    __device__ __forceinline__ int64_t total() const { return n_tiles; }
+    __device__ __forceinline__ YxTile tile(int64_t g, const CUtensorMap *in, const CUtensorMap *out, Cursor &) const {
+        YxTile t;
+        t.in = in;
+        t.out = out;
+        t.mask = mask;
+        t.out_u16 = out_u16;
+        t.field_out = field_out;
+        t.ny = ny;
+        t.nx = nx;
+        t.rows = nz * ny;
+        t.n_vox = nz * ny * nx;
+        t.rows_yzx = rows_yzx;
+        yx_decode((uint32_t) g, (uint32_t) n_tx, (uint32_t) n_ty, t);
+        return t;
+    }
+};
+
+// Many volumes (a batch group): maps and sizes from the device table; tile g
+// lies in the volume whose prefix-sum range holds it.  The next field goes to
+// the volume's other buffer in [y][z][x] rows.
+struct ManyVolumesYx {
+    const TcVol *vols;
+    const int64_t *prefix;  // n_vol + 1 prefix sums of the volumes' tiles
+    int n_vol, in_buf;
+    struct Cursor {
+        int64_t lo = 0, hi = 0;  // the current volume's tiles [lo, hi)
+        int v = 0;
+    };
+    __device__ __forceinline__ int64_t total() const { return __ldg(prefix + n_vol); }
+    __device__ __forceinline__ YxTile tile(int64_t g, const CUtensorMap *, const CUtensorMap *, Cursor &cur) const {
+        if (g < cur.lo || g >= cur.hi) {
+            cur.v = find_volume(prefix, n_vol, g);
+            cur.lo = __ldg(prefix + cur.v);
+            cur.hi = __ldg(prefix + cur.v + 1);
+        }
+        const TcVol &vol = vols[cur.v];
+        YxTile t;
+        t.in = &vol.map[1][in_buf];
+        t.out = &vol.yxrows[in_buf ^ 1];
+        t.mask = vol.mask;
+        t.out_u16 = vol.out_u16;
+        t.field_out = vol.field_out;
+        t.ny = vol.ny;
+        t.nx = vol.nx;
+        t.rows = vol.nz * vol.ny;
+        t.n_vox = vol.nz * vol.ny * vol.nx;
+        t.rows_yzx = 1;
+        yx_decode((uint32_t) (g - cur.lo), (uint32_t) vol.n_xt, (uint32_t) vol.n_at_y, t);
+        return t;
+    }
+};
+
+template <class Sched>
 struct YxLaunch {
     PassTaps t;  // ra = RA, kp = KP = 128 + RA + R rounded to 16, one coefficient set
     int final_pass;     // selects the FINAL instantiation
     int stages;         // F ring depth (tiles)
-    const void *mask;
-    // next field (not final), written through the store map: [z][y][x] rows
-    // (map dims x, y, z), or [y][z][x] rows when out_nz > 0 (map dims x, z, y)
-    uint16_t *out_u16;  // final
-    float *field_out;   // final, optional
-    int64_t nz, ny, nx, out_nz, out_z0;
-    int n_ty, n_tx;
-    int64_t n_tiles;
+    Sched sched;
 };
 
 // FINAL: the last repetition (uint16 output and FP32 field instead of the next
 // 16-bit field); a template parameter so that each form holds only its own
 // epilogue's registers.
-template <typename S, int FMT, bool FINAL>
+template <typename S, int FMT, bool FINAL, class Sched>
 __global__ void __launch_bounds__(kYxThreads, 1)
 tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap omap,
-             const __grid_constant__ YxLaunch p) {
+             const __grid_constant__ YxLaunch<Sched> p) {
     const PassTaps &tp = p.t;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
@@ -125,8 +203,8 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(yfull + 10);
     uint8_t *stage_out = reinterpret_cast<uint8_t *>(bars) + 1024;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t total = p.n_tiles;
-    const uint32_t n_tx = (uint32_t) p.n_tx, n_ty = (uint32_t) p.n_ty;
+    const Sched &sched = p.sched;
+    const int64_t total = sched.total();
 
     // T[n, j] = tap[j - n - RA + R]: the y pass's A (row n = output o, K = j)
     // and the x pass's B (row n = x-output, K = j) alike.
@@ -150,8 +228,10 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
         mbar_init(&drain[0], 1);
         mbar_init(&drain[1], 1);
         fence_barrier_init();
-        prefetch_tmap(&tmap);
-        if (!FINAL) prefetch_tmap(&omap);
+        if (std::is_same<Sched, OneVolumeYx>::value) {
+            prefetch_tmap(&tmap);
+            if (!FINAL) prefetch_tmap(&omap);
+        }
     }
     __syncwarp();
     if (warp == 0) {
@@ -164,15 +244,6 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    // Tile g: plane z, y-tile, x-tile (x fastest, so the CTAs in flight work on
-    // neighbouring tiles of one or two planes and share their halos in L2).
-    auto decode = [&](int64_t g, int &z, int &y0, int &x0) {
-        const uint32_t gg = (uint32_t) g, rest = gg / n_tx, t_y = rest % n_ty;
-        x0 = (int) (gg - rest * n_tx) * kXTN;
-        y0 = (int) t_y * kTM;
-        z = (int) (rest / n_ty);
-    };
-
     if (warp == 0 && lane == 0) {
         // TMA producer: one F tile (nch boxes) per ring stage; L2 prefetch ahead.
         // The stage and its phase advance incrementally (the ring depth is a
@@ -180,18 +251,18 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
         int64_t tl = 0;
         int s = 0;
         uint32_t ph = 0;
+        typename Sched::Cursor cur, pcur;
         for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
-            int z, y0, x0;
             const int64_t gp = g + kPrefetch * (int64_t) gridDim.x;
             if (gp < total) {
-                decode(gp, z, y0, x0);
-                for (int c = 0; c < nch; c++) tma_prefetch_3d(&tmap, x0 - tp.ra + 64 * c, y0 - tp.ra, z);
+                const YxTile q = sched.tile(gp, &tmap, &omap, pcur);
+                for (int c = 0; c < nch; c++) tma_prefetch_3d(q.in, q.x0 - tp.ra + 64 * c, q.y0 - tp.ra, q.z);
             }
-            decode(g, z, y0, x0);
+            const YxTile t = sched.tile(g, &tmap, &omap, cur);
             if (!mbar_wait(&empty[s], ph ^ 1, 1)) break;
             mbar_arrive_expect_tx(&full[s], tile_bytes);
             for (int c = 0; c < nch; c++)
-                tma_load_3d(ring + s * tile_bytes + c * chunk_bytes, &tmap, x0 - tp.ra + 64 * c, y0 - tp.ra, z,
+                tma_load_3d(ring + s * tile_bytes + c * chunk_bytes, t.in, t.x0 - tp.ra + 64 * c, t.y0 - tp.ra, t.z,
                             &full[s]);
             if (++s == stages) s = 0, ph ^= 1;
         }
@@ -313,20 +384,20 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
         const uint32_t lb = tmem + ((uint32_t) (quad * 32) << 16);
         uint8_t *stg = stage_out + ew * 2 * kXStageWarpBytes;
         int sbuf = 0;
-        const int64_t n_vox = p.nz * p.ny * p.nx, rows = p.nz * p.ny;
+        typename Sched::Cursor cur;
         int64_t tl = 0;
         for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
-            int z, y0, x0;
-            decode(g, z, y0, x0);
-            const int64_t y = y0 + quad * 32 + lane;
-            const bool live_row = y < p.ny;
-            const int64_t row = (int64_t) z * p.ny + y;
+            const YxTile t = sched.tile(g, &tmap, &omap, cur);
+            const int64_t y = t.y0 + quad * 32 + lane;
+            const bool live_row = y < t.ny;
+            const int64_t row = (int64_t) t.z * t.ny + y;
             MaskWords mw[2] = {};
 #pragma unroll
             for (int k = 0; k < 2; k++) {
-                const int64_t xb = x0 + part * 64 + 32 * k;
-                if (live_row && xb < p.nx)
-                    mw[k] = load_mask_words<FMT>(p.mask, row * p.nx + xb, p.nx - xb < 32 ? (int) (p.nx - xb) : 32, n_vox);
+                const int64_t xb = t.x0 + part * 64 + 32 * k;
+                if (live_row && xb < t.nx)
+                    mw[k] = load_mask_words<FMT>(t.mask, row * t.nx + xb, t.nx - xb < 32 ? (int) (t.nx - xb) : 32,
+                                                 t.n_vox);
             }
             if (!__all_sync(0xffffffffu, mbar_wait(xfull, (uint32_t) (tl & 1), 2))) break;
             tc_fence_after();
@@ -337,17 +408,17 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(xempty);
-            const uint32_t m0 = mask_flags<FMT>(mw[0], p.mask), m1 = mask_flags<FMT>(mw[1], p.mask);
+            const uint32_t m0 = mask_flags<FMT>(mw[0], t.mask), m1 = mask_flags<FMT>(mw[1], t.mask);
             // Non-final: both runs rounded together (two independent chains per step).
             uint32_t dd[2][16];
             if (!FINAL) narrow64_pairs_forced<S>(h, tp.inv_scale, tp.error_feedback, m0, m1, dd[0], dd[1]);
 #pragma unroll
             for (int k = 0; k < 2; k++) {
-                const int64_t xb = x0 + part * 64 + 32 * k;
+                const int64_t xb = t.x0 + part * 64 + 32 * k;
                 if (FINAL) {
                     const float(&hk)[32] = *reinterpret_cast<const float(*)[32]>(h + 32 * k);
-                    contig_final32(hk, k ? m1 : m0, live_row ? row : rows, rows, p.nx, xb, tp.inv_scale, p.out_u16,
-                                   p.field_out);
+                    contig_final32(hk, k ? m1 : m0, live_row ? row : t.rows, t.rows, t.nx, xb, tp.inv_scale,
+                                   t.out_u16, t.field_out);
                 } else {
                     // TMA store of the warp's 32 rows x 32 voxels (64-byte swizzle of the
                     // store map, which clips rows and columns outside the volume).  Every
@@ -365,10 +436,10 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
                     fence_proxy_async_smem();
                     __syncwarp();
                     if (lane == 0) {
-                        const int yq = y0 + quad * 32;
-                        if (xb < p.nx && yq < p.ny) {
-                            if (p.out_nz > 0) tma_store_3d(&omap, sb, (int) xb, z, yq);
-                            else tma_store_3d(&omap, sb, (int) xb, yq, z);
+                        const int yq = t.y0 + quad * 32;
+                        if (xb < t.nx && yq < t.ny) {
+                            if (t.rows_yzx) tma_store_3d(t.out, sb, (int) xb, t.z, yq);
+                            else tma_store_3d(t.out, sb, (int) xb, yq, t.z);
                         }
                         bulk_commit();
                     }

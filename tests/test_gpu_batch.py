@@ -28,23 +28,13 @@ def make_batch(field):
     return masks, outs, fouts, kernels
 
 
-def single(mask, kernel, reps, field, fused=False):
+def single(mask, kernel, reps, field):
     out = torch.empty(mask.shape, dtype=torch.uint16, device="cuda")
     fo = torch.empty(mask.shape, dtype=torch.float32, device="cuda")
-    # The batched launches run the y and x passes as separate kernels: compare
-    # with the same form of the single-volume call (a tensor-core group of one
-    # volume runs the single-volume launches with the fused y + x kernel).
-    device.diffuse(mask, kernel, reps, output=out, field=field, field_out=fo, fuse_passes=fused)
+    # The batched launches run the passes the single-volume call runs by
+    # default (the fused y + x kernel where it applies, else separate passes).
+    device.diffuse(mask, kernel, reps, output=out, field=field, field_out=fo)
     return out, fo
-
-
-def alone_in_group(i, shapes, sigmas, reps):
-    """Whether volume i is the only tensor-core-eligible volume of its
-    (kernel, repetitions) group (x extent a multiple of 8 and >= 64, radius <= 32)."""
-    def eligible(j):
-        return shapes[j][2] % 8 == 0 and shapes[j][2] >= 64 and round(4 * sigmas[j]) <= 32
-    return eligible(i) and sum(1 for j in range(len(shapes))
-                               if eligible(j) and sigmas[j] == sigmas[i] and reps[j] == reps[i]) == 1
 
 
 @pytest.mark.parametrize("field", ["bf16", "f16", "f32"])
@@ -56,7 +46,7 @@ def test_batch_equals_single_volume_runs(field):
     torch.cuda.synchronize()
     device.tensor_core_status()
     for i in range(len(SHAPES)):
-        o, f = single(masks[i], kernels[i], REPS[i], field, fused=alone_in_group(i, SHAPES, SIGMAS, REPS))
+        o, f = single(masks[i], kernels[i], REPS[i], field)
         torch.cuda.synchronize()
         assert torch.equal(outs[i], o), (i, text)
         assert torch.equal(fouts[i], f), (i, text)
@@ -86,7 +76,7 @@ def test_uneven_volumes_many_reps_batch_equals_single_and_repeats(field):
         runs = []
         for _ in range(2 if i < 4 else 1):
             fo = torch.empty(sh, dtype=torch.float32, device="cuda")
-            device.diffuse(masks[i], kernels[i], reps, field=field, field_out=fo, fuse_passes=False)
+            device.diffuse(masks[i], kernels[i], reps, field=field, field_out=fo)
             runs.append(fo)
         torch.cuda.synchronize()
         assert torch.equal(runs[0], runs[-1]), (i, sh)
@@ -108,7 +98,7 @@ def test_batch_with_wide_radius_volume_equals_single_runs():
     plan.close()
     for i, sh in enumerate(shapes):
         fo = torch.empty(sh, dtype=torch.float32, device="cuda")
-        device.diffuse(masks[i], kernels[i], 3, field="bf16", field_out=fo, fuse_passes=False)
+        device.diffuse(masks[i], kernels[i], 3, field="bf16", field_out=fo)
         torch.cuda.synchronize()
         assert torch.equal(fouts[i], fo), i
 

@@ -392,10 +392,10 @@ __device__ __forceinline__ void narrow64_pairs_forced(const float (&a)[64], floa
 // for the intermediate field of the fused y + x kernel, which the x MMAs
 // consume at once (its rounding noise, high-pass within 8 voxels, is removed
 // by the x convolution that follows).  d[j] holds voxels j (low) and 8 + j
-// (high); d[8 + j] holds 16 + j and 24 + j.
-template <typename S, bool MASKED>
-__device__ __forceinline__ void narrow32_quads(const float (&a)[32], float scale, bool ef, uint32_t force1,
-                                               uint32_t live, uint32_t (&d)[16]) {
+// (high); d[8 + j] holds 16 + j and 24 + j.  No masking: a run outside the
+// volume holds zeros, which round to zeros.
+template <typename S>
+__device__ __forceinline__ void narrow32_quads(const float (&a)[32], float scale, bool ef, uint32_t (&d)[16]) {
     float2 c0 = make_float2(0.0f, 0.0f), c1 = make_float2(0.0f, 0.0f);
     const float2 s2 = make_float2(scale, scale), m1 = make_float2(-1.0f, -1.0f);
 #pragma unroll
@@ -403,16 +403,6 @@ __device__ __forceinline__ void narrow32_quads(const float (&a)[32], float scale
         float2 w0 = make_float2(a[j], a[8 + j]), w1 = make_float2(a[16 + j], a[24 + j]);
         w0 = ef ? __ffma2_rn(w0, s2, c0) : __fmul2_rn(w0, s2);
         w1 = ef ? __ffma2_rn(w1, s2, c1) : __fmul2_rn(w1, s2);
-        if (MASKED) {
-            if (!((live >> j) & 1u)) w0.x = 0.0f;
-            if (!((live >> (8 + j)) & 1u)) w0.y = 0.0f;
-            if (!((live >> (16 + j)) & 1u)) w1.x = 0.0f;
-            if (!((live >> (24 + j)) & 1u)) w1.y = 0.0f;
-            if ((force1 >> j) & 1u) w0.x = 1.0f;
-            if ((force1 >> (8 + j)) & 1u) w0.y = 1.0f;
-            if ((force1 >> (16 + j)) & 1u) w1.x = 1.0f;
-            if ((force1 >> (24 + j)) & 1u) w1.y = 1.0f;
-        }
         const uint32_t q0 = Pair16<S>::cvt(w0.x, w0.y), q1 = Pair16<S>::cvt(w1.x, w1.y);
         if (ef) {
             c0 = __ffma2_rn(Pair16<S>::widen(q0), m1, w0);
@@ -423,7 +413,7 @@ __device__ __forceinline__ void narrow32_quads(const float (&a)[32], float scale
     }
 }
 
-// Two 32-voxel runs as narrow32_quads<S, false> each (a[0..31] -> d0,
+// Two 32-voxel runs as narrow32_quads<S> each (a[0..31] -> d0,
 // a[32..63] -> d1), their chains interleaved: four independent chains per step.
 template <typename S>
 __device__ __forceinline__ void narrow64_quads(const float (&a)[64], float scale, bool ef, uint32_t (&d0)[16],

@@ -348,7 +348,7 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
                 __syncwarp();
                 tmem_ld32(lb + kYxAccY + 32 * (c0 + 2), v);
                 uint32_t d[16], w[16];
-                narrow32_quads<S, false>(v, tp.inv_scale, tp.error_feedback, 0u, 0xffffffffu, d);
+                narrow32_quads<S>(v, tp.inv_scale, tp.error_feedback, d);
                 wait_yp();
                 if (!ok) break;
                 quads_to_adjacent(d, w);

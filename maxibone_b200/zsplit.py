@@ -18,9 +18,9 @@ z-slab of the field on its own GPU for the whole run:
   neighbour (torch.distributed P2P: NCCL over NVLink on GPUs, gloo on CPU
   tensors), H x ny x nx x 4 bytes per side and round.
 
-k is the largest count with k x radius no thicker than the thinnest slab, so
-halos only ever come from direct neighbours, and at most the requested
-repetitions.  FP32 results equal the single-volume form bit for bit (the core's
+k x radius is never thicker than the thinnest slab, so halos only ever come
+from direct neighbours; within that, split_plan picks k from an estimate of
+the planes computed and the per-round field passes.  FP32 results equal the single-volume form bit for bit (the core's
 planes see the same inputs in the same order); the 16-bit forms restart each
 round from the FP32 field (rounded to the storage type).
 
@@ -62,10 +62,21 @@ class SplitPlan:
         return max(1, -(-self.reps // self.k))
 
 
-def split_plan(nz: int, world: int, radius: int, reps: int, k: int | None = None) -> SplitPlan:
+def split_plan(nz: int, world: int, radius: int, reps: int, k: int | None = None,
+               round_cost: float = 0.25) -> SplitPlan:
     """Balanced contiguous z-slabs for `world` ranks and the repetitions per
     round.  Raises ValueError when a slab would be thinner than `radius` (the
-    halo of one repetition would have to come from beyond a neighbour)."""
+    halo of one repetition would have to come from beyond a neighbour).
+
+    k (when not given): a round of k repetitions computes on average
+    S + (k + 1) r planes per repetition on a slab of S planes with two cut
+    sides (its windows shrink by r per repetition), and exchanges k r planes
+    per side -- the same bytes per repetition for every k -- so small rounds
+    compute less, while each round also starts from and writes back the FP32
+    field over its S + 2 k r planes: `round_cost` is that work per plane
+    relative to one repetition's (the FP32 form's three CUDA-core passes
+    against about two memory passes: ~0.25).  k minimises
+    (S + (k + 1) r) + round_cost (S + 2 k r) / k."""
     if world < 1 or nz < world:
         raise ValueError(f"cannot split {nz} planes over {world} ranks")
     base, extra = divmod(nz, world)
@@ -78,7 +89,14 @@ def split_plan(nz: int, world: int, radius: int, reps: int, k: int | None = None
     if world > 1 and radius > thin:
         raise ValueError(f"slabs of {thin} planes are thinner than the kernel radius {radius}: use fewer ranks")
     k_max = max(1, reps) if world == 1 else max(1, min(max(1, reps), thin // max(1, radius)))
-    k = k_max if k is None else max(1, min(k, k_max))
+    if k is None:
+        if world == 1:
+            k = k_max
+        else:
+            def cost(kk):
+                return base + (kk + 1) * radius + round_cost * (base + 2 * kk * radius) / kk
+            k = min(range(1, k_max + 1), key=cost)
+    k = max(1, min(k, k_max))
     return SplitPlan(nz=nz, radius=radius, reps=reps, bounds=tuple(bounds), k=k)
 
 

@@ -109,18 +109,25 @@ def library_step(field: str = "f32", flags: int = 0, stream=None):
     or None (start from the mask); field_out float32 [ez, ny, nx] or None;
     output uint16 [ez, ny, nx] or None.  With shrinking, the last repetition
     writes only the planes it still computes (the core and up to `radius`
-    planes around it)."""
+    planes around it).  The step keeps one device workspace per slab shape, so
+    the rounds allocate nothing."""
     lib = _lib.lib()
+    workspaces = {}
 
     def step(mask, kernel, reps, init_field, field_out, output, shrink_lo, shrink_hi):
         nz, ny, nx = mask.shape
         k = np.ascontiguousarray(kernel, dtype=np.float32)
         st = stream if stream is not None else torch.cuda.current_stream(mask.device)
+        key = (tuple(mask.shape), mask.device)
+        if key not in workspaces:
+            n_ws = int(lib.maxi_diffusion_workspace_size(nz, ny, nx, _lib.FIELD_TYPES[field]))
+            workspaces[key] = torch.empty(n_ws, dtype=torch.uint8, device=mask.device)
+        ws = workspaces[key]
         _lib.check(lib.maxi_diffusion_device_ex(
             mask.data_ptr(), _lib.MASK_FORMATS["u8"], nz, ny, nx, k.ctypes.data, k.shape[0], int(reps),
             output.data_ptr() if output is not None else None,
             field_out.data_ptr() if field_out is not None else None,
-            _lib.FIELD_TYPES[field], flags, None, 0, st.cuda_stream,
+            _lib.FIELD_TYPES[field], flags, ws.data_ptr(), ws.numel(), st.cuda_stream,
             init_field.data_ptr() if init_field is not None else None, int(shrink_lo), int(shrink_hi)))
 
     return step

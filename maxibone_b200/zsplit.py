@@ -38,6 +38,14 @@ import torch
 from . import _lib
 
 
+def _device_bitpack(mask: torch.Tensor, stream) -> torch.Tensor:
+    """The diffusion's mask (set where > 0) as bit-packed words."""
+    from .device import bitpack
+    with torch.cuda.stream(stream):
+        binary = (mask > 0).to(torch.uint8)
+    return bitpack(binary, stream=stream)
+
+
 @dataclass(frozen=True)
 class SplitPlan:
     """Slab bounds of every rank and the rounds' repetition count."""
@@ -63,7 +71,7 @@ class SplitPlan:
 
 
 def split_plan(nz: int, world: int, radius: int, reps: int, k: int | None = None,
-               round_cost: float = 0.25) -> SplitPlan:
+               round_cost: float = 0.75) -> SplitPlan:
     """Balanced contiguous z-slabs for `world` ranks and the repetitions per
     round.  Raises ValueError when a slab would be thinner than `radius` (the
     halo of one repetition would have to come from beyond a neighbour).
@@ -74,8 +82,10 @@ def split_plan(nz: int, world: int, radius: int, reps: int, k: int | None = None
     per side -- the same bytes per repetition for every k -- so small rounds
     compute less, while each round also starts from and writes back the FP32
     field over its S + 2 k r planes: `round_cost` is that work per plane
-    relative to one repetition's (the FP32 form's three CUDA-core passes
-    against about two memory passes: ~0.25).  k minimises
+    relative to one repetition's (0.75 follows the FP32 form's slab rounds run
+    one after another on one B200, 1024^3, radius 32: for 2 slabs 1.45 / 1.49 /
+    1.50 times the single volume's work at k = 2 / 3 / 4, for 4 slabs 1.94 /
+    1.78 at k = 1 / 2, for 8 slabs 2.26 / 2.17 at k = 1 / 2).  k minimises
     (S + (k + 1) r) + round_cost (S + 2 k r) / k."""
     if world < 1 or nz < world:
         raise ValueError(f"cannot split {nz} planes over {world} ranks")
@@ -109,10 +119,11 @@ def library_step(field: str = "f32", flags: int = 0, stream=None):
     or None (start from the mask); field_out float32 [ez, ny, nx] or None;
     output uint16 [ez, ny, nx] or None.  With shrinking, the last repetition
     writes only the planes it still computes (the core and up to `radius`
-    planes around it).  The step keeps one device workspace per slab shape, so
-    the rounds allocate nothing."""
+    planes around it).  The step keeps one device workspace per slab shape and
+    the slab's mask packed to bits (it is the same every round), so the rounds
+    allocate and pack nothing."""
     lib = _lib.lib()
-    workspaces = {}
+    workspaces, packed = {}, {}
 
     def step(mask, kernel, reps, init_field, field_out, output, shrink_lo, shrink_hi):
         nz, ny, nx = mask.shape
@@ -123,8 +134,12 @@ def library_step(field: str = "f32", flags: int = 0, stream=None):
             n_ws = int(lib.maxi_diffusion_workspace_size(nz, ny, nx, _lib.FIELD_TYPES[field]))
             workspaces[key] = torch.empty(n_ws, dtype=torch.uint8, device=mask.device)
         ws = workspaces[key]
+        pkey = (mask.data_ptr(), tuple(mask.shape))
+        if pkey not in packed:  # one entry per slab; the mask is kept alive with its packed words
+            packed[pkey] = (mask, _device_bitpack(mask, st))
+        bits = packed[pkey][1]
         _lib.check(lib.maxi_diffusion_device_ex(
-            mask.data_ptr(), _lib.MASK_FORMATS["u8"], nz, ny, nx, k.ctypes.data, k.shape[0], int(reps),
+            bits.data_ptr(), _lib.MASK_FORMATS["bitpacked"], nz, ny, nx, k.ctypes.data, k.shape[0], int(reps),
             output.data_ptr() if output is not None else None,
             field_out.data_ptr() if field_out is not None else None,
             _lib.FIELD_TYPES[field], flags, ws.data_ptr(), ws.numel(), st.cuda_stream,

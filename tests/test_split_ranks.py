@@ -100,9 +100,9 @@ def test_split_plan_bounds_and_rounds():
     assert p.extended(0) == (0, 256) and p.extended(3) == (256, 640) and p.extended(7) == (768, 1024)
     # the chosen round length: thin slabs exchange every repetition, thick ones
     # less often (fewer round starts), never beyond the slab thickness
-    assert split_plan(1024, 8, 32, 100).k == 1
-    assert split_plan(1024, 2, 32, 100).k == 2
-    assert split_plan(1024, 2, 32, 100, round_cost=4.0).k > 2
+    assert split_plan(1024, 8, 32, 100).k == 2
+    assert split_plan(1024, 4, 32, 100).k == 2
+    assert split_plan(1024, 2, 32, 100, round_cost=4.0).k > 4
     assert split_plan(1024, 2, 32, 100, k=40).k == 16
     q = split_plan(37, 3, 4, 7, 2)
     assert [b[1] - b[0] for b in q.bounds] == [13, 12, 12] and q.k == 2 and q.rounds == 4

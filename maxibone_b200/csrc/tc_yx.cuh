@@ -32,11 +32,11 @@
 // passes).  Coefficients: one 16-bit set rounded to keep the kernel's sum and
 // second moment (tc_round_taps_matched).
 //
-// Tensor-core schedule.  A thread issues a tcgen05.mma of M = 128 about every
-// 100 cycles on B200 whatever its N (up to 192), while two issuing threads
-// reach the tensor cores' peak at N = 128: so every product is one chain of
-// the widest N (KP / 16 MMAs each for y and x per tile), and the y and the x
-// MMAs have an issuing thread each.  The conversion of tile t runs while the
+// Tensor-core schedule.  Narrow MMAs are bound by their issue (one thread
+// issues an M = 128, N = 64 MMA about every 60 cycles, twice the tensor pipe's
+// time), wide ones by the pipe: so every product is one chain of the widest N
+// (KP / 16 MMAs each for y and x per tile), and the y and the x MMAs have an
+// issuing thread each, so that neither waits on the other's issue.  The conversion of tile t runs while the
 // tensor cores do x(t - 1) and writes the other Y' buffer.  Tensor memory (512
 // columns): [0, 192) y accumulator, [192, 384) the two Y' buffers, [384, 512) x
 // accumulator.  Warp roles: 0 TMA producer, 1 y MMA issuer, 2-9 conversion (two
@@ -271,9 +271,8 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
         for (int64_t k = tl - stages; k < tl; k++)
             if (k >= 0) mbar_wait(&full[k % stages], (uint32_t) ((k / stages) & 1), 1);
     } else if ((warp == 1 || warp == kYxXWarp) && lane == 0) {
-        // MMA issuers.  A thread issues a tcgen05.mma about every 100 cycles
-        // whatever its N, so the y MMAs (warp 1) and the x MMAs (warp 18) have
-        // an issuing thread each; their ordering is through the barriers.
+        // MMA issuers: the y MMAs (warp 1) and the x MMAs (warp 18) have an
+        // issuing thread each; their ordering is through the barriers.
         const bool is_y = warp == 1;
         const uint32_t fmt = std::is_same<S, __nv_bfloat16>::value ? 1u : 0u;
         const uint32_t idesc_y = idesc_f16(fmt, 0 /*A K-major*/, 1 /*B MN-major*/, kTM, (uint32_t) kp);
@@ -342,31 +341,32 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
                 tc_fence_after();
                 yp_free = true;
             };
-            if (c1 == c0 + 3) {
-                // a third run first, so that the last two reads come together
+            // A third run first, narrowed and held as pairs, so that the last two
+            // reads come together and free the y accumulator for y(tl + 1) before
+            // this warp waits for its Y' buffer.
+            const bool third = c1 == c0 + 3;
+            uint32_t w3[16];
+            if (third) {
                 float v[32];
                 __syncwarp();
                 tmem_ld32(lb + kYxAccY + 32 * (c0 + 2), v);
-                uint32_t d[16], w[16];
+                uint32_t d[16];
                 narrow32_quads<S>(v, tp.inv_scale, tp.error_feedback, d);
-                wait_yp();
-                if (!ok) break;
-                quads_to_adjacent(d, w);
-                tmem_st16(yp + 16 * (c0 + 2), w);
+                quads_to_adjacent(d, w3);
             }
             {
-                // two runs together (four independent chains per step); the y
-                // accumulator is free once they are read
+                // two runs together (four independent chains per step)
                 float v[64];
                 __syncwarp();
                 tmem_ld64(lb + kYxAccY + 32 * c0, v);
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(yfree);
-                uint32_t d0[16], d1[16], w[16];
-                narrow64_quads<S>(v, tp.inv_scale, tp.error_feedback, d0, d1);
                 wait_yp();
                 if (!ok) break;
+                if (third) tmem_st16(yp + 16 * (c0 + 2), w3);
+                uint32_t d0[16], d1[16], w[16];
+                narrow64_quads<S>(v, tp.inv_scale, tp.error_feedback, d0, d1);
                 quads_to_adjacent(d0, w);
                 tmem_st16(yp + 16 * c0, w);
                 quads_to_adjacent(d1, w);
@@ -383,7 +383,6 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
         const int quad = warp & 3, part = ew >> 2;  // part: x-outputs part * 64 .. + 64 of the tile
         const uint32_t lb = tmem + ((uint32_t) (quad * 32) << 16);
         uint8_t *stg = stage_out + ew * 2 * kXStageWarpBytes;
-        int sbuf = 0;
         typename Sched::Cursor cur;
         int64_t tl = 0;
         for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
@@ -409,41 +408,49 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
             __syncwarp();
             if (lane == 0) mbar_arrive(xempty);
             const uint32_t m0 = mask_flags<FMT>(mw[0], t.mask), m1 = mask_flags<FMT>(mw[1], t.mask);
-            // Non-final: both runs rounded together (two independent chains per step).
-            uint32_t dd[2][16];
-            if (!FINAL) narrow64_pairs_forced<S>(h, tp.inv_scale, tp.error_feedback, m0, m1, dd[0], dd[1]);
+            if (FINAL) {
 #pragma unroll
-            for (int k = 0; k < 2; k++) {
-                const int64_t xb = t.x0 + part * 64 + 32 * k;
-                if (FINAL) {
+                for (int k = 0; k < 2; k++) {
+                    const int64_t xb = t.x0 + part * 64 + 32 * k;
                     const float(&hk)[32] = *reinterpret_cast<const float(*)[32]>(h + 32 * k);
                     contig_final32(hk, k ? m1 : m0, live_row ? row : t.rows, t.rows, t.nx, xb, tp.inv_scale,
                                    t.out_u16, t.field_out);
-                } else {
-                    // TMA store of the warp's 32 rows x 32 voxels (64-byte swizzle of the
-                    // store map, which clips rows and columns outside the volume).  Every
-                    // run commits one bulk group (an empty one outside the volume), so the
-                    // wait below always covers the store that last read the buffer.
+                }
+            } else {
+                // Both runs rounded together (two independent chains per step),
+                // then one TMA store per run of the warp's 32 rows x 32 voxels
+                // (64-byte swizzle of the store map, which clips rows and columns
+                // outside the volume) from the warp's two staging buffers.  The
+                // tile's stores form one bulk group, so the wait covers the
+                // previous tile's stores, the last readers of both buffers.
+                uint32_t dd[2][16];
+                narrow64_pairs_forced<S>(h, tp.inv_scale, tp.error_feedback, m0, m1, dd[0], dd[1]);
+                if (lane == 0) bulk_wait_read<0>();
+                __syncwarp();
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
                     uint32_t q[16];
                     pairs_to_adjacent(dd[k], q);
-                    if (lane == 0) bulk_wait_read<1>();
-                    __syncwarp();
-                    uint8_t *sb = stg + sbuf * kXStageWarpBytes;
+                    uint8_t *sb = stg + k * kXStageWarpBytes;
 #pragma unroll
                     for (int i = 0; i < 4; i++)
                         *reinterpret_cast<uint4 *>(sb + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) =
                             make_uint4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
-                    fence_proxy_async_smem();
-                    __syncwarp();
-                    if (lane == 0) {
-                        const int yq = t.y0 + quad * 32;
+                }
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) {
+                    const int yq = t.y0 + quad * 32;
+#pragma unroll
+                    for (int k = 0; k < 2; k++) {
+                        const int64_t xb = t.x0 + part * 64 + 32 * k;
                         if (xb < t.nx && yq < t.ny) {
+                            uint8_t *sb = stg + k * kXStageWarpBytes;
                             if (t.rows_yzx) tma_store_3d(t.out, sb, (int) xb, t.z, yq);
                             else tma_store_3d(t.out, sb, (int) xb, yq, t.z);
                         }
-                        bulk_commit();
                     }
-                    sbuf ^= 1;
+                    bulk_commit();
                 }
             }
         }

@@ -1016,9 +1016,9 @@ def main():
     per_kernel = {}
     for kind, (k_ms, k_n) in prof.items():
         if kind in kernel_bytes:
-            gbs = kernel_bytes[kind] * vox / (k_ms / k_n / 1e3) / 1e9
+            gbs = kernel_bytes[kind] * vox_local / (k_ms / k_n / 1e3) / 1e9
             per_kernel[kind] = {"launches": k_n, "ms_per_launch": k_ms / k_n, "alg_bytes_per_launch":
-                                kernel_bytes[kind] * vox, "gbs": gbs, "frac": gbs / peak}
+                                kernel_bytes[kind] * vox_local, "gbs": gbs, "frac": gbs / peak}
     dom = max(prof, key=lambda k: prof[k][0])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": per_voxel_traffic * vox if per_voxel_traffic else None,

@@ -284,7 +284,9 @@ int maxi_diffusion_batched(const maxi_volume *volumes, int64_t n_volumes, int32_
  * memory between rounds (8 bytes per voxel of pinned host memory; only when
  * that fits half of the host's available memory, MemAvailable, or
  * MAXIBONE_OOC_HOST_BUDGET bytes when that environment variable is set).  Planes of
- * a multiple of 32 voxels keep the whole mask bit-packed on the device.
+ * a multiple of 32 voxels keep the whole mask bit-packed on the device; from a
+ * pinned `voxels` buffer it is uploaded in chunks of about 1 GiB
+ * (MAXIBONE_OOC_UPLOAD_CHUNK_PLANES planes when set) while the first slabs run.
  * FP32 field; results equal maxi_diffusion_in_memory().
  */
 int maxi_diffusion_out_of_core(const uint8_t *voxels, int64_t total_z, int64_t total_y, int64_t total_x,

@@ -26,7 +26,10 @@
 // free device memory and a cost estimate (voxel-repetitions computed, bytes
 // crossing PCIe).  When the volume's plane is a multiple of 32 voxels the whole
 // mask is uploaded once and kept bit-packed on the device (1/8 byte per voxel),
-// so slabs need no mask uploads; the uint16 output of a slab is copied out on a
+// so slabs need no mask uploads; from a pinned caller buffer the upload runs on
+// its own stream in z order, and a slab's first kernel waits only for the
+// chunks its planes lie in, so later planes cross PCIe while the first slabs
+// compute.  The uint16 output of a slab is copied out on a
 // second stream while the next slab's repetitions run (only its last
 // repetition waits for that copy).  Pageable host buffers are staged through
 // pinned memory by the host thread.
@@ -212,7 +215,12 @@ static SlabPlan full_plan(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, in
     int64_t budget = free_b - reserve;
     // Resident bit-packed mask: whole 32-bit words per plane, and small enough.
     const int64_t packed_bytes = round_up(ceil_div(n, 32) * 4, 256);
-    const int64_t chunk_planes = std::max<int64_t>(1, std::min(nz, (int64_t(1) << 30) / plane));
+    // Upload chunks of about 1 GiB of mask (MAXIBONE_OOC_UPLOAD_CHUNK_PLANES planes when set).
+    int64_t chunk_planes = std::max<int64_t>(1, std::min(nz, (int64_t(1) << 30) / plane));
+    if (const char *env = getenv("MAXIBONE_OOC_UPLOAD_CHUNK_PLANES")) {
+        const long long v = atoll(env);
+        if (v > 0) chunk_planes = std::min<int64_t>(nz, v);
+    }
     const bool resident = !rebuild && plane % 32 == 0 && repititions > 0 &&
                           packed_bytes + 2 * chunk_planes * plane < budget / 4;
     if (resident) budget -= packed_bytes + 2 * chunk_planes * plane;
@@ -279,6 +287,8 @@ static int run_slabs(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, const f
     // Device and host buffers.
     struct Buffers {
         cudaStream_t cs = nullptr, ds = nullptr;  // compute, download
+        cudaStream_t us = nullptr;                // resident mask upload from a pinned caller buffer
+        std::vector<cudaEvent_t> up;              // chunk c of that upload packed
         cudaEvent_t ready = nullptr, freed = nullptr;
         uint32_t *packed = nullptr;               // resident mask
         uint8_t *stage[2] = {nullptr, nullptr};   // resident mask upload chunks
@@ -292,6 +302,7 @@ static int run_slabs(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, const f
         ~Buffers() {
             if (cs) cudaStreamSynchronize(cs);
             if (ds) cudaStreamSynchronize(ds);
+            if (us) cudaStreamSynchronize(us);
             cudaFree(packed);
             cudaFree(stage[0]);
             cudaFree(stage[1]);
@@ -305,8 +316,10 @@ static int run_slabs(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, const f
             cudaFreeHost(h_field[1]);
             if (ready) cudaEventDestroy(ready);
             if (freed) cudaEventDestroy(freed);
+            for (cudaEvent_t ev : up) cudaEventDestroy(ev);
             if (cs) cudaStreamDestroy(cs);
             if (ds) cudaStreamDestroy(ds);
+            if (us) cudaStreamDestroy(us);
         }
     } b;
     const int64_t ws_bytes = maxi_diffusion_workspace_size(E, ny, nx, field_type);
@@ -321,6 +334,18 @@ static int run_slabs(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, const f
         cudaEventCreateWithFlags(&b.ready, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b.freed, cudaEventDisableTiming) != cudaSuccess)
         return set_cuda_error(cudaGetLastError(), "out-of-core streams");
+    const bool overlap_upload = resident && direct_in;
+    if (overlap_upload) {
+        if (cudaStreamCreateWithFlags(&b.us, cudaStreamNonBlocking) != cudaSuccess)
+            return set_cuda_error(cudaGetLastError(), "out-of-core streams");
+        for (int64_t z = 0; z < nz; z += chunk_planes) {
+            b.up.push_back(nullptr);
+            if (cudaEventCreateWithFlags(&b.up.back(), cudaEventDisableTiming) != cudaSuccess) {
+                b.up.pop_back();
+                return set_cuda_error(cudaGetLastError(), "out-of-core streams");
+            }
+        }
+    }
     if (resident && (cudaMalloc(&b.packed, packed_bytes) != cudaSuccess ||
                      cudaMalloc(&b.stage[0], chunk_planes * plane) != cudaSuccess ||
                      cudaMalloc(&b.stage[1], chunk_planes * plane) != cudaSuccess))
@@ -343,8 +368,11 @@ static int run_slabs(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, const f
     }
     cudaError_t e;
 
-    // Whole mask -> resident bit-packed words, chunk by chunk.
+    // Whole mask -> resident bit-packed words, chunk by chunk (the two staging
+    // buffers alternate; the stream orders each refill after the previous
+    // packing of that buffer).
     if (resident) {
+        cudaStream_t ust = overlap_upload ? b.us : b.cs;
         for (int64_t z = 0, c = 0; z < nz; z += chunk_planes, c++) {
             const int64_t cz = std::min(chunk_planes, nz - z);
             uint8_t *st = b.stage[c & 1];
@@ -354,8 +382,9 @@ static int run_slabs(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, const f
                 int rc = read(z, cz, b.h_in);
                 if (rc) return rc;
             }
-            if ((e = cudaMemcpyAsync(st, src, cz * plane, cudaMemcpyHostToDevice, b.cs)) != cudaSuccess ||
-                (e = launch_bitpack_encode(st, cz * plane, b.packed + z * plane / 32, false, b.cs)) != cudaSuccess)
+            if ((e = cudaMemcpyAsync(st, src, cz * plane, cudaMemcpyHostToDevice, ust)) != cudaSuccess ||
+                (e = launch_bitpack_encode(st, cz * plane, b.packed + z * plane / 32, false, ust)) != cudaSuccess ||
+                (overlap_upload && (e = cudaEventRecord(b.up[c], ust)) != cudaSuccess))
                 return set_cuda_error(e, "mask upload");
         }
     }
@@ -387,6 +416,10 @@ static int run_slabs(int64_t nz, int64_t ny, int64_t nx, int64_t slab_z, const f
             const void *mask_ptr;
             int32_t mask_fmt;
             if (resident) {
+                // the chunks holding planes [e0, e1) are packed (all of them after the first round)
+                if (overlap_upload && round == 0 &&
+                    (e = cudaStreamWaitEvent(b.cs, b.up[(e1 - 1) / chunk_planes], 0)) != cudaSuccess)
+                    return set_cuda_error(e, "mask upload");
                 mask_ptr = b.packed + e0 * plane / 32;
                 mask_fmt = MAXI_MASK_BITPACKED;
             } else {

@@ -47,6 +47,25 @@ def test_out_of_core_pinned_buffers_and_bf16():
     assert np.all(o[mask > 0] == 65535)
 
 
+@pytest.mark.parametrize("chunk", [3, 16])
+def test_pinned_mask_uploaded_in_chunks_equals_in_memory_fp32(chunk, monkeypatch):
+    # From a pinned mask the resident upload runs on its own stream, chunk by
+    # chunk, and each slab waits only for the chunks it reads: small chunks
+    # and thin slabs make the first slabs compute while later chunks upload.
+    monkeypatch.setenv("MAXIBONE_OOC_UPLOAD_CHUNK_PLANES", str(chunk))
+    shape = (150, 64, 96)
+    mask = spheres_mask(shape, 12, (3, 9), seed=chunk)
+    kernel = gauss_kernel(2.0).astype(np.float32)
+    want = np.empty(shape, np.uint16)
+    diffusion(mask, kernel, want, 4)
+    pin_m = torch.empty(shape, dtype=torch.uint8, pin_memory=True)
+    pin_m.copy_(torch.from_numpy(mask))
+    pin_o = torch.zeros(shape, dtype=torch.int16, pin_memory=True)
+    got = pin_o.numpy().view(np.uint16)
+    diffusion_out_of_core(pin_m.numpy(), kernel, got, (25, 64, 96), 4)
+    np.testing.assert_array_equal(got, want)
+
+
 def test_on_disk_matches_reference_semantics(tmp_path):
     shape = (48, 30, 40)
     mask = spheres_mask(shape, 6, (2, 7), seed=3)

@@ -36,9 +36,9 @@
 // issues an M = 128, N = 64 MMA about every 60 cycles, twice the tensor pipe's
 // time), wide ones by the pipe: so every product is one chain of the widest N
 // (KP / 16 MMAs each for y and x per tile), and the y and the x MMAs have an
-// issuing thread each, so that neither waits on the other's issue.  The conversion of tile t runs while the
-// tensor cores do x(t - 1) and writes the other Y' buffer.  Tensor memory (512
-// columns): [0, 192) y accumulator, [192, 384) the two Y' buffers, [384, 512) x
+// issuing thread each, so that neither waits on the other's issue.  The
+// conversion of tile t runs while the tensor cores do x(t - 1) and writes the
+// other Y' buffer.  Tensor memory (512 columns): [0, 192) y accumulator, [192, 384) the two Y' buffers, [384, 512) x
 // accumulator.  Warp roles: 0 TMA producer, 1 y MMA issuer, 2-9 conversion (two
 // per TMEM lane quadrant), 10-17 epilogue (two per quadrant, 64 x-outputs
 // each), 18 x MMA issuer.  Every wait is bounded; on a timeout the kernel

@@ -386,6 +386,34 @@ __device__ __forceinline__ void narrow64_pairs_forced(const float (&a)[64], floa
     }
 }
 
+// narrow64_pairs_forced with the voxels of each step in adjacent elements:
+// a[2j], a[2j + 1] are voxels j and 16 + j of the first run, a[32 + 2j],
+// a[33 + 2j] those of the second (a permuted tensor-memory column order).
+// Bit for bit the same rounding as narrow64_pairs_forced.
+template <typename S>
+__device__ __forceinline__ void narrow64_pairs_forced_adjacent(const float (&a)[64], float scale, bool ef, uint32_t f0,
+                                                               uint32_t f1, uint32_t (&d0)[16], uint32_t (&d1)[16]) {
+    float2 c0 = make_float2(0.0f, 0.0f), c1 = make_float2(0.0f, 0.0f);
+    const float2 s2 = make_float2(scale, scale), m1 = make_float2(-1.0f, -1.0f);
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        const float2 v0 = make_float2(a[2 * j], a[2 * j + 1]), v1 = make_float2(a[32 + 2 * j], a[33 + 2 * j]);
+        float2 w0 = ef ? __ffma2_rn(v0, s2, c0) : __fmul2_rn(v0, s2);
+        float2 w1 = ef ? __ffma2_rn(v1, s2, c1) : __fmul2_rn(v1, s2);
+        if ((f0 >> j) & 1u) w0.x = 1.0f;
+        if ((f0 >> (16 + j)) & 1u) w0.y = 1.0f;
+        if ((f1 >> j) & 1u) w1.x = 1.0f;
+        if ((f1 >> (16 + j)) & 1u) w1.y = 1.0f;
+        const uint32_t q0 = Pair16<S>::cvt(w0.x, w0.y), q1 = Pair16<S>::cvt(w1.x, w1.y);
+        if (ef) {
+            c0 = __ffma2_rn(Pair16<S>::widen(q0), m1, w0);
+            c1 = __ffma2_rn(Pair16<S>::widen(q1), m1, w1);
+        }
+        d0[j] = q0;
+        d1[j] = q1;
+    }
+}
+
 // 32 voxels in four error-feedback chains of 8 (x = 8k + j, k = 0..3): chains
 // 0 / 1 and 2 / 3 advance together as two packed pairs, so each step has two
 // independent dependency chains and a run takes 8 steps instead of 16.  Used

@@ -63,6 +63,14 @@ constexpr uint32_t kYxYpCols = 96;
 constexpr uint32_t kYxAccX = 384;                                // x accumulator, 128 columns
 constexpr uint32_t kYxTmemCols = 512;
 
+// Output order of the Toeplitz rows: row n of the matrix in shared memory is
+// output (n & ~31) + P(n & 31) with P(2j) = j and P(2j + 1) = 16 + j.  The y
+// MMAs then leave y-output P(l) in TMEM lane l of each quadrant, and the x MMAs
+// leave x-output P(c) in column c of each 32-column run, so that the voxels the
+// epilogue rounds together (j and 16 + j of a run: two error-feedback chains)
+// arrive in adjacent registers of its tensor-memory loads.
+__host__ __device__ constexpr int yx_out_perm(int n) { return (n & ~31) | (((n & 31) >> 1) + ((n & 1) << 4)); }
+
 // One F tile: ceil(KP / 64) boxes of 64 x-columns x KP rows.
 __host__ __device__ constexpr int yx_tile_bytes(int kp) { return ((kp + 63) / 64) * kp * 128; }
 
@@ -210,7 +218,7 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
     // and the x pass's B (row n = x-output, K = j) alike.
     for (int e = threadIdx.x; e < kXTN * tp.kpa; e += kYxThreads) {
         const int n = e / tp.kpa, j = e - n * tp.kpa;
-        const int t = j - n - tp.ra + tp.radius;  // tap index 0..2R
+        const int t = j - yx_out_perm(n) - tp.ra + tp.radius;  // tap index 0..2R
         uint16_t v = 0;
         if (t >= 0 && t <= 2 * tp.radius && j < kp) v = tp.hi[t];
         *reinterpret_cast<uint16_t *>(tt + sw128_kmajor_offset(n, j, kXTN)) = v;
@@ -387,7 +395,8 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
         int64_t tl = 0;
         for (int64_t g = blockIdx.x; g < total; g += gridDim.x, tl++) {
             const YxTile t = sched.tile(g, &tmap, &omap, cur);
-            const int64_t y = t.y0 + quad * 32 + lane;
+            const int prow = yx_out_perm(lane);  // this lane's y-output within the quadrant
+            const int64_t y = t.y0 + quad * 32 + prow;
             const bool live_row = y < t.ny;
             const int64_t row = (int64_t) t.z * t.ny + y;
             MaskWords mw[2] = {};
@@ -412,7 +421,12 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
 #pragma unroll
                 for (int k = 0; k < 2; k++) {
                     const int64_t xb = t.x0 + part * 64 + 32 * k;
-                    const float(&hk)[32] = *reinterpret_cast<const float(*)[32]>(h + 32 * k);
+                    float hk[32];  // x order
+#pragma unroll
+                    for (int j = 0; j < 16; j++) {
+                        hk[j] = h[32 * k + 2 * j];
+                        hk[16 + j] = h[32 * k + 2 * j + 1];
+                    }
                     contig_final32(hk, k ? m1 : m0, live_row ? row : t.rows, t.rows, t.nx, xb, tp.inv_scale,
                                    t.out_u16, t.field_out);
                 }
@@ -424,7 +438,7 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
                 // tile's stores form one bulk group, so the wait covers the
                 // previous tile's stores, the last readers of both buffers.
                 uint32_t dd[2][16];
-                narrow64_pairs_forced<S>(h, tp.inv_scale, tp.error_feedback, m0, m1, dd[0], dd[1]);
+                narrow64_pairs_forced_adjacent<S>(h, tp.inv_scale, tp.error_feedback, m0, m1, dd[0], dd[1]);
                 if (lane == 0) bulk_wait_read<0>();
                 __syncwarp();
 #pragma unroll
@@ -434,7 +448,7 @@ tc_yx_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
                     uint8_t *sb = stg + k * kXStageWarpBytes;
 #pragma unroll
                     for (int i = 0; i < 4; i++)
-                        *reinterpret_cast<uint4 *>(sb + lane * 64 + ((i ^ ((lane >> 1) & 3)) << 4)) =
+                        *reinterpret_cast<uint4 *>(sb + prow * 64 + ((i ^ ((prow >> 1) & 3)) << 4)) =
                             make_uint4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
                 }
                 fence_proxy_async_smem();

@@ -921,6 +921,9 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
+        # A collective over every rank first, so that the communicator exists
+        # before the split's first grouped point-to-point exchange.
+        dist.barrier()
     shape, sigma, reps = WORKLOADS[args.workload]
     if args.shape:
         shape = tuple(int(v) for v in args.shape.lower().split("x"))

@@ -132,6 +132,10 @@ int maxi_profile_read(double *ms_by_kind, int64_t *launches_by_kind, int32_t n_k
  * bound by python_api::diffusion_in_memory, src/pybind/diffusion-pybind.cc:27-53.
  * voxels: uint8[nz][ny][nx] (set when > 0); kernel: float[kernel_size], odd
  * length; output: uint16[nz][ny][nx], written in place.  FP32 field.
+ * Pageable (not pinned) buffers of 64 MiB or more cross through two 32 MiB
+ * pinned staging buffers allocated for the call, several host threads moving
+ * each chunk while the previous one crosses PCIe; pinned buffers are copied
+ * directly.
  */
 int maxi_diffusion_in_memory(const uint8_t *voxels, int64_t nz, int64_t ny, int64_t nx,
                              const float *kernel, int64_t kernel_size, int64_t repititions,

@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "passes.cuh"
 #include "host_util.h"
+#include "host_copy.h"
 #include "unrolled.h"
 #include "profiler.h"
 #include "tc_pass.h"
@@ -379,7 +380,13 @@ int maxi_diffusion_in_memory(const uint8_t *voxels, int64_t nz, int64_t ny, int6
     uint8_t *d_mask = reinterpret_cast<uint8_t *>(base + mask_off);
     uint16_t *d_out = reinterpret_cast<uint16_t *>(base + out_off);
     cudaStream_t st = cache->stream;
-    cudaError_t e = cudaMemcpyAsync(d_mask, voxels, n, cudaMemcpyHostToDevice, st);
+    // Pageable caller buffers of some size go through pinned staging with
+    // several host threads; pinned ones are copied directly.
+    const int64_t stage_min = int64_t(64) << 20;
+    const bool stage_in = n >= stage_min && host_pageable(voxels);
+    const bool stage_out = 2 * n >= stage_min && host_pageable(output);
+    cudaError_t e = stage_in ? copy_to_device_staged(d_mask, voxels, n, st)
+                             : cudaMemcpyAsync(d_mask, voxels, n, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         rc = maxi_diffusion_device(d_mask, MAXI_MASK_U8, nz, ny, nx, kernel, kernel_size, repititions, d_out, nullptr,
                                    MAXI_FIELD_F32, 0, base + ws_off, need, st);
@@ -387,7 +394,8 @@ int maxi_diffusion_in_memory(const uint8_t *voxels, int64_t nz, int64_t ny, int6
             if (!g_keep_buffers.load()) cache_drop(cache);
             return rc;
         }
-        e = cudaMemcpyAsync(output, d_out, 2 * n, cudaMemcpyDeviceToHost, st);
+        e = stage_out ? copy_to_host_staged(output, d_out, 2 * n, st)
+                      : cudaMemcpyAsync(output, d_out, 2 * n, cudaMemcpyDeviceToHost, st);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (!g_keep_buffers.load()) cache_drop(cache);

@@ -23,14 +23,21 @@ void parallel_memcpy(void *dst, const void *src, size_t n, int threads) {
     const size_t slice = ((n + t - 1) / t + 65535) & ~size_t(65535);
     std::vector<std::thread> pool;
     pool.reserve(t);
-    for (int i = 0; i < t; i++) {
-        const size_t off = (size_t) i * slice;
-        if (off >= n) break;
-        const size_t len = std::min(slice, n - off);
-        pool.emplace_back([=]() {
-            std::memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off, len);
-        });
+    size_t done = 0;  // bytes handed to threads; the rest is copied here
+    try {
+        for (int i = 0; i < t; i++) {
+            const size_t off = (size_t) i * slice;
+            if (off >= n) break;
+            const size_t len = std::min(slice, n - off);
+            pool.emplace_back([=]() {
+                std::memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off, len);
+            });
+            done = off + len;
+        }
+    } catch (...) {
+        // no more threads: this thread copies what is left
     }
+    if (done < n) std::memcpy(static_cast<char *>(dst) + done, static_cast<const char *>(src) + done, n - done);
     for (auto &th : pool) th.join();
 }
 

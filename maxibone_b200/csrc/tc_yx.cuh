@@ -38,12 +38,12 @@
 // (KP / 16 MMAs each for y and x per tile), and the y and the x MMAs have an
 // issuing thread each, so that neither waits on the other's issue.  The
 // conversion of tile t runs while the tensor cores do x(t - 1) and writes the
-// other Y' buffer.  Tensor memory (512 columns): [0, 192) y accumulator, [192, 384) the two Y' buffers, [384, 512) x
-// accumulator.  Warp roles: 0 TMA producer, 1 y MMA issuer, 2-9 conversion (two
-// per TMEM lane quadrant), 10-17 epilogue (two per quadrant, 64 x-outputs
-// each), 18 x MMA issuer.  Every wait is bounded; on a timeout the kernel
-// records a code in g_tc_error, lets the copies and MMAs it started finish
-// (bounded) and winds down.
+// other Y' buffer.  Tensor memory (512 columns): [0, 192) y accumulator,
+// [192, 384) the two Y' buffers, [384, 512) x accumulator.  Warp roles: 0 TMA
+// producer, 1 y MMA issuer, 2-9 conversion (two per TMEM lane quadrant), 10-17
+// epilogue (two per quadrant, 64 x-outputs each), 18 x MMA issuer.  Every wait
+// is bounded; on a timeout the kernel records a code in g_tc_error, lets the
+// copies and MMAs it started finish (bounded) and winds down.
 #pragma once
 
 #include "tc_kernels.cuh"

@@ -67,12 +67,12 @@ typedef enum maxi_mask_format {
 #define MAXI_FLAG_SEPARATE_PASSES 0x20   /* BF16/FP16 tensor cores: the y and x passes as two
                                             kernels (two HBM round trips) instead of the fused
                                             y + x kernel, which is the default where it applies
-                                            (radius 12 to 32: the single coefficient set) */
+                                            (radius 4 to 32: the single coefficient set) */
 #define MAXI_FLAG_SPLIT_COEFFICIENTS 0x40 /* BF16/FP16 tensor cores: Toeplitz coefficients as high +
                                             low 16-bit halves (two MMAs per K step) instead of the
                                             single set whose taps are rounded so that the
                                             kernel's sum and second moment are kept (the default
-                                            from radius 12; smaller radii always use the halves);
+                                            from radius 4; smaller radii always use the halves);
                                             runs the separate y and x passes */
 
 const char *maxi_last_error(void);

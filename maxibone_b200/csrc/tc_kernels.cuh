@@ -1004,7 +1004,7 @@ inline void fill_pass_taps(PassTaps &t, const float *kernel, int radius, int ra,
     t.inv_scale = 1.0f / scale;
     t.hi_only = hi_only ? 1 : 0;
     if (hi_only) {
-        tc_round_taps_matched(kernel, radius, is_bf16, scale, t.hi);
+        t.inv_scale = 1.0f / tc_round_taps_scaled(kernel, radius, is_bf16, scale, t.hi);
         for (int i = 0; i < 2 * radius + 1; i++) t.lo[i] = 0;
     } else {
         tc_split_taps(kernel, radius, is_bf16, scale, t.hi, t.lo);

@@ -10,7 +10,10 @@
 #include "tc_kernels.cuh"
 #include "tc_yx.cuh"
 
+#include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <map>
 #include <vector>
 
 namespace maxi {
@@ -208,6 +211,58 @@ void tc_round_taps_matched(const float *kernel, int radius, bool is_bf16, float 
     }
     for (int g = 0; g < G; g++)
         for (int i : groups[g]) out[i] = flip[g] ? b1[i] : b0[i];
+}
+
+float tc_round_taps_scaled(const float *kernel, int radius, bool is_bf16, float base_scale, uint16_t *out) {
+    const int n = 2 * radius + 1;
+    // Results per kernel (the search costs milliseconds; launches repeat it).
+    static std::mutex mu;
+    static std::map<std::vector<uint32_t>, std::pair<float, std::vector<uint16_t>>> cache;
+    std::vector<uint32_t> key(n + 2);
+    key[0] = (uint32_t) is_bf16;
+    std::memcpy(&key[1], &base_scale, 4);
+    std::memcpy(&key[2], kernel, 4 * (size_t) n);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            std::copy(it->second.second.begin(), it->second.second.end(), out);
+            return it->second.first;
+        }
+    }
+    auto from = [&](uint16_t b) { return (double) (is_bf16 ? from_bf16(b) : from_f16(b)); };
+    double sum = 0.0, m2 = 0.0;
+    for (int i = 0; i < n; i++) {
+        sum += kernel[i];
+        m2 += (double) (i - radius) * (i - radius) * kernel[i];
+    }
+    const double w2 = 0.01 / std::max(1.0, (double) radius * radius);
+    // Candidate scales base x (1 + c / C): fewer for wide kernels, whose search is slower.
+    const int C = radius <= 32 ? 256 : radius <= 64 ? 32 : 1;
+    std::vector<uint16_t> bits(n), best_bits(n);
+    float best_s = base_scale;
+    double best_cost = -1.0;
+    for (int c = 0; c < C; c++) {
+        const float sc = base_scale * (1.0f + (float) c / (float) C);
+        tc_round_taps_matched(kernel, radius, is_bf16, sc, bits.data());
+        const double inv = (double) (1.0f / sc);  // the factor the epilogues apply
+        double s0 = 0.0, s2 = 0.0;
+        for (int i = 0; i < n; i++) {
+            const double q = from(bits[i]) * inv;
+            s0 += q;
+            s2 += (double) (i - radius) * (i - radius) * q;
+        }
+        const double cost = std::fabs(s0 - sum) + w2 * std::fabs(s2 - m2);
+        if (best_cost < 0.0 || cost < best_cost) {
+            best_cost = cost;
+            best_s = sc;
+            best_bits = bits;
+        }
+    }
+    std::copy(best_bits.begin(), best_bits.end(), out);
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = {best_s, best_bits};
+    return best_s;
 }
 
 bool tc_yx_supported(int radius, int64_t nz, int64_t ny, int64_t nx) {

@@ -17,11 +17,13 @@ constexpr int kTcMaxRadius = 32;
 // boxes; the x pass above radius 32 runs in its transposed form.
 constexpr int kTcMaxRadiusWide = 128;
 
-// Smallest radius served by one 16-bit coefficient set (tc_round_taps_matched);
-// below it the taps are large enough that their 16-bit rounding steps compound
-// past the error bound (BF16, sigma 2, R = 50: 2.4e-3 with one set, 1.4e-3 with
-// high + low halves), and the passes use the halves.
-constexpr int kTcSingleSetMinRadius = 12;
+// Smallest radius served by one 16-bit coefficient set (tc_round_taps_scaled):
+// the set's scale is searched so that its sum matches the kernel's to ~1e-9,
+// which keeps small-sigma kernels within the error bound too (BF16, sigma 2,
+// R = 50: 1.3e-3 over the batch's volumes; a set at scale 1 gave 2.4e-3).
+// Below radius 4 the 16-bit stores round to nearest and the passes use the
+// high + low halves.
+constexpr int kTcSingleSetMinRadius = 4;
 
 // Whether a pass of this radius uses the single coefficient set.
 inline bool tc_single_set(int radius, bool split_requested) {
@@ -77,6 +79,15 @@ cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool fina
 // to the FP32 kernel's.  Plain round-to-nearest changes the sum by ~1e-4, and
 // that gain error compounds over the 3 R passes of a diffusion.
 void tc_round_taps_matched(const float *kernel, int radius, bool is_bf16, float scale, uint16_t *out);
+
+// tc_round_taps_matched at the scale, among base_scale x (1 + c / C) for 256
+// values of c up to radius 32 (32 up to 64, 1 above), whose rounded taps times
+// the float 1 / scale the epilogues apply come closest to the FP32 kernel's sum
+// (first) and second moment.  A 16-bit grid cannot hit the sum at one scale
+// (BF16, sigma 2: 3e-5 off at best), but across scales it comes within ~1e-7:
+// the gain error that R repetitions compound.  Returns the scale; results are
+// cached per kernel.
+float tc_round_taps_scaled(const float *kernel, int radius, bool is_bf16, float base_scale, uint16_t *out);
 
 // Reads (and clears) the device error word of the tensor-core kernels:
 // 0 = fine, 1..3 = a bounded wait timed out, -1 = could not be read.

@@ -36,11 +36,11 @@ def diffuse(mask: torch.Tensor, kernel, repititions: int, output: torch.Tensor |
     workspace: uint8 CUDA tensor of at least workspace_bytes(shape, field), or None.
     tensor_cores: 16-bit fields: z and y passes on tcgen05 tensor cores where supported.
     error_feedback: 16-bit fields: error-feedback rounding along x (else round to nearest).
-    fuse_passes: 16-bit tensor-core fields, radius 12 to 32: the y and x passes in one
+    fuse_passes: 16-bit tensor-core fields, radius 4 to 32: the y and x passes in one
           kernel per z-plane tile (else two kernels, two HBM round trips).
     split_coefficients: 16-bit tensor-core passes: high + low 16-bit coefficient halves
           (two MMAs per K step, separate y and x passes) instead of one set whose
-          taps keep the kernel's sum and second moment (the default from radius 12;
+          taps keep the kernel's sum and second moment (the default from radius 4;
           smaller radii always use the halves).
     """
     if not mask.is_cuda:

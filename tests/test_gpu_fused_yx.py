@@ -7,7 +7,7 @@ agree with the separate y and x passes (both round the intermediate field to
 the same type, with error-feedback chains that start at different x), keep
 mask voxels exact, and be deterministic.  Every run asserts that the fused
 kernel is what ran (MAXI_PATH_FUSED_YX), so a fallback cannot pass unnoticed.
-The fused kernel uses the single coefficient set (the default from radius 12);
+The fused kernel uses the single coefficient set (the default from radius 4);
 the split high + low halves, which smaller radii always use, run the separate
 passes.
 """
@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 VS_F64 = {"bf16": 2e-3, "f16": 5e-4}
 FUSED_VS_SEPARATE = {"bf16": 4e-3, "f16": 1e-3}
 FUSED = _lib.PATH_TENSOR_CORES_ZY | _lib.PATH_FUSED_YX
-SINGLE_SET_MIN_RADIUS = 12
+SINGLE_SET_MIN_RADIUS = 4
 
 
 def run(mask, kernel, reps, field, fused=True, split=False, output=True, field_out=True, bitpacked=False):

@@ -26,10 +26,10 @@
 // ~1e-6: with single-rounded 16-bit coefficients the kernel's gain error
 // compounds over 3 x R passes.  FP16 coefficients are scaled by 2^10 to stay in
 // the normal range; the epilogue undoes the scale exactly.  With hi_only the
-// passes use one 16-bit set instead, each tap rounded up or down so that the
-// set keeps the kernel's sum and second moment (tc_round_taps_matched): one MMA
-// per K step.  Consecutive MMAs into one accumulator are latency-bound (about
-// 130 cycles each on B200 for N <= 192), so this halves the passes' tensor time.
+// passes use one 16-bit set instead, each tap rounded up or down at a searched
+// scale (undone by the epilogue like FP16's) so that the set keeps the kernel's
+// sum and second moment (tc_round_taps_scaled): one MMA per K step instead of
+// two, half the passes' tensor-core work.
 //
 // Row order of the 16-bit field between repetitions.  The z pass is the only
 // pass whose tile rows lie on different planes: read from the [z][y][x] volume

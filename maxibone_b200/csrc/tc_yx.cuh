@@ -29,8 +29,8 @@
 // type as the separate passes store it, so the arithmetic is that of the y
 // pass followed by the x pass; only the HBM round trip of the intermediate
 // field is gone (4 + 1/8 instead of 8 + 1/8 bytes per voxel for the two
-// passes).  Coefficients: one 16-bit set rounded to keep the kernel's sum and
-// second moment (tc_round_taps_matched).
+// passes).  Coefficients: one 16-bit set rounded, at a searched scale, to keep
+// the kernel's sum and second moment (tc_round_taps_scaled).
 //
 // Tensor-core schedule.  Narrow MMAs are bound by their issue (one thread
 // issues an M = 128, N = 64 MMA about every 60 cycles, twice the tensor pipe's

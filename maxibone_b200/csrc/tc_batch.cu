@@ -48,6 +48,8 @@ int tc_fill_volume(TcVol &vol, void *buf0, void *buf1, const uint32_t *packed_ma
     vol.cols_y = (int64_t) vol.n_xc_y * nz;
     vol.tiles_x = (int64_t) vol.n_xt * ceil_div(nz * ny, kTM);
     vol.tiles_yx = (int64_t) vol.n_xt * vol.n_at_y * nz;
+    vol.magic_xt = yx_div_magic((uint32_t) vol.n_xt);
+    vol.magic_at_y = yx_div_magic((uint32_t) vol.n_at_y);
     auto enc = tc_encode_fn();
     if (!enc) return -1;
     const CUtensorMapDataType dt = is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;

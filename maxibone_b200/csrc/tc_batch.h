@@ -28,6 +28,7 @@ struct alignas(64) TcVol {
     int64_t nz, ny, nx;
     int n_at_z, n_at_y, n_xc_z, n_xc_y, n_xt;
     int64_t cols_z, cols_y, tiles_x, tiles_yx;
+    uint64_t magic_xt, magic_at_y;  // fused kernel's tile decode: divisions by n_xt and n_at_y
 };
 
 // K extents of the strided (z/y) and contiguous (x) tensor-core passes.

@@ -294,6 +294,8 @@ cudaError_t tc_yx(const S *in, S *out, const void *mask, int mask_fmt, bool fina
     sc.n_ty = (int) ceil_div(ny, kTM);
     sc.n_tx = (int) ceil_div(nx, kXTN);
     sc.n_tiles = nz * sc.n_ty * sc.n_tx;
+    sc.magic_tx = yx_div_magic((uint32_t) sc.n_tx);
+    sc.magic_ty = yx_div_magic((uint32_t) sc.n_ty);
 
     CUtensorMap map;
     const cuuint64_t dims[3] = {(cuuint64_t) nx, (cuuint64_t) ny, (cuuint64_t) nz};

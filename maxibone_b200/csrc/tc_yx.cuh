@@ -100,13 +100,17 @@ struct YxTile {
     int z, y0, x0, rows_yzx;
 };
 
-// Tile g: plane z, y-tile, x-tile (x fastest, so the CTAs in flight work on
-// neighbouring tiles of one or two planes and share their halos in L2).
-__device__ __forceinline__ void yx_decode(uint32_t g, uint32_t n_tx, uint32_t n_ty, YxTile &t) {
-    const uint32_t rest = g / n_tx, t_y = rest % n_ty;
-    t.x0 = (int) (g - rest * n_tx) * kXTN;
-    t.y0 = (int) t_y * kTM;
-    t.z = (int) (rest / n_ty);
+// Tile g of a volume: x-tile g % n_tx, then y-tile, then plane (x fastest, so
+// the CTAs in flight work on neighbouring tiles of one or two planes and share
+// their halos in L2).  The divisions use the multiply below: floor(g / d) for
+// g < 2^32 as the high word of g * M, M = ceil(2^64 / d)
+// (d >= 2; yx_div_magic(1) = 0 marks d = 1): the product's excess over g / d
+// stays below g / 2^64 < 1 / d, so the floor is exact.
+__host__ __device__ constexpr uint64_t yx_div_magic(uint32_t d) {
+    return d <= 1 ? 0ull : ~0ull / d + 1ull;
+}
+__device__ __forceinline__ uint32_t yx_div(uint32_t g, uint32_t d, uint64_t magic) {
+    return magic ? (uint32_t) __umul64hi((uint64_t) g, magic) : g;
 }
 
 // One volume: maps are kernel parameters.  The next field goes to [z][y][x]
@@ -119,6 +123,7 @@ struct OneVolumeYx {
     int64_t nz, ny, nx;
     int n_ty, n_tx, rows_yzx;
     int64_t n_tiles;
+    uint64_t magic_tx, magic_ty;  // yx_div_magic(n_tx), yx_div_magic(n_ty)
     __device__ __forceinline__ int64_t total() const { return n_tiles; }
     __device__ __forceinline__ YxTile tile(int64_t g, const CUtensorMap *in, const CUtensorMap *out, Cursor &) const {
         YxTile t;
@@ -132,7 +137,12 @@ struct OneVolumeYx {
         t.rows = nz * ny;
         t.n_vox = nz * ny * nx;
         t.rows_yzx = rows_yzx;
-        yx_decode((uint32_t) g, (uint32_t) n_tx, (uint32_t) n_ty, t);
+        const uint32_t gg = (uint32_t) g;
+        const uint32_t rest = yx_div(gg, (uint32_t) n_tx, magic_tx);
+        const uint32_t z = yx_div(rest, (uint32_t) n_ty, magic_ty);
+        t.x0 = (int) (gg - rest * (uint32_t) n_tx) * kXTN;
+        t.y0 = (int) (rest - z * (uint32_t) n_ty) * kTM;
+        t.z = (int) z;
         return t;
     }
 };
@@ -167,7 +177,12 @@ struct ManyVolumesYx {
         t.rows = vol.nz * vol.ny;
         t.n_vox = vol.nz * vol.ny * vol.nx;
         t.rows_yzx = 1;
-        yx_decode((uint32_t) (g - cur.lo), (uint32_t) vol.n_xt, (uint32_t) vol.n_at_y, t);
+        const uint32_t gg = (uint32_t) (g - cur.lo);
+        const uint32_t rest = yx_div(gg, (uint32_t) vol.n_xt, vol.magic_xt);
+        const uint32_t z = yx_div(rest, (uint32_t) vol.n_at_y, vol.magic_at_y);
+        t.x0 = (int) (gg - rest * (uint32_t) vol.n_xt) * kXTN;
+        t.y0 = (int) (rest - z * (uint32_t) vol.n_at_y) * kTM;
+        t.z = (int) z;
         return t;
     }
 };

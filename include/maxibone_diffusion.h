@@ -103,6 +103,18 @@ int maxi_last_path(void);
  */
 int maxi_tensor_core_status(void);
 
+/*
+ * The single 16-bit coefficient set the tensor-core passes use for this
+ * kernel (no counterpart in the reference, whose passes use the FP32 kernel;
+ * for inspection and tests): taps[kernel_size] receives the BF16 or FP16 bit
+ * patterns (field_type MAXI_FIELD_BF16 / MAXI_FIELD_F16) and *inv_scale the
+ * factor the passes' epilogues apply to the accumulated sums, so that the
+ * pass computes sum_i from16(taps[i]) * inv_scale * field.  kernel_size odd,
+ * at most 257.
+ */
+int maxi_tensor_core_taps(const float *kernel, int64_t kernel_size, int32_t field_type, uint16_t *taps,
+                          float *inv_scale);
+
 /* Kernel kinds reported by maxi_profile_read(). */
 typedef enum maxi_kernel_kind {
     MAXI_KERNEL_INIT = 0,    /* mask -> field */

@@ -62,6 +62,7 @@ SIGNATURES = {
                                     _i64, _i64, ctypes.c_double, ctypes.c_double, _p]),
     "maxi_diffusion_device_noalloc": (_int, [_p, _i32, _i64, _i64, _i64, _p, _i64, _i64, _p, _p, _p]),
     "maxi_tensor_core_status": (_int, []),
+    "maxi_tensor_core_taps": (_int, [_p, _i64, _i32, _p, _p]),
     "maxi_release_cached_memory": (_int, []),
     "maxi_keep_device_buffers": (_int, [_int]),
     "maxi_last_path": (_int, []),

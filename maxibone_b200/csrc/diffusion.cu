@@ -229,6 +229,22 @@ int maxi_tensor_core_status(void) {
     return MAXI_OK;
 }
 
+int maxi_tensor_core_taps(const float *kernel, int64_t kernel_size, int32_t field_type, uint16_t *taps,
+                          float *inv_scale) {
+    clear_error();
+    if (!kernel || !taps || !inv_scale) return set_error(MAXI_ERR_INVALID_ARGUMENT, "NULL pointer");
+    if (kernel_size < 1 || kernel_size % 2 == 0 || kernel_size > 2 * tc::kTcMaxRadiusWide + 1)
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "kernel_size must be odd and at most %d",
+                         2 * tc::kTcMaxRadiusWide + 1);
+    if (field_type != MAXI_FIELD_BF16 && field_type != MAXI_FIELD_F16)
+        return set_error(MAXI_ERR_INVALID_ARGUMENT, "field_type must be MAXI_FIELD_BF16 or MAXI_FIELD_F16");
+    const bool bf16 = field_type == MAXI_FIELD_BF16;
+    // the base scale of the passes' taps (fill_pass_taps): FP16 taps are lifted into the normal range
+    const float s = tc::tc_round_taps_scaled(kernel, (int) (kernel_size / 2), bf16, bf16 ? 1.0f : 1024.0f, taps);
+    *inv_scale = 1.0f / s;
+    return MAXI_OK;
+}
+
 int64_t maxi_diffusion_workspace_size(int64_t nz, int64_t ny, int64_t nx, int32_t field_type) {
     if (nz <= 0 || ny <= 0 || nx <= 0 || field_bytes(field_type) == 0) return -1;
     return workspace_bytes_for(nz * ny * nx, field_type);

@@ -18,9 +18,10 @@ constexpr int kTcMaxRadius = 32;
 constexpr int kTcMaxRadiusWide = 128;
 
 // Smallest radius served by one 16-bit coefficient set (tc_round_taps_scaled):
-// the set's scale is searched so that its sum matches the kernel's to ~1e-9,
-// which keeps small-sigma kernels within the error bound too (BF16, sigma 2,
-// R = 50: 1.3e-3 over the batch's volumes; a set at scale 1 gave 2.4e-3).
+// the set's scale is searched so that its sum matches the kernel's (to 2e-7 at
+// sigma 1, 2e-8 from sigma 2), which keeps small-sigma kernels within the
+// error bound too (BF16, sigma 2, R = 50: 1.3e-3 over the batch's volumes; a
+// set at scale 1 gave 2.4e-3).
 // Below radius 4 the 16-bit stores round to nearest and the passes use the
 // high + low halves.
 constexpr int kTcSingleSetMinRadius = 4;
@@ -84,7 +85,7 @@ void tc_round_taps_matched(const float *kernel, int radius, bool is_bf16, float 
 // values of c up to radius 32 (32 up to 64, 1 above), whose rounded taps times
 // the float 1 / scale the epilogues apply come closest to the FP32 kernel's sum
 // (first) and second moment.  A 16-bit grid cannot hit the sum at one scale
-// (BF16, sigma 2: 3e-5 off at best), but across scales it comes within ~1e-7:
+// (BF16, sigma 2: 3e-5 off at best), but across scales it comes within 2e-7:
 // the gain error that R repetitions compound.  Returns the scale; results are
 // cached per kernel.
 float tc_round_taps_scaled(const float *kernel, int radius, bool is_bf16, float base_scale, uint16_t *out);
